@@ -1,0 +1,207 @@
+/*
+ * mpcd_gpu.h -- C ABI of libmpcd_gpu.so, the B200 (sm_100a) solvent timestep
+ * of multi-particle collision dynamics (MPCD).
+ *
+ * The library replaces one call of the reference program, the serial solvent
+ * timestep
+ *
+ *   void timestep(cell ***CL, particleMPC *SRDparticles, spec SP[], bc WALL[],
+ *                 simptr simMD, specSwimmer *SS, swimmer swimmers[],
+ *                 double AVNOW[3], double AVV[3], double avDIR[3],
+ *                 inputList in, double *KBTNOW, double *AVS, int runtime,
+ *                 int MD_mode, outputFlagsList outFlags,
+ *                 outputFilesList outFiles);
+ *
+ * (mpcd/headers/mpc.h:16, mpcd/subroutines/mpc.c:4496), called once per
+ * iteration from mpcd/mpcd.c:268 (warm-up) and mpcd/mpcd.c:298 (main loop).
+ * Where the reference keeps its state in host structures (particles in a
+ * 128-byte AoS array threaded through per-cell linked lists, globals such as
+ * DIM/XYZ/GnDNST, a static RNG), a handle here owns the state in device
+ * memory, and every entry point takes plain pointers and sizes.
+ *
+ * Conventions: every function returns an int status, 0 on success and a
+ * negative MPCD_ERR_* code on failure (the reference prints and calls exit(1)
+ * instead, e.g. mpc.c:2805-2808, bc.c:700-711).  Nothing here calls exit().
+ * A handle is used by one host thread at a time; its GPU work is ordered on
+ * one CUDA stream owned by the handle.
+ */
+#ifndef MPCD_GPU_H
+#define MPCD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPCD_ABI_VERSION 1
+
+#define MPCD_MAX_SPECIES 10 /* reference MAXSPECI, definitions.h:66 */
+#define MPCD_MAX_WALLS 16
+
+/* status codes */
+#define MPCD_OK 0
+#define MPCD_ERR_ARG (-1)         /* bad argument / null pointer            */
+#define MPCD_ERR_UNSUPPORTED (-2) /* option outside the GPU path            */
+#define MPCD_ERR_CUDA (-3)        /* CUDA runtime error                     */
+#define MPCD_ERR_NOMEM (-4)       /* device allocation failed               */
+#define MPCD_ERR_STATE (-5)       /* call out of order (e.g. no particles)  */
+#define MPCD_ERR_SIZE (-6)        /* size above a compiled-in maximum       */
+
+/* collision operators: the reference's collOp codes (definitions.h:261-303)
+ * that this library implements */
+#define MPCD_COLL_ARBAXIS 0        /* SRD, random axis                     */
+#define MPCD_COLL_MPCAT 2          /* Andersen MPC-AT                      */
+#define MPCD_COLL_RAT 3            /* Andersen MPC-AT+a                    */
+#define MPCD_COLL_DIPOLE_DIR_SUM 16 /* nematic, dipole activity summed    */
+#define MPCD_COLL_DIPOLE_DIR_AV 17  /* nematic, dipole activity averaged  */
+
+/* nematic switch: the reference's in.LC values (definitions.h:194-200) */
+#define MPCD_LC_ISOTROPIC 0
+#define MPCD_LC_LOCAL 1
+
+/* precision of the particle state */
+#define MPCD_PREC_FP64 0  /* positions and velocities in FP64 (reference) */
+#define MPCD_PREC_MIXED 1 /* int cell + FP32 offset, FP32 velocity;
+                             cell sums and 3x3 inverses in FP64          */
+
+/* One species of MPCD particle: the fields of the reference's spec struct
+ * (SRDclss.h:56-83) that the timestep reads. */
+typedef struct mpcd_species {
+    double mass;        /* MASS   (json 'mass')      */
+    double damp;        /* DAMP   (json 'damp')      */
+    double rfc;         /* RFC    (json 'rfc')       */
+    double tumble;      /* TUMBLE (json 'tumble')    */
+    double chihi;       /* CHIHI  (json 'shearSusc') */
+    double act;         /* ACT    (json 'act')       */
+    double mfpot;       /* MFPOT  (json 'mfpot')     */
+    double sigwidth;    /* SIGWIDTH                  */
+    double sigpos;      /* SIGPOS                    */
+    double minactratio; /* MINACTRATIO               */
+} mpcd_species;
+
+/* One planar boundary: the fields of the reference's bc struct
+ * (SRDclss.h:140-200) used for a static, axis-aligned plane (P = 1,
+ * exactly one non-zero component of A; PLANAR flag of read.c:1417-1428).
+ * Surface W = sum_i A_i (x_i - Q_i) - R, times -1 if inv (calcW_PLANE,
+ * bc.c:306-316); a particle is inside the wall when W < 0. */
+typedef struct mpcd_wall {
+    double A[3];     /* normal (1/aInv), points into the fluid             */
+    double Q[3];     /* point on the plane                                 */
+    double R;        /* offset                                             */
+    int inv;         /* INV                                                */
+    int phantom;     /* PHANTOM: ghost particles fill cut cells            */
+    int coll_type;   /* COLL_TYPE: only 1 (BC_SURF_RULES) is implemented   */
+    int pad_;
+    double DN, DT;   /* position shift normal / tangential                 */
+    double DVN, DVT; /* velocity shift normal / tangential                 */
+    double MVN, MVT; /* velocity multiplier normal / tangential            */
+    double DVxyz[3]; /* cartesian velocity shift                           */
+    double MUN, MUT; /* orientation multiplier normal / tangential         */
+    double MUxyz[3]; /* cartesian orientation multiplier                   */
+    double DUxyz[3]; /* cartesian orientation shift                        */
+    int inter[MPCD_MAX_SPECIES]; /* INTER: 1 if species interacts       */
+} mpcd_wall;
+
+/* Simulation parameters: the parts of the reference's inputList
+ * (SRDclss.h:389-425) and globals (globals.h:24-65) the timestep uses. */
+typedef struct mpcd_config {
+    int dim;          /* DIM: 2 or 3                                       */
+    int L[3];         /* XYZ: box size in cells (L[2] = 1 in 2D)            */
+    double dt;        /* in.dt                                             */
+    double kbt;       /* in.KBT                                            */
+    int coll_op;      /* in.RTECH, one of MPCD_COLL_*                      */
+    int lc;           /* in.LC, MPCD_LC_*                                  */
+    double rot_ang;   /* in.RA in radians (SRD rotation angle)             */
+    int galinv;       /* in.GALINV: 1 = random grid shift each step        */
+    int precision;    /* MPCD_PREC_*                                       */
+    double grav[3];   /* in.GRAV                                           */
+    double gndnst;    /* GnDNST; <= 0 means: compute at upload as
+                         globalDensities (init.c:1002-1018) does           */
+    uint64_t seed;    /* key of the counter-based generator               */
+    uint32_t replica; /* replica index folded into every draw              */
+    int n_species;
+    mpcd_species species[MPCD_MAX_SPECIES];
+    int n_walls;
+    mpcd_wall walls[MPCD_MAX_WALLS];
+    int capacity;     /* maximum number of particles                       */
+} mpcd_config;
+
+/* Per-handle error counters (the reference prints warnings instead). */
+typedef struct mpcd_status {
+    uint64_t steps;         /* steps executed                               */
+    uint64_t escaped;       /* particles binned outside the grid (bin(),
+                               mpc.c:970-982)                               */
+    uint64_t bounce_limit;  /* particles that hit the NBOUNCE limit
+                               (bc.c:1461-1488)                             */
+    uint64_t nonfinite;     /* non-finite velocities seen by the step       */
+} mpcd_status;
+
+typedef struct mpcd_handle mpcd_handle;
+
+/* Library version (MPCD_ABI_VERSION). */
+int mpcd_abi_version(void);
+
+/* Create a handle on the current CUDA device.  Replaces the reference's
+ * readJson (read.c:973) + initializeSIM (init.c:2048) state set-up; the
+ * particles are supplied separately by mpcd_upload_state. */
+int mpcd_create(const mpcd_config *cfg, mpcd_handle **out);
+
+/* Release all device memory of the handle. */
+int mpcd_destroy(mpcd_handle *h);
+
+/* Copy n particles (AoS, 3 doubles per vector; U and spid may be NULL) to
+ * the device.  Replaces binin (mpc.c:924) and the initial localPROP. */
+int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
+                      const double *U, const int *spid);
+
+/* Same, reading an array of records with a byte stride, so a caller can pass
+ * the reference's particleMPC array (SRDclss.h:34-44) directly:
+ * stride = sizeof(particleMPC), offsets = offsetof(particleMPC, Q/V/U/SPID).
+ * off_U may be (size_t)-1 to skip orientations. */
+int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *base,
+                                  size_t stride, size_t off_Q, size_t off_V,
+                                  size_t off_U, size_t off_spid);
+
+/* Copy the particle state back in the caller's original particle order. */
+int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double *U);
+
+/* Strided counterpart of mpcd_download_state (writes Q, V, U fields only). */
+int mpcd_download_particles_strided(mpcd_handle *h, void *base, size_t stride,
+                                    size_t off_Q, size_t off_V, size_t off_U);
+
+/* Enqueue nsteps timesteps with step numbers step0, step0+1, ...  The step
+ * number keys every random draw.  Asynchronous on the handle's stream. */
+int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0);
+
+/* Drop-in for one call of timestep() (mpc.c:4496): one step numbered
+ * 'runtime', then the step's global measures copied to the host:
+ * AVNOW = avVel (therm.c:362-367), KBTNOW = TEMP (therm.c:209-235). */
+int mpcd_timestep(mpcd_handle *h, uint32_t runtime, double AVNOW[3],
+                  double *KBTNOW);
+
+/* Global measures of the last executed step (blocks until it finishes). */
+int mpcd_globals(mpcd_handle *h, double *kbtnow, double avnow[3]);
+
+/* Re-bin on the unshifted grid and compute per-cell properties for output
+ * (the re-bin + localPROP at the end of timestep, mpc.c:4936-4942).
+ * Arrays hold (L0+1)(L1+1)(L2+1) cells, index (a*(L1+1)+b)*(L2+1)+c; any
+ * pointer may be NULL.  vcm/cm hold 3 doubles per cell. */
+int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
+                    double *cm);
+
+/* Error counters accumulated so far. */
+int mpcd_get_status(mpcd_handle *h, mpcd_status *st);
+
+/* Use the caller's CUDA stream (cudaStream_t passed as void*) from now on. */
+int mpcd_set_stream(mpcd_handle *h, void *stream);
+
+/* Number of kernel launches the last mpcd_step issued per step. */
+int mpcd_launches_per_step(mpcd_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPCD_GPU_H */

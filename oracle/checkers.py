@@ -1,0 +1,181 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes wrappers of the CPU checkers.
+
+- Oracle: oracle/libmpcd_oracle.so, the plain-C restatement of the reference
+  solvent timestep (oracle/mpcd_oracle.c).
+- Reference: oracle/_ref/libmpcdref.so, the reference's own timestep built
+  from its sources with injected counter-based draws
+  (oracle/ref/ref_harness.c); libmpcdref_time.so is the same with the
+  reference's own Mersenne-Twister generator, for timing.
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg, never by the product.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "libmpcd_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libmpcdref.so")
+REF_TIME_LIB = os.path.join(HERE, "_ref", "libmpcdref_time.so")
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Oracle:
+    """CPU restatement of the reference timestep."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = C.CDLL(ORACLE_LIB)
+            lib.oracle_create.restype = C.c_void_p
+            lib.oracle_create.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 4
+            lib.oracle_destroy.argtypes = [C.c_void_p]
+            lib.oracle_step.argtypes = [C.c_void_p, C.c_uint32]
+            lib.oracle_get_particles.argtypes = [C.c_void_p] * 4
+            lib.oracle_get_globals.argtypes = [C.c_void_p] * 3
+            lib.oracle_get_cells.argtypes = [C.c_void_p] * 5
+            lib.oracle_gndnst.restype = C.c_double
+            lib.oracle_gndnst.argtypes = [C.c_void_p]
+            lib.oracle_ncells.argtypes = [C.c_void_p]
+            lib.oracle_escaped.restype = C.c_long
+            lib.oracle_escaped.argtypes = [C.c_void_p]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, cfg, Q, V, U=None, spid=None):
+        self.cfg = cfg
+        lib = self.lib()
+        self.n = len(Q)
+        Q, V = _f64(Q), _f64(V)
+        U = None if U is None else _f64(U)
+        spid = None if spid is None else np.ascontiguousarray(spid, dtype=np.int32)
+        self.h = lib.oracle_create(C.byref(cfg), self.n, _p(Q), _p(V), _p(U), _p(spid))
+        if not self.h:
+            raise RuntimeError("oracle_create failed")
+
+    def step(self, step):
+        r = self.lib().oracle_step(self.h, step)
+        if r != 0:
+            raise RuntimeError(f"oracle_step returned {r}")
+
+    def particles(self):
+        Q = np.zeros((self.n, 3))
+        V = np.zeros((self.n, 3))
+        U = np.zeros((self.n, 3))
+        self.lib().oracle_get_particles(self.h, _p(Q), _p(V), _p(U))
+        return Q, V, U
+
+    def globals(self):
+        kb = C.c_double()
+        av = np.zeros(3)
+        self.lib().oracle_get_globals(self.h, C.byref(kb), _p(av))
+        return kb.value, av
+
+    def cells(self):
+        nc = self.lib().oracle_ncells(self.h)
+        pop = np.zeros(nc, dtype=np.int32)
+        mass = np.zeros(nc)
+        vcm = np.zeros((nc, 3))
+        cm = np.zeros((nc, 3))
+        self.lib().oracle_get_cells(self.h, _p(pop), _p(mass), _p(vcm), _p(cm))
+        return pop, mass, vcm, cm
+
+    def gndnst(self):
+        return self.lib().oracle_gndnst(self.h)
+
+    def escaped(self):
+        return self.lib().oracle_escaped(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib().oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Reference:
+    """The reference's own timestep (process-global state: one at a time)."""
+
+    _libs = {}
+
+    @classmethod
+    def available(cls, timing=False):
+        return os.path.exists(REF_TIME_LIB if timing else REF_LIB)
+
+    @classmethod
+    def lib(cls, timing=False):
+        path = REF_TIME_LIB if timing else REF_LIB
+        if path not in cls._libs:
+            lib = C.CDLL(path)
+            lib.ref_init.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 4
+            lib.ref_step.argtypes = [C.c_uint32]
+            lib.ref_run_timed.restype = C.c_double
+            lib.ref_run_timed.argtypes = [C.c_int, C.c_uint32]
+            lib.ref_get_particles.argtypes = [C.c_void_p] * 3
+            lib.ref_get_globals.argtypes = [C.c_void_p] * 2
+            lib.ref_get_cells.argtypes = [C.c_void_p] * 4
+            lib.ref_gndnst.restype = C.c_double
+            lib.ref_unexpected_draws.restype = C.c_long
+            cls._libs[path] = lib
+        return cls._libs[path]
+
+    def __init__(self, cfg, Q, V, U=None, spid=None, timing=False):
+        self.cfg = cfg
+        self.n = len(Q)
+        self._lib = self.lib(timing)
+        Q, V = _f64(Q), _f64(V)
+        U = None if U is None else _f64(U)
+        spid = None if spid is None else np.ascontiguousarray(spid, dtype=np.int32)
+        r = self._lib.ref_init(C.byref(cfg), self.n, _p(Q), _p(V), _p(U), _p(spid))
+        if r != 0:
+            raise RuntimeError("ref_init failed")
+
+    def step(self, step):
+        self._lib.ref_step(step)
+
+    def run_timed(self, nsteps, step0=1):
+        return self._lib.ref_run_timed(nsteps, step0)
+
+    def particles(self):
+        Q = np.zeros((self.n, 3))
+        V = np.zeros((self.n, 3))
+        U = np.zeros((self.n, 3))
+        self._lib.ref_get_particles(_p(Q), _p(V), _p(U))
+        return Q, V, U
+
+    def globals(self):
+        kb = C.c_double()
+        av = np.zeros(3)
+        self._lib.ref_get_globals(C.byref(kb), _p(av))
+        return kb.value, av
+
+    def cells(self):
+        nc = self._lib.ref_ncells()
+        pop = np.zeros(nc, dtype=np.int32)
+        mass = np.zeros(nc)
+        vcm = np.zeros((nc, 3))
+        cm = np.zeros((nc, 3))
+        self._lib.ref_get_cells(_p(pop), _p(mass), _p(vcm), _p(cm))
+        return pop, mass, vcm, cm
+
+    def gndnst(self):
+        return self._lib.ref_gndnst()
+
+    def unexpected_draws(self):
+        return self._lib.ref_unexpected_draws()

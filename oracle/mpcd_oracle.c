@@ -1,0 +1,644 @@
+/*
+ * mpcd_oracle.c -- TEST INFRASTRUCTURE ONLY: a plain-C, serial, FP64
+ * restatement of the reference's solvent timestep (NIAMH-MPCD,
+ * mpcd/subroutines/mpc.c:4496-4954 and the helpers it calls), used by the
+ * tests, smoke() and the benchmark's CPU baseline as the checker for the GPU
+ * library.  The product never links or calls this file.
+ *
+ * Random numbers come from niamh-mpcd_b200/csrc/mpcd_rng.h keyed by
+ * (seed, replica, step, stream, cell or particle id), the same values the GPU
+ * uses and the reference harness (oracle/ref/ref_harness.c) injects into the
+ * reference, so all three consume identical draws.
+ *
+ * Stage order follows timestep() for the paths without MD, swimmers,
+ * thermostats or moving walls:
+ *   grid shift        ranshift + gridShift_all     mpc.c:4567-4575, 720-766
+ *   bin (shifted)     bin(...,1)                   mpc.c:4596, 948-992
+ *   acceleration      acc_all                      mpc.c:4621, 697-700
+ *   cell moments      localPROP                    mpc.c:4630, 64-216
+ *   phantom particles ghostPart                    mpc.c:4634, 351-567
+ *   nematic           LCcollision, jefferysTorque  mpc.c:4640-4678
+ *   collision         MPCcollision per cell        mpc.c:4699-4714
+ *   globals           avVel, TEMP                  mpc.c:4738-4752
+ *   shift back        gridShift_all(...,1)         mpc.c:4793-4799
+ *   stream            stream_all                   mpc.c:4815-4817
+ *   walls             MPC_BCcollision              mpc.c:4834, bc.c:1363
+ *   re-bin            bin(...,0) + localPROP       mpc.c:4936-4942
+ * Within a cell, particles are visited in ascending particle index; the
+ * reference visits them in linked-list order, so sums differ only by
+ * rounding.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mpcd_gpu.h"
+#include "mpcd_rng.h"
+#include "mpcd_oracle.h"
+
+#define TOL 1e-8    /* definitions.h:56 */
+#define NBOUNCE 50  /* definitions.h:62 */
+
+struct oracle {
+    mpcd_config cfg;
+    int dim, n;
+    int L[3], N1[3], ncells;
+    int pbc[3];
+    double vol, gndnst;
+    double *Q, *V, *U, *T;
+    int *spid;
+    int *key, *start, *list, *cnt;
+    int *pop;
+    double *mass, *vcm, *cm, *I, *S, *dir, *E;
+    double wallQ[MPCD_MAX_WALLS][3];
+    double avnow[3], kbtnow;
+    long escaped, bounce_limit;
+};
+
+/* ------------------------------------------------------------ small math */
+static double dot3(const double *a, const double *b, int n) {
+    double r = 0.0;
+    for (int i = 0; i < n; i++) r += a[i] * b[i];
+    return r;
+}
+static void cross3(const double *x, const double *y, double *r) {
+    r[0] = x[1] * y[2] - x[2] * y[1];
+    r[1] = x[2] * y[0] - x[0] * y[2];
+    r[2] = x[0] * y[1] - x[1] * y[0];
+}
+/* inverse of a 3x3 matrix through its adjugate and determinant (the
+ * method of invert3x3, mtools.c:1031-1038) */
+static void inv3(const double m[9], double r[9]) {
+    double c00 = m[4] * m[8] - m[5] * m[7];
+    double c01 = m[3] * m[8] - m[5] * m[6];
+    double c02 = m[3] * m[7] - m[4] * m[6];
+    double det = m[0] * c00 - m[1] * c01 + m[2] * c02;
+    double c10 = m[1] * m[8] - m[2] * m[7];
+    double c11 = m[0] * m[8] - m[2] * m[6];
+    double c12 = m[0] * m[7] - m[1] * m[6];
+    double c20 = m[1] * m[5] - m[2] * m[4];
+    double c21 = m[0] * m[5] - m[2] * m[3];
+    double c22 = m[0] * m[4] - m[1] * m[3];
+    /* r[j][i] = (-1)^(i+j) minor(i,j) / det */
+    r[0] = c00 / det;
+    r[3] = -c01 / det;
+    r[6] = c02 / det;
+    r[1] = -c10 / det;
+    r[4] = c11 / det;
+    r[7] = -c12 / det;
+    r[2] = c20 / det;
+    r[5] = -c21 / det;
+    r[8] = c22 / det;
+}
+
+static int cell_index(const oracle_t *o, int a, int b, int c) {
+    return (a * o->N1[1] + b) * o->N1[2] + c;
+}
+
+static double wall_W(const oracle_t *o, int w, const double *q) {
+    /* calcW_PLANE, bc.c:306-316 */
+    const mpcd_wall *wl = &o->cfg.walls[w];
+    double W = 0.0;
+    for (int i = 0; i < o->dim; i++) W += wl->A[i] * (q[i] - o->wallQ[w][i]);
+    W -= wl->R;
+    if (wl->inv) W *= -1.0;
+    return W;
+}
+
+/* ----------------------------------------------------------- create/free */
+void oracle_destroy(oracle_t *o) {
+    if (!o) return;
+    free(o->Q);
+    free(o->V);
+    free(o->U);
+    free(o->T);
+    free(o->spid);
+    free(o->key);
+    free(o->start);
+    free(o->list);
+    free(o->cnt);
+    free(o->pop);
+    free(o->mass);
+    free(o->vcm);
+    free(o->cm);
+    free(o->I);
+    free(o->S);
+    free(o->dir);
+    free(o->E);
+    free(o);
+}
+
+static void bin_cells(oracle_t *o, int shifted);
+static void local_prop(oracle_t *o);
+
+oracle_t *oracle_create(const mpcd_config *cfg, int n, const double *Q,
+                        const double *V, const double *U, const int *spid) {
+    oracle_t *o = (oracle_t *)calloc(1, sizeof(oracle_t));
+    if (!o) return NULL;
+    o->cfg = *cfg;
+    o->dim = cfg->dim;
+    o->n = n;
+    for (int d = 0; d < 3; d++) {
+        o->L[d] = d < o->dim ? cfg->L[d] : 1;
+        o->N1[d] = o->L[d] + 1; /* (L+1)^D grid, read.c:1053 */
+    }
+    o->ncells = o->N1[0] * o->N1[1] * o->N1[2];
+    o->vol = 1.0;
+    for (int d = 0; d < o->dim; d++) o->vol *= o->L[d];
+    /* periodic axes as setPBC (read.c:584-603) */
+    for (int w = 0; w < cfg->n_walls; w++) {
+        const mpcd_wall *wl = &cfg->walls[w];
+        for (int d = 0; d < 3; d++) {
+            o->wallQ[w][d] = wl->Q[d];
+            if (fabs(fabs(wl->A[d]) - 1.0) <= TOL && wl->MVN > 0.0 &&
+                wl->MVT > 0.0 && (fabs(wl->DN) >= TOL || fabs(wl->DT) >= TOL))
+                o->pbc[d] = 1;
+        }
+    }
+    size_t n3 = (size_t)3 * (size_t)(n > 0 ? n : 1);
+    o->Q = (double *)malloc(n3 * sizeof(double));
+    o->V = (double *)malloc(n3 * sizeof(double));
+    o->U = (double *)calloc(n3, sizeof(double));
+    o->T = (double *)calloc(n3, sizeof(double));
+    o->spid = (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int));
+    o->key = (int *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int));
+    o->list = (int *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int));
+    o->start = (int *)malloc((size_t)(o->ncells + 1) * sizeof(int));
+    o->cnt = (int *)malloc((size_t)o->ncells * sizeof(int));
+    o->pop = (int *)calloc((size_t)o->ncells, sizeof(int));
+    o->mass = (double *)calloc((size_t)o->ncells, sizeof(double));
+    o->vcm = (double *)calloc((size_t)o->ncells * 3, sizeof(double));
+    o->cm = (double *)calloc((size_t)o->ncells * 3, sizeof(double));
+    o->I = (double *)calloc((size_t)o->ncells * 9, sizeof(double));
+    o->S = (double *)calloc((size_t)o->ncells, sizeof(double));
+    o->dir = (double *)calloc((size_t)o->ncells * 3, sizeof(double));
+    o->E = (double *)calloc((size_t)o->ncells * 9, sizeof(double));
+    memcpy(o->Q, Q, (size_t)3 * n * sizeof(double));
+    memcpy(o->V, V, (size_t)3 * n * sizeof(double));
+    if (U) memcpy(o->U, U, (size_t)3 * n * sizeof(double));
+    if (spid) memcpy(o->spid, spid, (size_t)n * sizeof(int));
+    /* initial binning + localPROP + globalDensities (init.c:2114-2127) */
+    bin_cells(o, 0);
+    local_prop(o);
+    if (cfg->gndnst > 0.0) {
+        o->gndnst = cfg->gndnst;
+    } else {
+        /* globalDensities, init.c:1002-1018: mean POPSRD over occupied cells
+         * of the L^D box (the extra layer excluded) */
+        double cnt = 0.0, sumN = 0.0;
+        for (int a = 0; a < o->L[0]; a++)
+            for (int b = 0; b < o->L[1]; b++)
+                for (int c = 0; c < o->L[2]; c++) {
+                    int ci = cell_index(o, a, b, c);
+                    if (o->pop[ci] > 0) {
+                        cnt += 1.0;
+                        sumN += (double)o->pop[ci];
+                    }
+                }
+        o->gndnst = cnt > 0.0 ? sumN / cnt : 0.0;
+    }
+    return o;
+}
+
+double oracle_gndnst(const oracle_t *o) { return o->gndnst; }
+int oracle_ncells(const oracle_t *o) { return o->ncells; }
+
+/* -------------------------------------------------------------- binning */
+/* Cell key by truncation; on shifted grids periodic axes map index L to 0
+ * (bin, mpc.c:958-968).  Particles outside the grid are counted as escaped
+ * and clamped (the reference re-places them at random, mpc.c:970-982). */
+static void bin_cells(oracle_t *o, int shifted) {
+    int n = o->n;
+    memset(o->cnt, 0, (size_t)o->ncells * sizeof(int));
+    for (int i = 0; i < n; i++) {
+        int idx[3];
+        for (int d = 0; d < 3; d++) {
+            int a = (int)o->Q[3 * i + d];
+            if (shifted && o->pbc[d] && a == o->L[d]) a = 0;
+            if (a < 0 || a > o->L[d]) {
+                o->escaped++;
+                a = a < 0 ? 0 : o->L[d];
+            }
+            idx[d] = a;
+        }
+        int k = cell_index(o, idx[0], idx[1], idx[2]);
+        o->key[i] = k;
+        o->cnt[k]++;
+    }
+    o->start[0] = 0;
+    for (int c = 0; c < o->ncells; c++) o->start[c + 1] = o->start[c] + o->cnt[c];
+    memset(o->cnt, 0, (size_t)o->ncells * sizeof(int));
+    for (int i = 0; i < n; i++) {
+        int k = o->key[i];
+        o->list[o->start[k] + o->cnt[k]++] = i;
+    }
+}
+
+static int compute_cm(int op, int lc) {
+    /* localPROP, mpc.c:75 */
+    return op == MPCD_COLL_RAT || lc != 0 || op == 15 || op == 16 || op == 17;
+}
+
+/* localPROP (mpc.c:64-216) for MPCD particles: POP, MASS, VCM, CM and the
+ * moment of inertia about CM (localMomInertiaTensor, mpc.c:4209-4299). */
+static void local_prop(oracle_t *o) {
+    int dim = o->dim, op = o->cfg.coll_op, lc = o->cfg.lc;
+    int ccm = compute_cm(op, lc);
+    for (int c = 0; c < o->ncells; c++) {
+        int s = o->start[c], e = o->start[c + 1];
+        double M = 0.0, v[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+        for (int j = s; j < e; j++) {
+            int i = o->list[j];
+            double m = o->cfg.species[o->spid[i]].mass;
+            M += m;
+            for (int d = 0; d < dim; d++) v[d] += o->V[3 * i + d] * m;
+            if (ccm)
+                for (int d = 0; d < dim; d++) q[d] += o->Q[3 * i + d] * m;
+        }
+        o->pop[c] = e - s;
+        o->mass[c] = M;
+        for (int d = 0; d < dim; d++) {
+            if (M > 0.0) {
+                v[d] /= M;
+                if (ccm) q[d] /= M;
+            }
+            o->vcm[3 * c + d] = v[d];
+            if (ccm) o->cm[3 * c + d] = q[d];
+        }
+        if (op == MPCD_COLL_RAT || lc != 0) {
+            double I[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int j = s; j < e; j++) {
+                int i = o->list[j];
+                double m = o->cfg.species[o->spid[i]].mass;
+                double r[3] = {0, 0, 0};
+                for (int d = 0; d < dim; d++) r[d] = o->Q[3 * i + d] - o->cm[3 * c + d];
+                I[0] += m * (r[1] * r[1] + r[2] * r[2]);
+                I[4] += m * (r[0] * r[0] + r[2] * r[2]);
+                I[8] += m * (r[0] * r[0] + r[1] * r[1]);
+                I[1] += m * r[0] * r[1];
+                I[2] += m * r[0] * r[2];
+                I[5] += m * r[1] * r[2];
+            }
+            I[1] = -I[1];
+            I[2] = -I[2];
+            I[5] = -I[5];
+            I[3] = I[1];
+            I[6] = I[2];
+            I[7] = I[5];
+            memcpy(&o->I[9 * c], I, sizeof(I));
+        }
+    }
+}
+
+/* ------------------------------------------------------------ phantoms */
+/* ghostPart (mpc.c:351-567), momentum part: a cell cut by a phantom wall
+ * (some corner with W < 0, walls at their shifted position) holding
+ * 0 < POP < GnDNST gets VCM <- (VCM + N(0, kT (GnDNST-POP))) / GnDNST. */
+static void ghost_part(oracle_t *o, uint32_t step) {
+    int dim = o->dim, nc = 1 << dim;
+    int any = 0;
+    for (int w = 0; w < o->cfg.n_walls; w++) any |= o->cfg.walls[w].phantom;
+    if (!any) return;
+    for (int a = 0; a <= o->L[0]; a++)
+        for (int b = 0; b <= o->L[1]; b++)
+            for (int c = 0; c <= o->L[2]; c++) {
+                int ci = cell_index(o, a, b, c);
+                if (o->pop[ci] <= 0) continue;
+                int cut = 0;
+                for (int w = 0; w < o->cfg.n_walls; w++) {
+                    if (!o->cfg.walls[w].phantom) continue;
+                    for (int j = 0; j < nc; j++) {
+                        double q[3] = {(double)a + (double)(j & 1),
+                                       (double)b + (double)((j >> 1) & 1),
+                                       (double)c + (double)((j >> 2) & 1)};
+                        if (wall_W(o, w, q) < 0.0) cut = 1;
+                    }
+                }
+                if (cut && o->pop[ci] < o->gndnst) {
+                    double invN = 1.0 / (o->gndnst - (double)o->pop[ci]);
+                    double sig = sqrt(o->cfg.kbt / invN);
+                    for (int d = 0; d < dim; d++) {
+                        float g = mpcd_rng_normal(o->cfg.seed, o->cfg.replica, step,
+                                                  MPCD_STREAM_GHOST, (uint32_t)ci,
+                                                  (uint32_t)d);
+                        o->vcm[3 * ci + d] += sig * (double)g;
+                        o->vcm[3 * ci + d] /= o->gndnst;
+                    }
+                }
+            }
+}
+
+/* ------------------------------------------------------------ collisions */
+/* SRD (stochrotMPC, mpc.c:1275-1333 with rotate, mpc.c:1181-1257): the
+ * rotation sign draw (long)genrand_real() is always 0, so the angle is
+ * always -RA; in 2D the random axis is unused. */
+static void collide_srd(oracle_t *o, int c, uint32_t step) {
+    int dim = o->dim;
+    double Cs = cos(o->cfg.rot_ang), Sn = -1.0 * sin(o->cfg.rot_ang);
+    double R[9];
+    if (dim == 3) {
+        double L[3];
+        mpcd_rng_axis3(o->cfg.seed, o->cfg.replica, step, (uint32_t)c, L);
+        R[0] = L[0] * L[0] + (1. - L[0] * L[0]) * Cs;
+        R[1] = L[0] * L[1] * (1. - Cs) - L[2] * Sn;
+        R[2] = L[0] * L[2] * (1. - Cs) + L[1] * Sn;
+        R[3] = L[0] * L[1] * (1. - Cs) + L[2] * Sn;
+        R[4] = L[1] * L[1] + (1. - L[1] * L[1]) * Cs;
+        R[5] = L[1] * L[2] * (1. - Cs) - L[0] * Sn;
+        R[6] = L[0] * L[2] * (1. - Cs) - L[1] * Sn;
+        R[7] = L[1] * L[2] * (1. - Cs) + L[0] * Sn;
+        R[8] = L[2] * L[2] + (1. - L[2] * L[2]) * Cs;
+    } else {
+        R[0] = Cs;
+        R[1] = -1. * Sn;
+        R[3] = Sn;
+        R[4] = Cs;
+    }
+    const double *u = &o->vcm[3 * c];
+    for (int j = o->start[c]; j < o->start[c + 1]; j++) {
+        int i = o->list[j];
+        double w[3] = {0, 0, 0}, t[3] = {0, 0, 0};
+        for (int d = 0; d < dim; d++) w[d] = o->V[3 * i + d] - u[d];
+        for (int a = 0; a < dim; a++)
+            for (int b = 0; b < dim; b++) t[a] += R[a * 3 + b] * w[b];
+        for (int d = 0; d < dim; d++) o->V[3 * i + d] = u[d] + t[d];
+    }
+}
+
+static void thermal_draw(const oracle_t *o, int i, uint32_t step, double *rv) {
+    double m = o->cfg.species[o->spid[i]].mass;
+    double sig = sqrt(o->cfg.kbt / m); /* genrand_gaussMB, rand.c:510-513 */
+    for (int d = 0; d < o->dim; d++)
+        rv[d] = sig * (double)mpcd_rng_normal(o->cfg.seed, o->cfg.replica, step,
+                                              MPCD_STREAM_THERMAL, (uint32_t)i,
+                                              (uint32_t)d);
+}
+
+/* Andersen MPC-AT (andersenMPC, mpc.c:1353-1444):
+ * v' = VCM + RV - RS - DAMP*VCM/POP, RS = sum(m RV)/M. */
+static void collide_mpcat(oracle_t *o, int c, uint32_t step) {
+    int dim = o->dim, s = o->start[c], e = o->start[c + 1];
+    double RS[3] = {0, 0, 0};
+    const double *u = &o->vcm[3 * c];
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double rv[3];
+        thermal_draw(o, i, step, rv);
+        double m = o->cfg.species[o->spid[i]].mass;
+        for (int d = 0; d < dim; d++) RS[d] += m * rv[d];
+    }
+    for (int d = 0; d < dim; d++) RS[d] /= o->mass[c];
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double rv[3];
+        thermal_draw(o, i, step, rv);
+        double damp = o->cfg.species[o->spid[i]].damp;
+        for (int d = 0; d < dim; d++)
+            o->V[3 * i + d] =
+                u[d] + rv[d] - RS[d] - damp * u[d] / (double)(e - s);
+    }
+}
+
+/* Andersen MPC-AT+a (andersenROT, mpc.c:1461-1657): as MPC-AT with the
+ * damping not divided by POP, plus the angular-momentum restoring term
+ * W x (r - CM), W = I^-1 sum (r-CM) x m(v - RV).  3D: I inverted by
+ * adjugate, zero for POP < 3; 2D: only 1/I_zz. */
+static void collide_rat(oracle_t *o, int c, uint32_t step) {
+    int dim = o->dim, s = o->start[c], e = o->start[c + 1];
+    int pop = e - s;
+    double RS[3] = {0, 0, 0}, Lm[3] = {0, 0, 0}, W[3] = {0, 0, 0};
+    double II[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double *u = &o->vcm[3 * c], *cm = &o->cm[3 * c];
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double rv[3];
+        thermal_draw(o, i, step, rv);
+        double m = o->cfg.species[o->spid[i]].mass;
+        for (int d = 0; d < dim; d++) RS[d] += m * rv[d];
+    }
+    for (int d = 0; d < dim; d++) RS[d] /= o->mass[c];
+    if (dim == 3) {
+        if (pop >= 3) inv3(&o->I[9 * c], II);
+    } else {
+        II[8] = 1. / o->I[9 * c + 8];
+    }
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double rv[3] = {0, 0, 0}, r[3] = {0, 0, 0}, dv[3] = {0, 0, 0}, am[3];
+        thermal_draw(o, i, step, rv);
+        double m = o->cfg.species[o->spid[i]].mass;
+        for (int d = 0; d < dim; d++) {
+            r[d] = o->Q[3 * i + d] - cm[d];
+            dv[d] = m * (o->V[3 * i + d] - rv[d]);
+        }
+        cross3(r, dv, am);
+        for (int d = 0; d < 3; d++) Lm[d] += am[d];
+    }
+    for (int a = 0; a < 3; a++) {
+        W[a] = 0.0;
+        for (int b = 0; b < 3; b++) W[a] += II[a * 3 + b] * Lm[b];
+    }
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double rv[3] = {0, 0, 0}, r[3] = {0, 0, 0}, ang[3];
+        thermal_draw(o, i, step, rv);
+        double damp = o->cfg.species[o->spid[i]].damp;
+        for (int d = 0; d < dim; d++) r[d] = o->Q[3 * i + d] - cm[d];
+        cross3(W, r, ang);
+        for (int d = 0; d < dim; d++)
+            o->V[3 * i + d] = u[d] + rv[d] - RS[d] - damp * u[d] + ang[d];
+    }
+}
+
+/* ----------------------------------------------------------------- walls */
+/* MPC_BCcollision (bc.c:1363-1496) for static planar walls with rule-based
+ * collisions (COLL_TYPE 1): repeatedly find the wall crossed earliest
+ * (chooseBC, bc.c:1252-1334), rewind to it, transform velocity (velBC,
+ * bc.c:598-746) and position (posBC, bc.c:760-774), stream the rest. */
+static void wall_collisions(oracle_t *o, int i) {
+    int dim = o->dim, nw = o->cfg.n_walls;
+    double *q = &o->Q[3 * i], *v = &o->V[3 * i];
+    double dt = o->cfg.dt, t_left = dt, t_coll = 0.0;
+    int chosen = 0, cnt = 0, cnt2 = 0;
+    double m = o->cfg.species[o->spid[i]].mass;
+    for (;;) {
+        double t_min = t_left, W = 1.0;
+        for (int w = 0; w < nw; w++) {
+            const mpcd_wall *wl = &o->cfg.walls[w];
+            if (!wl->inter[o->spid[i]]) continue;
+            double tw = wall_W(o, w, q);
+            if (tw < 0.0) {
+                /* crosstimeReverse, planar branch (bc.c:257-262) */
+                double t1 = wl->R;
+                for (int d = 0; d < dim; d++) t1 += wl->A[d] * (o->wallQ[w][d] - q[d]);
+                t1 /= (wl->A[0] * (-v[0]) + wl->A[1] * (-v[1]) + wl->A[2] * (-v[2]));
+                double tc = t_left - t1;
+                if (tc < t_min) {
+                    t_min = tc;
+                    chosen = w;
+                    W = tw;
+                }
+            }
+        }
+        t_coll = t_min;
+        if (W > -TOL) break;
+        cnt++;
+        const mpcd_wall *wl = &o->cfg.walls[chosen];
+        if (t_coll > -TOL) {
+            double n[3] = {0, 0, 0}, vn[3] = {0, 0, 0}, vt[3] = {0, 0, 0};
+            double V[3] = {0, 0, 0};
+            for (int d = 0; d < dim; d++) q[d] = q[d] - (t_left - t_coll) * v[d];
+            for (int d = 0; d < dim; d++) n[d] = wl->A[d];
+            double len = sqrt(dot3(n, n, dim));
+            if (fabs(len) >= TOL)
+                for (int d = 0; d < dim; d++) n[d] = n[d] / len;
+            /* velBC, rule branch: walls at rest, no spin */
+            for (int d = 0; d < dim; d++) V[d] = v[d] - 0.0 - 0.0;
+            double x = dot3(V, n, dim);
+            for (int d = 0; d < dim; d++) vn[d] = x * n[d];
+            for (int d = 0; d < dim; d++) vt[d] = V[d] - vn[d];
+            for (int d = 0; d < dim; d++) {
+                vn[d] *= wl->MVN;
+                vn[d] += wl->DVN * n[d];
+                vt[d] *= wl->MVT;
+                vt[d] += wl->DVT;
+            }
+            for (int d = 0; d < dim; d++) V[d] = vn[d] + vt[d];
+            for (int d = 0; d < dim; d++) V[d] += wl->DVxyz[d];
+            for (int d = 0; d < dim; d++) V[d] += 0.0 + 0.0;
+            for (int d = 0; d < dim; d++) {
+                V[d] -= v[d];
+                V[d] *= m;
+            }
+            double imp = 1.0 / m;
+            for (int d = 0; d < dim; d++) v[d] += V[d] * 1.0 * imp;
+            /* posBC */
+            double pn[3], pt[3];
+            double xq = dot3(q, n, dim);
+            for (int d = 0; d < dim; d++) pn[d] = xq * n[d];
+            for (int d = 0; d < dim; d++) pt[d] = q[d] - pn[d];
+            for (int d = 0; d < dim; d++) {
+                pn[d] += wl->DN * n[d] * (1. - 2. * TOL);
+                pt[d] += wl->DT;
+            }
+            for (int d = 0; d < dim; d++) q[d] = pn[d] + pt[d];
+            t_left -= t_coll;
+            for (int d = 0; d < dim; d++) q[d] = q[d] + t_left * v[d];
+            if (wall_W(o, chosen, q) < -TOL)
+                for (int d = 0; d < dim; d++) q[d] = q[d] - t_left * v[d];
+        } else {
+            for (int d = 0; d < dim; d++) q[d] = q[d] - (t_left - t_coll) * v[d];
+        }
+        if (cnt > NBOUNCE) {
+            if (cnt < 2 * NBOUNCE && cnt2 == 0) {
+                if (t_left > TOL) {
+                    t_left *= 1.1;
+                } else {
+                    t_left = 0.9 * dt;
+                    t_coll = 0.1 * dt;
+                }
+            } else {
+                /* the reference re-thermalises here (bc.c:1478-1488) */
+                o->bounce_limit++;
+                break;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ step */
+int oracle_step(oracle_t *o, uint32_t step) {
+    int dim = o->dim, n = o->n, op = o->cfg.coll_op;
+    double s[3] = {0, 0, 0};
+    if (o->cfg.lc != 0) return MPCD_ERR_UNSUPPORTED;
+    if (o->cfg.galinv) mpcd_rng_shift(o->cfg.seed, o->cfg.replica, step, dim, s);
+    /* gridShift_all(...,0), mpc.c:728-736 and walls :765 */
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < dim; d++) {
+            double *q = &o->Q[3 * i + d];
+            *q += s[d];
+            if (*q > o->L[d] && *q <= o->L[d] + s[d]) *q -= o->L[d];
+        }
+    for (int w = 0; w < o->cfg.n_walls; w++)
+        for (int d = 0; d < dim; d++) o->wallQ[w][d] += s[d];
+    bin_cells(o, 1);
+    /* acc_all, mpc.c:697-700 (GRAV_FLAG as initializeSIM, init.c:2059) */
+    const double *g = o->cfg.grav;
+    if (fabs(g[0]) >= TOL || fabs(g[1]) >= TOL || fabs(g[2]) >= TOL)
+        for (int i = 0; i < n; i++)
+            for (int d = 0; d < dim; d++) o->V[3 * i + d] = o->V[3 * i + d] + o->cfg.dt * g[d];
+    local_prop(o);
+    ghost_part(o, step);
+    for (int c = 0; c < o->ncells; c++) {
+        if (o->pop[c] <= 1) continue;
+        if (op == MPCD_COLL_ARBAXIS)
+            collide_srd(o, c, step);
+        else if (op == MPCD_COLL_MPCAT)
+            collide_mpcat(o, c, step);
+        else if (op == MPCD_COLL_RAT)
+            collide_rat(o, c, step);
+        else
+            return MPCD_ERR_UNSUPPORTED;
+    }
+    /* avVel (therm.c:362-367) over every cell; TEMP (therm.c:209-235) */
+    for (int d = 0; d < 3; d++) o->avnow[d] = 0.0;
+    for (int c = 0; c < o->ncells; c++)
+        for (int d = 0; d < dim; d++) o->avnow[d] += o->vcm[3 * c + d];
+    for (int d = 0; d < dim; d++) o->avnow[d] /= o->vol;
+    double kbt = 0.0;
+    for (int i = 0; i < n; i++) {
+        const double *v = &o->V[3 * i];
+        double t = (v[0] - 0.0) * (v[0] - 0.0);
+        t += (v[1] - 0.0) * (v[1] - 0.0);
+        t += (v[2] - 0.0) * (v[2] - 0.0);
+        kbt += o->cfg.species[o->spid[i]].mass * t;
+    }
+    o->kbtnow = kbt / (double)(n * dim);
+    /* gridShift_all(...,1) */
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < dim; d++) {
+            double *q = &o->Q[3 * i + d];
+            *q += -1.0 * s[d];
+            if (*q < 0.0 && *q >= -1.0 * s[d]) *q += o->L[d];
+        }
+    for (int w = 0; w < o->cfg.n_walls; w++)
+        for (int d = 0; d < dim; d++) o->wallQ[w][d] += -1.0 * s[d];
+    /* stream_all, mpc.c:680-687 */
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < dim; d++) o->Q[3 * i + d] = o->Q[3 * i + d] + o->cfg.dt * o->V[3 * i + d];
+    for (int i = 0; i < n; i++) wall_collisions(o, i);
+    /* re-bin on the unshifted grid + localPROP, mpc.c:4936-4942 */
+    bin_cells(o, 0);
+    local_prop(o);
+    return 0;
+}
+
+int oracle_get_particles(const oracle_t *o, double *Q, double *V, double *U) {
+    if (Q) memcpy(Q, o->Q, (size_t)3 * o->n * sizeof(double));
+    if (V) memcpy(V, o->V, (size_t)3 * o->n * sizeof(double));
+    if (U) memcpy(U, o->U, (size_t)3 * o->n * sizeof(double));
+    return 0;
+}
+
+int oracle_get_globals(const oracle_t *o, double *kbtnow, double *avnow) {
+    *kbtnow = o->kbtnow;
+    for (int d = 0; d < 3; d++) avnow[d] = o->avnow[d];
+    return 0;
+}
+
+int oracle_get_cells(const oracle_t *o, int *pop, double *mass, double *vcm,
+                     double *cm) {
+    for (int c = 0; c < o->ncells; c++) {
+        if (pop) pop[c] = o->pop[c];
+        if (mass) mass[c] = o->mass[c];
+        for (int d = 0; d < 3; d++) {
+            if (vcm) vcm[3 * c + d] = o->vcm[3 * c + d];
+            if (cm) cm[3 * c + d] = o->cm[3 * c + d];
+        }
+    }
+    return 0;
+}
+
+long oracle_escaped(const oracle_t *o) { return o->escaped; }

@@ -1,0 +1,486 @@
+/*
+ * ref_harness.c -- TEST INFRASTRUCTURE ONLY.  Drives the reference program's
+ * own solvent timestep (NIAMH-MPCD, compiled unmodified from its sources into
+ * oracle/_ref/) on state built here, so its outputs can pin the CPU oracle and
+ * be committed as golden fixtures.  Nothing in the product links this file.
+ *
+ * Two builds of this file exist (oracle/ref/Makefile):
+ *
+ *  - libmpcdref.so (REF_INJECT defined): the reference's rand.c is replaced by
+ *    the functions below, which hand out the counter-based draws of
+ *    niamh-mpcd_b200/csrc/mpcd_rng.h.  The reference visits cells and
+ *    particles in its own serial order, so the harness interposes the
+ *    per-cell entry points (MPCcollision, ghostPart, LCcollision,
+ *    genrand_maierSaupe) to learn which cell or particle a draw belongs to.
+ *    Interposition works because the reference objects are built -fPIC with
+ *    GCC's default semantic interposition: their calls to these global
+ *    functions go through the PLT and resolve to the definitions here first.
+ *
+ *  - libmpcdref_time.so: the reference's own rand.c (Mersenne Twister) and
+ *    no interposers, built -fno-semantic-interposition, to time the
+ *    reference's serial timestep as the CPU baseline.
+ *
+ * State is built directly (positions, velocities, walls) instead of through
+ * readJson, skipping accessibleVolume (init.c:954-989), which takes minutes.
+ * Walls are filled as readJson fills a JSON "BC" entry (read.c:1141-1428).
+ */
+#define _GNU_SOURCE
+#include <dlfcn.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+/* product headers first: the reference headers define macros named e, pi
+ * and real (definitions.h:73-75, md/mdtypes.h:52) */
+#include "mpcd_gpu.h"
+#include "mpcd_rng.h"
+
+#include "definitions.h"
+#include "SRDclss.h"
+#include "mpc.h"
+#include "init.h"
+#include "therm.h"
+
+/* reference globals (globals.h:24-65, common symbols of the core library) */
+extern int DBUG, DIM, MDmode, GPOP, NSPECI, NBC, NS;
+extern double VOL, GnDNST, GmDNST, GMASS;
+extern int XYZ[_3D], XYZ_P1[_3D], XYZPBC[_3D], maxXYZ;
+extern int BMHASSPARE;
+extern double BMSPARE;
+
+void setPBC(bc *WALL);                         /* read.c:584 */
+double calcW(bc WALL, particleMPC P);          /* bc.c:55    */
+unsigned long RandomSeedSRD(unsigned long s);  /* rand.c:293 */
+
+/* ------------------------------------------------------------------ state */
+static cell ***g_CL = NULL;
+static cell *g_cells = NULL;
+static particleMPC *g_pp = NULL;
+static spec *g_SP = NULL;
+static bc *g_WALL = NULL;
+static specSwimmer *g_SS = NULL;
+static inputList g_in;
+static outputFlagsList g_oflags;
+static outputFilesList g_ofiles;
+static double g_AVNOW[3], g_AVV[3], g_avDIR[3], g_KBTNOW, g_AVS;
+static int g_ncells = 0;
+
+/* draw bookkeeping */
+static uint64_t g_seed = 0;
+static uint32_t g_replica = 0, g_step = 0;
+enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC };
+static int g_phase = PH_NONE;
+static int g_cell = 0;
+static particleMPC *g_cursor = NULL;
+static int g_comp = 0;
+static int g_pid = 0;
+static uint32_t g_k = 0;
+static int *g_ghost = NULL;
+static int g_ghost_n = 0, g_ghost_pos = 0;
+static long g_unexpected = 0;
+
+static int cell_id(const cell *c) { return (int)(c - g_cells); }
+
+/* ------------------------------------------------------------ set-up/API */
+int ref_free(void) {
+    if (g_CL) {
+        for (int i = 0; i < XYZ_P1[0]; i++) free(g_CL[i]);
+        free(g_CL);
+    }
+    free(g_cells);
+    free(g_pp);
+    free(g_SP);
+    free(g_WALL);
+    free(g_SS);
+    free(g_ghost);
+    g_CL = NULL;
+    g_cells = NULL;
+    g_pp = NULL;
+    g_SP = NULL;
+    g_WALL = NULL;
+    g_SS = NULL;
+    g_ghost = NULL;
+    return 0;
+}
+
+/* Build the reference's state from a config and particle arrays (AoS, 3
+ * doubles per vector).  Returns 0 on success. */
+int ref_init(const mpcd_config *cfg, int n, const double *Q, const double *V,
+             const double *U, const int *spid) {
+    int i, j, d;
+    ref_free();
+    DBUG = 0;
+    DIM = cfg->dim;
+    MDmode = 0;
+    NS = 0;
+    GPOP = n;
+    NSPECI = cfg->n_species;
+    NBC = cfg->n_walls;
+    for (d = 0; d < 3; d++) {
+        XYZ[d] = (d < DIM) ? cfg->L[d] : 1; /* read.c:1040-1044 */
+        XYZ_P1[d] = XYZ[d] + 1;
+    }
+    VOL = 1.0;
+    for (d = 0; d < DIM; d++) VOL *= XYZ[d];
+    maxXYZ = (int)sqrt((double)(XYZ[0] * XYZ[0] + XYZ[1] * XYZ[1] + XYZ[2] * XYZ[2]));
+    BMHASSPARE = 0;
+    BMSPARE = 0.0;
+
+    g_SP = (spec *)calloc((size_t)NSPECI, sizeof(spec));
+    for (i = 0; i < NSPECI; i++) {
+        const mpcd_species *s = &cfg->species[i];
+        g_SP[i].MASS = s->mass;
+        g_SP[i].DAMP = s->damp;
+        g_SP[i].RFC = s->rfc;
+        g_SP[i].TUMBLE = s->tumble;
+        g_SP[i].CHIHI = s->chihi;
+        g_SP[i].ACT = s->act;
+        g_SP[i].MFPOT = s->mfpot;
+        g_SP[i].SIGWIDTH = s->sigwidth;
+        g_SP[i].SIGPOS = s->sigpos;
+        g_SP[i].MINACTRATIO = s->minactratio;
+        g_SP[i].LEN = 0.007;
+        g_SP[i].POP = 0;
+    }
+    for (i = 0; i < n; i++) g_SP[spid ? spid[i] : 0].POP++;
+
+    g_WALL = (bc *)calloc((size_t)(NBC > 0 ? NBC : 1), sizeof(bc));
+    for (i = 0; i < NBC; i++) {
+        const mpcd_wall *w = &cfg->walls[i];
+        bc *b = &g_WALL[i];
+        b->COLL_TYPE = w->coll_type;
+        b->PHANTOM = w->phantom;
+        b->E = -1.0;
+        for (d = 0; d < 3; d++) {
+            b->Q[d] = w->Q[d];
+            b->A[d] = w->A[d];
+            b->AINV[d] = (w->A[d] != 0.0) ? 1.0 / w->A[d] : 0.0;
+            b->DVxyz[d] = w->DVxyz[d];
+            b->MUxyz[d] = w->MUxyz[d];
+            b->DUxyz[d] = w->DUxyz[d];
+        }
+        for (d = 0; d < 4; d++) b->P[d] = 1.0;
+        b->ROTSYMM[0] = 4.0;
+        b->ROTSYMM[1] = 4.0;
+        b->R = w->R;
+        b->INV = w->inv;
+        b->DN = w->DN;
+        b->DT = w->DT;
+        b->DVN = w->DVN;
+        b->DVT = w->DVT;
+        b->MVN = w->MVN;
+        b->MVT = w->MVT;
+        b->MUN = w->MUN;
+        b->MUT = w->MUT;
+        b->KBT = 1.0;
+        b->MASS = 1.0;
+        b->DSPLC = 0;
+        b->REORIENT = 0; /* init.c:2063-2065: static walls with O = 0 */
+        for (j = 0; j < MAXSPECI; j++) b->INTER[j] = w->inter[j];
+        b->INTER[MAXSPECI] = BCON;
+        b->INTER[MAXSPECI + 1] = BCON;
+        /* PLANAR flag as read.c:1417-1428 */
+        b->PLANAR = 0;
+        if ((b->A[0] != 0.0) + (b->A[1] != 0.0) + (b->A[2] != 0.0) == 1) b->PLANAR = 1;
+    }
+    for (d = 0; d < 3; d++) XYZPBC[d] = 0;
+    for (i = 0; i < NBC; i++) setPBC(&g_WALL[i]);
+
+    g_pp = (particleMPC *)calloc((size_t)(n > 0 ? n : 1), sizeof(particleMPC));
+    for (i = 0; i < n; i++) {
+        for (d = 0; d < 3; d++) {
+            g_pp[i].Q[d] = Q[3 * i + d];
+            g_pp[i].V[d] = V[3 * i + d];
+            g_pp[i].U[d] = U ? U[3 * i + d] : 0.0;
+        }
+        g_pp[i].SPID = spid ? spid[i] : 0;
+        g_pp[i].S_flag = STREAM;
+    }
+
+    g_ncells = XYZ_P1[0] * XYZ_P1[1] * XYZ_P1[2];
+    g_cells = (cell *)calloc((size_t)g_ncells, sizeof(cell));
+    g_CL = (cell ***)malloc((size_t)XYZ_P1[0] * sizeof(cell **));
+    for (i = 0; i < XYZ_P1[0]; i++) {
+        g_CL[i] = (cell **)malloc((size_t)XYZ_P1[1] * sizeof(cell *));
+        for (j = 0; j < XYZ_P1[1]; j++)
+            g_CL[i][j] = g_cells + ((size_t)i * XYZ_P1[1] + j) * XYZ_P1[2];
+    }
+    g_ghost = (int *)malloc((size_t)g_ncells * sizeof(int));
+    g_SS = (specSwimmer *)calloc(1, sizeof(specSwimmer));
+
+    memset(&g_in, 0, sizeof(g_in));
+    g_in.KBT = cfg->kbt;
+    g_in.dt = cfg->dt;
+    g_in.RA = cfg->rot_ang;
+    g_in.C = cos(cfg->rot_ang); /* initvar, init.c:1194-1195 */
+    g_in.S = sin(cfg->rot_ang);
+    g_in.RTECH = cfg->coll_op;
+    g_in.LC = cfg->lc;
+    g_in.GALINV = cfg->galinv;
+    g_in.TSTECH = NOTHERM;
+    g_in.TAU = 0.5;
+    g_in.noHI = HION;
+    g_in.inCOMP = INCOMPOFF;
+    g_in.MULTIPHASE = MPHOFF;
+    g_in.seed = (unsigned long)cfg->seed;
+    for (d = 0; d < 3; d++) g_in.GRAV[d] = cfg->grav[d];
+    g_in.GRAV_FLAG = (fabs(g_in.GRAV[0]) >= TOL || fabs(g_in.GRAV[1]) >= TOL ||
+                      fabs(g_in.GRAV[2]) >= TOL);
+    memset(&g_oflags, 0, sizeof(g_oflags));
+    memset(&g_ofiles, 0, sizeof(g_ofiles));
+    for (d = 0; d < 3; d++) g_AVNOW[d] = g_AVV[d] = g_avDIR[d] = 0.0;
+    g_KBTNOW = 0.0;
+    g_AVS = 0.0;
+
+    g_seed = cfg->seed;
+    g_replica = cfg->replica;
+#ifndef REF_INJECT
+    RandomSeedSRD((unsigned long)(cfg->seed ? cfg->seed : 1));
+#endif
+    binin(g_pp, g_CL);
+    localPROP(g_CL, g_SP, *g_SS, g_in.RTECH, g_in.LC);
+    globalDensities(g_CL, g_SP);
+    if (cfg->gndnst > 0.0) GnDNST = cfg->gndnst;
+    return 0;
+}
+
+double ref_gndnst(void) { return GnDNST; }
+int ref_ncells(void) { return g_ncells; }
+long ref_unexpected_draws(void) { return g_unexpected; }
+
+/* One call of the reference timestep() (mpc.c:4496) numbered 'step'. */
+int ref_step(uint32_t step) {
+    if (!g_pp) return -1;
+    g_step = step;
+    timestep(g_CL, g_pp, g_SP, g_WALL, NULL, g_SS, NULL, g_AVNOW, g_AVV, g_avDIR,
+             g_in, &g_KBTNOW, &g_AVS, (int)step, 0, g_oflags, g_ofiles);
+    return 0;
+}
+
+/* Run nsteps and return the elapsed wall time in seconds (CPU baseline). */
+double ref_run_timed(int nsteps, uint32_t step0) {
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    for (int s = 0; s < nsteps; s++) ref_step(step0 + (uint32_t)s);
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+}
+
+int ref_get_particles(double *Q, double *V, double *U) {
+    for (int i = 0; i < GPOP; i++)
+        for (int d = 0; d < 3; d++) {
+            if (Q) Q[3 * i + d] = g_pp[i].Q[d];
+            if (V) V[3 * i + d] = g_pp[i].V[d];
+            if (U) U[3 * i + d] = g_pp[i].U[d];
+        }
+    return 0;
+}
+
+int ref_get_globals(double *kbtnow, double *avnow) {
+    *kbtnow = g_KBTNOW;
+    for (int d = 0; d < 3; d++) avnow[d] = g_AVNOW[d];
+    return 0;
+}
+
+/* Cell properties as left by the last timestep (re-bin + localPROP on the
+ * unshifted grid, mpc.c:4936-4942), cells in (a,b,c) row-major order. */
+int ref_get_cells(int *pop, double *mass, double *vcm, double *cm) {
+    for (int c = 0; c < g_ncells; c++) {
+        if (pop) pop[c] = g_cells[c].POP;
+        if (mass) mass[c] = g_cells[c].MASS;
+        for (int d = 0; d < 3; d++) {
+            if (vcm) vcm[3 * c + d] = g_cells[c].VCM[d];
+            if (cm) cm[3 * c + d] = g_cells[c].CM[d];
+        }
+    }
+    return 0;
+}
+
+#ifdef REF_INJECT
+/* ======================================================================
+ * Replacement of mpcd/subroutines/rand.c: every symbol another reference
+ * translation unit calls, serving the counter-based draws.
+ * ====================================================================== */
+static float next_normal(void) {
+    float g = 0.0f;
+    if (g_phase == PH_COLLIDE && g_cursor) {
+        int pid = (int)(g_cursor - g_pp);
+        g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_THERMAL,
+                            (uint32_t)pid, (uint32_t)g_comp);
+        if (++g_comp == DIM) {
+            g_comp = 0;
+            g_cursor = g_cursor->next;
+        }
+    } else if (g_phase == PH_GHOST && g_ghost_pos < g_ghost_n) {
+        g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_GHOST,
+                            (uint32_t)g_ghost[g_ghost_pos], (uint32_t)g_comp);
+        if (++g_comp == DIM) {
+            g_comp = 0;
+            g_ghost_pos++;
+        }
+    } else {
+        g_unexpected++;
+    }
+    return g;
+}
+
+unsigned long RandomSeedSRD(unsigned long seed) { return seed; }
+void init_genrand(unsigned long s) { (void)s; }
+unsigned long genrand_int32(void) {
+    g_unexpected++;
+    return 0x80000000ul;
+}
+long genrand_int31(void) { return (long)(genrand_int32() >> 1); }
+
+double genrand_real(void) {
+    if (g_phase == PH_LC)
+        return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_LC,
+                                (uint32_t)g_pid, g_k++);
+    /* stochrotMPC draws a uniform only for the rotation sign, which
+     * (long)genrand_real() truncates to 0 (mpc.c:1291) */
+    if (g_phase == PH_COLLIDE) return 0.0;
+    g_unexpected++;
+    return 0.5;
+}
+double genrand_pmOne(void) { return genrand_real() <= 0.5 ? -1.0 : 1.0; }
+float genrand_gauss(void) { return next_normal(); }
+double genrand_gaussMB(double KBT, double M) {
+    double sigma = sqrt(KBT / M);
+    return sigma * next_normal();
+}
+double genrand_gaussGen(double mu, double sigma) { return sigma * next_normal() + mu; }
+double genrand_exp(double lambda) {
+    g_unexpected++;
+    return lambda;
+}
+int genrand_poisson(double lambda) {
+    g_unexpected++;
+    return (int)lambda;
+}
+float genrand_rayleigh(float std) {
+    g_unexpected++;
+    return std;
+}
+void genrand_sphere(double vec[], int dimension) {
+    g_unexpected++;
+    for (int i = 0; i < dimension; i++) vec[i] = (i == 0);
+}
+void genrand_coneNP(double vec[], double theta, int dimension) {
+    (void)theta;
+    genrand_sphere(vec, dimension);
+}
+void genrand_cone(double axis[], double vecOut[], double theta, int dimension) {
+    (void)axis;
+    genrand_coneNP(vecOut, theta, dimension);
+}
+double *ranvec3D(double *v) {
+    mpcd_rng_axis3(g_seed, g_replica, g_step, (uint32_t)g_cell, v);
+    return v;
+}
+double *ranvec2D(double *v) {
+    v[0] = 1.0;
+    v[1] = 0.0;
+    return v;
+}
+double *ranvec(double *v, int dimension) {
+    if (g_phase != PH_COLLIDE) g_unexpected++;
+    if (dimension == _3D) ranvec3D(v);
+    if (dimension == _2D) ranvec2D(v);
+    return v;
+}
+double *ranshift(double *v, int doShift, int dimension) {
+    if (doShift) {
+        mpcd_rng_shift(g_seed, g_replica, g_step, dimension, v);
+    } else {
+        v[0] = v[1] = v[2] = 0.0;
+    }
+    return v;
+}
+int rand_particle(int POP) {
+    g_unexpected++;
+    return POP / 2;
+}
+
+/* ======================================================================
+ * Interposers: set the cursor, then call the reference's own function.
+ * ====================================================================== */
+typedef void (*mpccoll_fn)(cell *, spec *, specSwimmer, double, int, double,
+                           double, double, double, int, int, double, double *,
+                           int);
+void MPCcollision(cell *CL, spec *SP, specSwimmer SS, double KBT, int RTECH,
+                  double C, double S, double FRICCO, double TimeStep,
+                  int MD_mode, int LC, double RELAX, double *CLQ, int outP) {
+    static mpccoll_fn orig = NULL;
+    if (!orig) orig = (mpccoll_fn)dlsym(RTLD_NEXT, "MPCcollision");
+    g_phase = PH_COLLIDE;
+    g_cell = cell_id(CL);
+    g_cursor = CL->pp;
+    g_comp = 0;
+    orig(CL, SP, SS, KBT, RTECH, C, S, FRICCO, TimeStep, MD_mode, LC, RELAX, CLQ,
+         outP);
+    g_phase = PH_NONE;
+}
+
+/* The cells ghostPart (mpc.c:351-567) fills: cut by a phantom wall (some
+ * corner with W < 0) and 0 < POP < GnDNST, in its x->y->z order. */
+typedef void (*ghost_fn)(cell ***, bc *, double, int, spec *);
+void ghostPart(cell ***CL, bc WALL[], double KBT, int LC, spec *SP) {
+    static ghost_fn orig = NULL;
+    if (!orig) orig = (ghost_fn)dlsym(RTLD_NEXT, "ghostPart");
+    int ncorner = 1 << DIM;
+    particleMPC tp;
+    memset(&tp, 0, sizeof(tp));
+    g_ghost_n = 0;
+    for (int a = 0; a <= XYZ[0]; a++)
+        for (int b = 0; b <= XYZ[1]; b++)
+            for (int c = 0; c <= XYZ[2]; c++) {
+                cell *cl = &CL[a][b][c];
+                if (cl->POP <= 0) continue;
+                int flagW = 0;
+                for (int i = 0; i < NBC; i++) {
+                    if (!WALL[i].PHANTOM) continue;
+                    for (int j = 0; j < ncorner; j++) {
+                        tp.Q[0] = (double)a + (double)(j & 1);
+                        tp.Q[1] = (double)b + (double)((j >> 1) & 1);
+                        tp.Q[2] = (double)c + (double)((j >> 2) & 1);
+                        if (calcW(WALL[i], tp) < 0.0) flagW = 1;
+                    }
+                }
+                if (flagW && cl->POP < GnDNST && cl->POP > 0)
+                    g_ghost[g_ghost_n++] = cell_id(cl);
+            }
+    g_phase = PH_GHOST;
+    g_ghost_pos = 0;
+    g_comp = 0;
+    orig(CL, WALL, KBT, LC, SP);
+    if (g_ghost_pos != g_ghost_n) g_unexpected++;
+    g_phase = PH_NONE;
+}
+
+typedef void (*lccoll_fn)(cell *, spec *, double, int, double, double, int);
+void LCcollision(cell *CL, spec *SP, double KBT, int zeroMFPot, double dt,
+                 double SG, int LC) {
+    static lccoll_fn orig = NULL;
+    if (!orig) orig = (lccoll_fn)dlsym(RTLD_NEXT, "LCcollision");
+    g_phase = PH_LC;
+    g_cell = cell_id(CL);
+    orig(CL, SP, KBT, zeroMFPot, dt, SG, LC);
+    g_phase = PH_NONE;
+}
+
+typedef void (*ms_fn)(double *, double *, double, double *, double, double,
+                      double);
+void genrand_maierSaupe(double DIR[], double rotAx[], double rotAngle,
+                        double U[], double KBT, double S, double effM) {
+    static ms_fn orig = NULL;
+    if (!orig) orig = (ms_fn)dlsym(RTLD_NEXT, "genrand_maierSaupe");
+    particleMPC *p =
+        (particleMPC *)((char *)U - offsetof(particleMPC, U));
+    g_pid = (int)(p - g_pp);
+    g_k = 0;
+    orig(DIR, rotAx, rotAngle, U, KBT, S, effM);
+}
+#endif /* REF_INJECT */
