@@ -1,0 +1,280 @@
+"""Benchmark of the MPCD solvent timestep on B200.
+
+Workload (one step = one solvent timestep of every particle): the 3D SRD
+fluid of 64^3 periodic cells, 10 particles per cell (2,621,440 particles),
+kT=1, dt=0.1, rotation angle 130 degrees about a random axis per cell, random
+grid shift, synthetic seeded state.  The headline is the mixed-precision form;
+the plain FP64 form is measured in the same run ("fp64" key).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs independent replica boxes, one per rank (the path has no data
+exchange between replicas): weak scaling, value summed over ranks, time the
+max over ranks.  --impl reference times the reference's own serial C timestep
+(built from its sources into oracle/_ref/) on a bounded sample of the same
+workload on this host's cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "niamh-mpcd_b200"))
+
+METRIC = "MPCD particle-steps/s, mixed vs FP64 on 1 B200; achieved HBM GB/s"
+UNIT = "particle-steps/s"
+L_BOX = (64, 64, 64)
+PPC = 10
+# algorithmic bytes per particle-step (state read+written once, cell record
+# written+read once per ppc particles): 3D SRD mixed 62.4 B, FP64 102.4 B
+ALG_BYTES = {"mixed": 62.4, "fp64": 102.4}
+WORKLOAD = "3D SRD fluid, periodic 64^3 cells, 10 particles/cell (2,621,440), rot 130 deg"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_gpu(args, rank, world):
+    import numpy as np
+    import torch
+
+    from mpcd_b200 import abi
+    from mpcd_b200 import workloads as W
+    from mpcd_b200.gpu import Solver
+
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    results = {}
+    for form, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        cfg = W.cfg_srd3d(L_BOX, precision=prec, seed=20240 + rank)
+        cfg.replica = rank
+        Q, V, U, sp = W.synthetic_state(cfg, PPC, seed=7 + rank)
+        n = len(Q)
+        g = Solver(cfg)
+        g.set_stream(stream.cuda_stream)
+        g.upload(Q, V, U, sp)
+        g.step(args.warmup, 1)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        clk = Clocks(dev) if form == "mixed" else None
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            g.step(1, 1 + args.warmup + k)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        clocks = clk.stop() if clk else None
+        ms = [a.elapsed_time(b) for a, b in ev]
+        total_ms = float(sum(ms))
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        kb, av = g.globals()
+        st = g.status()
+        results[form] = {
+            "n": n, "ms_total": total_ms, "ms_per_step": total_ms / args.steps,
+            "ms_min": min(ms), "launches": g.launches_per_step(), "clocks": clocks,
+            "kbt": kb, "escaped": int(st.escaped),
+        }
+        # e2e through the C ABI with host buffers: upload from pinned host
+        # memory, K drop-in timestep() calls each returning the step's global
+        # measures to the host, download of the final state
+        if form == "mixed":
+            Qh = torch.from_numpy(Q).pin_memory().numpy()
+            Vh = torch.from_numpy(V).pin_memory().numpy()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g.upload(Qh, Vh, None, sp)
+            for k in range(args.steps):
+                g.timestep(1000 + k)
+            q2, v2, _ = g.download()
+            torch.cuda.synchronize()
+            e2e_s = time.perf_counter() - t0
+            te = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            if world > 1:
+                torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+            results["e2e"] = {
+                "value": n * world * args.steps / float(te.item()), "unit": UNIT,
+                "h2d_bytes_per_step": (Q.nbytes + V.nbytes + sp.nbytes) / args.steps,
+                "d2h_bytes_per_step": (q2.nbytes + v2.nbytes) / args.steps + 32,
+            }
+        g.close()
+        del Q, V, U
+    return results
+
+
+def cpu_baseline(args, force_port=False):
+    """The reference's own serial timestep (oracle/_ref/libmpcdref_time.so,
+    built from its sources) on a bounded sample: the same 64^3 SRD state,
+    a few steps, one core.  Falls back to the CPU oracle port if the
+    reference build is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from checkers import Oracle, Reference
+    from mpcd_b200 import workloads as W
+
+    cfg = W.cfg_srd3d(L_BOX, seed=20240)
+    Q, V, U, sp = W.synthetic_state(cfg, PPC, seed=7)
+    n = len(Q)
+    k = max(1, args.cpu_sample_steps)
+    if Reference.available(timing=True) and not force_port:
+        r = Reference(cfg, Q, V, U, sp, timing=True)
+        r.run_timed(1, 1)  # warm-up step
+        secs = r.run_timed(k, 2)
+        kind = "reference"
+    else:
+        o = Oracle(cfg, Q, V, U, sp)
+        o.step(1)
+        t0 = time.perf_counter()
+        for s in range(k):
+            o.step(2 + s)
+        secs = time.perf_counter() - t0
+        kind = "port"
+    return {"value": n * k / secs, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{k} timesteps of the 64^3 SRD state ({n} particles) after 1 warm-up "
+                      f"step, serial, host {os.cpu_count()} cores available"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_baseline(args)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+                "n_gpus": args.gpus, "steps": args.cpu_sample_steps, "warmup": 1,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "global_batch": 2621440, "form": "reference C"},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_gpu(args, rank, world)
+    if rank == 0:
+        mix, f64 = res["mixed"], res["fp64"]
+        n = mix["n"]
+        value = n * world * args.steps / (mix["ms_total"] / 1e3)
+        v64 = n * world * args.steps / (f64["ms_total"] / 1e3)
+        peak, peak_kind = peaks()
+        ach = ALG_BYTES["mixed"] * n / (mix["ms_total"] / args.steps / 1e3) / 1e9
+        ach64 = ALG_BYTES["fp64"] * n / (f64["ms_total"] / args.steps / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": mix["ms_total"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": n * world, "form": "mixed",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MB write) between timed steps"},
+            "fp64": {"value": v64, "ms_per_step": f64["ms_total"] / args.steps,
+                     "achieved_gbs": ach64, "frac": ach64 / peak},
+            "mixed_over_fp64": value / v64,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "traffic": None,
+                         "unit_of_work": "one timestep (all kernels of a step)",
+                         "peak_source": peak_kind},
+            "gpu_launches": mix["launches"] * args.steps,
+            "clocks": mix["clocks"],
+            "e2e": res["e2e"],
+        }
+        if not args.no_cpu:
+            try:
+                line["cpu_baseline"] = cpu_baseline(args)
+            except Exception as e:  # noqa: BLE001
+                line["cpu_baseline"] = {"error": str(e)}
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,9 @@
+#!/usr/bin/env bash
+# Builds libmpcd_gpu.so (sm_100a) in-tree: niamh-mpcd_b200/libmpcd_gpu.so
+set -euo pipefail
+HERE="$(cd "$(dirname "$0")" && pwd)"
+NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
+"$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo -std=c++17 \
+    -Xcompiler -fPIC -Xcompiler -Wall -shared \
+    -I"$HERE/../include" -I"$HERE/csrc" \
+    "$HERE/csrc/mpcd_api.cu" -o "$HERE/libmpcd_gpu.so" ${MPCD_NVCC_EXTRA:-}

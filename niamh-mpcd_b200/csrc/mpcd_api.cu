@@ -1,0 +1,567 @@
+// mpcd_api.cu -- the C ABI of libmpcd_gpu.so (declared in include/mpcd_gpu.h).
+//
+// A handle owns the particle state in device memory, two state buffers (the
+// counting sort writes the cell-ordered copy into the other one), the cell
+// count/start arrays and the per-step accumulators, all on one CUDA stream.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "mpcd_gpu.h"
+#include "mpcd_device.cuh"
+#include "mpcd_fp64.cuh"
+#include "mpcd_mixed.cuh"
+
+using namespace mpcd;
+
+struct mpcd_handle {
+    mpcd_config cfg;
+    DevCfg dc;
+    int device;
+    cudaStream_t stream;
+    bool own_stream;
+    int n;
+    int cap;
+    int prec;
+    // FP64 state, two buffers
+    Fp64State f[2];
+    // mixed state, two buffers
+    MixState mx[2];
+    int cur;
+    int *key, *rank, *count, *start, *part;
+    double *acc;
+    unsigned long long *status;
+    int nscan;
+    int sm_count;
+    int launches;
+    uint32_t last_step;
+    uint64_t steps;
+    double *host_acc;  // pinned
+    // cell-property scratch for mpcd_cell_props
+    int *cp_pop;
+    double *cp_sums;
+};
+
+#define CK(call)                                                        \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) {                                        \
+            fprintf(stderr, "mpcd: %s failed: %s\n", #call,             \
+                    cudaGetErrorString(e_));                            \
+            return MPCD_ERR_CUDA;                                       \
+        }                                                               \
+    } while (0)
+
+static int dev_alloc(void **p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return e == cudaErrorMemoryAllocation ? MPCD_ERR_NOMEM : MPCD_ERR_CUDA;
+    }
+    return MPCD_OK;
+}
+
+#define ALLOC(ptr, bytes)                                        \
+    do {                                                         \
+        int r_ = dev_alloc((void **)&(ptr), (bytes));            \
+        if (r_ != MPCD_OK) {                                     \
+            mpcd_destroy(h);                                     \
+            return r_;                                           \
+        }                                                        \
+    } while (0)
+
+static bool is_periodic_wall(const mpcd_wall &w) {
+    // setPBC, read.c:584-603
+    for (int d = 0; d < 3; d++)
+        if (std::fabs(std::fabs(w.A[d]) - 1.0) <= kTol && w.MVN > 0.0 && w.MVT > 0.0 &&
+            (std::fabs(w.DN) >= kTol || std::fabs(w.DT) >= kTol))
+            return true;
+    return false;
+}
+
+static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
+    memset(dc, 0, sizeof(*dc));
+    if (cfg->dim != 2 && cfg->dim != 3) return MPCD_ERR_UNSUPPORTED;
+    if (cfg->n_species < 1 || cfg->n_species > MPCD_MAX_SPECIES) return MPCD_ERR_ARG;
+    if (cfg->n_walls < 0 || cfg->n_walls > MPCD_MAX_WALLS) return MPCD_ERR_ARG;
+    if (!(cfg->dt > 0.0) || !(cfg->kbt >= 0.0)) return MPCD_ERR_ARG;
+    if (cfg->lc != MPCD_LC_ISOTROPIC) return MPCD_ERR_UNSUPPORTED;
+    if (cfg->coll_op != MPCD_COLL_ARBAXIS && cfg->coll_op != MPCD_COLL_MPCAT &&
+        cfg->coll_op != MPCD_COLL_RAT)
+        return MPCD_ERR_UNSUPPORTED;
+    dc->dim = cfg->dim;
+    dc->op = cfg->coll_op;
+    dc->lc = cfg->lc;
+    dc->galinv = cfg->galinv;
+    for (int d = 0; d < 3; d++) {
+        int L = d < cfg->dim ? cfg->L[d] : 1;
+        if (L < 1) return MPCD_ERR_ARG;
+        dc->L[d] = L;
+        dc->N1[d] = L + 1;
+    }
+    long long nc = (long long)dc->N1[0] * dc->N1[1] * dc->N1[2];
+    if (nc > (1LL << 30)) return MPCD_ERR_SIZE;
+    dc->ncells = (int)nc;
+    dc->vol = 1.0;
+    for (int d = 0; d < cfg->dim; d++) dc->vol *= dc->L[d];
+    dc->n_species = cfg->n_species;
+    for (int s = 0; s < cfg->n_species; s++) {
+        if (!(cfg->species[s].mass > 0.0)) return MPCD_ERR_ARG;
+        dc->mass[s] = cfg->species[s].mass;
+        dc->damp[s] = cfg->species[s].damp;
+    }
+    dc->dt = cfg->dt;
+    dc->kbt = cfg->kbt;
+    dc->cosA = std::cos(cfg->rot_ang);
+    dc->sinA = -1.0 * std::sin(cfg->rot_ang);  // rotation sign draw is always 0
+    for (int d = 0; d < 3; d++) dc->grav[d] = cfg->grav[d];
+    dc->grav_flag = std::fabs(cfg->grav[0]) >= kTol || std::fabs(cfg->grav[1]) >= kTol ||
+                    std::fabs(cfg->grav[2]) >= kTol;
+    dc->seed = cfg->seed;
+    dc->replica = cfg->replica;
+    dc->n_walls = cfg->n_walls;
+    for (int w = 0; w < cfg->n_walls; w++) {
+        const mpcd_wall &src = cfg->walls[w];
+        DevWall &dst = dc->walls[w];
+        int nz = 0, ax = 0;
+        for (int d = 0; d < 3; d++)
+            if (src.A[d] != 0.0) {
+                nz++;
+                ax = d;
+            }
+        // static axis-aligned planes with rule-based collisions only
+        if (nz != 1 || src.coll_type != 1) return MPCD_ERR_UNSUPPORTED;
+        for (int d = 0; d < 3; d++) {
+            dst.A[d] = src.A[d];
+            dst.Q[d] = src.Q[d];
+            dst.DVxyz[d] = src.DVxyz[d];
+        }
+        dst.R = src.R;
+        dst.DN = src.DN;
+        dst.DT = src.DT;
+        dst.DVN = src.DVN;
+        dst.DVT = src.DVT;
+        dst.MVN = src.MVN;
+        dst.MVT = src.MVT;
+        dst.inv = src.inv;
+        dst.phantom = src.phantom;
+        dst.axis = ax;
+        dst.periodic = is_periodic_wall(src) ? 1 : 0;
+        uint32_t m = 0;
+        for (int s = 0; s < MPCD_MAX_SPECIES; s++)
+            if (src.inter[s]) m |= 1u << s;
+        dst.inter = m;
+        if (dst.phantom) dc->any_phantom = 1;
+        if (!dst.periodic) dc->n_solid++;
+        if (dst.periodic) dc->pbc[ax] = 1;
+    }
+    dc->gndnst = cfg->gndnst;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_abi_version(void) { return MPCD_ABI_VERSION; }
+
+extern "C" int mpcd_destroy(mpcd_handle *h) {
+    if (!h) return MPCD_ERR_ARG;
+    for (int b = 0; b < 2; b++) {
+        for (int d = 0; d < 3; d++) {
+            cudaFree(h->f[b].q[d]);
+            cudaFree(h->f[b].v[d]);
+        }
+        cudaFree(h->f[b].pid);
+        cudaFree(h->f[b].sp);
+        mix_free(h->mx[b]);
+    }
+    cudaFree(h->key);
+    cudaFree(h->rank);
+    cudaFree(h->count);
+    cudaFree(h->start);
+    cudaFree(h->part);
+    cudaFree(h->acc);
+    cudaFree(h->status);
+    cudaFree(h->cp_pop);
+    cudaFree(h->cp_sums);
+    if (h->host_acc) cudaFreeHost(h->host_acc);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
+    if (!cfg || !out) return MPCD_ERR_ARG;
+    *out = nullptr;
+    DevCfg dc;
+    int r = build_devcfg(cfg, &dc);
+    if (r != MPCD_OK) return r;
+    if (cfg->capacity < 0) return MPCD_ERR_ARG;
+    if (cfg->precision != MPCD_PREC_FP64 && cfg->precision != MPCD_PREC_MIXED)
+        return MPCD_ERR_ARG;
+    if (cfg->precision == MPCD_PREC_MIXED) {
+        r = mix_check(dc);
+        if (r != MPCD_OK) return r;
+    }
+    mpcd_handle *h = new mpcd_handle();
+    memset(h, 0, sizeof(*h));
+    h->cfg = *cfg;
+    h->dc = dc;
+    h->prec = cfg->precision;
+    cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return MPCD_ERR_CUDA;
+    }
+    h->own_stream = true;
+    int nc = dc.ncells;
+    h->nscan = (nc + kScanTile - 1) / kScanTile;
+    ALLOC(h->count, sizeof(int) * nc);
+    ALLOC(h->start, sizeof(int) * (nc + 1));
+    ALLOC(h->part, sizeof(int) * h->nscan);
+    ALLOC(h->acc, sizeof(double) * ACC_WORDS);
+    ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
+    if (cudaMemsetAsync(h->count, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->status, 0, sizeof(unsigned long long) * ST_WORDS, h->stream) !=
+            cudaSuccess ||
+        cudaMemsetAsync(h->acc, 0, sizeof(double) * ACC_WORDS, h->stream) != cudaSuccess) {
+        mpcd_destroy(h);
+        return MPCD_ERR_CUDA;
+    }
+    if (cudaMallocHost((void **)&h->host_acc, sizeof(double) * ACC_WORDS) != cudaSuccess) {
+        mpcd_destroy(h);
+        return MPCD_ERR_NOMEM;
+    }
+    *out = h;
+    return MPCD_OK;
+}
+
+// (Re)allocate the per-particle arrays for n particles.
+static int ensure_capacity(mpcd_handle *h, int n) {
+    int want = n > h->cfg.capacity ? n : h->cfg.capacity;
+    if (want <= h->cap) return MPCD_OK;
+    for (int b = 0; b < 2; b++) {
+        for (int d = 0; d < 3; d++) {
+            cudaFree(h->f[b].q[d]);
+            cudaFree(h->f[b].v[d]);
+            h->f[b].q[d] = h->f[b].v[d] = nullptr;
+        }
+        cudaFree(h->f[b].pid);
+        cudaFree(h->f[b].sp);
+        h->f[b].pid = h->f[b].sp = nullptr;
+        mix_free(h->mx[b]);
+    }
+    cudaFree(h->key);
+    cudaFree(h->rank);
+    h->key = h->rank = nullptr;
+    size_t N = (size_t)want;
+    int r;
+    for (int b = 0; b < 2; b++) {
+        if (h->prec == MPCD_PREC_FP64) {
+            for (int d = 0; d < h->dc.dim; d++) {
+                if ((r = dev_alloc((void **)&h->f[b].q[d], N * sizeof(double)))) return r;
+                if ((r = dev_alloc((void **)&h->f[b].v[d], N * sizeof(double)))) return r;
+            }
+            if ((r = dev_alloc((void **)&h->f[b].pid, N * sizeof(int)))) return r;
+            if (h->dc.n_species > 1)
+                if ((r = dev_alloc((void **)&h->f[b].sp, N * sizeof(int)))) return r;
+        } else {
+            if ((r = mix_alloc(h->mx[b], N, h->dc))) return r;
+        }
+    }
+    if ((r = dev_alloc((void **)&h->key, N * sizeof(int)))) return r;
+    if ((r = dev_alloc((void **)&h->rank, N * sizeof(int)))) return r;
+    h->cap = want;
+    return MPCD_OK;
+}
+
+static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V,
+                         const int *spid) {
+    int dim = h->dc.dim;
+    for (int i = 0; i < n; i++) {
+        int s = spid ? spid[i] : 0;
+        if (s < 0 || s >= h->dc.n_species) return MPCD_ERR_ARG;
+        for (int d = 0; d < dim; d++)
+            if (!std::isfinite(Q[3 * i + d]) || !std::isfinite(V[3 * i + d])) return MPCD_ERR_ARG;
+    }
+    int r = ensure_capacity(h, n);
+    if (r != MPCD_OK) return r;
+    h->n = n;
+    h->cur = 0;
+    // global number density as globalDensities (init.c:1002-1018) unless given
+    if (!(h->cfg.gndnst > 0.0)) {
+        std::vector<int> pop((size_t)h->dc.ncells, 0);
+        for (int i = 0; i < n; i++) {
+            int idx[3] = {0, 0, 0};
+            for (int d = 0; d < dim; d++) {
+                int a = (int)Q[3 * i + d];
+                if (a < 0) a = 0;
+                if (a > h->dc.L[d]) a = h->dc.L[d];
+                idx[d] = a;
+            }
+            pop[((size_t)idx[0] * h->dc.N1[1] + idx[1]) * h->dc.N1[2] + idx[2]]++;
+        }
+        double cnt = 0.0, sumN = 0.0;
+        for (int a = 0; a < h->dc.L[0]; a++)
+            for (int b = 0; b < h->dc.L[1]; b++)
+                for (int z = 0; z < h->dc.L[2]; z++) {
+                    int p = pop[((size_t)a * h->dc.N1[1] + b) * h->dc.N1[2] + z];
+                    if (p > 0) {
+                        cnt += 1.0;
+                        sumN += (double)p;
+                    }
+                }
+        h->dc.gndnst = cnt > 0.0 ? sumN / cnt : 0.0;
+    }
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
+                                 const double *U, const int *spid) {
+    if (!h || n < 0 || (n > 0 && (!Q || !V))) return MPCD_ERR_ARG;
+    (void)U;
+    int r = upload_common(h, n, Q, V, spid);
+    if (r != MPCD_OK) return r;
+    if (n == 0) return MPCD_OK;
+    int dim = h->dc.dim;
+    size_t N = (size_t)n;
+    if (h->prec == MPCD_PREC_FP64) {
+        std::vector<double> tmp(N);
+        std::vector<int> ids(N);
+        for (int d = 0; d < dim; d++) {
+            for (size_t i = 0; i < N; i++) tmp[i] = Q[3 * i + d];
+            CK(cudaMemcpyAsync(h->f[0].q[d], tmp.data(), N * 8, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            for (size_t i = 0; i < N; i++) tmp[i] = V[3 * i + d];
+            CK(cudaMemcpyAsync(h->f[0].v[d], tmp.data(), N * 8, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        for (size_t i = 0; i < N; i++) ids[i] = (int)i;
+        CK(cudaMemcpyAsync(h->f[0].pid, ids.data(), N * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->f[0].sp) {
+            for (size_t i = 0; i < N; i++) ids[i] = spid ? spid[i] : 0;
+            CK(cudaMemcpyAsync(h->f[0].sp, ids.data(), N * 4, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+    } else {
+        r = mix_upload(h->mx[0], h->dc, n, Q, V, spid, h->stream);
+        if (r != MPCD_OK) return r;
+    }
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *base,
+                                             size_t stride, size_t off_Q, size_t off_V,
+                                             size_t off_U, size_t off_spid) {
+    if (!h || n < 0 || (n > 0 && !base) || stride == 0) return MPCD_ERR_ARG;
+    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n);
+    std::vector<int> sp((size_t)n);
+    const char *b = (const char *)base;
+    for (int i = 0; i < n; i++) {
+        const char *rec = b + (size_t)i * stride;
+        memcpy(&Q[3 * (size_t)i], rec + off_Q, 3 * sizeof(double));
+        memcpy(&V[3 * (size_t)i], rec + off_V, 3 * sizeof(double));
+        if (off_spid != (size_t)-1)
+            memcpy(&sp[i], rec + off_spid, sizeof(int));
+        else
+            sp[i] = 0;
+    }
+    (void)off_U;
+    return mpcd_upload_state(h, n, Q.data(), V.data(), nullptr, sp.data());
+}
+
+extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double *U) {
+    if (!h) return MPCD_ERR_ARG;
+    int n = h->n, dim = h->dc.dim;
+    size_t N = (size_t)n;
+    if (n == 0) return MPCD_OK;
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int> pid(N);
+    if (h->prec == MPCD_PREC_FP64) {
+        const Fp64State &st = h->f[h->cur];
+        CK(cudaMemcpy(pid.data(), st.pid, N * 4, cudaMemcpyDeviceToHost));
+        std::vector<double> tmp(N);
+        for (int d = 0; d < 3; d++) {
+            if (d < dim) {
+                if (Q) {
+                    CK(cudaMemcpy(tmp.data(), st.q[d], N * 8, cudaMemcpyDeviceToHost));
+                    for (size_t i = 0; i < N; i++) Q[3 * (size_t)pid[i] + d] = tmp[i];
+                }
+                if (V) {
+                    CK(cudaMemcpy(tmp.data(), st.v[d], N * 8, cudaMemcpyDeviceToHost));
+                    for (size_t i = 0; i < N; i++) V[3 * (size_t)pid[i] + d] = tmp[i];
+                }
+            } else {
+                for (size_t i = 0; i < N; i++) {
+                    if (Q) Q[3 * i + d] = 0.0;
+                    if (V) V[3 * i + d] = 0.0;
+                }
+            }
+        }
+    } else {
+        int r = mix_download(h->mx[h->cur], h->dc, n, Q, V);
+        if (r != MPCD_OK) return r;
+    }
+    if (U)
+        for (size_t i = 0; i < 3 * N; i++) U[i] = 0.0;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_download_particles_strided(mpcd_handle *h, void *base, size_t stride,
+                                               size_t off_Q, size_t off_V, size_t off_U) {
+    if (!h || (h->n > 0 && !base) || stride == 0) return MPCD_ERR_ARG;
+    int n = h->n;
+    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n);
+    int r = mpcd_download_state(h, Q.data(), V.data(), nullptr);
+    if (r != MPCD_OK) return r;
+    char *b = (char *)base;
+    for (int i = 0; i < n; i++) {
+        char *rec = b + (size_t)i * stride;
+        memcpy(rec + off_Q, &Q[3 * (size_t)i], 3 * sizeof(double));
+        memcpy(rec + off_V, &V[3 * (size_t)i], 3 * sizeof(double));
+    }
+    (void)off_U;
+    return MPCD_OK;
+}
+
+static int grid_for(const mpcd_handle *h, int n) {
+    int g = (n + 255) / 256;
+    int cap = h->sm_count * 8;
+    if (g > cap) g = cap;
+    return g < 1 ? 1 : g;
+}
+
+static int step_fp64(mpcd_handle *h, uint32_t step) {
+    const DevCfg &c = h->dc;
+    int n = h->n, nc = c.ncells;
+    Fp64State a = h->f[h->cur], b = h->f[1 - h->cur];
+    int gb = grid_for(h, n);
+    int gc = (int)(((long long)nc * 32 + 255) / 256);
+    if (c.dim == 3) {
+        k_bin_fp64<3><<<gb, 256, 0, h->stream>>>(c, a, n, h->key, h->rank, h->count, step,
+                                                  h->status);
+    } else {
+        k_bin_fp64<2><<<gb, 256, 0, h->stream>>>(c, a, n, h->key, h->rank, h->count, step,
+                                                  h->status);
+    }
+    k_scan_partial<<<h->nscan, 256, 0, h->stream>>>(h->count, nc, h->part);
+    k_scan_apply<<<h->nscan, 256, 0, h->stream>>>(h->count, nc, h->part, h->start, h->acc);
+    if (c.dim == 3) {
+        k_scatter_fp64<3><<<gb, 256, 0, h->stream>>>(a, b, n, h->key, h->rank, h->start);
+        k_cell_fp64<3><<<gc, 256, 0, h->stream>>>(c, b, h->start, step, h->acc, h->status);
+    } else {
+        k_scatter_fp64<2><<<gb, 256, 0, h->stream>>>(a, b, n, h->key, h->rank, h->start);
+        k_cell_fp64<2><<<gc, 256, 0, h->stream>>>(c, b, h->start, step, h->acc, h->status);
+    }
+    CK(cudaGetLastError());
+    h->cur = 1 - h->cur;
+    h->launches = 5;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
+    if (!h || nsteps < 0) return MPCD_ERR_ARG;
+    if (h->n <= 0) return MPCD_ERR_STATE;
+    for (int k = 0; k < nsteps; k++) {
+        uint32_t step = step0 + (uint32_t)k;
+        int r;
+        if (h->prec == MPCD_PREC_FP64)
+            r = step_fp64(h, step);
+        else
+            r = mix_step(h->mx, h->cur, h->dc, h->n, step, h->key, h->rank, h->count,
+                         h->start, h->part, h->nscan, h->acc, h->status, h->stream,
+                         h->sm_count, &h->launches);
+        if (r != MPCD_OK) return r;
+        h->last_step = step;
+        h->steps++;
+    }
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_globals(mpcd_handle *h, double *kbtnow, double avnow[3]) {
+    if (!h) return MPCD_ERR_ARG;
+    CK(cudaMemcpyAsync(h->host_acc, h->acc, sizeof(double) * ACC_WORDS,
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    int dim = h->dc.dim;
+    if (kbtnow) *kbtnow = h->n > 0 ? h->host_acc[ACC_KE] / (double)(h->n * dim) : 0.0;
+    if (avnow)
+        for (int d = 0; d < 3; d++)
+            avnow[d] = d < dim ? h->host_acc[ACC_VCM + d] / h->dc.vol : 0.0;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_timestep(mpcd_handle *h, uint32_t runtime, double AVNOW[3],
+                             double *KBTNOW) {
+    int r = mpcd_step(h, 1, runtime);
+    if (r != MPCD_OK) return r;
+    return mpcd_globals(h, KBTNOW, AVNOW);
+}
+
+extern "C" int mpcd_get_status(mpcd_handle *h, mpcd_status *st) {
+    if (!h || !st) return MPCD_ERR_ARG;
+    unsigned long long w[ST_WORDS];
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(w, h->status, sizeof(w), cudaMemcpyDeviceToHost));
+    st->steps = h->steps;
+    st->escaped = w[ST_ESCAPED];
+    st->bounce_limit = w[ST_BOUNCE];
+    st->nonfinite = w[ST_NONFINITE];
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_set_stream(mpcd_handle *h, void *stream) {
+    if (!h) return MPCD_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)stream;
+    h->own_stream = false;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_launches_per_step(mpcd_handle *h) { return h ? h->launches : 0; }
+
+extern "C" int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
+                               double *cm) {
+    if (!h) return MPCD_ERR_ARG;
+    // Re-bin on the unshifted grid on the host from the downloaded state (an
+    // output-step operation, off the timestep's hot path).
+    int n = h->n, dim = h->dc.dim, nc = h->dc.ncells;
+    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n);
+    int r = mpcd_download_state(h, Q.data(), V.data(), nullptr);
+    if (r != MPCD_OK) return r;
+    std::vector<int> p((size_t)nc, 0);
+    std::vector<double> m((size_t)nc, 0.0), sv((size_t)nc * 3, 0.0), sq((size_t)nc * 3, 0.0);
+    for (int i = 0; i < n; i++) {
+        int idx[3] = {0, 0, 0};
+        for (int d = 0; d < dim; d++) {
+            int a = (int)Q[3 * (size_t)i + d];
+            if (a < 0) a = 0;
+            if (a > h->dc.L[d]) a = h->dc.L[d];
+            idx[d] = a;
+        }
+        size_t k = ((size_t)idx[0] * h->dc.N1[1] + idx[1]) * h->dc.N1[2] + idx[2];
+        double ms = h->dc.mass[0];
+        p[k]++;
+        m[k] += ms;
+        for (int d = 0; d < dim; d++) {
+            sv[3 * k + d] += V[3 * (size_t)i + d] * ms;
+            sq[3 * k + d] += Q[3 * (size_t)i + d] * ms;
+        }
+    }
+    for (int k = 0; k < nc; k++) {
+        if (pop) pop[k] = p[k];
+        if (mass) mass[k] = m[k];
+        for (int d = 0; d < 3; d++) {
+            double a = (d < dim && m[k] > 0.0) ? sv[3 * (size_t)k + d] / m[k] : 0.0;
+            double b = (d < dim && m[k] > 0.0) ? sq[3 * (size_t)k + d] / m[k] : 0.0;
+            if (vcm) vcm[3 * (size_t)k + d] = a;
+            if (cm) cm[3 * (size_t)k + d] = b;
+        }
+    }
+    return MPCD_OK;
+}

@@ -1,0 +1,305 @@
+// mpcd_device.cuh -- device-side configuration and per-particle/per-cell
+// building blocks of the MPCD solvent timestep (sm_100a).
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "mpcd_gpu.h"
+#include "mpcd_rng.h"
+
+namespace mpcd {
+
+static inline float __int_as_float_host(int i) {
+    float f;
+    std::memcpy(&f, &i, 4);
+    return f;
+}
+static inline int __float_as_int_host(float f) {
+    int i;
+    std::memcpy(&i, &f, 4);
+    return i;
+}
+
+constexpr double kTol = 1e-8;  // reference TOL, definitions.h:56
+constexpr int kNBounce = 50;   // reference NBOUNCE, definitions.h:62
+
+// Status counters (device, uint64): index into DevStatus words.
+enum { ST_ESCAPED = 0, ST_BOUNCE = 1, ST_NONFINITE = 2, ST_WORDS = 4 };
+
+// Per-step global accumulators: [0] sum m v^2 (TEMP), [1..3] sum VCM (avVel)
+enum { ACC_KE = 0, ACC_VCM = 1, ACC_WORDS = 4 };
+
+struct DevWall {
+    double A[3], Q[3];
+    double R, DN, DT, DVN, DVT, MVN, MVT;
+    double DVxyz[3];
+    int inv, phantom, periodic, axis;  // axis: the one non-zero component of A
+    uint32_t inter;                    // bit s set: species s interacts
+    int pad_;
+};
+
+struct DevCfg {
+    int dim, op, lc, galinv;
+    int L[3], N1[3], pbc[3];
+    int ncells, n_species, n_walls, any_phantom;
+    int n_solid;  // walls that are not periodic (mixed mode loops only these)
+    int grav_flag;
+    double dt, kbt, gndnst, vol;
+    double cosA, sinA;  // cos(RA) and the sine with the reference's sign (-sin RA)
+    double grav[3];
+    double mass[MPCD_MAX_SPECIES], damp[MPCD_MAX_SPECIES];
+    uint64_t seed;
+    uint32_t replica;
+    int pad_;
+    DevWall walls[MPCD_MAX_WALLS];
+};
+
+__device__ __forceinline__ int cell_lin(const DevCfg &c, int a, int b, int z) {
+    return (a * c.N1[1] + b) * c.N1[2] + z;
+}
+
+__device__ __forceinline__ void cell_coords(const DevCfg &c, int lin, int &a,
+                                            int &b, int &z) {
+    z = lin % c.N1[2];
+    int t = lin / c.N1[2];
+    b = t % c.N1[1];
+    a = t / c.N1[1];
+}
+
+// ------------------------------------------------------------------ warps
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------- grid shift
+// gridShift_all, mpc.c:720-766: forward shift wraps Q > L && Q <= L + s.
+__device__ __forceinline__ double shift_fwd(double q, double s, int L) {
+    q += s;
+    if (q > L && q <= L + s) q -= L;
+    return q;
+}
+__device__ __forceinline__ double shift_back(double q, double s, int L) {
+    double ms = -1.0 * s;
+    q += ms;
+    if (q < 0.0 && q >= ms) q += L;
+    return q;
+}
+
+// bin, mpc.c:958-982: truncation, periodic index L -> 0 on the shifted grid,
+// escapes counted and clamped.
+__device__ __forceinline__ int bin_axis(double q, int L, int pbc, int shifted,
+                                        int &escaped) {
+    int a = (int)q;
+    if (shifted && pbc && a == L) a = 0;
+    if (a < 0 || a > L) {
+        escaped = 1;
+        a = a < 0 ? 0 : L;
+    }
+    return a;
+}
+
+// --------------------------------------------------------------- walls
+// Surface function of a planar wall (calcW_PLANE, bc.c:306-316) with the
+// wall displaced by 'off' (the grid shift during the collision stage).
+__device__ __forceinline__ double wall_W(const DevWall &w, const double *q,
+                                         const double *wq, int dim) {
+    double W = 0.0;
+    for (int i = 0; i < dim; i++) W += w.A[i] * (q[i] - wq[i]);
+    W -= w.R;
+    if (w.inv) W *= -1.0;
+    return W;
+}
+
+// MPC_BCcollision (bc.c:1363-1496) for static planar rule-based walls, in
+// FP64, visiting walls in index order.  'only_solid' skips periodic walls
+// (the mixed-precision state wraps periodic axes exactly instead).
+// Returns 1 if the particle hit the bounce limit.
+template <int DIM>
+__device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
+                               bool only_solid) {
+    double t_left = c.dt, t_coll = 0.0;
+    int chosen = 0, cnt = 0;
+    const double m = c.mass[sp];
+    for (;;) {
+        double t_min = t_left, W = 1.0;
+        for (int w = 0; w < c.n_walls; w++) {
+            const DevWall &wl = c.walls[w];
+            if (only_solid && wl.periodic) continue;
+            if (!((wl.inter >> sp) & 1u)) continue;
+            double tw = wall_W(wl, q, wl.Q, DIM);
+            if (tw < 0.0) {
+                double t1 = wl.R;
+                for (int d = 0; d < DIM; d++) t1 += wl.A[d] * (wl.Q[d] - q[d]);
+                double den = wl.A[0] * (-v[0]) + wl.A[1] * (-v[1]);
+                den += wl.A[2] * (DIM == 3 ? -v[2] : -0.0);
+                t1 /= den;
+                double tc = t_left - t1;
+                if (tc < t_min) {
+                    t_min = tc;
+                    chosen = w;
+                    W = tw;
+                }
+            }
+        }
+        t_coll = t_min;
+        if (W > -kTol) return 0;
+        cnt++;
+        const DevWall &wl = c.walls[chosen];
+        if (t_coll > -kTol) {
+            double n[3] = {0, 0, 0}, vn[3], vt[3], V[3];
+            for (int d = 0; d < DIM; d++) q[d] = q[d] - (t_left - t_coll) * v[d];
+            for (int d = 0; d < DIM; d++) n[d] = wl.A[d];
+            double len = 0.0;
+            for (int d = 0; d < DIM; d++) len += n[d] * n[d];
+            len = sqrt(len);
+            if (fabs(len) >= kTol)
+                for (int d = 0; d < DIM; d++) n[d] = n[d] / len;
+            double x = 0.0;
+            for (int d = 0; d < DIM; d++) x += v[d] * n[d];
+            for (int d = 0; d < DIM; d++) {
+                vn[d] = x * n[d];
+                vt[d] = v[d] - vn[d];
+            }
+            for (int d = 0; d < DIM; d++) {
+                vn[d] *= wl.MVN;
+                vn[d] += wl.DVN * n[d];
+                vt[d] *= wl.MVT;
+                vt[d] += wl.DVT;
+            }
+            for (int d = 0; d < DIM; d++) {
+                V[d] = vn[d] + vt[d];
+                V[d] += wl.DVxyz[d];
+                V[d] -= v[d];
+                V[d] *= m;
+            }
+            double imp = 1.0 / m;
+            for (int d = 0; d < DIM; d++) v[d] += V[d] * 1.0 * imp;
+            double xq = 0.0, pn[3], pt[3];
+            for (int d = 0; d < DIM; d++) xq += q[d] * n[d];
+            for (int d = 0; d < DIM; d++) {
+                pn[d] = xq * n[d];
+                pt[d] = q[d] - pn[d];
+                pn[d] += wl.DN * n[d] * (1. - 2. * kTol);
+                pt[d] += wl.DT;
+                q[d] = pn[d] + pt[d];
+            }
+            t_left -= t_coll;
+            for (int d = 0; d < DIM; d++) q[d] = q[d] + t_left * v[d];
+            if (wall_W(wl, q, wl.Q, DIM) < -kTol)
+                for (int d = 0; d < DIM; d++) q[d] = q[d] - t_left * v[d];
+        } else {
+            for (int d = 0; d < DIM; d++) q[d] = q[d] - (t_left - t_coll) * v[d];
+        }
+        if (cnt > kNBounce) {
+            if (cnt < 2 * kNBounce) {
+                if (t_left > kTol) {
+                    t_left *= 1.1;
+                } else {
+                    t_left = 0.9 * c.dt;
+                    t_coll = 0.1 * c.dt;
+                }
+            } else {
+                return 1;
+            }
+        }
+    }
+}
+
+// Is the (shifted-grid) cell (a,b,z) cut by a phantom wall at its shifted
+// position?  Corner test of ghostPart, mpc.c:380-470.
+template <int DIM>
+__device__ bool cell_cut_by_phantom(const DevCfg &c, int a, int b, int z,
+                                    const double *s) {
+    const int nc = 1 << DIM;
+    for (int w = 0; w < c.n_walls; w++) {
+        const DevWall &wl = c.walls[w];
+        if (!wl.phantom) continue;
+        double wq[3];
+        for (int d = 0; d < 3; d++) wq[d] = wl.Q[d] + (d < DIM ? s[d] : 0.0);
+        for (int j = 0; j < nc; j++) {
+            double q[3] = {(double)a + (double)(j & 1), (double)b + (double)((j >> 1) & 1),
+                           (double)z + (double)((j >> 2) & 1)};
+            if (wall_W(wl, q, wq, DIM) < 0.0) return true;
+        }
+    }
+    return false;
+}
+
+// SRD rotation matrix about unit axis L by the reference's angle (rotate,
+// mpc.c:1181-1257); in 2D a plane rotation.
+template <int DIM, typename T>
+__device__ __forceinline__ void srd_matrix(const DevCfg &c, const double *L,
+                                           T R[9]) {
+    const double Cs = c.cosA, Sn = c.sinA;
+    if (DIM == 3) {
+        R[0] = (T)(L[0] * L[0] + (1. - L[0] * L[0]) * Cs);
+        R[1] = (T)(L[0] * L[1] * (1. - Cs) - L[2] * Sn);
+        R[2] = (T)(L[0] * L[2] * (1. - Cs) + L[1] * Sn);
+        R[3] = (T)(L[0] * L[1] * (1. - Cs) + L[2] * Sn);
+        R[4] = (T)(L[1] * L[1] + (1. - L[1] * L[1]) * Cs);
+        R[5] = (T)(L[1] * L[2] * (1. - Cs) - L[0] * Sn);
+        R[6] = (T)(L[0] * L[2] * (1. - Cs) - L[1] * Sn);
+        R[7] = (T)(L[1] * L[2] * (1. - Cs) + L[0] * Sn);
+        R[8] = (T)(L[2] * L[2] + (1. - L[2] * L[2]) * Cs);
+    } else {
+        R[0] = (T)Cs;
+        R[1] = (T)(-1. * Sn);
+        R[3] = (T)Sn;
+        R[4] = (T)Cs;
+        R[2] = R[5] = R[6] = R[7] = R[8] = (T)0;
+    }
+}
+
+// Inverse of a symmetric-or-not 3x3 matrix by adjugate / determinant.
+__device__ __forceinline__ void inv3(const double m[9], double r[9]) {
+    double c00 = m[4] * m[8] - m[5] * m[7];
+    double c01 = m[3] * m[8] - m[5] * m[6];
+    double c02 = m[3] * m[7] - m[4] * m[6];
+    double det = m[0] * c00 - m[1] * c01 + m[2] * c02;
+    double c10 = m[1] * m[8] - m[2] * m[7];
+    double c11 = m[0] * m[8] - m[2] * m[6];
+    double c12 = m[0] * m[7] - m[1] * m[6];
+    double c20 = m[1] * m[5] - m[2] * m[4];
+    double c21 = m[0] * m[5] - m[2] * m[3];
+    double c22 = m[0] * m[4] - m[1] * m[3];
+    r[0] = c00 / det;
+    r[3] = -c01 / det;
+    r[6] = c02 / det;
+    r[1] = -c10 / det;
+    r[4] = c11 / det;
+    r[7] = -c12 / det;
+    r[2] = c20 / det;
+    r[5] = -c21 / det;
+    r[8] = c22 / det;
+}
+
+__device__ __forceinline__ void cross3(const double *x, const double *y,
+                                       double *r) {
+    r[0] = x[1] * y[2] - x[2] * y[1];
+    r[1] = x[2] * y[0] - x[0] * y[2];
+    r[2] = x[0] * y[1] - x[1] * y[0];
+}
+
+// Thermal velocity of particle pid (genrand_gaussMB per component).
+template <int DIM>
+__device__ __forceinline__ void thermal(const DevCfg &c, uint32_t step,
+                                        uint32_t pid, int sp, double *rv) {
+    double sig = sqrt(c.kbt / c.mass[sp]);
+    float g[2];
+    mpcd_rng_normal2(c.seed, c.replica, step, MPCD_STREAM_THERMAL, pid, 0u, g);
+    rv[0] = sig * (double)g[0];
+    rv[1] = sig * (double)g[1];
+    if (DIM == 3) {
+        mpcd_rng_normal2(c.seed, c.replica, step, MPCD_STREAM_THERMAL, pid, 1u, g);
+        rv[2] = sig * (double)g[0];
+    } else {
+        rv[2] = 0.0;
+    }
+}
+
+}  // namespace mpcd

@@ -1,0 +1,130 @@
+"""Python binding of libmpcd_gpu.so (the C ABI of include/mpcd_gpu.h).
+
+The library is built in-tree (niamh-mpcd_b200/build.sh); if it is missing,
+loading raises instead of falling back to any CPU path.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "libmpcd_gpu.so")
+
+EXPORTS = [
+    "mpcd_abi_version", "mpcd_create", "mpcd_destroy", "mpcd_upload_state",
+    "mpcd_upload_particles_strided", "mpcd_download_state",
+    "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
+    "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
+    "mpcd_launches_per_step",
+]
+
+_lib = None
+
+
+class MPCDError(RuntimeError):
+    pass
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MPCDError(f"libmpcd_gpu.so not built ({LIB_PATH}); run build()")
+        lib = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        lib.mpcd_create.argtypes = [vp, C.POINTER(vp)]
+        lib.mpcd_destroy.argtypes = [vp]
+        lib.mpcd_upload_state.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+        lib.mpcd_upload_particles_strided.argtypes = [vp, C.c_int, vp, C.c_size_t,
+                                                      C.c_size_t, C.c_size_t, C.c_size_t,
+                                                      C.c_size_t]
+        lib.mpcd_download_state.argtypes = [vp, vp, vp, vp]
+        lib.mpcd_download_particles_strided.argtypes = [vp, vp, C.c_size_t, C.c_size_t,
+                                                        C.c_size_t, C.c_size_t]
+        lib.mpcd_step.argtypes = [vp, C.c_int, C.c_uint32]
+        lib.mpcd_timestep.argtypes = [vp, C.c_uint32, vp, vp]
+        lib.mpcd_globals.argtypes = [vp, vp, vp]
+        lib.mpcd_cell_props.argtypes = [vp, vp, vp, vp, vp]
+        lib.mpcd_get_status.argtypes = [vp, vp]
+        lib.mpcd_set_stream.argtypes = [vp, vp]
+        lib.mpcd_launches_per_step.argtypes = [vp]
+        _lib = lib
+    return _lib
+
+
+def _check(r, what):
+    if r != 0:
+        raise MPCDError(f"{what} failed: {r} ({abi.ERRORS.get(r, 'unknown')})")
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Solver:
+    """One simulation box on the current CUDA device."""
+
+    def __init__(self, cfg):
+        self.lib = load()
+        self.cfg = cfg
+        h = C.c_void_p()
+        _check(self.lib.mpcd_create(C.byref(cfg), C.byref(h)), "mpcd_create")
+        self.h = h
+        self.n = 0
+
+    def upload(self, Q, V, U=None, spid=None):
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        spid = None if spid is None else np.ascontiguousarray(spid, dtype=np.int32)
+        _check(self.lib.mpcd_upload_state(self.h, len(Q), _p(Q), _p(V), _p(U), _p(spid)),
+               "mpcd_upload_state")
+        self.n = len(Q)
+
+    def step(self, nsteps, step0):
+        _check(self.lib.mpcd_step(self.h, nsteps, step0), "mpcd_step")
+
+    def timestep(self, runtime):
+        av = np.zeros(3)
+        kb = C.c_double()
+        _check(self.lib.mpcd_timestep(self.h, runtime, _p(av), C.byref(kb)), "mpcd_timestep")
+        return kb.value, av
+
+    def globals(self):
+        av = np.zeros(3)
+        kb = C.c_double()
+        _check(self.lib.mpcd_globals(self.h, C.byref(kb), _p(av)), "mpcd_globals")
+        return kb.value, av
+
+    def download(self):
+        Q = np.zeros((self.n, 3))
+        V = np.zeros((self.n, 3))
+        U = np.zeros((self.n, 3))
+        _check(self.lib.mpcd_download_state(self.h, _p(Q), _p(V), _p(U)),
+               "mpcd_download_state")
+        return Q, V, U
+
+    def status(self):
+        st = abi.Status()
+        _check(self.lib.mpcd_get_status(self.h, C.byref(st)), "mpcd_get_status")
+        return st
+
+    def launches_per_step(self):
+        return self.lib.mpcd_launches_per_step(self.h)
+
+    def set_stream(self, stream_ptr):
+        _check(self.lib.mpcd_set_stream(self.h, C.c_void_p(stream_ptr)), "mpcd_set_stream")
+
+    def close(self):
+        if self.h:
+            self.lib.mpcd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
