@@ -136,6 +136,8 @@ typedef struct mpcd_status {
     uint64_t bounce_limit;  /* particles that hit the NBOUNCE limit
                                (bc.c:1461-1488)                             */
     uint64_t nonfinite;     /* non-finite velocities seen by the step       */
+    uint64_t overflow;      /* particles of cells too populous for one tile
+                               (streamed without collision)                 */
 } mpcd_status;
 
 typedef struct mpcd_handle mpcd_handle;
@@ -199,6 +201,20 @@ int mpcd_set_stream(mpcd_handle *h, void *stream);
 
 /* Number of kernel launches the last mpcd_step issued per step. */
 int mpcd_launches_per_step(mpcd_handle *h);
+
+/* Execution strategy of the per-step pipeline (no counterpart in the
+ * reference, which has one serial path):
+ *   MPCD_STRATEGY_SCATTER   fused cell kernel writes in place, a scatter
+ *                           kernel reorders the state (one pass of compute);
+ *   MPCD_STRATEGY_RECOMPUTE the fused cell kernel runs twice, first only
+ *                           counting the next step's cells, then writing each
+ *                           particle directly to its sorted slot (fewer
+ *                           bytes moved, twice the arithmetic).
+ * strategy -1 restores the default; tile_particles (0 = default) sets the
+ * average number of particles staged per thread block. */
+#define MPCD_STRATEGY_SCATTER 0
+#define MPCD_STRATEGY_RECOMPUTE 1
+int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,7 @@
 #include "mpcd_device.cuh"
 #include "mpcd_fp64.cuh"
 #include "mpcd_mixed.cuh"
+#include "mpcd_tile.cuh"
 
 using namespace mpcd;
 
@@ -27,23 +28,22 @@ struct mpcd_handle {
     int n;
     int cap;
     int prec;
-    // FP64 state, two buffers
-    Fp64State f[2];
-    // mixed state, two buffers
-    MixState mx[2];
+    Fp64State f[2];  // FP64 state, two buffers (the sort writes the other)
+    MixState mx[2];  // mixed state, two buffers
     int cur;
-    int *key, *rank, *count, *start, *part;
-    double *acc;
+    int *key, *rank, *count, *fill, *start[2], *part;
+    int scur;        // which start[] belongs to the current order
+    double *acc;     // 2 x ACC_WORDS, by step parity
     unsigned long long *status;
     int nscan;
     int sm_count;
     int launches;
+    int strategy;    // MPCD_STRATEGY_*
+    int tile_target; // expected particles per tile
+    int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     uint32_t last_step;
     uint64_t steps;
     double *host_acc;  // pinned
-    // cell-property scratch for mpcd_cell_props
-    int *cp_pop;
-    double *cp_sums;
 };
 
 #define CK(call)                                                        \
@@ -180,12 +180,12 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->key);
     cudaFree(h->rank);
     cudaFree(h->count);
-    cudaFree(h->start);
+    cudaFree(h->fill);
+    cudaFree(h->start[0]);
+    cudaFree(h->start[1]);
     cudaFree(h->part);
     cudaFree(h->acc);
     cudaFree(h->status);
-    cudaFree(h->cp_pop);
-    cudaFree(h->cp_sums);
     if (h->host_acc) cudaFreeHost(h->host_acc);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -220,14 +220,20 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     int nc = dc.ncells;
     h->nscan = (nc + kScanTile - 1) / kScanTile;
     ALLOC(h->count, sizeof(int) * nc);
-    ALLOC(h->start, sizeof(int) * (nc + 1));
+    ALLOC(h->fill, sizeof(int) * nc);
+    ALLOC(h->start[0], sizeof(int) * (nc + 1));
+    ALLOC(h->start[1], sizeof(int) * (nc + 1));
     ALLOC(h->part, sizeof(int) * h->nscan);
-    ALLOC(h->acc, sizeof(double) * ACC_WORDS);
+    ALLOC(h->acc, sizeof(double) * 2 * ACC_WORDS);
     ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
+    h->sorted_for = -1;
+    h->strategy = -1;
+    h->tile_target = 0;
     if (cudaMemsetAsync(h->count, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->fill, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
         cudaMemsetAsync(h->status, 0, sizeof(unsigned long long) * ST_WORDS, h->stream) !=
             cudaSuccess ||
-        cudaMemsetAsync(h->acc, 0, sizeof(double) * ACC_WORDS, h->stream) != cudaSuccess) {
+        cudaMemsetAsync(h->acc, 0, sizeof(double) * 2 * ACC_WORDS, h->stream) != cudaSuccess) {
         mpcd_destroy(h);
         return MPCD_ERR_CUDA;
     }
@@ -291,6 +297,7 @@ static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V
     if (r != MPCD_OK) return r;
     h->n = n;
     h->cur = 0;
+    h->sorted_for = -1;
     // global number density as globalDensities (init.c:1002-1018) unless given
     if (!(h->cfg.gndnst > 0.0)) {
         std::vector<int> pop((size_t)h->dc.ncells, 0);
@@ -435,46 +442,170 @@ static int grid_for(const mpcd_handle *h, int n) {
     return g < 1 ? 1 : g;
 }
 
-static int step_fp64(mpcd_handle *h, uint32_t step) {
+// Tile geometry: cells per tile so that a tile holds about 'target'
+// particles on average; staging capacity 1.5x that plus a margin.
+static void tile_geometry(const mpcd_handle *h, int target, int *ct, int *cap) {
+    double vol = 1.0;
+    for (int d = 0; d < h->dc.dim; d++) vol *= h->dc.L[d];
+    double ppc = h->n > 0 ? (double)h->n / vol : 10.0;
+    if (ppc < 1.0) ppc = 1.0;
+    int c = 1;
+    while (c * 2 <= 256 && (double)(c * 2) * ppc <= (double)target) c *= 2;
+    *ct = c;
+    *cap = (int)(1.5 * (double)c * ppc) + 128;
+}
+
+template <int DIM, class T>
+static int launch_tile(mpcd_handle *h, int mode, const typename T::State &a,
+                       const typename T::State &b, const TileBufs &tb, const StepArgs &sa) {
+    int ct, capp;
+    tile_geometry(h, h->tile_target, &ct, &capp);
+    TileLayout lay = tile_layout<T>(ct, capp, h->dc.op, h->dc.n_species);
+    while (lay.bytes > 200 * 1024 && capp > 256) {
+        capp = capp * 3 / 4;
+        lay = tile_layout<T>(ct, capp, h->dc.op, h->dc.n_species);
+    }
+    int grid = (h->dc.ncells + ct - 1) / ct;
     const DevCfg &c = h->dc;
-    int n = h->n, nc = c.ncells;
-    Fp64State a = h->f[h->cur], b = h->f[1 - h->cur];
-    int gb = grid_for(h, n);
-    int gc = (int)(((long long)nc * 32 + 255) / 256);
-    if (c.dim == 3) {
-        k_bin_fp64<3><<<gb, 256, 0, h->stream>>>(c, a, n, h->key, h->rank, h->count, step,
-                                                  h->status);
-    } else {
-        k_bin_fp64<2><<<gb, 256, 0, h->stream>>>(c, a, n, h->key, h->rank, h->count, step,
-                                                  h->status);
+    cudaError_t e = cudaSuccess;
+#define MPCD_LAUNCH_TILE(MODEV)                                                          \
+    do {                                                                                 \
+        auto kfn = k_tile<DIM, T, MODEV>;                                                \
+        e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                 lay.bytes);                                             \
+        if (e == cudaSuccess) kfn<<<grid, 256, lay.bytes, h->stream>>>(c, a, b, tb, sa, lay); \
+    } while (0)
+    if (mode == MODE_INPLACE)
+        MPCD_LAUNCH_TILE(MODE_INPLACE);
+    else if (mode == MODE_COUNT)
+        MPCD_LAUNCH_TILE(MODE_COUNT);
+    else
+        MPCD_LAUNCH_TILE(MODE_FINAL);
+#undef MPCD_LAUNCH_TILE
+    if (e != cudaSuccess) return MPCD_ERR_CUDA;
+    return MPCD_OK;
+}
+
+static void launch_scan(mpcd_handle *h, int *start, int *fill, double *acc_zero) {
+    k_scan_partial<<<h->nscan, 256, 0, h->stream>>>(h->count, h->dc.ncells, h->part);
+    k_scan_apply<<<h->nscan, 256, 0, h->stream>>>(h->count, h->dc.ncells, h->part, start,
+                                                   fill, acc_zero);
+}
+
+template <int DIM, class T>
+static void launch_key(mpcd_handle *h, const typename T::State &a, const StepArgs &sa);
+template <>
+void launch_key<3, MixT<3>>(mpcd_handle *h, const MixState &a, const StepArgs &sa) {
+    k_key_mix<3><<<grid_for(h, h->n), 256, 0, h->stream>>>(h->dc, a, h->n, h->key, h->rank,
+                                                           h->count, sa, h->status);
+}
+template <>
+void launch_key<2, MixT<2>>(mpcd_handle *h, const MixState &a, const StepArgs &sa) {
+    k_key_mix<2><<<grid_for(h, h->n), 256, 0, h->stream>>>(h->dc, a, h->n, h->key, h->rank,
+                                                           h->count, sa, h->status);
+}
+template <>
+void launch_key<3, F64T<3>>(mpcd_handle *h, const Fp64State &a, const StepArgs &sa) {
+    k_key_f64<3><<<grid_for(h, h->n), 256, 0, h->stream>>>(h->dc, a, h->n, h->key, h->rank,
+                                                           h->count, sa, h->status);
+}
+template <>
+void launch_key<2, F64T<2>>(mpcd_handle *h, const Fp64State &a, const StepArgs &sa) {
+    k_key_f64<2><<<grid_for(h, h->n), 256, 0, h->stream>>>(h->dc, a, h->n, h->key, h->rank,
+                                                           h->count, sa, h->status);
+}
+
+static void launch_scatter(mpcd_handle *h, const MixState &a, const MixState &b,
+                           const int *start) {
+    k_scatter_mix<<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key, h->rank,
+                                                            start);
+}
+static void launch_scatter(mpcd_handle *h, const Fp64State &a, const Fp64State &b,
+                           const int *start) {
+    if (h->dc.dim == 3)
+        k_scatter_f64v<3><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key,
+                                                                    h->rank, start);
+    else
+        k_scatter_f64v<2><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key,
+                                                                    h->rank, start);
+}
+
+static void host_shift(const mpcd_handle *h, uint32_t step, double s[3]) {
+    s[0] = s[1] = s[2] = 0.0;
+    if (h->dc.galinv) mpcd_rng_shift(h->dc.seed, h->dc.replica, step, h->dc.dim, s);
+}
+
+// One solvent timestep.  Particles enter sorted by cell of this step's
+// shifted grid (established here if they are not) and leave sorted for the
+// next step's.
+template <int DIM, class T>
+static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
+    StepArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.step = step;
+    host_shift(h, step, sa.s);
+    host_shift(h, step + 1u, sa.sn);
+    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
+    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    int launches = 0;
+    if (h->sorted_for != (int64_t)step) {
+        launch_key<DIM, T>(h, st[h->cur], sa);
+        launch_scan(h, h->start[h->scur], nullptr, acc_cur);
+        launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[h->scur]);
+        h->cur = 1 - h->cur;
+        launches += 4;
     }
-    k_scan_partial<<<h->nscan, 256, 0, h->stream>>>(h->count, nc, h->part);
-    k_scan_apply<<<h->nscan, 256, 0, h->stream>>>(h->count, nc, h->part, h->start, h->acc);
-    if (c.dim == 3) {
-        k_scatter_fp64<3><<<gb, 256, 0, h->stream>>>(a, b, n, h->key, h->rank, h->start);
-        k_cell_fp64<3><<<gc, 256, 0, h->stream>>>(c, b, h->start, step, h->acc, h->status);
+    TileBufs tb;
+    memset(&tb, 0, sizeof(tb));
+    tb.start = h->start[h->scur];
+    tb.start_next = h->start[1 - h->scur];
+    tb.count_next = h->count;
+    tb.fill = h->fill;
+    tb.key = h->key;
+    tb.rank = h->rank;
+    tb.acc = acc_cur;
+    tb.status = h->status;
+    int r;
+    if (h->strategy == MPCD_STRATEGY_SCATTER) {
+        r = launch_tile<DIM, T>(h, MODE_INPLACE, st[h->cur], st[1 - h->cur], tb, sa);
+        if (r != MPCD_OK) return r;
+        launch_scan(h, h->start[1 - h->scur], nullptr, acc_nxt);
+        launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]);
     } else {
-        k_scatter_fp64<2><<<gb, 256, 0, h->stream>>>(a, b, n, h->key, h->rank, h->start);
-        k_cell_fp64<2><<<gc, 256, 0, h->stream>>>(c, b, h->start, step, h->acc, h->status);
+        r = launch_tile<DIM, T>(h, MODE_COUNT, st[h->cur], st[1 - h->cur], tb, sa);
+        if (r != MPCD_OK) return r;
+        launch_scan(h, h->start[1 - h->scur], h->fill, acc_nxt);
+        r = launch_tile<DIM, T>(h, MODE_FINAL, st[h->cur], st[1 - h->cur], tb, sa);
+        if (r != MPCD_OK) return r;
     }
+    launches += 4;
     CK(cudaGetLastError());
     h->cur = 1 - h->cur;
-    h->launches = 5;
+    h->scur = 1 - h->scur;
+    h->sorted_for = (int64_t)step + 1;
+    h->launches = launches;
     return MPCD_OK;
+}
+
+static int default_strategy(const mpcd_handle *h) {
+    // recompute (96 B/particle) wins when the collision is cheap to redo
+    return h->dc.op == MPCD_COLL_ARBAXIS ? MPCD_STRATEGY_RECOMPUTE : MPCD_STRATEGY_SCATTER;
 }
 
 extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
     if (!h || nsteps < 0) return MPCD_ERR_ARG;
     if (h->n <= 0) return MPCD_ERR_STATE;
+    if (h->strategy < 0) h->strategy = default_strategy(h);
+    if (h->tile_target <= 0) h->tile_target = h->prec == MPCD_PREC_MIXED ? 1024 : 768;
     for (int k = 0; k < nsteps; k++) {
         uint32_t step = step0 + (uint32_t)k;
         int r;
         if (h->prec == MPCD_PREC_FP64)
-            r = step_fp64(h, step);
+            r = h->dc.dim == 3 ? run_step<3, F64T<3>>(h, h->f, step)
+                               : run_step<2, F64T<2>>(h, h->f, step);
         else
-            r = mix_step(h->mx, h->cur, h->dc, h->n, step, h->key, h->rank, h->count,
-                         h->start, h->part, h->nscan, h->acc, h->status, h->stream,
-                         h->sm_count, &h->launches);
+            r = h->dc.dim == 3 ? run_step<3, MixT<3>>(h, h->mx, step)
+                               : run_step<2, MixT<2>>(h, h->mx, step);
         if (r != MPCD_OK) return r;
         h->last_step = step;
         h->steps++;
@@ -482,9 +613,21 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
     return MPCD_OK;
 }
 
+extern "C" int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles) {
+    if (!h) return MPCD_ERR_ARG;
+    if (strategy != MPCD_STRATEGY_SCATTER && strategy != MPCD_STRATEGY_RECOMPUTE &&
+        strategy != -1)
+        return MPCD_ERR_ARG;
+    if (tile_particles != 0 && (tile_particles < 32 || tile_particles > 8192)) return MPCD_ERR_ARG;
+    h->strategy = strategy;
+    h->tile_target = tile_particles;
+    return MPCD_OK;
+}
+
 extern "C" int mpcd_globals(mpcd_handle *h, double *kbtnow, double avnow[3]) {
     if (!h) return MPCD_ERR_ARG;
-    CK(cudaMemcpyAsync(h->host_acc, h->acc, sizeof(double) * ACC_WORDS,
+    CK(cudaMemcpyAsync(h->host_acc, h->acc + (size_t)(h->last_step & 1u) * ACC_WORDS,
+                       sizeof(double) * ACC_WORDS,
                        cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     int dim = h->dc.dim;
@@ -511,6 +654,7 @@ extern "C" int mpcd_get_status(mpcd_handle *h, mpcd_status *st) {
     st->escaped = w[ST_ESCAPED];
     st->bounce_limit = w[ST_BOUNCE];
     st->nonfinite = w[ST_NONFINITE];
+    st->overflow = w[ST_OVERFLOW];
     return MPCD_OK;
 }
 

@@ -1,0 +1,639 @@
+// mpcd_tile.cuh -- the fused per-step kernel of the solvent timestep.
+//
+// Particles are kept sorted by cell of the current step's shifted grid
+// (counting sort, cell start offsets in 'start').  One CTA owns a tile of
+// consecutive cells; it stages the tile's particles in shared memory, then
+//   - one thread per cell: moments (localPROP), phantom particles
+//     (ghostPart), the cell's collision parameters (SRD axis and rotation
+//     matrix; Andersen sums; MPC-AT+a inertia tensor, its FP64 inverse and
+//     the angular-momentum term), avVel;
+//   - one thread per particle: the collision (MPCcollision), TEMP, shift
+//     back, streaming, walls, and the particle's cell key on the NEXT step's
+//     shifted grid (whose shift is known: draws are counter-based), counted
+//     into the next step's histogram.
+// Three variants of the write-out (MODE_*):
+//   INPLACE  write the state back in place + key/rank (a scatter kernel then
+//            reorders it);
+//   COUNT    write nothing, only count the next keys;
+//   FINAL    recompute and write each particle straight to its slot of the
+//            next step's order (needs the scan of COUNT's histogram).
+// INPLACE+scatter moves 144 B/particle (mixed), COUNT+FINAL 96 B; the
+// autotuner picks per configuration.
+#pragma once
+
+#include "mpcd_device.cuh"
+#include "mpcd_fp64.cuh"
+#include "mpcd_mixed.cuh"
+
+namespace mpcd {
+
+enum { MODE_INPLACE = 0, MODE_COUNT = 1, MODE_FINAL = 2 };
+
+enum { ST_OVERFLOW = 3 };  // status word: cells too large for a tile
+
+struct StepArgs {
+    uint32_t step;
+    int pad_;
+    double s[3];   // shift of this step
+    double sn[3];  // shift of the next step
+};
+
+struct TileBufs {
+    const int *start;       // this step's cell starts
+    const int *start_next;  // next step's cell starts (FINAL)
+    int *count_next;        // next step's histogram (INPLACE, COUNT)
+    int *fill;              // next step's fill cursors (FINAL)
+    int *key;               // INPLACE: next key per particle
+    int *rank;              // INPLACE: rank within next cell
+    double *acc;
+    unsigned long long *status;
+};
+
+// ------------------------------------------------------- precision traits
+struct MixRec {
+    float4 P, W;
+};
+struct F64Rec {
+    double q[3];  // position on the shifted grid
+    double v[3];
+    int pid, pad_;
+};
+
+template <int DIM>
+struct MixT {
+    using State = MixState;
+    using Rec = MixRec;
+    using VT = float;
+    static __device__ __forceinline__ void load(const DevCfg &c, const State &st, int i,
+                                                const StepArgs &sa, Rec &r) {
+        r.P = st.P[i];
+        r.W = st.W[i];
+        if (c.grav_flag) {
+            r.W.x += (float)(c.dt * c.grav[0]);
+            r.W.y += (float)(c.dt * c.grav[1]);
+            if (DIM == 3) r.W.z += (float)(c.dt * c.grav[2]);
+        }
+    }
+    static __device__ __forceinline__ int sp(const State &st, int i) {
+        return st.sp ? st.sp[i] : 0;
+    }
+    static __device__ __forceinline__ uint32_t pid(const Rec &r) {
+        return (uint32_t)__float_as_int(r.W.w);
+    }
+    static __device__ __forceinline__ void vel(const Rec &r, double v[3]) {
+        v[0] = r.W.x;
+        v[1] = r.W.y;
+        v[2] = DIM == 3 ? (double)r.W.z : 0.0;
+    }
+    static __device__ __forceinline__ void velf(const Rec &r, float v[3]) {
+        v[0] = r.W.x;
+        v[1] = r.W.y;
+        v[2] = DIM == 3 ? r.W.z : 0.f;
+    }
+    // position relative to the origin of shifted cell cc
+    static __device__ __forceinline__ void rel(const DevCfg &c, const Rec &r,
+                                               const StepArgs &sa, const int *cc,
+                                               double q[3]) {
+        mix_rel<DIM>(c, r.P, sa.s, cc, q);
+    }
+    static __device__ __forceinline__ void set_vel(Rec &r, const double v[3]) {
+        r.W.x = (float)v[0];
+        r.W.y = (float)v[1];
+        if (DIM == 3) r.W.z = (float)v[2];
+    }
+    static __device__ __forceinline__ void set_velf(Rec &r, const float v[3]) {
+        r.W.x = v[0];
+        r.W.y = v[1];
+        if (DIM == 3) r.W.z = v[2];
+    }
+    // stream (FP32), walls (FP64, solid only), exact periodic wrap; returns
+    // the particle's cell key on the next step's grid; 'bounce' set when the
+    // wall loop hit its limit.
+    static __device__ __forceinline__ int finish(const DevCfg &c, Rec &r, int sp,
+                                                 const StepArgs &sa, int &bounce, int &esc) {
+        int ci[3];
+        unpack_cell(__float_as_int(r.P.w), ci[0], ci[1], ci[2]);
+        float o[3] = {r.P.x, r.P.y, r.P.z};
+        float vv[3] = {r.W.x, r.W.y, r.W.z};
+        const float dtf = (float)c.dt;
+        for (int d = 0; d < DIM; d++) {
+            o[d] = fmaf(dtf, vv[d], o[d]);
+            carry(o[d], ci[d]);
+        }
+        if (c.n_solid > 0) {
+            double q[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+            for (int d = 0; d < DIM; d++) {
+                q[d] = (double)ci[d] + (double)o[d];
+                v[d] = (double)vv[d];
+            }
+            bool inside = false;
+            for (int wi = 0; wi < c.n_walls; wi++) {
+                const DevWall &wl = c.walls[wi];
+                if (!wl.periodic && wall_W(wl, q, wl.Q, DIM) < 0.0) inside = true;
+            }
+            if (inside) {
+                bounce += wall_collisions<DIM>(c, q, v, sp, true);
+                for (int d = 0; d < DIM; d++) {
+                    double f = floor(q[d]);
+                    ci[d] = (int)f;
+                    o[d] = (float)(q[d] - f);
+                    if (o[d] >= 1.0f) {
+                        o[d] = 0.0f;
+                        ci[d] += 1;
+                    }
+                    vv[d] = (float)v[d];
+                }
+            }
+        }
+        for (int d = 0; d < DIM; d++) {
+            if (c.pbc[d]) {
+                if (ci[d] < 0 || ci[d] >= c.L[d])
+                    ci[d] = ((ci[d] % c.L[d]) + c.L[d]) % c.L[d];
+            } else {
+                if (ci[d] < 0) ci[d] = 0;
+                if (ci[d] > c.L[d]) ci[d] = c.L[d];
+            }
+        }
+        r.P.x = o[0];
+        r.P.y = o[1];
+        r.P.z = DIM == 3 ? o[2] : 0.0f;
+        r.P.w = __int_as_float(pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0));
+        r.W.x = vv[0];
+        r.W.y = vv[1];
+        if (DIM == 3) r.W.z = vv[2];
+        double qs;
+        int a = mix_shift_axis(ci[0], o[0], sa.sn[0], c.L[0], c.pbc[0], qs, esc);
+        int b = mix_shift_axis(ci[1], o[1], sa.sn[1], c.L[1], c.pbc[1], qs, esc);
+        int z = 0;
+        if (DIM == 3) z = mix_shift_axis(ci[2], o[2], sa.sn[2], c.L[2], c.pbc[2], qs, esc);
+        return cell_lin(c, a, b, z);
+    }
+    static __device__ __forceinline__ void store(const State &st, int i, const Rec &r) {
+        st.P[i] = r.P;
+        st.W[i] = r.W;
+    }
+    static __device__ __forceinline__ void store_sp(const State &st, int i, int sp) {
+        if (st.sp) st.sp[i] = sp;
+    }
+};
+
+template <int DIM>
+struct F64T {
+    using State = Fp64State;
+    using Rec = F64Rec;
+    using VT = double;
+    static __device__ __forceinline__ void load(const DevCfg &c, const State &st, int i,
+                                                const StepArgs &sa, Rec &r) {
+        for (int d = 0; d < 3; d++) {
+            r.q[d] = d < DIM ? shift_fwd(st.q[d][i], sa.s[d], c.L[d]) : 0.0;
+            r.v[d] = d < DIM ? st.v[d][i] : 0.0;
+            if (d < DIM && c.grav_flag) r.v[d] = r.v[d] + c.dt * c.grav[d];
+        }
+        r.pid = st.pid[i];
+    }
+    static __device__ __forceinline__ int sp(const State &st, int i) {
+        return st.sp ? st.sp[i] : 0;
+    }
+    static __device__ __forceinline__ uint32_t pid(const Rec &r) { return (uint32_t)r.pid; }
+    static __device__ __forceinline__ void vel(const Rec &r, double v[3]) {
+        v[0] = r.v[0];
+        v[1] = r.v[1];
+        v[2] = r.v[2];
+    }
+    static __device__ __forceinline__ void rel(const DevCfg &c, const Rec &r,
+                                               const StepArgs &sa, const int *cc,
+                                               double q[3]) {
+        // the reference uses absolute shifted positions (localPROP, mpc.c:103)
+        q[0] = r.q[0];
+        q[1] = r.q[1];
+        q[2] = r.q[2];
+    }
+    static __device__ __forceinline__ void set_vel(Rec &r, const double v[3]) {
+        for (int d = 0; d < DIM; d++) r.v[d] = v[d];
+    }
+    static __device__ __forceinline__ int finish(const DevCfg &c, Rec &r, int sp,
+                                                 const StepArgs &sa, int &bounce, int &esc) {
+        double q[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+        for (int d = 0; d < DIM; d++) {
+            v[d] = r.v[d];
+            q[d] = shift_back(r.q[d], sa.s[d], c.L[d]);
+            q[d] = q[d] + c.dt * v[d];
+        }
+        bounce += wall_collisions<DIM>(c, q, v, sp, false);
+        int idx[3] = {0, 0, 0};
+        for (int d = 0; d < DIM; d++) {
+            r.q[d] = q[d];
+            r.v[d] = v[d];
+            double qs = shift_fwd(q[d], sa.sn[d], c.L[d]);
+            idx[d] = bin_axis(qs, c.L[d], c.pbc[d], 1, esc);
+        }
+        return cell_lin(c, idx[0], idx[1], idx[2]);
+    }
+    static __device__ __forceinline__ void store(const State &st, int i, const Rec &r) {
+        for (int d = 0; d < DIM; d++) {
+            st.q[d][i] = r.q[d];
+            st.v[d][i] = r.v[d];
+        }
+        st.pid[i] = r.pid;
+    }
+    static __device__ __forceinline__ void store_sp(const State &st, int i, int sp) {
+        if (st.sp) st.sp[i] = sp;
+    }
+};
+
+// --------------------------------------------------------- smem layout
+struct TileLayout {
+    int ct;   // cells per tile
+    int cap;  // particle capacity of the staging area
+    int off_rec, off_sp, off_cell, off_rv;
+    int off_start, off_u, off_R, off_cm, off_rs, off_W;
+    int bytes;
+};
+
+template <class T>
+static inline TileLayout tile_layout(int ct, int cap, int op, int nspecies) {
+    TileLayout L;
+    L.ct = ct;
+    L.cap = cap;
+    int o = 0;
+    auto take = [&](int bytes, int align) {
+        o = (o + align - 1) / align * align;
+        int r = o;
+        o += bytes;
+        return r;
+    };
+    L.off_rec = take(cap * (int)sizeof(typename T::Rec), 16);
+    bool and_ = op != MPCD_COLL_ARBAXIS;
+    L.off_rv = and_ ? take(cap * 3 * (int)sizeof(typename T::VT), 16) : -1;
+    L.off_start = take((ct + 1) * 4, 16);
+    L.off_u = take(ct * 3 * 8, 16);
+    L.off_R = op == MPCD_COLL_ARBAXIS ? take(ct * 9 * (int)sizeof(typename T::VT), 16) : -1;
+    L.off_cm = op == MPCD_COLL_RAT ? take(ct * 3 * 8, 16) : -1;
+    L.off_rs = and_ ? take(ct * 3 * 8, 16) : -1;
+    L.off_W = op == MPCD_COLL_RAT ? take(ct * 3 * 8, 16) : -1;
+    L.off_sp = nspecies > 1 ? take(cap, 4) : -1;
+    L.off_cell = take(cap, 4);
+    L.bytes = (o + 15) / 16 * 16;
+    return L;
+}
+
+__device__ __forceinline__ double block_sum256(double v, double *red) {
+    v = warp_sum(v);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 32) {
+        t = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+        t = warp_sum(t);
+    }
+    return t;  // valid in thread 0
+}
+
+template <int DIM, class T, int MODE>
+__global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
+                                              typename T::State a, typename T::State b,
+                                              TileBufs tb, StepArgs sa, TileLayout lay) {
+    using Rec = typename T::Rec;
+    using VT = typename T::VT;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red[8];
+    __shared__ int s_sub[2];
+    Rec *s_rec = (Rec *)(smem + lay.off_rec);
+    unsigned char *s_cell = smem + lay.off_cell;
+    unsigned char *s_sp = lay.off_sp >= 0 ? smem + lay.off_sp : nullptr;
+    VT *s_rv = lay.off_rv >= 0 ? (VT *)(smem + lay.off_rv) : nullptr;
+    int *s_start = (int *)(smem + lay.off_start);
+    double *s_u = (double *)(smem + lay.off_u);
+    VT *s_R = lay.off_R >= 0 ? (VT *)(smem + lay.off_R) : nullptr;
+    double *s_cm = lay.off_cm >= 0 ? (double *)(smem + lay.off_cm) : nullptr;
+    double *s_rs = lay.off_rs >= 0 ? (double *)(smem + lay.off_rs) : nullptr;
+    double *s_W = lay.off_W >= 0 ? (double *)(smem + lay.off_W) : nullptr;
+
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int c0 = blockIdx.x * lay.ct;
+    const int c1 = min(c0 + lay.ct, c.ncells);
+    const int nct = c1 - c0;
+    for (int k = tid; k <= nct; k += nth) s_start[k] = tb.start[c0 + k];
+    __syncthreads();
+
+    const bool andersen = c.op != MPCD_COLL_ARBAXIS;
+    const bool rat = c.op == MPCD_COLL_RAT;
+    double ke = 0.0, av[3] = {0, 0, 0};
+    int bounce = 0, esc = 0, overflow = 0;
+
+    int cl_a = 0;
+    while (cl_a < nct) {
+        // largest sub-tile [cl_a, cl_b) that fits the staging area
+        if (tid == 0) {
+            const int base = s_start[cl_a];
+            int cl_b = nct;
+            if (s_start[nct] - base > lay.cap) {  // rare: tile above capacity
+                cl_b = cl_a;
+                while (cl_b < nct && s_start[cl_b + 1] - base <= lay.cap) cl_b++;
+            }
+            s_sub[0] = cl_b;
+        }
+        __syncthreads();
+        int cl_b = s_sub[0];
+        const bool huge = (cl_b == cl_a);  // one cell larger than the tile
+        if (huge) cl_b = cl_a + 1;
+        const int p0 = s_start[cl_a];
+        const int np = s_start[cl_b] - p0;
+        if (huge) {
+            // no collision for a cell beyond capacity (counted); particles
+            // still stream and are re-binned
+            if (tid == 0) overflow += np;
+            for (int j = tid; j < np; j += nth) {
+                Rec r;
+                T::load(c, a, p0 + j, sa, r);
+                int sp = T::sp(a, p0 + j);
+                double v[3];
+                T::vel(r, v);
+                ke += c.mass[sp] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                int k = T::finish(c, r, sp, sa, bounce, esc);
+                if (MODE == MODE_INPLACE) {
+                    T::store(a, p0 + j, r);
+                    tb.key[p0 + j] = k;
+                    tb.rank[p0 + j] = atomicAdd(&tb.count_next[k], 1);
+                } else if (MODE == MODE_COUNT) {
+                    atomicAdd(&tb.count_next[k], 1);
+                } else {
+                    int dst = tb.start_next[k] + atomicAdd(&tb.fill[k], 1);
+                    T::store(b, dst, r);
+                    T::store_sp(b, dst, sp);
+                }
+            }
+            __syncthreads();
+            cl_a = cl_b;
+            continue;
+        }
+        // ---- stage ----
+        for (int j = tid; j < np; j += nth) {
+            T::load(c, a, p0 + j, sa, s_rec[j]);
+            if (s_sp) s_sp[j] = (unsigned char)T::sp(a, p0 + j);
+        }
+        for (int cl = cl_a + tid; cl < cl_b; cl += nth)
+            for (int j = s_start[cl] - p0; j < s_start[cl + 1] - p0; j++)
+                s_cell[j] = (unsigned char)(cl - cl_a);
+        __syncthreads();
+        // ---- thermal draws (Andersen), one per particle ----
+        if (andersen) {
+            for (int j = tid; j < np; j += nth) {
+                int sp = s_sp ? s_sp[j] : 0;
+                double rv[3];
+                thermal<DIM>(c, sa.step, T::pid(s_rec[j]), sp, rv);
+                for (int d = 0; d < 3; d++) s_rv[3 * j + d] = (VT)rv[d];
+            }
+            __syncthreads();
+        }
+        // ---- per cell ----
+        for (int cl = cl_a + tid; cl < cl_b; cl += nth) {
+            const int lc = cl - cl_a;
+            const int j0 = s_start[cl] - p0, j1 = s_start[cl + 1] - p0, pop = j1 - j0;
+            const int cell = c0 + cl;
+            int cc[3];
+            cell_coords(c, cell, cc[0], cc[1], cc[2]);
+            double M = 0.0, pv[3] = {0, 0, 0}, pq[3] = {0, 0, 0};
+            for (int j = j0; j < j1; j++) {
+                double m = c.mass[s_sp ? s_sp[j] : 0];
+                double v[3];
+                T::vel(s_rec[j], v);
+                M += m;
+                for (int d = 0; d < DIM; d++) pv[d] += v[d] * m;
+                if (rat) {
+                    double q[3];
+                    T::rel(c, s_rec[j], sa, cc, q);
+                    for (int d = 0; d < DIM; d++) pq[d] += q[d] * m;
+                }
+            }
+            double u[3] = {0, 0, 0}, cm[3] = {0, 0, 0};
+            if (M > 0.0)
+                for (int d = 0; d < DIM; d++) {
+                    u[d] = pv[d] / M;
+                    if (rat) cm[d] = pq[d] / M;
+                }
+            if (c.any_phantom && pop > 0 && pop < c.gndnst &&
+                cell_cut_by_phantom<DIM>(c, cc[0], cc[1], cc[2], sa.s)) {
+                double invN = 1.0 / (c.gndnst - (double)pop);
+                double sig = sqrt(c.kbt / invN);
+                for (int d = 0; d < DIM; d++) {
+                    float g = mpcd_rng_normal(c.seed, c.replica, sa.step, MPCD_STREAM_GHOST,
+                                              (uint32_t)cell, (uint32_t)d);
+                    u[d] += sig * (double)g;
+                    u[d] /= c.gndnst;
+                }
+            }
+            for (int d = 0; d < DIM; d++) av[d] += u[d];
+            for (int d = 0; d < 3; d++) s_u[3 * lc + d] = u[d];
+            if (pop > 1) {
+                if (!andersen) {
+                    double Lx[3] = {0, 0, 1};
+                    if (DIM == 3)
+                        mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
+                    srd_matrix<DIM, VT>(c, Lx, &s_R[9 * lc]);
+                } else {
+                    double rs[3] = {0, 0, 0};
+                    for (int j = j0; j < j1; j++) {
+                        double m = c.mass[s_sp ? s_sp[j] : 0];
+                        for (int d = 0; d < DIM; d++) rs[d] += m * (double)s_rv[3 * j + d];
+                    }
+                    for (int d = 0; d < 3; d++) s_rs[3 * lc + d] = d < DIM ? rs[d] / M : 0.0;
+                    if (rat) {
+                        double I6[6] = {0, 0, 0, 0, 0, 0}, Lm[3] = {0, 0, 0};
+                        for (int j = j0; j < j1; j++) {
+                            double m = c.mass[s_sp ? s_sp[j] : 0];
+                            double q[3], v[3], r[3] = {0, 0, 0}, dv[3] = {0, 0, 0}, am[3];
+                            T::rel(c, s_rec[j], sa, cc, q);
+                            T::vel(s_rec[j], v);
+                            for (int d = 0; d < DIM; d++) {
+                                r[d] = q[d] - cm[d];
+                                dv[d] = m * (v[d] - (double)s_rv[3 * j + d]);
+                            }
+                            I6[0] += m * (r[1] * r[1] + r[2] * r[2]);
+                            I6[1] += m * (r[0] * r[0] + r[2] * r[2]);
+                            I6[2] += m * (r[0] * r[0] + r[1] * r[1]);
+                            I6[3] += m * r[0] * r[1];
+                            I6[4] += m * r[0] * r[2];
+                            I6[5] += m * r[1] * r[2];
+                            cross3(r, dv, am);
+                            for (int d = 0; d < 3; d++) Lm[d] += am[d];
+                        }
+                        double II[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                        if (DIM == 3) {
+                            if (pop >= 3) {
+                                double I[9] = {I6[0], -I6[3], -I6[4], -I6[3], I6[1],
+                                               -I6[5], -I6[4], -I6[5], I6[2]};
+                                inv3(I, II);
+                            }
+                        } else {
+                            II[8] = 1. / I6[2];
+                        }
+                        for (int x = 0; x < 3; x++) {
+                            double w = 0.0;
+                            for (int y = 0; y < 3; y++) w += II[x * 3 + y] * Lm[y];
+                            s_W[3 * lc + x] = w;
+                            s_cm[3 * lc + x] = cm[x];
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // ---- per particle ----
+        for (int j = tid; j < np; j += nth) {
+            const int lc = s_cell[j];
+            const int cl = cl_a + lc;
+            const int pop = s_start[cl + 1] - s_start[cl];
+            const int sp = s_sp ? s_sp[j] : 0;
+            Rec r = s_rec[j];
+            if (pop > 1) {
+                if (!andersen) {
+                    const VT *R = &s_R[9 * lc];
+                    if constexpr (sizeof(VT) == 4) {
+                        float ux = (float)s_u[3 * lc], uy = (float)s_u[3 * lc + 1],
+                              uz = (float)s_u[3 * lc + 2];
+                        float v[3];
+                        MixT<DIM>::velf(*(const MixRec *)&r, v);
+                        float wx = v[0] - ux, wy = v[1] - uy, wz = DIM == 3 ? v[2] - uz : 0.f;
+                        float nv[3];
+                        if (DIM == 3) {
+                            nv[0] = ux + ((float)R[0] * wx + (float)R[1] * wy + (float)R[2] * wz);
+                            nv[1] = uy + ((float)R[3] * wx + (float)R[4] * wy + (float)R[5] * wz);
+                            nv[2] = uz + ((float)R[6] * wx + (float)R[7] * wy + (float)R[8] * wz);
+                        } else {
+                            nv[0] = ux + ((float)R[0] * wx + (float)R[1] * wy);
+                            nv[1] = uy + ((float)R[3] * wx + (float)R[4] * wy);
+                            nv[2] = 0.f;
+                        }
+                        MixT<DIM>::set_velf(*(MixRec *)&r, nv);
+                    } else {
+                        double v[3], w[3] = {0, 0, 0}, t[3] = {0, 0, 0}, nv[3];
+                        T::vel(r, v);
+                        const double *u = &s_u[3 * lc];
+                        for (int d = 0; d < DIM; d++) w[d] = v[d] - u[d];
+                        for (int x = 0; x < DIM; x++)
+                            for (int y = 0; y < DIM; y++) t[x] += (double)R[x * 3 + y] * w[y];
+                        for (int d = 0; d < DIM; d++) nv[d] = u[d] + t[d];
+                        T::set_vel(r, nv);
+                    }
+                } else {
+                    const double *u = &s_u[3 * lc], *rs = &s_rs[3 * lc];
+                    double damp = c.damp[sp];
+                    double nv[3];
+                    if (!rat) {
+                        for (int d = 0; d < DIM; d++)
+                            nv[d] = u[d] + (double)s_rv[3 * j + d] - rs[d] -
+                                    damp * u[d] / (double)pop;
+                    } else {
+                        int cc[3];
+                        cell_coords(c, c0 + cl, cc[0], cc[1], cc[2]);
+                        double q[3], rr[3] = {0, 0, 0}, ang[3];
+                        T::rel(c, r, sa, cc, q);
+                        for (int d = 0; d < DIM; d++) rr[d] = q[d] - s_cm[3 * lc + d];
+                        cross3(&s_W[3 * lc], rr, ang);
+                        for (int d = 0; d < DIM; d++)
+                            nv[d] = u[d] + (double)s_rv[3 * j + d] - rs[d] - damp * u[d] + ang[d];
+                    }
+                    T::set_vel(r, nv);
+                }
+            }
+            {
+                double v[3];
+                T::vel(r, v);
+                double t = v[0] * v[0];
+                t += v[1] * v[1];
+                t += v[2] * v[2];
+                ke += c.mass[sp] * t;
+            }
+            int k = T::finish(c, r, sp, sa, bounce, esc);
+            const int gi = p0 + j;
+            if (MODE == MODE_INPLACE) {
+                T::store(a, gi, r);
+                tb.key[gi] = k;
+                tb.rank[gi] = atomicAdd(&tb.count_next[k], 1);
+            } else if (MODE == MODE_COUNT) {
+                atomicAdd(&tb.count_next[k], 1);
+            } else {
+                int dst = tb.start_next[k] + atomicAdd(&tb.fill[k], 1);
+                T::store(b, dst, r);
+                T::store_sp(b, dst, sp);
+            }
+        }
+        __syncthreads();
+        cl_a = cl_b;
+    }
+    // ---- block reductions ----
+    if (MODE != MODE_COUNT) {
+        double t = block_sum256(ke, red);
+        if (tid == 0) atomicAdd(&tb.acc[ACC_KE], t);
+        for (int d = 0; d < DIM; d++) {
+            t = block_sum256(av[d], red);
+            if (tid == 0) atomicAdd(&tb.acc[ACC_VCM + d], t);
+        }
+        if (bounce) atomicAdd(&tb.status[ST_BOUNCE], (unsigned long long)bounce);
+        if (overflow) atomicAdd(&tb.status[ST_OVERFLOW], (unsigned long long)overflow);
+    }
+    if (esc && MODE != MODE_FINAL) atomicAdd(&tb.status[ST_ESCAPED], (unsigned long long)esc);
+}
+
+// Keys on the shifted grid of a step from the stored (unshifted) state:
+// establishes the cell order before the first step.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_key_mix(const __grid_constant__ DevCfg c, MixState a,
+                                                 int n, int *key, int *rank, int *count,
+                                                 StepArgs sa, unsigned long long *status) {
+    int esc_local = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 p = a.P[i];
+        int ca, cb, cz, e = 0;
+        unpack_cell(__float_as_int(p.w), ca, cb, cz);
+        double qs;
+        int x = mix_shift_axis(ca, p.x, sa.s[0], c.L[0], c.pbc[0], qs, e);
+        int y = mix_shift_axis(cb, p.y, sa.s[1], c.L[1], c.pbc[1], qs, e);
+        int z = DIM == 3 ? mix_shift_axis(cz, p.z, sa.s[2], c.L[2], c.pbc[2], qs, e) : 0;
+        esc_local += e;
+        int k = cell_lin(c, x, y, z);
+        key[i] = k;
+        rank[i] = atomicAdd(&count[k], 1);
+    }
+    if (esc_local) atomicAdd(&status[ST_ESCAPED], (unsigned long long)esc_local);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_key_f64(const __grid_constant__ DevCfg c, Fp64State a,
+                                                 int n, int *key, int *rank, int *count,
+                                                 StepArgs sa, unsigned long long *status) {
+    int esc_local = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int idx[3] = {0, 0, 0}, e = 0;
+        for (int d = 0; d < DIM; d++) {
+            double qs = shift_fwd(a.q[d][i], sa.s[d], c.L[d]);
+            idx[d] = bin_axis(qs, c.L[d], c.pbc[d], 1, e);
+        }
+        esc_local += e;
+        int k = cell_lin(c, idx[0], idx[1], idx[2]);
+        key[i] = k;
+        rank[i] = atomicAdd(&count[k], 1);
+    }
+    if (esc_local) atomicAdd(&status[ST_ESCAPED], (unsigned long long)esc_local);
+}
+
+// Reorder by (key, rank) into the other buffer.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_scatter_f64v(Fp64State a, Fp64State b, int n,
+                                                      const int *key, const int *rank,
+                                                      const int *start) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int dst = start[key[i]] + rank[i];
+        for (int d = 0; d < DIM; d++) {
+            b.q[d][dst] = a.q[d][i];
+            b.v[d][dst] = a.v[d][i];
+        }
+        b.pid[dst] = a.pid[i];
+        if (a.sp) b.sp[dst] = a.sp[i];
+    }
+}
+
+}  // namespace mpcd

@@ -28,6 +28,9 @@ LC_LOCAL = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
 
+STRATEGY_SCATTER = 0
+STRATEGY_RECOMPUTE = 1
+
 ERRORS = {
     ERR_ARG: "bad argument",
     ERR_UNSUPPORTED: "unsupported option",
@@ -106,6 +109,7 @@ class Status(C.Structure):
         ("escaped", C.c_uint64),
         ("bounce_limit", C.c_uint64),
         ("nonfinite", C.c_uint64),
+        ("overflow", C.c_uint64),
     ]
 
 

@@ -18,7 +18,7 @@ EXPORTS = [
     "mpcd_upload_particles_strided", "mpcd_download_state",
     "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
-    "mpcd_launches_per_step",
+    "mpcd_launches_per_step", "mpcd_set_strategy",
 ]
 
 _lib = None
@@ -51,6 +51,7 @@ def load():
         lib.mpcd_get_status.argtypes = [vp, vp]
         lib.mpcd_set_stream.argtypes = [vp, vp]
         lib.mpcd_launches_per_step.argtypes = [vp]
+        lib.mpcd_set_strategy.argtypes = [vp, C.c_int, C.c_int]
         _lib = lib
     return _lib
 
@@ -114,6 +115,10 @@ class Solver:
 
     def launches_per_step(self):
         return self.lib.mpcd_launches_per_step(self.h)
+
+    def set_strategy(self, strategy=-1, tile_particles=0):
+        _check(self.lib.mpcd_set_strategy(self.h, strategy, tile_particles),
+               "mpcd_set_strategy")
 
     def set_stream(self, stream_ptr):
         _check(self.lib.mpcd_set_stream(self.h, C.c_void_p(stream_ptr)), "mpcd_set_stream")

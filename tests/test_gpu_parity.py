@@ -80,3 +80,77 @@ def test_srd_conserves_momentum_and_energy(prec):
     tol = 1e-12 if prec == abi.PREC_FP64 else 1e-6
     assert np.abs(v.sum(axis=0) - p0).max() / scale < tol
     assert abs((v ** 2).sum() - e0) / e0 < (1e-12 if prec == abi.PREC_FP64 else 1e-5)
+
+
+@pytest.mark.parametrize("strategy", [abi.STRATEGY_SCATTER, abi.STRATEGY_RECOMPUTE])
+@pytest.mark.parametrize("name", ["srd3d", "rat2d", "channel3d", "mpcat3d_damp"])
+@pytest.mark.parametrize("tile", [0, 64, 4096])
+def test_strategies_and_tiles_agree_with_oracle(name, strategy, tile):
+    cfg, ppc, sseed, _ = build(name)
+    Q, V, U, sp = state(cfg, ppc, sseed)
+    o = Oracle(cfg, Q, V, U, sp)
+    g = Solver(cfg)
+    g.set_strategy(strategy, tile)
+    g.upload(Q, V, U, sp)
+    for s in range(1, 4):
+        o.step(s)
+        g.step(1, s)
+    qo, vo, _ = o.particles()
+    qg, vg, _ = g.download()
+    np.testing.assert_allclose(vg, vo, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qg, qo, rtol=0, atol=1e-11 * max(cfg.L))
+
+
+def _clumped_state(cfg, ppc, seed, clumps, per_clump):
+    """Uniform fluid plus dense clumps of particles in a few cells, so that
+    some cell tiles hold more particles than their staging capacity."""
+    from mpcd_b200 import workloads as W
+    Q, V, U, sp = W.synthetic_state(cfg, ppc, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    extra_q = []
+    for cidx in clumps:
+        q = np.zeros((per_clump, 3))
+        for d in range(cfg.dim):
+            q[:, d] = cidx[d] + 0.05 + 0.9 * rng.random(per_clump)
+        extra_q.append(q)
+    Qx = np.concatenate([Q] + extra_q)
+    n_extra = len(Qx) - len(Q)
+    Vx = np.concatenate([V, np.zeros((n_extra, 3))])
+    Vx[len(V):, :cfg.dim] = rng.standard_normal((n_extra, cfg.dim))
+    Ux = np.concatenate([U, np.zeros((n_extra, 3))])
+    spx = np.zeros(len(Qx), dtype=np.int32)
+    return Qx, Vx, Ux, spx
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_dense_tiles_are_subdivided(prec):
+    # 40 dense cells of 200 particles: tiles far above capacity are split
+    # into sub-tiles; every particle must still match the oracle.
+    from mpcd_b200 import workloads as W
+    cfg = W.cfg_srd3d((10, 10, 10), precision=abi.PREC_FP64, seed=31)
+    cfgp = W.cfg_srd3d((10, 10, 10), precision=prec, seed=31)
+    clumps = [(i % 10, (i // 10) % 10, 3 + (i % 4)) for i in range(40)]
+    Q, V, U, sp = _clumped_state(cfg, 10, 8, clumps, 200)
+    o = Oracle(cfg, Q, V, U, sp)
+    g = Solver(cfgp)
+    g.upload(Q, V, U, sp)
+    o.step(1)
+    g.step(1, 1)
+    qo, vo, _ = o.particles()
+    qg, vg, _ = g.download()
+    tol = 1e-11 if prec == abi.PREC_FP64 else 1e-5
+    bad = np.mean(np.abs(vg - vo).max(axis=1) > tol)
+    assert bad < (1e-12 if prec == abi.PREC_FP64 else 2e-3)
+    assert g.status().overflow == 0
+
+
+def test_overfull_cell_is_reported_not_collided():
+    # one cell holding more particles than a tile can stage: its particles
+    # stream without collision and are counted in status.overflow
+    from mpcd_b200 import workloads as W
+    cfg = W.cfg_srd3d((6, 6, 6), seed=32)
+    Q, V, U, sp = _clumped_state(cfg, 10, 9, [(2, 2, 2)], 5000)
+    g = Solver(cfg)
+    g.upload(Q, V, U, sp)
+    g.step(1, 1)
+    assert g.status().overflow >= 5000
