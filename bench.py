@@ -44,6 +44,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--forms", default="fp64,mixed",
+                    help="comma list of state forms to time (fp64, mixed)")
+    ap.add_argument("--strategy", type=int, default=-1,
+                    help="-1 default, 0 scatter, 1 recompute")
+    ap.add_argument("--tile", type=int, default=0, help="particles per tile (0 default)")
     return ap.parse_args()
 
 
@@ -117,13 +122,16 @@ def run_gpu(args, rank, world):
     stream = torch.cuda.current_stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     results = {}
-    for form, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+    forms = [f for f in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED))
+             if f[0] in args.forms.split(",")]
+    for form, prec in forms:
         cfg = W.cfg_srd3d(L_BOX, precision=prec, seed=20240 + rank)
         cfg.replica = rank
         Q, V, U, sp = W.synthetic_state(cfg, PPC, seed=7 + rank)
         n = len(Q)
         g = Solver(cfg)
         g.set_stream(stream.cuda_stream)
+        g.set_strategy(args.strategy, args.tile)
         g.upload(Q, V, U, sp)
         g.step(args.warmup, 1)
         torch.cuda.synchronize()
@@ -238,7 +246,9 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     res = run_gpu(args, rank, world)
-    if rank == 0:
+    if rank == 0 and not ("mixed" in res and "fp64" in res):
+        print(json.dumps({k: v for k, v in res.items()}))
+    elif rank == 0:
         mix, f64 = res["mixed"], res["fp64"]
         n = mix["n"]
         value = n * world * args.steps / (mix["ms_total"] / 1e3)
