@@ -216,6 +216,15 @@ int mpcd_launches_per_step(mpcd_handle *h);
 #define MPCD_STRATEGY_RECOMPUTE 1
 int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
 
+/* Cell-kernel family (no counterpart in the reference):
+ *   MPCD_KERNEL_AUTO  warp-per-32-cell-group kernel where the operator
+ *                     allows it (SRD without phantom walls), block-per-tile
+ *                     kernel otherwise;
+ *   MPCD_KERNEL_TILE  always the block-per-tile kernel. */
+#define MPCD_KERNEL_AUTO 0
+#define MPCD_KERNEL_TILE 1
+int mpcd_set_kernel(mpcd_handle *h, int kernel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,7 @@
 #include "mpcd_fp64.cuh"
 #include "mpcd_mixed.cuh"
 #include "mpcd_tile.cuh"
+#include "mpcd_group.cuh"
 
 using namespace mpcd;
 
@@ -40,6 +41,7 @@ struct mpcd_handle {
     int launches;
     int strategy;    // MPCD_STRATEGY_*
     int tile_target; // expected particles per tile
+    int kernel;      // MPCD_KERNEL_*: cell kernel family
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     uint32_t last_step;
     uint64_t steps;
@@ -455,9 +457,51 @@ static void tile_geometry(const mpcd_handle *h, int target, int *ct, int *cap) {
     *cap = (int)(1.5 * (double)c * ppc) + 128;
 }
 
+// Staging capacity of a warp's 32-cell group: mean + ~4 sigma + margin.
+static int group_capacity(const mpcd_handle *h) {
+    double vol = 1.0;
+    for (int d = 0; d < h->dc.dim; d++) vol *= h->dc.L[d];
+    double mean = 32.0 * (h->n > 0 ? (double)h->n / vol : 10.0);
+    int capw = (int)(mean + 4.0 * std::sqrt(mean) + 32.0);
+    capw = (capw + 31) / 32 * 32;
+    return capw < 64 ? 64 : (capw > 2048 ? 2048 : capw);
+}
+
+template <int DIM, class T>
+static int launch_group(mpcd_handle *h, int mode, const typename T::State &a,
+                        const typename T::State &b, const TileBufs &tb, const StepArgs &sa) {
+    int capw = group_capacity(h);
+    int bytes = GroupLayout<T>::kWarps * GroupLayout<T>::per_warp_bytes(capw);
+    int groups = (h->dc.ncells + 31) / 32;
+    int grid = (groups + GroupLayout<T>::kWarps - 1) / GroupLayout<T>::kWarps;
+    const DevCfg &c = h->dc;
+    cudaError_t e = cudaSuccess;
+#define MPCD_LAUNCH_GROUP(MODEV)                                                         \
+    do {                                                                                 \
+        auto kfn = k_group<DIM, T, MODEV>;                                               \
+        e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); \
+        if (e == cudaSuccess)                                                            \
+            e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, \
+                                     100);                                               \
+        if (e == cudaSuccess)                                                            \
+            kfn<<<grid, 32 * GroupLayout<T>::kWarps, bytes, h->stream>>>(c, a, b, tb, sa, capw); \
+    } while (0)
+    if (mode == MODE_INPLACE)
+        MPCD_LAUNCH_GROUP(MODE_INPLACE);
+    else if (mode == MODE_COUNT)
+        MPCD_LAUNCH_GROUP(MODE_COUNT);
+    else
+        MPCD_LAUNCH_GROUP(MODE_FINAL);
+#undef MPCD_LAUNCH_GROUP
+    if (e != cudaSuccess) return MPCD_ERR_CUDA;
+    return MPCD_OK;
+}
+
 template <int DIM, class T>
 static int launch_tile(mpcd_handle *h, int mode, const typename T::State &a,
                        const typename T::State &b, const TileBufs &tb, const StepArgs &sa) {
+    if (h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom && h->kernel != MPCD_KERNEL_TILE)
+        return launch_group<DIM, T>(h, mode, a, b, tb, sa);
     int ct, capp;
     tile_geometry(h, h->tile_target, &ct, &capp);
     TileLayout lay = tile_layout<T>(ct, capp, h->dc.op, h->dc.n_species);
@@ -473,6 +517,9 @@ static int launch_tile(mpcd_handle *h, int mode, const typename T::State &a,
         auto kfn = k_tile<DIM, T, MODEV>;                                                \
         e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
                                  lay.bytes);                                             \
+        if (e == cudaSuccess)                                                            \
+            e = cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, \
+                                     100);                                               \
         if (e == cudaSuccess) kfn<<<grid, 256, lay.bytes, h->stream>>>(c, a, b, tb, sa, lay); \
     } while (0)
     if (mode == MODE_INPLACE)
@@ -610,6 +657,12 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
         h->last_step = step;
         h->steps++;
     }
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_set_kernel(mpcd_handle *h, int kernel) {
+    if (!h || (kernel != MPCD_KERNEL_AUTO && kernel != MPCD_KERNEL_TILE)) return MPCD_ERR_ARG;
+    h->kernel = kernel;
     return MPCD_OK;
 }
 

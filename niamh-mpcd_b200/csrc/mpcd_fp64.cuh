@@ -65,14 +65,13 @@ __global__ void __launch_bounds__(256) k_scan_partial(const int *count, int ncel
 __global__ void __launch_bounds__(256) k_scan_apply(int *count, int ncells,
                                                     const int *part, int *start,
                                                     int *fill, double *acc) {
-    __shared__ int s_off;
-    if (threadIdx.x == 0) {
-        int off = 0;
-        for (int b = 0; b < (int)blockIdx.x; b++) off += part[b];
-        s_off = off;
-    }
+    // offset of this block: sum of the partial sums of the blocks before it,
+    // loaded and reduced by all threads
+    int mine = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += 256) mine += part[b];
+    int s_off;
+    block_excl_scan256(mine, s_off);
     if (acc && blockIdx.x == 0 && threadIdx.x < ACC_WORDS) acc[threadIdx.x] = 0.0;
-    __syncthreads();
     int base = blockIdx.x * kScanTile + threadIdx.x * 8;
     int v[8], sum = 0;
 #pragma unroll

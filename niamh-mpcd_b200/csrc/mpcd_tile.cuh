@@ -393,8 +393,8 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             const int lc = cl - cl_a;
             const int j0 = s_start[cl] - p0, j1 = s_start[cl + 1] - p0, pop = j1 - j0;
             const int cell = c0 + cl;
-            int cc[3];
-            cell_coords(c, cell, cc[0], cc[1], cc[2]);
+            int cc[3] = {0, 0, 0};
+            if (c.any_phantom || rat) cell_coords(c, cell, cc[0], cc[1], cc[2]);
             double M = 0.0, pv[3] = {0, 0, 0}, pq[3] = {0, 0, 0};
             for (int j = j0; j < j1; j++) {
                 double m = c.mass[s_sp ? s_sp[j] : 0];

@@ -28,6 +28,9 @@ LC_LOCAL = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
 
+KERNEL_AUTO = 0
+KERNEL_TILE = 1
+
 STRATEGY_SCATTER = 0
 STRATEGY_RECOMPUTE = 1
 

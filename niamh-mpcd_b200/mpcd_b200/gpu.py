@@ -18,7 +18,7 @@ EXPORTS = [
     "mpcd_upload_particles_strided", "mpcd_download_state",
     "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
-    "mpcd_launches_per_step", "mpcd_set_strategy",
+    "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
 ]
 
 _lib = None
@@ -52,6 +52,7 @@ def load():
         lib.mpcd_set_stream.argtypes = [vp, vp]
         lib.mpcd_launches_per_step.argtypes = [vp]
         lib.mpcd_set_strategy.argtypes = [vp, C.c_int, C.c_int]
+        lib.mpcd_set_kernel.argtypes = [vp, C.c_int]
         _lib = lib
     return _lib
 
@@ -119,6 +120,9 @@ class Solver:
     def set_strategy(self, strategy=-1, tile_particles=0):
         _check(self.lib.mpcd_set_strategy(self.h, strategy, tile_particles),
                "mpcd_set_strategy")
+
+    def set_kernel(self, kernel):
+        _check(self.lib.mpcd_set_kernel(self.h, kernel), "mpcd_set_kernel")
 
     def set_stream(self, stream_ptr):
         _check(self.lib.mpcd_set_stream(self.h, C.c_void_p(stream_ptr)), "mpcd_set_stream")

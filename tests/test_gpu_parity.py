@@ -83,14 +83,16 @@ def test_srd_conserves_momentum_and_energy(prec):
 
 
 @pytest.mark.parametrize("strategy", [abi.STRATEGY_SCATTER, abi.STRATEGY_RECOMPUTE])
-@pytest.mark.parametrize("name", ["srd3d", "rat2d", "channel3d", "mpcat3d_damp"])
+@pytest.mark.parametrize("name", ["srd3d", "srd2d", "rat2d", "channel3d", "mpcat3d_damp"])
 @pytest.mark.parametrize("tile", [0, 64, 4096])
-def test_strategies_and_tiles_agree_with_oracle(name, strategy, tile):
+@pytest.mark.parametrize("kernel", [abi.KERNEL_AUTO, abi.KERNEL_TILE])
+def test_strategies_and_tiles_agree_with_oracle(name, strategy, tile, kernel):
     cfg, ppc, sseed, _ = build(name)
     Q, V, U, sp = state(cfg, ppc, sseed)
     o = Oracle(cfg, Q, V, U, sp)
     g = Solver(cfg)
     g.set_strategy(strategy, tile)
+    g.set_kernel(kernel)
     g.upload(Q, V, U, sp)
     for s in range(1, 4):
         o.step(s)
@@ -122,17 +124,20 @@ def _clumped_state(cfg, ppc, seed, clumps, per_clump):
     return Qx, Vx, Ux, spx
 
 
+@pytest.mark.parametrize("kernel", [abi.KERNEL_AUTO, abi.KERNEL_TILE])
 @pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
-def test_dense_tiles_are_subdivided(prec):
+def test_dense_tiles_are_subdivided(prec, kernel):
     # 40 dense cells of 200 particles: tiles far above capacity are split
     # into sub-tiles; every particle must still match the oracle.
     from mpcd_b200 import workloads as W
     cfg = W.cfg_srd3d((10, 10, 10), precision=abi.PREC_FP64, seed=31)
     cfgp = W.cfg_srd3d((10, 10, 10), precision=prec, seed=31)
     clumps = [(i % 10, (i // 10) % 10, 3 + (i % 4)) for i in range(40)]
+    clumps += [(0, 0, z) for z in range(8)]  # one 32-cell group far above capacity
     Q, V, U, sp = _clumped_state(cfg, 10, 8, clumps, 200)
     o = Oracle(cfg, Q, V, U, sp)
     g = Solver(cfgp)
+    g.set_kernel(kernel)
     g.upload(Q, V, U, sp)
     o.step(1)
     g.step(1, 1)
@@ -147,8 +152,9 @@ def test_dense_tiles_are_subdivided(prec):
 def test_overfull_cell_is_reported_not_collided():
     # one cell holding more particles than a tile can stage: its particles
     # stream without collision and are counted in status.overflow
+    # (no grid shift, so the clump stays in one cell)
     from mpcd_b200 import workloads as W
-    cfg = W.cfg_srd3d((6, 6, 6), seed=32)
+    cfg = W.cfg_srd3d((6, 6, 6), seed=32, galinv=0)
     Q, V, U, sp = _clumped_state(cfg, 10, 9, [(2, 2, 2)], 5000)
     g = Solver(cfg)
     g.upload(Q, V, U, sp)
