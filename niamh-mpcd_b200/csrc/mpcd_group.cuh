@@ -18,31 +18,41 @@
 
 #include "mpcd_tile.cuh"
 
+#ifndef MPCD_GROUP_BATCH
+#define MPCD_GROUP_BATCH 2  // particles per lane in flight
+#endif
+#ifndef MPCD_GROUP_MINB
+#define MPCD_GROUP_MINB 1  // minimum resident blocks per SM (register cap)
+#endif
+
 namespace mpcd {
 
 template <class T>
 struct GroupVel;
+// mixed: the whole 32-byte record is staged, so the per-particle phase
+// reads only shared memory
 template <int DIM>
 struct GroupVel<MixT<DIM>> {
-    using S = float4;  // vx, vy, vz, pid
+    using S = MixRec;
     static __device__ __forceinline__ S load(const DevCfg &c, const MixState &st, int i) {
-        float4 w = st.W[i];
+        MixRec r;
+        r.P = st.P[i];
+        r.W = st.W[i];
         if (c.grav_flag) {
-            w.x += (float)(c.dt * c.grav[0]);
-            w.y += (float)(c.dt * c.grav[1]);
-            if (DIM == 3) w.z += (float)(c.dt * c.grav[2]);
+            r.W.x += (float)(c.dt * c.grav[0]);
+            r.W.y += (float)(c.dt * c.grav[1]);
+            if (DIM == 3) r.W.z += (float)(c.dt * c.grav[2]);
         }
-        return w;
+        return r;
     }
     static __device__ __forceinline__ void vel(const S &s, double v[3]) {
-        v[0] = s.x;
-        v[1] = s.y;
-        v[2] = DIM == 3 ? (double)s.z : 0.0;
+        v[0] = s.W.x;
+        v[1] = s.W.y;
+        v[2] = DIM == 3 ? (double)s.W.z : 0.0;
     }
     static __device__ __forceinline__ void compose(const DevCfg &c, const MixState &st, int i,
                                                    const StepArgs &sa, const S &s, MixRec &r) {
-        r.P = st.P[i];
-        r.W = s;
+        r = s;
     }
 };
 template <int DIM>
@@ -91,7 +101,7 @@ struct GroupLayout {
 };
 
 template <int DIM, class T, int MODE>
-__global__ void __launch_bounds__(128) k_group(const __grid_constant__ DevCfg c,
+__global__ void __launch_bounds__(128, MPCD_GROUP_MINB) k_group(const __grid_constant__ DevCfg c,
                                                typename T::State a, typename T::State b,
                                                TileBufs tb, StepArgs sa, int capw) {
     using GV = GroupVel<T>;
@@ -176,8 +186,10 @@ __global__ void __launch_bounds__(128) k_group(const __grid_constant__ DevCfg c,
                     sCell[j] = (unsigned char)lane;
                 }
                 double u[3] = {0, 0, 0};
-                if (M > 0.0)
-                    for (int d = 0; d < DIM; d++) u[d] = pv[d] / M;
+                if (M > 0.0) {
+                    const double iM = 1.0 / M;
+                    for (int d = 0; d < DIM; d++) u[d] = pv[d] * iM;
+                }
                 for (int d = 0; d < DIM; d++) av[d] += u[d];
                 VT *ur = &sUR[12 * lane];
                 for (int d = 0; d < 3; d++) ur[d] = (VT)u[d];
@@ -189,60 +201,93 @@ __global__ void __launch_bounds__(128) k_group(const __grid_constant__ DevCfg c,
                 }
             }
             __syncwarp();
-            // ---- lane = particle ----
-            for (int j = lane; j < np; j += 32) {
-                const int gi = base + j;
-                const int lc = sCell[j];
-                const VT *ur = &sUR[12 * lc];
-                const int sp = T::sp(a, gi);
-                Rec r;
-                GV::compose(c, a, gi, sa, sV[j], r);
-                if (sPop[lc] > 1) {
-                    if constexpr (sizeof(VT) == 4) {
-                        const MixRec &m = *(const MixRec *)&r;
-                        float w0 = m.W.x - ur[0], w1 = m.W.y - ur[1];
-                        float w2 = DIM == 3 ? m.W.z - ur[2] : 0.f;
-                        float nv[3];
-                        const float *R = ur + 3;
-                        if (DIM == 3) {
-                            nv[0] = ur[0] + (R[0] * w0 + R[1] * w1 + R[2] * w2);
-                            nv[1] = ur[1] + (R[3] * w0 + R[4] * w1 + R[5] * w2);
-                            nv[2] = ur[2] + (R[6] * w0 + R[7] * w1 + R[8] * w2);
+            // ---- lane = particle, kBatch particles per lane in flight ----
+            constexpr int kBatch = MPCD_GROUP_BATCH;
+            for (int j0 = lane; j0 < np; j0 += 32 * kBatch) {
+                Rec r[kBatch];
+                int k[kBatch], spv[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; u++) {
+                    const int j = j0 + 32 * u;
+                    k[u] = -1;
+                    if (j >= np) continue;
+                    const int gi = base + j;
+                    const int lc = sCell[j];
+                    const VT *ur = &sUR[12 * lc];
+                    const int sp = T::sp(a, gi);
+                    spv[u] = sp;
+                    GV::compose(c, a, gi, sa, sV[j], r[u]);
+                    if (sPop[lc] > 1) {
+                        if constexpr (sizeof(VT) == 4) {
+                            MixRec &m = *(MixRec *)&r[u];
+                            float w0 = m.W.x - ur[0], w1 = m.W.y - ur[1];
+                            float w2 = DIM == 3 ? m.W.z - ur[2] : 0.f;
+                            const float *R = ur + 3;
+                            if (DIM == 3) {
+                                m.W.x = ur[0] + (R[0] * w0 + R[1] * w1 + R[2] * w2);
+                                m.W.y = ur[1] + (R[3] * w0 + R[4] * w1 + R[5] * w2);
+                                m.W.z = ur[2] + (R[6] * w0 + R[7] * w1 + R[8] * w2);
+                            } else {
+                                m.W.x = ur[0] + (R[0] * w0 + R[1] * w1);
+                                m.W.y = ur[1] + (R[3] * w0 + R[4] * w1);
+                            }
                         } else {
-                            nv[0] = ur[0] + (R[0] * w0 + R[1] * w1);
-                            nv[1] = ur[1] + (R[3] * w0 + R[4] * w1);
-                            nv[2] = 0.f;
+                            double v[3], w[3] = {0, 0, 0}, t[3] = {0, 0, 0}, nv[3];
+                            T::vel(r[u], v);
+                            for (int d = 0; d < DIM; d++) w[d] = v[d] - (double)ur[d];
+                            for (int x = 0; x < DIM; x++)
+                                for (int y = 0; y < DIM; y++)
+                                    t[x] += (double)ur[3 + x * 3 + y] * w[y];
+                            for (int d = 0; d < DIM; d++) nv[d] = (double)ur[d] + t[d];
+                            T::set_vel(r[u], nv);
                         }
-                        MixT<DIM>::set_velf(*(MixRec *)&r, nv);
-                    } else {
-                        double v[3], w[3] = {0, 0, 0}, t[3] = {0, 0, 0}, nv[3];
-                        T::vel(r, v);
-                        for (int d = 0; d < DIM; d++) w[d] = v[d] - (double)ur[d];
-                        for (int x = 0; x < DIM; x++)
-                            for (int y = 0; y < DIM; y++) t[x] += (double)ur[3 + x * 3 + y] * w[y];
-                        for (int d = 0; d < DIM; d++) nv[d] = (double)ur[d] + t[d];
-                        T::set_vel(r, nv);
                     }
+                    if (MODE != MODE_COUNT) {
+                        if constexpr (sizeof(VT) == 4) {
+                            const MixRec &m = *(const MixRec *)&r[u];
+                            float t = m.W.x * m.W.x + m.W.y * m.W.y;
+                            if (DIM == 3) t += m.W.z * m.W.z;
+                            ke += c.mass[sp] * (double)t;
+                        } else {
+                            double v[3];
+                            T::vel(r[u], v);
+                            double t = v[0] * v[0];
+                            t += v[1] * v[1];
+                            t += v[2] * v[2];
+                            ke += c.mass[sp] * t;
+                        }
+                    }
+                    k[u] = T::finish(c, r[u], sp, sa, bounce, esc);
                 }
-                if (MODE != MODE_COUNT) {
-                    double v[3];
-                    T::vel(r, v);
-                    double t = v[0] * v[0];
-                    t += v[1] * v[1];
-                    t += v[2] * v[2];
-                    ke += c.mass[sp] * t;
-                }
-                int k = T::finish(c, r, sp, sa, bounce, esc);
-                if (MODE == MODE_INPLACE) {
-                    T::store(a, gi, r);
-                    tb.key[gi] = k;
-                    tb.rank[gi] = atomicAdd(&tb.count_next[k], 1);
-                } else if (MODE == MODE_COUNT) {
-                    atomicAdd(&tb.count_next[k], 1);
+                if (MODE == MODE_COUNT) {
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++)
+                        if (k[u] >= 0) atomicAdd(&tb.count_next[k[u]], 1);
+                } else if (MODE == MODE_INPLACE) {
+                    int rk[kBatch];
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++)
+                        if (k[u] >= 0) rk[u] = atomicAdd(&tb.count_next[k[u]], 1);
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++)
+                        if (k[u] >= 0) {
+                            const int gi = base + j0 + 32 * u;
+                            T::store(a, gi, r[u]);
+                            tb.key[gi] = k[u];
+                            tb.rank[gi] = rk[u];
+                        }
                 } else {
-                    int dst = tb.start_next[k] + atomicAdd(&tb.fill[k], 1);
-                    T::store(b, dst, r);
-                    T::store_sp(b, dst, sp);
+                    int slot[kBatch];
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++)
+                        if (k[u] >= 0) slot[u] = atomicAdd(&tb.fill[k[u]], 1);
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++)
+                        if (k[u] >= 0) {
+                            const int dst = tb.start_next[k[u]] + slot[u];
+                            T::store(b, dst, r[u]);
+                            T::store_sp(b, dst, spv[u]);
+                        }
                 }
             }
             __syncwarp();

@@ -57,13 +57,49 @@ static inline int mix_alloc(MixState &s, size_t n, const DevCfg &c) {
     return MPCD_OK;
 }
 
-// Shifted-grid coordinate of one axis, exactly as gridShift_all + bin.
-__device__ __forceinline__ int mix_shift_axis(int cidx, float o, double s, int L, int pbc,
-                                              double &qs, int &esc) {
-    double q = (double)cidx + (double)o;
-    q = shift_fwd(q, s, L);
-    qs = q;
-    return bin_axis(q, L, pbc, 1, esc);
+// Shifted-grid cell index of one axis from (cell ci, offset o) and the grid
+// shift s, following gridShift_all + bin (mpc.c:728-736, 958-968): with
+// Q = ci + o and Q' = Q + s, Q' is wrapped by -L when L < Q' <= L + s, the
+// cell is trunc(Q'), and index L maps to 0 on periodic axes.  Only t = o + s
+// is formed in FP64 (exact in every case that can change the outcome); 'rel'
+// returns Q' relative to the origin of the returned cell.
+__device__ __forceinline__ int mix_shift_axis(int ci, float o, double s, int L, int pbc,
+                                              double &rel, int &esc) {
+    const double t = (double)o + s;
+    int a;
+    if (ci <= L - 2) {
+        const bool cy = t >= 1.0;
+        a = ci + (cy ? 1 : 0);
+        rel = cy ? t - 1.0 : t;
+    } else if (ci == L - 1) {
+        if (t > 1.0) {  // Q' > L: wrapped into cell 0
+            a = 0;
+            rel = t - 1.0;
+        } else if (t == 1.0) {  // Q' == L exactly: not wrapped
+            a = L;
+            rel = 0.0;
+        } else {
+            a = L - 1;
+            rel = t;
+        }
+    } else {  // ci == L: possible on non-periodic axes only
+        if (o == 0.0f && s > 0.0) {
+            a = 0;
+            rel = t;
+        } else if (t >= 1.0) {
+            a = L + 1;
+            rel = t - 1.0;
+        } else {
+            a = L;
+            rel = t;
+        }
+    }
+    if (pbc && a == L) a = 0;
+    if (a < 0 || a > L) {
+        esc = 1;
+        a = a < 0 ? 0 : L;
+    }
+    return a;
 }
 
 __global__ void __launch_bounds__(256) k_scatter_mix(MixState a, MixState b, int n,
@@ -85,16 +121,10 @@ __device__ __forceinline__ void mix_rel(const DevCfg &c, const float4 &p, const 
     int ca, cb, cz;
     unpack_cell(__float_as_int(p.w), ca, cb, cz);
     int e = 0;
-    double qs;
-    mix_shift_axis(ca, p.x, s[0], c.L[0], c.pbc[0], qs, e);
-    r[0] = qs - (double)cellc[0];
-    mix_shift_axis(cb, p.y, s[1], c.L[1], c.pbc[1], qs, e);
-    r[1] = qs - (double)cellc[1];
+    mix_shift_axis(ca, p.x, s[0], c.L[0], c.pbc[0], r[0], e);
+    mix_shift_axis(cb, p.y, s[1], c.L[1], c.pbc[1], r[1], e);
     r[2] = 0.0;
-    if (DIM == 3) {
-        mix_shift_axis(cz, p.z, s[2], c.L[2], c.pbc[2], qs, e);
-        r[2] = qs - (double)cellc[2];
-    }
+    if (DIM == 3) mix_shift_axis(cz, p.z, s[2], c.L[2], c.pbc[2], r[2], e);
 }
 
 // Stream an offset by dt*v in FP32 and carry whole cells into the index.

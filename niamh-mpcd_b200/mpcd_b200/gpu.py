@@ -10,8 +10,9 @@ import numpy as np
 
 from . import abi
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
-                        "libmpcd_gpu.so")
+LIB_PATH = os.environ.get(
+    "MPCD_GPU_LIB",
+    os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "libmpcd_gpu.so"))
 
 EXPORTS = [
     "mpcd_abi_version", "mpcd_create", "mpcd_destroy", "mpcd_upload_state",
