@@ -592,6 +592,10 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
     sa.step = step;
     host_shift(h, step, sa.s);
     host_shift(h, step + 1u, sa.sn);
+    for (int d = 0; d < 3; d++) {  // s = k * 2^-32 exactly
+        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0);
+        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0);
+    }
     double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
     double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
     int launches = 0;

@@ -1,15 +1,19 @@
 // mpcd_mixed.cuh -- the mixed-precision form of the solvent timestep.
 //
-// Particle state, 32 bytes per particle in two float4 records:
-//   P = {ox, oy, oz, cell}   position = integer cell (10 bits per axis,
-//                            packed) + FP32 offset in [0,1) within it
-//   W = {vx, vy, vz, pid}    FP32 velocity + original particle index
-// Positions never lose precision with box size, and the periodic wrap is an
-// exact integer wrap (the reference shifts by L(1-2e-8) instead, bc.c:769).
-// Shifted coordinates are formed exactly in FP64 (int + float + 32-bit
-// shift fit in 53 bits), so cell keys follow the reference's gridShift/bin
-// rules (mpc.c:728-736, 958-968) exactly.  Cell sums, the MPC-AT+a inertia
-// tensor and its inverse are FP64; the SRD rotation and streaming are FP32.
+// Particle state, 32 bytes per particle in two 16-byte records:
+//   P = {fx, fy, fz, cell} (uint4)  position = integer cell (10 bits per
+//                          axis, packed) + 32-bit fixed-point offset within
+//                          the cell (value f * 2^-32 in [0,1))
+//   W = {vx, vy, vz, pid} (float4)  FP32 velocity + original particle index
+// The sub-cell offset has a uniform resolution of 2^-32 cell whatever the box
+// size, and the grid shift (a 32-bit uniform, s = k * 2^-32 exactly, as the
+// reference's genrand_real, rand.c:365-368) adds to it exactly in integer
+// arithmetic, so shifting, wrapping and binning follow the reference's
+// gridShift_all/bin rules (mpc.c:728-736, 958-968) without rounding.  The
+// periodic wrap is an exact integer wrap (the reference shifts by L(1-2e-8)
+// instead, bc.c:769).  Streaming adds the FP32 displacement dt*v converted
+// to fixed point.  Cell sums, the MPC-AT+a inertia tensor and its inverse
+// are FP64; the SRD rotation and streaming are FP32.
 #pragma once
 
 #include "mpcd_device.cuh"
@@ -18,13 +22,15 @@
 namespace mpcd {
 
 struct MixState {
-    float4 *P;
+    uint4 *P;
     float4 *W;
     int *sp;  // species (nullptr for one species)
 };
 
 constexpr int kCellBits = 10;
 constexpr int kCellMask = (1 << kCellBits) - 1;
+constexpr double kFx = 4294967296.0;               // 2^32
+constexpr double kFxInv = 2.3283064365386963e-10;  // 2^-32
 
 __host__ __device__ __forceinline__ int pack_cell(int a, int b, int z) {
     return a | (b << kCellBits) | (z << (2 * kCellBits));
@@ -45,54 +51,44 @@ static inline void mix_free(MixState &s) {
     cudaFree(s.P);
     cudaFree(s.W);
     cudaFree(s.sp);
-    s.P = s.W = nullptr;
+    s.P = nullptr;
+    s.W = nullptr;
     s.sp = nullptr;
 }
 
 static inline int mix_alloc(MixState &s, size_t n, const DevCfg &c) {
-    if (cudaMalloc((void **)&s.P, n * sizeof(float4)) != cudaSuccess) return MPCD_ERR_NOMEM;
+    if (cudaMalloc((void **)&s.P, n * sizeof(uint4)) != cudaSuccess) return MPCD_ERR_NOMEM;
     if (cudaMalloc((void **)&s.W, n * sizeof(float4)) != cudaSuccess) return MPCD_ERR_NOMEM;
     if (c.n_species > 1 && cudaMalloc((void **)&s.sp, n * sizeof(int)) != cudaSuccess)
         return MPCD_ERR_NOMEM;
     return MPCD_OK;
 }
 
-// Shifted-grid cell index of one axis from (cell ci, offset o) and the grid
-// shift s, following gridShift_all + bin (mpc.c:728-736, 958-968): with
-// Q = ci + o and Q' = Q + s, Q' is wrapped by -L when L < Q' <= L + s, the
-// cell is trunc(Q'), and index L maps to 0 on periodic axes.  Only t = o + s
-// is formed in FP64 (exact in every case that can change the outcome); 'rel'
-// returns Q' relative to the origin of the returned cell.
-__device__ __forceinline__ int mix_shift_axis(int ci, float o, double s, int L, int pbc,
-                                              double &rel, int &esc) {
-    const double t = (double)o + s;
+// Shifted-grid cell index of one axis for the position ci + f*2^-32 and the
+// shift k*2^-32, following gridShift_all + bin: with Q' = Q + s, Q' is
+// wrapped by -L when L < Q' <= L + s, the cell is trunc(Q'), and index L maps
+// to 0 on periodic axes.  'rel' returns the fixed-point position of Q'
+// within the returned cell.
+__device__ __forceinline__ int fx_shift_axis(int ci, uint32_t f, uint32_t k, int L, int pbc,
+                                             uint32_t &rel, int &esc) {
+    const uint32_t t = f + k;  // fraction of f + k
+    const bool cy = t < f;     // f + k >= 2^32, i.e. o + s >= 1
     int a;
+    rel = t;
     if (ci <= L - 2) {
-        const bool cy = t >= 1.0;
         a = ci + (cy ? 1 : 0);
-        rel = cy ? t - 1.0 : t;
     } else if (ci == L - 1) {
-        if (t > 1.0) {  // Q' > L: wrapped into cell 0
-            a = 0;
-            rel = t - 1.0;
-        } else if (t == 1.0) {  // Q' == L exactly: not wrapped
-            a = L;
-            rel = 0.0;
-        } else {
+        if (cy && t != 0u)
+            a = 0;  // Q' > L: wrapped into cell 0
+        else if (cy)
+            a = L;  // Q' == L exactly: not wrapped
+        else
             a = L - 1;
-            rel = t;
-        }
     } else {  // ci == L: possible on non-periodic axes only
-        if (o == 0.0f && s > 0.0) {
-            a = 0;
-            rel = t;
-        } else if (t >= 1.0) {
-            a = L + 1;
-            rel = t - 1.0;
-        } else {
-            a = L;
-            rel = t;
-        }
+        if (f == 0u && k != 0u)
+            a = 0;  // L < Q' <= L + s: wrapped
+        else
+            a = L + (cy ? 1 : 0);
     }
     if (pbc && a == L) a = 0;
     if (a < 0 || a > L) {
@@ -100,6 +96,46 @@ __device__ __forceinline__ int mix_shift_axis(int ci, float o, double s, int L, 
         a = a < 0 ? 0 : L;
     }
     return a;
+}
+
+// Position of record p on the shifted grid relative to the origin of its
+// shifted cell, in cell units (exact in FP64).
+template <int DIM>
+__device__ __forceinline__ void mix_rel(const DevCfg &c, const uint4 &p, const uint32_t *k,
+                                        double *r) {
+    int ca, cb, cz, e = 0;
+    uint32_t t;
+    unpack_cell((int)p.w, ca, cb, cz);
+    fx_shift_axis(ca, p.x, k[0], c.L[0], c.pbc[0], t, e);
+    r[0] = (double)t * kFxInv;
+    fx_shift_axis(cb, p.y, k[1], c.L[1], c.pbc[1], t, e);
+    r[1] = (double)t * kFxInv;
+    r[2] = 0.0;
+    if (DIM == 3) {
+        fx_shift_axis(cz, p.z, k[2], c.L[2], c.pbc[2], t, e);
+        r[2] = (double)t * kFxInv;
+    }
+}
+
+// Stream one axis by the FP32 displacement dx: exact fixed-point add.
+__device__ __forceinline__ void fx_stream(uint32_t &f, int &ci, float dx) {
+    const long long disp = __float2ll_rn(dx * 4294967296.0f);
+    const long long nq = (long long)f + disp;
+    ci += (int)(nq >> 32);
+    f = (uint32_t)nq;
+}
+
+// Fixed-point representation of a coordinate (host and device).
+__host__ __device__ __forceinline__ void fx_from_double(double q, int &ci, uint32_t &f) {
+    double fl = floor(q);
+    double fr = (q - fl) * kFx;
+    long long r = (long long)(fr + 0.5);
+    ci = (int)fl;
+    if (r >= (1LL << 32)) {
+        ci += 1;
+        r = 0;
+    }
+    f = (uint32_t)r;
 }
 
 __global__ void __launch_bounds__(256) k_scatter_mix(MixState a, MixState b, int n,
@@ -113,69 +149,36 @@ __global__ void __launch_bounds__(256) k_scatter_mix(MixState a, MixState b, int
     }
 }
 
-// Position of particle record p on the shifted grid relative to the origin
-// of its shifted cell (exact in FP64).
-template <int DIM>
-__device__ __forceinline__ void mix_rel(const DevCfg &c, const float4 &p, const double *s,
-                                        const int *cellc, double *r) {
-    int ca, cb, cz;
-    unpack_cell(__float_as_int(p.w), ca, cb, cz);
-    int e = 0;
-    mix_shift_axis(ca, p.x, s[0], c.L[0], c.pbc[0], r[0], e);
-    mix_shift_axis(cb, p.y, s[1], c.L[1], c.pbc[1], r[1], e);
-    r[2] = 0.0;
-    if (DIM == 3) mix_shift_axis(cz, p.z, s[2], c.L[2], c.pbc[2], r[2], e);
-}
-
-// Stream an offset by dt*v in FP32 and carry whole cells into the index.
-__device__ __forceinline__ void carry(float &o, int &ci) {
-    float f = floorf(o);
-    if (f != 0.0f) {
-        o -= f;
-        ci += (int)f;
-        if (o >= 1.0f) {  // rounding at the top edge
-            o = 0.0f;
-            ci += 1;
-        }
-    }
-}
-
 // Host-side conversion to and from the packed representation.
 static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *Q,
                              const double *V, const int *spid, cudaStream_t stream) {
-    std::vector<float4> P((size_t)n), W((size_t)n);
+    std::vector<uint4> P((size_t)n);
+    std::vector<float4> W((size_t)n);
     for (int i = 0; i < n; i++) {
         int ci[3] = {0, 0, 0};
-        float o[3] = {0.f, 0.f, 0.f};
+        uint32_t f[3] = {0u, 0u, 0u};
         for (int d = 0; d < c.dim; d++) {
-            double q = Q[3 * (size_t)i + d];
-            double f = std::floor(q);
-            ci[d] = (int)f;
-            o[d] = (float)(q - f);
-            if (o[d] >= 1.0f) {
-                o[d] = 0.0f;
-                ci[d] += 1;
-            }
+            fx_from_double(Q[3 * (size_t)i + d], ci[d], f[d]);
             if (ci[d] < 0 || ci[d] > c.L[d]) return MPCD_ERR_ARG;
         }
-        P[i] = make_float4(o[0], o[1], o[2], __int_as_float_host(pack_cell(ci[0], ci[1], ci[2])));
+        P[i] = make_uint4(f[0], f[1], f[2], (unsigned)pack_cell(ci[0], ci[1], ci[2]));
         W[i] = make_float4((float)V[3 * (size_t)i], (float)V[3 * (size_t)i + 1],
                            c.dim == 3 ? (float)V[3 * (size_t)i + 2] : 0.f,
                            __int_as_float_host(i));
     }
-    if (cudaMemcpyAsync(s.P, P.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice,
+    if (cudaMemcpyAsync(s.P, P.data(), (size_t)n * sizeof(uint4), cudaMemcpyHostToDevice,
                         stream) != cudaSuccess)
         return MPCD_ERR_CUDA;
     if (cudaMemcpyAsync(s.W, W.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice,
                         stream) != cudaSuccess)
         return MPCD_ERR_CUDA;
+    std::vector<int> sp;
     if (s.sp) {
-        std::vector<int> sp((size_t)n);
+        sp.resize((size_t)n);
         for (int i = 0; i < n; i++) sp[i] = spid ? spid[i] : 0;
         if (cudaMemcpyAsync(s.sp, sp.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice,
                             stream) != cudaSuccess)
             return MPCD_ERR_CUDA;
-        if (cudaStreamSynchronize(stream) != cudaSuccess) return MPCD_ERR_CUDA;
     }
     if (cudaStreamSynchronize(stream) != cudaSuccess) return MPCD_ERR_CUDA;
     return MPCD_OK;
@@ -183,8 +186,9 @@ static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *
 
 static inline int mix_download(const MixState &s, const DevCfg &c, int n, double *Q,
                                double *V) {
-    std::vector<float4> P((size_t)n), W((size_t)n);
-    if (cudaMemcpy(P.data(), s.P, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost) !=
+    std::vector<uint4> P((size_t)n);
+    std::vector<float4> W((size_t)n);
+    if (cudaMemcpy(P.data(), s.P, (size_t)n * sizeof(uint4), cudaMemcpyDeviceToHost) !=
         cudaSuccess)
         return MPCD_ERR_CUDA;
     if (cudaMemcpy(W.data(), s.W, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost) !=
@@ -194,11 +198,11 @@ static inline int mix_download(const MixState &s, const DevCfg &c, int n, double
         int pid = __float_as_int_host(W[i].w);
         if (pid < 0 || pid >= n) return MPCD_ERR_STATE;
         int ci[3];
-        unpack_cell(__float_as_int_host(P[i].w), ci[0], ci[1], ci[2]);
-        float o[3] = {P[i].x, P[i].y, P[i].z};
+        unpack_cell((int)P[i].w, ci[0], ci[1], ci[2]);
+        uint32_t f[3] = {P[i].x, P[i].y, P[i].z};
         float v[3] = {W[i].x, W[i].y, W[i].z};
         for (int d = 0; d < 3; d++) {
-            if (Q) Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)o[d] : 0.0;
+            if (Q) Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;
             if (V) V[3 * (size_t)pid + d] = d < c.dim ? (double)v[d] : 0.0;
         }
     }

@@ -34,8 +34,10 @@ enum { ST_OVERFLOW = 3 };  // status word: cells too large for a tile
 struct StepArgs {
     uint32_t step;
     int pad_;
-    double s[3];   // shift of this step
-    double sn[3];  // shift of the next step
+    double s[3];     // shift of this step
+    double sn[3];    // shift of the next step
+    uint32_t ks[3];  // the same shifts as 32-bit fractions (s = k * 2^-32)
+    uint32_t ksn[3];
 };
 
 struct TileBufs {
@@ -51,7 +53,8 @@ struct TileBufs {
 
 // ------------------------------------------------------- precision traits
 struct MixRec {
-    float4 P, W;
+    uint4 P;
+    float4 W;
 };
 struct F64Rec {
     double q[3];  // position on the shifted grid
@@ -90,11 +93,11 @@ struct MixT {
         v[1] = r.W.y;
         v[2] = DIM == 3 ? r.W.z : 0.f;
     }
-    // position relative to the origin of shifted cell cc
+    // position relative to the origin of its shifted cell
     static __device__ __forceinline__ void rel(const DevCfg &c, const Rec &r,
                                                const StepArgs &sa, const int *cc,
                                                double q[3]) {
-        mix_rel<DIM>(c, r.P, sa.s, cc, q);
+        mix_rel<DIM>(c, r.P, sa.ks, q);
     }
     static __device__ __forceinline__ void set_vel(Rec &r, const double v[3]) {
         r.W.x = (float)v[0];
@@ -106,24 +109,21 @@ struct MixT {
         r.W.y = v[1];
         if (DIM == 3) r.W.z = v[2];
     }
-    // stream (FP32), walls (FP64, solid only), exact periodic wrap; returns
-    // the particle's cell key on the next step's grid; 'bounce' set when the
-    // wall loop hit its limit.
+    // stream (fixed point), walls (FP64, solid only), exact periodic wrap;
+    // returns the particle's cell key on the next step's grid; 'bounce' set
+    // when the wall loop hit its limit.
     static __device__ __forceinline__ int finish(const DevCfg &c, Rec &r, int sp,
                                                  const StepArgs &sa, int &bounce, int &esc) {
         int ci[3];
-        unpack_cell(__float_as_int(r.P.w), ci[0], ci[1], ci[2]);
-        float o[3] = {r.P.x, r.P.y, r.P.z};
+        unpack_cell((int)r.P.w, ci[0], ci[1], ci[2]);
+        uint32_t f[3] = {r.P.x, r.P.y, r.P.z};
         float vv[3] = {r.W.x, r.W.y, r.W.z};
         const float dtf = (float)c.dt;
-        for (int d = 0; d < DIM; d++) {
-            o[d] = fmaf(dtf, vv[d], o[d]);
-            carry(o[d], ci[d]);
-        }
+        for (int d = 0; d < DIM; d++) fx_stream(f[d], ci[d], dtf * vv[d]);
         if (c.n_solid > 0) {
             double q[3] = {0, 0, 0}, v[3] = {0, 0, 0};
             for (int d = 0; d < DIM; d++) {
-                q[d] = (double)ci[d] + (double)o[d];
+                q[d] = (double)ci[d] + (double)f[d] * kFxInv;
                 v[d] = (double)vv[d];
             }
             bool inside = false;
@@ -134,13 +134,7 @@ struct MixT {
             if (inside) {
                 bounce += wall_collisions<DIM>(c, q, v, sp, true);
                 for (int d = 0; d < DIM; d++) {
-                    double f = floor(q[d]);
-                    ci[d] = (int)f;
-                    o[d] = (float)(q[d] - f);
-                    if (o[d] >= 1.0f) {
-                        o[d] = 0.0f;
-                        ci[d] += 1;
-                    }
+                    fx_from_double(q[d], ci[d], f[d]);
                     vv[d] = (float)v[d];
                 }
             }
@@ -149,23 +143,25 @@ struct MixT {
             if (c.pbc[d]) {
                 if (ci[d] < 0 || ci[d] >= c.L[d])
                     ci[d] = ((ci[d] % c.L[d]) + c.L[d]) % c.L[d];
-            } else {
-                if (ci[d] < 0) ci[d] = 0;
-                if (ci[d] > c.L[d]) ci[d] = c.L[d];
+            } else if (ci[d] < 0) {
+                ci[d] = 0;
+                f[d] = 0u;
+            } else if (ci[d] > c.L[d]) {
+                ci[d] = c.L[d];
             }
         }
-        r.P.x = o[0];
-        r.P.y = o[1];
-        r.P.z = DIM == 3 ? o[2] : 0.0f;
-        r.P.w = __int_as_float(pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0));
+        r.P.x = f[0];
+        r.P.y = f[1];
+        r.P.z = DIM == 3 ? f[2] : 0u;
+        r.P.w = (unsigned)pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
         r.W.x = vv[0];
         r.W.y = vv[1];
         if (DIM == 3) r.W.z = vv[2];
-        double qs;
-        int a = mix_shift_axis(ci[0], o[0], sa.sn[0], c.L[0], c.pbc[0], qs, esc);
-        int b = mix_shift_axis(ci[1], o[1], sa.sn[1], c.L[1], c.pbc[1], qs, esc);
+        uint32_t t;
+        int a = fx_shift_axis(ci[0], f[0], sa.ksn[0], c.L[0], c.pbc[0], t, esc);
+        int b = fx_shift_axis(ci[1], f[1], sa.ksn[1], c.L[1], c.pbc[1], t, esc);
         int z = 0;
-        if (DIM == 3) z = mix_shift_axis(ci[2], o[2], sa.sn[2], c.L[2], c.pbc[2], qs, esc);
+        if (DIM == 3) z = fx_shift_axis(ci[2], f[2], sa.ksn[2], c.L[2], c.pbc[2], t, esc);
         return cell_lin(c, a, b, z);
     }
     static __device__ __forceinline__ void store(const State &st, int i, const Rec &r) {
@@ -586,13 +582,13 @@ __global__ void __launch_bounds__(256) k_key_mix(const __grid_constant__ DevCfg 
                                                  StepArgs sa, unsigned long long *status) {
     int esc_local = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 p = a.P[i];
+        uint4 p = a.P[i];
         int ca, cb, cz, e = 0;
-        unpack_cell(__float_as_int(p.w), ca, cb, cz);
-        double qs;
-        int x = mix_shift_axis(ca, p.x, sa.s[0], c.L[0], c.pbc[0], qs, e);
-        int y = mix_shift_axis(cb, p.y, sa.s[1], c.L[1], c.pbc[1], qs, e);
-        int z = DIM == 3 ? mix_shift_axis(cz, p.z, sa.s[2], c.L[2], c.pbc[2], qs, e) : 0;
+        uint32_t t;
+        unpack_cell((int)p.w, ca, cb, cz);
+        int x = fx_shift_axis(ca, p.x, sa.ks[0], c.L[0], c.pbc[0], t, e);
+        int y = fx_shift_axis(cb, p.y, sa.ks[1], c.L[1], c.pbc[1], t, e);
+        int z = DIM == 3 ? fx_shift_axis(cz, p.z, sa.ks[2], c.L[2], c.pbc[2], t, e) : 0;
         esc_local += e;
         int k = cell_lin(c, x, y, z);
         key[i] = k;
