@@ -29,6 +29,10 @@ namespace mpcd {
 
 template <class T>
 struct GroupVel;
+#ifndef MPCD_GROUP_STAGE_FULL
+#define MPCD_GROUP_STAGE_FULL 1  // mixed: stage position and velocity records
+#endif
+#if MPCD_GROUP_STAGE_FULL
 // mixed: the whole 32-byte record is staged, so the per-particle phase
 // reads only shared memory
 template <int DIM>
@@ -55,6 +59,33 @@ struct GroupVel<MixT<DIM>> {
         r = s;
     }
 };
+#else
+// mixed: only the velocity record is staged; positions are read in the
+// per-particle phase
+template <int DIM>
+struct GroupVel<MixT<DIM>> {
+    using S = float4;
+    static __device__ __forceinline__ S load(const DevCfg &c, const MixState &st, int i) {
+        float4 w = st.W[i];
+        if (c.grav_flag) {
+            w.x += (float)(c.dt * c.grav[0]);
+            w.y += (float)(c.dt * c.grav[1]);
+            if (DIM == 3) w.z += (float)(c.dt * c.grav[2]);
+        }
+        return w;
+    }
+    static __device__ __forceinline__ void vel(const S &s, double v[3]) {
+        v[0] = s.x;
+        v[1] = s.y;
+        v[2] = DIM == 3 ? (double)s.z : 0.0;
+    }
+    static __device__ __forceinline__ void compose(const DevCfg &c, const MixState &st, int i,
+                                                   const StepArgs &sa, const S &s, MixRec &r) {
+        r.P = st.P[i];
+        r.W = s;
+    }
+};
+#endif
 template <int DIM>
 struct GroupVel<F64T<DIM>> {
     struct S {
