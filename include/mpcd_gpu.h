@@ -216,13 +216,20 @@ int mpcd_launches_per_step(mpcd_handle *h);
 #define MPCD_STRATEGY_RECOMPUTE 1
 int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
 
-/* Cell-kernel family (no counterpart in the reference):
- *   MPCD_KERNEL_AUTO  warp-per-32-cell-group kernel where the operator
- *                     allows it (SRD without phantom walls), block-per-tile
- *                     kernel otherwise;
- *   MPCD_KERNEL_TILE  always the block-per-tile kernel. */
+/* Cell-kernel family (no counterpart in the reference).  For the SRD
+ * operator without phantom walls:
+ *   MPCD_KERNEL_SPLIT  a thread-per-cell pass writes each cell's centre-of-
+ *                      mass velocity and rotation, then a thread-per-particle
+ *                      pass collides, streams and re-bins (the default);
+ *   MPCD_KERNEL_GROUP  one warp per group of 32 cells does both, staging the
+ *                      group in shared memory;
+ *   MPCD_KERNEL_TILE   one block per tile of cells (the kernel every other
+ *                      operator uses).
+ * MPCD_KERNEL_AUTO picks SPLIT where it applies and TILE elsewhere. */
 #define MPCD_KERNEL_AUTO 0
 #define MPCD_KERNEL_TILE 1
+#define MPCD_KERNEL_GROUP 2
+#define MPCD_KERNEL_SPLIT 3
 int mpcd_set_kernel(mpcd_handle *h, int kernel);
 
 #ifdef __cplusplus

@@ -17,6 +17,7 @@
 #include "mpcd_mixed.cuh"
 #include "mpcd_tile.cuh"
 #include "mpcd_group.cuh"
+#include "mpcd_split.cuh"
 
 using namespace mpcd;
 
@@ -42,6 +43,7 @@ struct mpcd_handle {
     int strategy;    // MPCD_STRATEGY_*
     int tile_target; // expected particles per tile
     int kernel;      // MPCD_KERNEL_*: cell kernel family
+    void *crec;      // per-cell SRD records (split kernel family)
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     uint32_t last_step;
     uint64_t steps;
@@ -188,6 +190,7 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->part);
     cudaFree(h->acc);
     cudaFree(h->status);
+    cudaFree(h->crec);
     if (h->host_acc) cudaFreeHost(h->host_acc);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -228,6 +231,7 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     ALLOC(h->part, sizeof(int) * h->nscan);
     ALLOC(h->acc, sizeof(double) * 2 * ACC_WORDS);
     ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
+    ALLOC(h->crec, (size_t)nc * 128);
     h->sorted_for = -1;
     h->strategy = -1;
     h->tile_target = 0;
@@ -497,11 +501,42 @@ static int launch_group(mpcd_handle *h, int mode, const typename T::State &a,
     return MPCD_OK;
 }
 
+static int kernel_family(const mpcd_handle *h) {
+    bool srd_plain = h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom;
+    if (!srd_plain) return MPCD_KERNEL_TILE;
+    return h->kernel == MPCD_KERNEL_AUTO ? MPCD_KERNEL_SPLIT : h->kernel;
+}
+
+template <int DIM, class T>
+static int launch_srd_cells(mpcd_handle *h, const typename T::State &a, const int *start,
+                            const StepArgs &sa, double *acc) {
+    int grid = (h->dc.ncells + 255) / 256;
+    k_srd_cells<DIM, T><<<grid, 256, 0, h->stream>>>(
+        h->dc, a, start, (typename SrdCell<T>::Rec *)h->crec, sa, acc);
+    return cudaGetLastError() == cudaSuccess ? MPCD_OK : MPCD_ERR_CUDA;
+}
+
+template <int DIM, class T>
+static int launch_srd_parts(mpcd_handle *h, int mode, const typename T::State &a,
+                            const typename T::State &b, const TileBufs &tb,
+                            const StepArgs &sa) {
+    int grid = (h->n + 255) / 256;
+    const typename SrdCell<T>::Rec *cr = (const typename SrdCell<T>::Rec *)h->crec;
+    if (mode == MODE_INPLACE)
+        k_srd_parts<DIM, T, MODE_INPLACE><<<grid, 256, 0, h->stream>>>(h->dc, a, b, h->n, cr, tb, sa);
+    else if (mode == MODE_COUNT)
+        k_srd_parts<DIM, T, MODE_COUNT><<<grid, 256, 0, h->stream>>>(h->dc, a, b, h->n, cr, tb, sa);
+    else
+        k_srd_parts<DIM, T, MODE_FINAL><<<grid, 256, 0, h->stream>>>(h->dc, a, b, h->n, cr, tb, sa);
+    return cudaGetLastError() == cudaSuccess ? MPCD_OK : MPCD_ERR_CUDA;
+}
+
 template <int DIM, class T>
 static int launch_tile(mpcd_handle *h, int mode, const typename T::State &a,
                        const typename T::State &b, const TileBufs &tb, const StepArgs &sa) {
-    if (h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom && h->kernel != MPCD_KERNEL_TILE)
-        return launch_group<DIM, T>(h, mode, a, b, tb, sa);
+    int fam = kernel_family(h);
+    if (fam == MPCD_KERNEL_SPLIT) return launch_srd_parts<DIM, T>(h, mode, a, b, tb, sa);
+    if (fam == MPCD_KERNEL_GROUP) return launch_group<DIM, T>(h, mode, a, b, tb, sa);
     int ct, capp;
     tile_geometry(h, h->tile_target, &ct, &capp);
     TileLayout lay = tile_layout<T>(ct, capp, h->dc.op, h->dc.n_species);
@@ -617,6 +652,11 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
     tb.acc = acc_cur;
     tb.status = h->status;
     int r;
+    if (kernel_family(h) == MPCD_KERNEL_SPLIT) {
+        r = launch_srd_cells<DIM, T>(h, st[h->cur], tb.start, sa, acc_cur);
+        if (r != MPCD_OK) return r;
+        launches += 1;
+    }
     if (h->strategy == MPCD_STRATEGY_SCATTER) {
         r = launch_tile<DIM, T>(h, MODE_INPLACE, st[h->cur], st[1 - h->cur], tb, sa);
         if (r != MPCD_OK) return r;
@@ -665,7 +705,7 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
 }
 
 extern "C" int mpcd_set_kernel(mpcd_handle *h, int kernel) {
-    if (!h || (kernel != MPCD_KERNEL_AUTO && kernel != MPCD_KERNEL_TILE)) return MPCD_ERR_ARG;
+    if (!h || kernel < MPCD_KERNEL_AUTO || kernel > MPCD_KERNEL_SPLIT) return MPCD_ERR_ARG;
     h->kernel = kernel;
     return MPCD_OK;
 }

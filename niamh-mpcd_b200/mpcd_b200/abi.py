@@ -30,6 +30,8 @@ PREC_MIXED = 1
 
 KERNEL_AUTO = 0
 KERNEL_TILE = 1
+KERNEL_GROUP = 2
+KERNEL_SPLIT = 3
 
 STRATEGY_SCATTER = 0
 STRATEGY_RECOMPUTE = 1

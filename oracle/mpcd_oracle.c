@@ -40,6 +40,7 @@
 
 #define TOL 1e-8    /* definitions.h:56 */
 #define NBOUNCE 50  /* definitions.h:62 */
+#define MPCD_PI 3.14159265358979323846 /* pi = MPCD_PI, definitions.h:72 */
 
 struct oracle {
     mpcd_config cfg;
@@ -132,6 +133,8 @@ void oracle_destroy(oracle_t *o) {
 
 static void bin_cells(oracle_t *o, int shifted);
 static void local_prop(oracle_t *o);
+static void vel_grad_2d(oracle_t *o);
+static void order_param_2d(oracle_t *o, int c);
 
 oracle_t *oracle_create(const mpcd_config *cfg, int n, const double *Q,
                         const double *V, const double *U, const int *spid) {
@@ -290,6 +293,128 @@ static void local_prop(oracle_t *o) {
             memcpy(&o->I[9 * c], I, sizeof(I));
         }
     }
+    if (lc != 0) {
+        for (int c = 0; c < o->ncells; c++)
+            if (o->start[c + 1] - o->start[c] > 1) order_param_2d(o, c);
+        vel_grad_2d(o);
+    }
+}
+
+
+/* ---------------------------------------------------------------- nematic */
+static double len3(const double *v, int n) { return sqrt(dot3(v, v, n)); }
+static void norm_n(double *v, int n) {
+    /* norm, mtools.c:246-251 */
+    double l = len3(v, n);
+    if (fabs(l) >= TOL)
+        for (int i = 0; i < n; i++) v[i] = v[i] / l;
+}
+/* rodriguesRotation, mtools.c:1572-1585 (renormalises to the old length) */
+static void rodrigues(double *vec, double *ax, double th) {
+    double cp[3], dp, old, nw;
+    norm_n(ax, 3);
+    old = len3(vec, 3);
+    cross3(ax, vec, cp);
+    dp = dot3(ax, vec, 3);
+    for (int i = 0; i < 3; i++)
+        vec[i] = vec[i] * cos(th) + cp[i] * sin(th) + ax[i] * dp * (1.0 - cos(th));
+    nw = len3(vec, 3);
+    for (int i = 0; i < 3; i++) vec[i] *= (old / nw);
+}
+
+/* 2x2 eigen-decomposition of the order tensor, eigenvalues2x2 and
+ * eigenvectors2x2 (mtools.c:1225-1300), including their special cases.
+ * Returns the largest eigenvalue; dir receives eigenvector 0. */
+static double eigen2(const double m[4], double dir[2]) {
+    double det = m[0] * m[3] - m[2] * m[1];
+    double tr = m[0] + m[3];
+    double sq = sqrt(tr * tr * 0.25 - det);
+    double ev0 = tr * 0.5 + sq, ev1 = tr * 0.5 - sq;
+    double e0[2] = {0, 0}, e1[2] = {0, 0};
+    (void)ev1;
+    if (fabs(m[2] - 0.0) >= TOL) {
+        e0[0] = ev0 - m[3];
+        e0[1] = m[2];
+        norm_n(e0, 2);
+    } else if (fabs(m[1] - 0.0) >= TOL) {
+        e0[0] = m[1];
+        e0[1] = ev0 - m[0];
+        norm_n(e0, 2);
+    } else {
+        if (fabs(m[0] - m[3]) <= TOL) {
+            e0[0] = sqrt(2.);
+            e0[1] = e0[0];
+        } else if (fabs(m[0] - ev0) <= TOL) {
+            e0[0] = 1.0;
+            e0[1] = 0.0;
+        } else if (fabs(m[3] - ev0) <= TOL) {
+            /* the reference writes row 0 twice here, ending at (1, 0) */
+            e0[0] = 1.0;
+            e0[1] = 0.0;
+        }
+    }
+    (void)e1;
+    dir[0] = e0[0];
+    dir[1] = e0[1];
+    return ev0;
+}
+
+/* velGradD2Q9, lc.c:2130-2162: E_ij = 3 sum_k w_k e_kj VCM_i(x + e_k) on
+ * bulk cells 1..L-1, then edges copied from their neighbour in the
+ * reference's order; corner (L, L) keeps its old value. */
+static void vel_grad_2d(oracle_t *o) {
+    static const int ev[8][2] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}, {1, 1}, {-1, 1}, {-1, -1}, {1, -1}};
+    const double w[8] = {1. / 9., 1. / 9., 1. / 9., 1. / 9., 1. / 36., 1. / 36., 1. / 36., 1. / 36.};
+    int Lx = o->L[0], Ly = o->L[1];
+    for (int a = 1; a < Lx; a++)
+        for (int b = 1; b < Ly; b++) {
+            double *E = &o->E[9 * cell_index(o, a, b, 0)];
+            for (int i = 0; i < 2; i++)
+                for (int j = 0; j < 2; j++) {
+                    double e = 0.0;
+                    for (int k = 0; k < 8; k++)
+                        e += w[k] * ev[k][j] *
+                             o->vcm[3 * cell_index(o, a + ev[k][0], b + ev[k][1], 0) + i];
+                    e *= 3.;
+                    E[3 * i + j] = e;
+                }
+        }
+#define COPYE(dst, src)                                                       \
+    for (int i = 0; i < 2; i++)                                                \
+        for (int j = 0; j < 2; j++) o->E[9 * (dst) + 3 * i + j] = o->E[9 * (src) + 3 * i + j];
+    for (int b = 0; b < Ly; b++) COPYE(cell_index(o, 0, b, 0), cell_index(o, 1, b, 0));
+    for (int b = 0; b < Ly; b++) COPYE(cell_index(o, Lx, b, 0), cell_index(o, Lx - 1, b, 0));
+    for (int a = 0; a < Lx; a++) COPYE(cell_index(o, a, 0, 0), cell_index(o, a, 1, 0));
+    for (int a = 0; a < Lx; a++) COPYE(cell_index(o, a, Ly, 0), cell_index(o, a, Ly - 1, 0));
+#undef COPYE
+}
+
+/* order tensor, director and scalar order parameter of a cell with more
+ * than one particle (tensOrderParam lc.c:1125-1148, localPROP mpc.c:176-213),
+ * 2D */
+static void order_param_2d(oracle_t *o, int c) {
+    int s = o->start[c], e = o->start[c + 1];
+    double Sm[4] = {0, 0, 0, 0};
+    double cc = 1. / (2.0 - 1.), popinv = 1. / (double)(e - s);
+    for (int j = s; j < e; j++) {
+        const double *u = &o->U[3 * o->list[j]];
+        Sm[0] += u[0] * u[0];
+        Sm[1] += u[0] * u[1];
+        Sm[3] += u[1] * u[1];
+    }
+    Sm[0] *= cc * 2.0 * popinv;
+    Sm[1] *= cc * 2.0 * popinv;
+    Sm[3] *= cc * 2.0 * popinv;
+    Sm[0] -= cc;
+    Sm[3] -= cc;
+    Sm[2] = Sm[1];
+    double dir[2];
+    double S = eigen2(Sm, dir);
+    o->dir[3 * c + 0] = dir[0];
+    o->dir[3 * c + 1] = dir[1];
+    o->dir[3 * c + 2] = 0.0;
+    if (S > 1.0) S = 1.0;
+    o->S[c] = S;
 }
 
 /* ------------------------------------------------------------ phantoms */
@@ -452,6 +577,243 @@ static void collide_rat(oracle_t *o, int c, uint32_t step) {
     }
 }
 
+
+/* LCcollision (lc.c:427-544) with genrand_maierSaupeMetropolis_2D
+ * (lc.c:341-411): Metropolis sampling of each orientation in the cell's
+ * mean-field potential, rotated onto the director; torque T = rfc U x dU/dt.
+ * Uniforms: the particle's own sequence of the LC stream. */
+static void lc_collision_cell(oracle_t *o, int c, uint32_t step) {
+    const double KBT = o->cfg.kbt, dt = o->cfg.dt;
+    int s = o->start[c], e = o->start[c + 1], pop = e - s;
+    double S = o->S[c];
+    double DIR[3] = {o->dir[3 * c], o->dir[3 * c + 1], 0.0};
+    double xaxis[3] = {1.0, 0.0, 0.0}, rotAx[3];
+    cross3(DIR, xaxis, rotAx);
+    double ca = dot3(DIR, xaxis, 2) / len3(DIR, 2) / len3(xaxis, 2);
+    double rotAngle = -1. * acos(ca);
+    norm_n(rotAx, 3);
+    double av = 0.0;
+    for (int j = s; j < e; j++) av += o->cfg.species[o->spid[o->list[j]]].mfpot;
+    if (pop > 1) av /= (float)pop;
+    double effM = av * 0.5 * 2.0;
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double *U = &o->U[3 * i], *T = &o->T[3 * i];
+        double rfc = o->cfg.species[o->spid[i]].rfc;
+        double dU[3] = {U[0], U[1], 0.0};
+        for (int d = 0; d < 3; d++) T[d] = 0.;
+        uint32_t k = 0;
+        /* genrand_maierSaupeMetropolis_2D */
+        double newU[3] = {U[0], U[1], 0.0};
+        double A[3] = {DIR[0], DIR[1], 0}, B[3] = {U[0], U[1], 0}, cr[3];
+        cross3(A, B, cr);
+        double ang0 = atan2(len3(cr, 3), dot3(A, B, 2));
+        if (fabs(ang0 - 0.5 * MPCD_PI) <= TOL || fabs(ang0 + 0.5 * MPCD_PI) <= TOL)
+            ang0 = MPCD_PI * (0.5 - mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step,
+                                                  MPCD_STREAM_LC, (uint32_t)i, k++));
+        double uz0 = dot3(DIR, U, 2);
+        int anneal = (int)(5 + 0.1 * effM * S / KBT);
+        int cnt = 0;
+        for (int a = 0; a < anneal; a++) {
+            int acc = 0;
+            double w0 = effM * S * uz0 * uz0 / KBT;
+            double ang1 = MPCD_PI * (0.5 - mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step,
+                                                        MPCD_STREAM_LC, (uint32_t)i, k++));
+            double uz1 = cos(ang1);
+            double w1 = effM * S * uz1 * uz1 / KBT;
+            double dw = w1 - w0;
+            if (dw >= 0.) {
+                acc = 1;
+            } else {
+                double R = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_LC,
+                                            (uint32_t)i, k++);
+                if (R <= exp(dw)) acc = 1;
+            }
+            if (acc) {
+                cnt += 1;
+                ang0 = ang1;
+                uz0 = uz1;
+            }
+        }
+        newU[0] = uz0;
+        newU[1] = sin(ang0);
+        if (cnt > 0) {
+            double ax[3] = {rotAx[0], rotAx[1], rotAx[2]};
+            rodrigues(newU, ax, rotAngle);
+            U[0] = newU[0];
+            U[1] = newU[1];
+        }
+        for (int d = 0; d < 2; d++) dU[d] = (U[d] - dU[d]) / dt;
+        cross3(U, dU, T);
+        for (int d = 0; d < 3; d++) T[d] *= rfc;
+    }
+}
+
+/* jefferysTorque (lc.c:559-607) with larsonRotRate (lc.c:622-718):
+ * du/dt = u.W + lambda (u.D - u u u:D), rotation by chi dt |u x du/dt|. */
+static void jeffery_cell(oracle_t *o, int c) {
+    const double *E = &o->E[9 * c];
+    for (int j = o->start[c]; j < o->start[c + 1]; j++) {
+        int p = o->list[j];
+        double tumble = o->cfg.species[o->spid[p]].tumble;
+        double chihi = o->cfg.species[o->spid[p]].chihi;
+        double *U = &o->U[3 * p];
+        double u[3] = {U[0], U[1], U[2]};
+        double D[3][3], W[3][3], uuuD[3] = {0, 0, 0}, uw[3] = {0, 0, 0}, uD[3] = {0, 0, 0};
+        double dudt[3], w[3];
+        for (int i = 0; i < 3; i++)
+            for (int jj = 0; jj < 3; jj++) {
+                D[jj][i] = 0.5 * (E[3 * i + jj] + E[3 * jj + i]);
+                W[jj][i] = 0.5 * (E[3 * i + jj] - E[3 * jj + i]);
+            }
+        for (int jj = 0; jj < 3; jj++) {
+            for (int i = 0; i < 3; i++) {
+                for (int k = 0; k < 3; k++) uuuD[jj] += u[jj] * (u[i] * D[i][k] * u[k]);
+                uD[jj] += u[i] * D[i][jj];
+                uw[jj] += u[i] * W[i][jj];
+            }
+            dudt[jj] = uw[jj] + tumble * (uD[jj] - uuuD[jj]);
+        }
+        cross3(u, dudt, w);
+        for (int i = 0; i < 3; i++) w[i] *= chihi;
+        for (int i = 0; i < 3; i++) w[i] *= o->cfg.dt;
+        double theta = len3(w, 3);
+        norm_n(w, 3);
+        rodrigues(U, w, theta);
+    }
+}
+
+/* Andersen-ROT for nematic fluids: andersenROT_LC (lc.c:1515-1728) and
+ * dipoleAndersenROT_LC (lc.c:1749-2043, collOp 16/17/20/21: active dipole
+ * kick +-ACT dt DIR by the side of the plane through CM normal to DIR).
+ * Angular momentum includes the orientational torques sum T dt. */
+static void collide_lc(oracle_t *o, int c, uint32_t step) {
+    int op = o->cfg.coll_op, s = o->start[c], e = o->start[c + 1], pop = e - s;
+    int dipole = (op == 16 || op == 17 || op == 20 || op == 21);
+    const double dt = o->cfg.dt;
+    double RS[3] = {0, 0, 0}, AS[3] = {0, 0, 0}, Llm[3] = {0, 0, 0}, Lnm[3] = {0, 0, 0};
+    double W[3] = {0, 0, 0}, II[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double *u = &o->vcm[3 * c], *cm = &o->cm[3 * c], *dir = &o->dir[3 * c];
+    double ACT = 0.0, sigW = 0.0, sigP = 0.0;
+    if (dipole) {
+        int spcnt[MPCD_MAX_SPECIES] = {0};
+        for (int j = s; j < e; j++) spcnt[o->spid[o->list[j]]]++;
+        for (int j = s; j < e; j++) {
+            const mpcd_species *sp = &o->cfg.species[o->spid[o->list[j]]];
+            if (sp->minactratio == 0.0 ||
+                sp->minactratio * o->gndnst < (double)spcnt[o->spid[o->list[j]]]) {
+                ACT += sp->act / sp->mass;
+                sigW += sp->sigwidth;
+                sigP += sp->sigpos;
+            }
+        }
+        if (op == 17 || op == 20) ACT *= o->gndnst / ((double)pop);
+        if (op == 20 || op == 21) {
+            sigW /= (double)pop;
+            sigP /= (double)pop;
+            double fall = (1 - tanh(((double)pop - o->gndnst * (1 + sigP)) / (o->gndnst * sigW)));
+            ACT *= fall / 2;
+        }
+        ACT *= dt;
+    }
+    int act_on = dipole && fabs(ACT - 0.0) >= TOL;
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double m = o->cfg.species[o->spid[i]].mass;
+        double rv[3];
+        thermal_draw(o, i, step, rv);
+        for (int d = 0; d < 2; d++) RS[d] += m * rv[d];
+        if (act_on) {
+            double pW = 0.0;
+            for (int d = 0; d < 2; d++) pW += dir[d] * (o->Q[3 * i + d] - cm[d]);
+            pW -= 0.0;
+            double pm = pW <= 0 ? -1. : 1.;
+            for (int d = 0; d < 2; d++) AS[d] += m * (pm * ACT * dir[d]);
+        }
+    }
+    for (int d = 0; d < 2; d++) {
+        RS[d] /= o->mass[c];
+        AS[d] /= o->mass[c];
+    }
+    II[8] = 1. / o->I[9 * c + 8];
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double m = o->cfg.species[o->spid[i]].mass;
+        double rv[3] = {0, 0, 0}, r[3] = {0, 0, 0}, dv[3] = {0, 0, 0}, am[3], av[3] = {0, 0, 0};
+        thermal_draw(o, i, step, rv);
+        if (act_on) {
+            double pW = 0.0;
+            for (int d = 0; d < 2; d++) pW += dir[d] * (o->Q[3 * i + d] - cm[d]);
+            pW -= 0.0;
+            double pm = pW <= 0 ? -1. : 1.;
+            for (int d = 0; d < 2; d++) av[d] = pm * ACT * dir[d];
+        }
+        for (int d = 0; d < 2; d++) {
+            r[d] = o->Q[3 * i + d] - cm[d];
+            dv[d] = dipole ? m * (o->V[3 * i + d] - rv[d] - av[d]) : m * (o->V[3 * i + d] - rv[d]);
+        }
+        cross3(r, dv, am);
+        for (int d = 0; d < 3; d++) Llm[d] += am[d];
+        for (int d = 0; d < 3; d++) Lnm[d] += o->T[3 * i + d] * dt;
+    }
+    double L[3];
+    for (int d = 0; d < 3; d++) L[d] = Llm[d] + Lnm[d];
+    for (int a = 0; a < 3; a++) {
+        W[a] = 0.0;
+        for (int b = 0; b < 3; b++) W[a] += II[a * 3 + b] * L[b];
+    }
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double rv[3] = {0, 0, 0}, r[3] = {0, 0, 0}, ang[3], av[3] = {0, 0, 0};
+        thermal_draw(o, i, step, rv);
+        double damp = o->cfg.species[o->spid[i]].damp;
+        for (int d = 0; d < 2; d++) r[d] = o->Q[3 * i + d] - cm[d];
+        cross3(W, r, ang);
+        if (dipole) {
+            if (act_on) {
+                double pW = 0.0;
+                for (int d = 0; d < 2; d++) pW += dir[d] * (o->Q[3 * i + d] - cm[d]);
+                pW -= 0.0;
+                double pm = pW <= 0 ? -1. : 1.;
+                for (int d = 0; d < 2; d++) av[d] = pm * ACT * dir[d];
+            }
+            for (int d = 0; d < 2; d++)
+                o->V[3 * i + d] = u[d] + rv[d] - RS[d] + ang[d] + av[d] - AS[d] - damp * u[d];
+        } else {
+            for (int d = 0; d < 2; d++) o->V[3 * i + d] = u[d] + rv[d] - RS[d] + ang[d];
+        }
+    }
+}
+
+/* oriBC (lc.c:1290-1405) for a static wall: orientation made unit, turned to
+ * point out of the wall, its normal/tangential parts scaled by MUN/MUT (or
+ * replaced by DUxyz when both are 0), scaled by MUxyz and renormalised. */
+static void ori_bc(oracle_t *o, int i, const mpcd_wall *wl, const double *n) {
+    int dim = o->dim;
+    double *U = &o->U[3 * i], UN[3] = {0, 0, 0}, UT[3] = {0, 0, 0};
+    norm_n(U, dim);
+    if (dot3(U, n, dim) >= 0.0)
+        for (int d = 0; d < dim; d++) U[d] *= 1.;
+    else
+        for (int d = 0; d < dim; d++) U[d] *= -1.;
+    double x = dot3(U, n, dim);
+    for (int d = 0; d < dim; d++) UN[d] = x * n[d];
+    for (int d = 0; d < dim; d++) UT[d] = U[d] - UN[d];
+    if (fabs(wl->MUN - 0.0) <= TOL && fabs(wl->MUT - 0.0) <= TOL) {
+        for (int d = 0; d < dim; d++) U[d] = wl->DUxyz[d];
+    } else {
+        for (int d = 0; d < dim; d++) {
+            UN[d] *= wl->MUN;
+            UT[d] *= wl->MUT;
+        }
+        for (int d = 0; d < dim; d++) U[d] = UN[d] + UT[d];
+        U[0] *= wl->MUxyz[0];
+        if (dim >= 2) U[1] *= wl->MUxyz[1];
+        if (dim >= 3) U[2] *= wl->MUxyz[2];
+    }
+    norm_n(U, dim);
+}
+
 /* ----------------------------------------------------------------- walls */
 /* MPC_BCcollision (bc.c:1363-1496) for static planar walls with rule-based
  * collisions (COLL_TYPE 1): repeatedly find the wall crossed earliest
@@ -524,6 +886,7 @@ static void wall_collisions(oracle_t *o, int i) {
                 pt[d] += wl->DT;
             }
             for (int d = 0; d < dim; d++) q[d] = pn[d] + pt[d];
+            if (o->cfg.lc != 0) ori_bc(o, i, wl, n);
             t_left -= t_coll;
             for (int d = 0; d < dim; d++) q[d] = q[d] + t_left * v[d];
             if (wall_W(o, chosen, q) < -TOL)
@@ -552,7 +915,7 @@ static void wall_collisions(oracle_t *o, int i) {
 int oracle_step(oracle_t *o, uint32_t step) {
     int dim = o->dim, n = o->n, op = o->cfg.coll_op;
     double s[3] = {0, 0, 0};
-    if (o->cfg.lc != 0) return MPCD_ERR_UNSUPPORTED;
+    if (o->cfg.lc != 0 && dim != 2) return MPCD_ERR_UNSUPPORTED;
     if (o->cfg.galinv) mpcd_rng_shift(o->cfg.seed, o->cfg.replica, step, dim, s);
     /* gridShift_all(...,0), mpc.c:728-736 and walls :765 */
     for (int i = 0; i < n; i++)
@@ -571,9 +934,18 @@ int oracle_step(oracle_t *o, uint32_t step) {
             for (int d = 0; d < dim; d++) o->V[3 * i + d] = o->V[3 * i + d] + o->cfg.dt * g[d];
     local_prop(o);
     ghost_part(o, step);
+    if (o->cfg.lc != 0) {
+        /* mpc.c:4640-4678 */
+        for (int c = 0; c < o->ncells; c++)
+            if (o->pop[c] > 1) lc_collision_cell(o, c, step);
+        for (int c = 0; c < o->ncells; c++)
+            if (o->pop[c] > 1) jeffery_cell(o, c);
+    }
     for (int c = 0; c < o->ncells; c++) {
         if (o->pop[c] <= 1) continue;
-        if (op == MPCD_COLL_ARBAXIS)
+        if (o->cfg.lc != 0)
+            collide_lc(o, c, step);
+        else if (op == MPCD_COLL_ARBAXIS)
             collide_srd(o, c, step);
         else if (op == MPCD_COLL_MPCAT)
             collide_mpcat(o, c, step);

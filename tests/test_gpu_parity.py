@@ -85,7 +85,7 @@ def test_srd_conserves_momentum_and_energy(prec):
 @pytest.mark.parametrize("strategy", [abi.STRATEGY_SCATTER, abi.STRATEGY_RECOMPUTE])
 @pytest.mark.parametrize("name", ["srd3d", "srd2d", "rat2d", "channel3d", "mpcat3d_damp"])
 @pytest.mark.parametrize("tile", [0, 64, 4096])
-@pytest.mark.parametrize("kernel", [abi.KERNEL_AUTO, abi.KERNEL_TILE])
+@pytest.mark.parametrize("kernel", [abi.KERNEL_AUTO, abi.KERNEL_TILE, abi.KERNEL_GROUP])
 def test_strategies_and_tiles_agree_with_oracle(name, strategy, tile, kernel):
     cfg, ppc, sseed, _ = build(name)
     Q, V, U, sp = state(cfg, ppc, sseed)
@@ -124,7 +124,7 @@ def _clumped_state(cfg, ppc, seed, clumps, per_clump):
     return Qx, Vx, Ux, spx
 
 
-@pytest.mark.parametrize("kernel", [abi.KERNEL_AUTO, abi.KERNEL_TILE])
+@pytest.mark.parametrize("kernel", [abi.KERNEL_AUTO, abi.KERNEL_TILE, abi.KERNEL_GROUP])
 @pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
 def test_dense_tiles_are_subdivided(prec, kernel):
     # 40 dense cells of 200 particles: tiles far above capacity are split
