@@ -18,6 +18,9 @@ CASES = {
     "channel3d": (W.cfg_channel3d, dict(L=(8, 6, 4), g=1e-2), 20, 17, 4),
     "srd3d_heavy": (W.cfg_srd3d, dict(L=(4, 4, 4), species=[W._species(mass=2.5)],
                                       kbt=1.7, dt=0.25), 10, 18, 4),
+    "nematic2d_dipole": (W.cfg_nematic2d, dict(L=(8, 7), coll_op=16), 20, 19, 4),
+    "nematic2d_av": (W.cfg_nematic2d, dict(L=(7, 6), coll_op=17), 20, 20, 4),
+    "nematic2d_rat": (W.cfg_nematic2d, dict(L=(6, 8), coll_op=3), 20, 21, 4),
 }
 
 

@@ -22,15 +22,17 @@ from cases import CASES, build, state  # noqa: E402
 from checkers import Reference  # noqa: E402
 
 
-def main():
-    for name in CASES:
+def main(names=None):
+    for name in (names or CASES):
         cfg, ppc, sseed, nsteps = build(name)
         Q, V, U, sp = state(cfg, ppc, sseed)
         ref = Reference(cfg, Q, V, U, sp)
-        out = {"Q0": Q, "V0": V, "gndnst": ref.gndnst()}
+        out = {"Q0": Q, "V0": V, "U0": U, "gndnst": ref.gndnst()}
         for s in range(1, nsteps + 1):
             ref.step(s)
-            q, v, _ = ref.particles()
+            q, v, u = ref.particles()
+            if cfg.lc:
+                out[f"U{s}"] = u
             kb, av = ref.globals()
             pop, _, _, _ = ref.cells()
             out[f"Q{s}"] = q
@@ -44,4 +46,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

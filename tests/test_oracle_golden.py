@@ -27,8 +27,10 @@ def test_oracle_matches_reference_golden(name):
     assert o.gndnst() == pytest.approx(float(g["gndnst"]), abs=0)
     for s in range(1, nsteps + 1):
         o.step(s)
-        q, v, _ = o.particles()
+        q, v, u = o.particles()
         kb, av = o.globals()
+        if cfg.lc:
+            np.testing.assert_allclose(u, g[f"U{s}"], rtol=0, atol=1e-11)
         pop, _, _, _ = o.cells()
         np.testing.assert_allclose(q, g[f"Q{s}"], rtol=0, atol=ATOL * max(cfg.L))
         np.testing.assert_allclose(v, g[f"V{s}"], rtol=0, atol=ATOL * 10)
