@@ -185,16 +185,30 @@ __global__ void __launch_bounds__(256) k_srd_parts(const __grid_constant__ DevCf
             }
         }
         const int k = T::finish(c, r, sp, sa, bounce, esc);
-        if (MODE == MODE_INPLACE) {
-            T::store(a, i, r);
-            tb.key[i] = k;
-            tb.rank[i] = atomicAdd(&tb.count_next[k], 1);
-        } else if (MODE == MODE_COUNT) {
-            atomicAdd(&tb.count_next[k], 1);
+        // warp-aggregated counting: lanes with the same next cell take one
+        // atomic (particles of a cell are adjacent and move together)
+        const unsigned act = __activemask();
+        const unsigned peers = __match_any_sync(act, k);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        const int below = __popc(peers & ((1u << lane) - 1u));
+        if (MODE == MODE_COUNT) {
+            if (lane == leader) atomicAdd(&tb.count_next[k], __popc(peers));
         } else {
-            const int dst = tb.start_next[k] + atomicAdd(&tb.fill[k], 1);
-            T::store(b, dst, r);
-            T::store_sp(b, dst, sp);
+            int base = 0;
+            if (lane == leader)
+                base = atomicAdd(MODE == MODE_INPLACE ? &tb.count_next[k] : &tb.fill[k],
+                                 __popc(peers));
+            base = __shfl_sync(peers, base, leader) + below;
+            if (MODE == MODE_INPLACE) {
+                T::store(a, i, r);
+                tb.key[i] = k;
+                tb.rank[i] = base;
+            } else {
+                const int dst = tb.start_next[k] + base;
+                T::store(b, dst, r);
+                T::store_sp(b, dst, sp);
+            }
         }
     }
     if (MODE != MODE_COUNT) {

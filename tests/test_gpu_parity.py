@@ -149,7 +149,8 @@ def test_dense_tiles_are_subdivided(prec, kernel):
     assert g.status().overflow == 0
 
 
-def test_overfull_cell_is_reported_not_collided():
+@pytest.mark.parametrize("kernel", [abi.KERNEL_TILE, abi.KERNEL_GROUP])
+def test_overfull_cell_is_reported_not_collided(kernel):
     # one cell holding more particles than a tile can stage: its particles
     # stream without collision and are counted in status.overflow
     # (no grid shift, so the clump stays in one cell)
@@ -157,6 +158,23 @@ def test_overfull_cell_is_reported_not_collided():
     cfg = W.cfg_srd3d((6, 6, 6), seed=32, galinv=0)
     Q, V, U, sp = _clumped_state(cfg, 10, 9, [(2, 2, 2)], 5000)
     g = Solver(cfg)
+    g.set_kernel(kernel)
     g.upload(Q, V, U, sp)
     g.step(1, 1)
     assert g.status().overflow >= 5000
+
+
+def test_split_kernel_collides_any_cell_population():
+    # the thread-per-cell pass has no staging limit: a 5000-particle cell
+    # collides exactly like the oracle's
+    from mpcd_b200 import workloads as W
+    cfg = W.cfg_srd3d((6, 6, 6), seed=32, galinv=0)
+    Q, V, U, sp = _clumped_state(cfg, 10, 9, [(2, 2, 2)], 5000)
+    o = Oracle(cfg, Q, V, U, sp)
+    g = Solver(cfg)
+    g.set_kernel(abi.KERNEL_SPLIT)
+    g.upload(Q, V, U, sp)
+    o.step(1)
+    g.step(1, 1)
+    np.testing.assert_allclose(g.download()[1], o.particles()[1], rtol=0, atol=1e-11)
+    assert g.status().overflow == 0
