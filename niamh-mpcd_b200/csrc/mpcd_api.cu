@@ -18,6 +18,7 @@
 #include "mpcd_tile.cuh"
 #include "mpcd_group.cuh"
 #include "mpcd_split.cuh"
+#include "mpcd_lc.cuh"
 
 using namespace mpcd;
 
@@ -44,6 +45,8 @@ struct mpcd_handle {
     int tile_target; // expected particles per tile
     int kernel;      // MPCD_KERNEL_*: cell kernel family
     void *crec;      // per-cell SRD records (split kernel family)
+    LcCells lcc;     // per-cell nematic arrays (lc != 0)
+    double *lcbuf;
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     uint32_t last_step;
     uint64_t steps;
@@ -94,9 +97,10 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     if (cfg->n_species < 1 || cfg->n_species > MPCD_MAX_SPECIES) return MPCD_ERR_ARG;
     if (cfg->n_walls < 0 || cfg->n_walls > MPCD_MAX_WALLS) return MPCD_ERR_ARG;
     if (!(cfg->dt > 0.0) || !(cfg->kbt >= 0.0)) return MPCD_ERR_ARG;
-    if (cfg->lc != MPCD_LC_ISOTROPIC) return MPCD_ERR_UNSUPPORTED;
-    if (cfg->coll_op != MPCD_COLL_ARBAXIS && cfg->coll_op != MPCD_COLL_MPCAT &&
-        cfg->coll_op != MPCD_COLL_RAT)
+    if (cfg->lc != MPCD_LC_ISOTROPIC && !(cfg->lc == MPCD_LC_LOCAL && cfg->dim == 2))
+        return MPCD_ERR_UNSUPPORTED;
+    if (cfg->lc == MPCD_LC_ISOTROPIC && cfg->coll_op != MPCD_COLL_ARBAXIS &&
+        cfg->coll_op != MPCD_COLL_MPCAT && cfg->coll_op != MPCD_COLL_RAT)
         return MPCD_ERR_UNSUPPORTED;
     dc->dim = cfg->dim;
     dc->op = cfg->coll_op;
@@ -118,6 +122,14 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         if (!(cfg->species[s].mass > 0.0)) return MPCD_ERR_ARG;
         dc->mass[s] = cfg->species[s].mass;
         dc->damp[s] = cfg->species[s].damp;
+        dc->rfc[s] = cfg->species[s].rfc;
+        dc->tumble[s] = cfg->species[s].tumble;
+        dc->chihi[s] = cfg->species[s].chihi;
+        dc->act[s] = cfg->species[s].act;
+        dc->mfpot[s] = cfg->species[s].mfpot;
+        dc->sigwidth[s] = cfg->species[s].sigwidth;
+        dc->sigpos[s] = cfg->species[s].sigpos;
+        dc->minactratio[s] = cfg->species[s].minactratio;
     }
     dc->dt = cfg->dt;
     dc->kbt = cfg->kbt;
@@ -144,7 +156,15 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
             dst.A[d] = src.A[d];
             dst.Q[d] = src.Q[d];
             dst.DVxyz[d] = src.DVxyz[d];
+            dst.MUxyz[d] = src.MUxyz[d];
+            dst.DUxyz[d] = src.DUxyz[d];
         }
+        dst.MUN = src.MUN;
+        dst.MUT = src.MUT;
+        // nematic anchoring by phantom walls (ghostPart's ghost anchoring) is
+        // not implemented
+        if (cfg->lc && src.phantom && (std::fabs(src.MUN) <= kTol || std::fabs(src.MUT) <= kTol))
+            return MPCD_ERR_UNSUPPORTED;
         dst.R = src.R;
         dst.DN = src.DN;
         dst.DT = src.DT;
@@ -179,6 +199,8 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
         }
         cudaFree(h->f[b].pid);
         cudaFree(h->f[b].sp);
+        cudaFree(h->f[b].u[0]);
+        cudaFree(h->f[b].u[1]);
         mix_free(h->mx[b]);
     }
     cudaFree(h->key);
@@ -191,6 +213,7 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->acc);
     cudaFree(h->status);
     cudaFree(h->crec);
+    cudaFree(h->lcbuf);
     if (h->host_acc) cudaFreeHost(h->host_acc);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -232,6 +255,22 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     ALLOC(h->acc, sizeof(double) * 2 * ACC_WORDS);
     ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
     ALLOC(h->crec, (size_t)nc * 128);
+    if (dc.lc) {
+        ALLOC(h->lcbuf, (size_t)nc * 13 * sizeof(double));
+        if (cudaMemsetAsync(h->lcbuf, 0, (size_t)nc * 13 * sizeof(double), h->stream) !=
+            cudaSuccess) {
+            mpcd_destroy(h);
+            return MPCD_ERR_CUDA;
+        }
+        double *b = h->lcbuf;
+        h->lcc.vcm = b;
+        h->lcc.cm = b + 2 * (size_t)nc;
+        h->lcc.izz = b + 4 * (size_t)nc;
+        h->lcc.mass = b + 5 * (size_t)nc;
+        h->lcc.S = b + 6 * (size_t)nc;
+        h->lcc.dir = b + 7 * (size_t)nc;
+        h->lcc.E = b + 9 * (size_t)nc;
+    }
     h->sorted_for = -1;
     h->strategy = -1;
     h->tile_target = 0;
@@ -264,6 +303,10 @@ static int ensure_capacity(mpcd_handle *h, int n) {
         cudaFree(h->f[b].pid);
         cudaFree(h->f[b].sp);
         h->f[b].pid = h->f[b].sp = nullptr;
+        for (int d = 0; d < 2; d++) {
+            cudaFree(h->f[b].u[d]);
+            h->f[b].u[d] = nullptr;
+        }
         mix_free(h->mx[b]);
     }
     cudaFree(h->key);
@@ -278,6 +321,9 @@ static int ensure_capacity(mpcd_handle *h, int n) {
                 if ((r = dev_alloc((void **)&h->f[b].v[d], N * sizeof(double)))) return r;
             }
             if ((r = dev_alloc((void **)&h->f[b].pid, N * sizeof(int)))) return r;
+            if (h->dc.lc)
+                for (int d = 0; d < 2; d++)
+                    if ((r = dev_alloc((void **)&h->f[b].u[d], N * sizeof(double)))) return r;
             if (h->dc.n_species > 1)
                 if ((r = dev_alloc((void **)&h->f[b].sp, N * sizeof(int)))) return r;
         } else {
@@ -335,7 +381,6 @@ static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V
 extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
                                  const double *U, const int *spid) {
     if (!h || n < 0 || (n > 0 && (!Q || !V))) return MPCD_ERR_ARG;
-    (void)U;
     int r = upload_common(h, n, Q, V, spid);
     if (r != MPCD_OK) return r;
     if (n == 0) return MPCD_OK;
@@ -360,8 +405,15 @@ extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const d
             CK(cudaMemcpyAsync(h->f[0].sp, ids.data(), N * 4, cudaMemcpyHostToDevice, h->stream));
             CK(cudaStreamSynchronize(h->stream));
         }
+        if (h->f[0].u[0])
+            for (int d = 0; d < 2; d++) {
+                for (size_t i = 0; i < N; i++) tmp[i] = U ? U[3 * i + d] : (d == 0 ? 1.0 : 0.0);
+                CK(cudaMemcpyAsync(h->f[0].u[d], tmp.data(), N * 8, cudaMemcpyHostToDevice,
+                                   h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+            }
     } else {
-        r = mix_upload(h->mx[0], h->dc, n, Q, V, spid, h->stream);
+        r = mix_upload(h->mx[0], h->dc, n, Q, V, U, spid, h->stream);
         if (r != MPCD_OK) return r;
     }
     return MPCD_OK;
@@ -415,12 +467,18 @@ extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double 
                 }
             }
         }
+        if (U) {
+            for (size_t i = 0; i < 3 * N; i++) U[i] = 0.0;
+            if (st.u[0])
+                for (int d = 0; d < 2; d++) {
+                    CK(cudaMemcpy(tmp.data(), st.u[d], N * 8, cudaMemcpyDeviceToHost));
+                    for (size_t i = 0; i < N; i++) U[3 * (size_t)pid[i] + d] = tmp[i];
+                }
+        }
     } else {
-        int r = mix_download(h->mx[h->cur], h->dc, n, Q, V);
+        int r = mix_download(h->mx[h->cur], h->dc, n, Q, V, U);
         if (r != MPCD_OK) return r;
     }
-    if (U)
-        for (size_t i = 0; i < 3 * N; i++) U[i] = 0.0;
     return MPCD_OK;
 }
 
@@ -683,6 +741,73 @@ static int default_strategy(const mpcd_handle *h) {
     return h->dc.op == MPCD_COLL_ARBAXIS ? MPCD_STRATEGY_RECOMPUTE : MPCD_STRATEGY_SCATTER;
 }
 
+// One nematic (2D) timestep: moments + order parameter, velocity gradient,
+// the tile kernel (orientation update, collision, streaming), re-sort.
+template <class T>
+static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
+    StepArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.step = step;
+    host_shift(h, step, sa.s);
+    host_shift(h, step + 1u, sa.sn);
+    for (int d = 0; d < 3; d++) {
+        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0);
+        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0);
+    }
+    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
+    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    int launches = 0;
+    if (h->sorted_for != (int64_t)step) {
+        launch_key<2, T>(h, st[h->cur], sa);
+        launch_scan(h, h->start[h->scur], nullptr, acc_cur);
+        launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[h->scur]);
+        h->cur = 1 - h->cur;
+        launches += 4;
+    }
+    const DevCfg &c = h->dc;
+    const int *start = h->start[h->scur];
+    k_lc_moments<T><<<(c.ncells + 255) / 256, 256, 0, h->stream>>>(c, st[h->cur], start,
+                                                                   h->lcc, sa, acc_cur);
+    int nb = (c.L[0] - 1) * (c.L[1] - 1);
+    if (nb > 0) k_lc_grad<<<(nb + 255) / 256, 256, 0, h->stream>>>(c, h->lcc);
+    k_lc_edges<<<(c.L[1] + 255) / 256, 256, 0, h->stream>>>(c, h->lcc, 0);
+    k_lc_edges<<<(c.L[0] + 255) / 256, 256, 0, h->stream>>>(c, h->lcc, 1);
+    // tile: about 640 particles on average
+    int ct, capp;
+    tile_geometry(h, h->tile_target > 0 ? h->tile_target : 640, &ct, &capp);
+    LcTileLayout lay;
+    lay.ct = ct;
+    lay.cap = capp;
+    lay.bytes = (int)((size_t)capp * sizeof(LcPart) + (size_t)((ct + 1) * 4 + 15) / 16 * 16 +
+                      (size_t)ct * 9 * sizeof(double) + (size_t)capp + 16);
+    while (lay.bytes > 200 * 1024 && lay.cap > 256) {
+        lay.cap = lay.cap * 3 / 4;
+        lay.bytes = (int)((size_t)lay.cap * sizeof(LcPart) + (size_t)((ct + 1) * 4 + 15) / 16 * 16 +
+                          (size_t)ct * 9 * sizeof(double) + (size_t)lay.cap + 16);
+    }
+    TileBufs tb;
+    memset(&tb, 0, sizeof(tb));
+    tb.start = start;
+    tb.count_next = h->count;
+    tb.key = h->key;
+    tb.rank = h->rank;
+    tb.acc = acc_cur;
+    tb.status = h->status;
+    auto kfn = k_lc_tile<T>;
+    CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.bytes));
+    kfn<<<(c.ncells + ct - 1) / ct, 256, lay.bytes, h->stream>>>(c, st[h->cur], h->lcc, tb, sa,
+                                                                 lay);
+    launch_scan(h, h->start[1 - h->scur], nullptr, acc_nxt);
+    launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]);
+    launches += 9;
+    CK(cudaGetLastError());
+    h->cur = 1 - h->cur;
+    h->scur = 1 - h->scur;
+    h->sorted_for = (int64_t)step + 1;
+    h->launches = launches;
+    return MPCD_OK;
+}
+
 extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
     if (!h || nsteps < 0) return MPCD_ERR_ARG;
     if (h->n <= 0) return MPCD_ERR_STATE;
@@ -691,7 +816,10 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
     for (int k = 0; k < nsteps; k++) {
         uint32_t step = step0 + (uint32_t)k;
         int r;
-        if (h->prec == MPCD_PREC_FP64)
+        if (h->dc.lc)
+            r = h->prec == MPCD_PREC_FP64 ? run_step_lc<F64T<2>>(h, h->f, step)
+                                          : run_step_lc<MixT<2>>(h, h->mx, step);
+        else if (h->prec == MPCD_PREC_FP64)
             r = h->dc.dim == 3 ? run_step<3, F64T<3>>(h, h->f, step)
                                : run_step<2, F64T<2>>(h, h->f, step);
         else

@@ -36,6 +36,7 @@ struct DevWall {
     double A[3], Q[3];
     double R, DN, DT, DVN, DVT, MVN, MVT;
     double DVxyz[3];
+    double MUN, MUT, MUxyz[3], DUxyz[3];  // orientation rules (nematic)
     int inv, phantom, periodic, axis;  // axis: the one non-zero component of A
     uint32_t inter;                    // bit s set: species s interacts
     int pad_;
@@ -51,6 +52,9 @@ struct DevCfg {
     double cosA, sinA;  // cos(RA) and the sine with the reference's sign (-sin RA)
     double grav[3];
     double mass[MPCD_MAX_SPECIES], damp[MPCD_MAX_SPECIES];
+    double rfc[MPCD_MAX_SPECIES], tumble[MPCD_MAX_SPECIES], chihi[MPCD_MAX_SPECIES];
+    double act[MPCD_MAX_SPECIES], mfpot[MPCD_MAX_SPECIES], sigwidth[MPCD_MAX_SPECIES];
+    double sigpos[MPCD_MAX_SPECIES], minactratio[MPCD_MAX_SPECIES];
     uint64_t seed;
     uint32_t replica;
     int pad_;
@@ -115,13 +119,55 @@ __device__ __forceinline__ double wall_W(const DevWall &w, const double *q,
     return W;
 }
 
+// oriBC (lc.c:1290-1405) for a static wall: the orientation is made unit,
+// turned to point out of the wall, its normal and tangential parts scaled by
+// MUN/MUT (or replaced by DUxyz when both are 0), scaled by MUxyz and
+// renormalised.
+template <int DIM>
+__device__ void ori_bc(const DevWall &wl, const double *n, double *U) {
+    double l = 0.0;
+    for (int d = 0; d < DIM; d++) l += U[d] * U[d];
+    l = sqrt(l);
+    if (fabs(l) >= kTol)
+        for (int d = 0; d < DIM; d++) U[d] = U[d] / l;
+    double x = 0.0;
+    for (int d = 0; d < DIM; d++) x += U[d] * n[d];
+    if (x >= 0.0)
+        for (int d = 0; d < DIM; d++) U[d] *= 1.;
+    else
+        for (int d = 0; d < DIM; d++) U[d] *= -1.;
+    double un[3], ut[3];
+    x = 0.0;
+    for (int d = 0; d < DIM; d++) x += U[d] * n[d];
+    for (int d = 0; d < DIM; d++) {
+        un[d] = x * n[d];
+        ut[d] = U[d] - un[d];
+    }
+    if (fabs(wl.MUN - 0.0) <= kTol && fabs(wl.MUT - 0.0) <= kTol) {
+        for (int d = 0; d < DIM; d++) U[d] = wl.DUxyz[d];
+    } else {
+        for (int d = 0; d < DIM; d++) {
+            un[d] *= wl.MUN;
+            ut[d] *= wl.MUT;
+        }
+        for (int d = 0; d < DIM; d++) U[d] = un[d] + ut[d];
+        for (int d = 0; d < DIM; d++) U[d] *= wl.MUxyz[d];
+    }
+    l = 0.0;
+    for (int d = 0; d < DIM; d++) l += U[d] * U[d];
+    l = sqrt(l);
+    if (fabs(l) >= kTol)
+        for (int d = 0; d < DIM; d++) U[d] = U[d] / l;
+}
+
 // MPC_BCcollision (bc.c:1363-1496) for static planar rule-based walls, in
 // FP64, visiting walls in index order.  'only_solid' skips periodic walls
-// (the mixed-precision state wraps periodic axes exactly instead).
-// Returns 1 if the particle hit the bounce limit.
+// (the mixed-precision state wraps periodic axes exactly instead).  U, if
+// given, is the nematic orientation, transformed by oriBC at each
+// collision.  Returns 1 if the particle hit the bounce limit.
 template <int DIM>
 __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
-                               bool only_solid) {
+                               bool only_solid, double *U = nullptr) {
     double t_left = c.dt, t_coll = 0.0;
     int chosen = 0, cnt = 0;
     const double m = c.mass[sp];
@@ -188,6 +234,7 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
                 pt[d] += wl.DT;
                 q[d] = pn[d] + pt[d];
             }
+            if (U) ori_bc<DIM>(wl, n, U);
             t_left -= t_coll;
             for (int d = 0; d < DIM; d++) q[d] = q[d] + t_left * v[d];
             if (wall_W(wl, q, wl.Q, DIM) < -kTol)

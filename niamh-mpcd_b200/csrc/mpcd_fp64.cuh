@@ -16,7 +16,8 @@ struct Fp64State {
     double *q[3];
     double *v[3];
     int *pid;
-    int *sp;  // species (nullptr when there is one species)
+    int *sp;      // species (nullptr when there is one species)
+    double *u[2]; // nematic orientation (2D; nullptr when isotropic)
 };
 
 constexpr int kScanTile = 2048;  // cells per scan block (256 threads x 8)

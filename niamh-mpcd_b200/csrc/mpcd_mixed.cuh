@@ -24,7 +24,8 @@ namespace mpcd {
 struct MixState {
     uint4 *P;
     float4 *W;
-    int *sp;  // species (nullptr for one species)
+    int *sp;    // species (nullptr for one species)
+    float2 *U;  // nematic orientation (2D; nullptr when isotropic)
 };
 
 constexpr int kCellBits = 10;
@@ -51,15 +52,19 @@ static inline void mix_free(MixState &s) {
     cudaFree(s.P);
     cudaFree(s.W);
     cudaFree(s.sp);
+    cudaFree(s.U);
     s.P = nullptr;
     s.W = nullptr;
     s.sp = nullptr;
+    s.U = nullptr;
 }
 
 static inline int mix_alloc(MixState &s, size_t n, const DevCfg &c) {
     if (cudaMalloc((void **)&s.P, n * sizeof(uint4)) != cudaSuccess) return MPCD_ERR_NOMEM;
     if (cudaMalloc((void **)&s.W, n * sizeof(float4)) != cudaSuccess) return MPCD_ERR_NOMEM;
     if (c.n_species > 1 && cudaMalloc((void **)&s.sp, n * sizeof(int)) != cudaSuccess)
+        return MPCD_ERR_NOMEM;
+    if (c.lc && cudaMalloc((void **)&s.U, n * sizeof(float2)) != cudaSuccess)
         return MPCD_ERR_NOMEM;
     return MPCD_OK;
 }
@@ -146,12 +151,14 @@ __global__ void __launch_bounds__(256) k_scatter_mix(MixState a, MixState b, int
         b.P[dst] = a.P[i];
         b.W[dst] = a.W[i];
         if (a.sp) b.sp[dst] = a.sp[i];
+        if (a.U) b.U[dst] = a.U[i];
     }
 }
 
 // Host-side conversion to and from the packed representation.
 static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *Q,
-                             const double *V, const int *spid, cudaStream_t stream) {
+                             const double *V, const double *Uo, const int *spid,
+                             cudaStream_t stream) {
     std::vector<uint4> P((size_t)n);
     std::vector<float4> W((size_t)n);
     for (int i = 0; i < n; i++) {
@@ -172,6 +179,16 @@ static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *
     if (cudaMemcpyAsync(s.W, W.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice,
                         stream) != cudaSuccess)
         return MPCD_ERR_CUDA;
+    std::vector<float2> Uh;
+    if (s.U) {
+        Uh.resize((size_t)n);
+        for (int i = 0; i < n; i++)
+            Uh[i] = Uo ? make_float2((float)Uo[3 * (size_t)i], (float)Uo[3 * (size_t)i + 1])
+                       : make_float2(1.f, 0.f);
+        if (cudaMemcpyAsync(s.U, Uh.data(), (size_t)n * sizeof(float2), cudaMemcpyHostToDevice,
+                            stream) != cudaSuccess)
+            return MPCD_ERR_CUDA;
+    }
     std::vector<int> sp;
     if (s.sp) {
         sp.resize((size_t)n);
@@ -185,9 +202,16 @@ static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *
 }
 
 static inline int mix_download(const MixState &s, const DevCfg &c, int n, double *Q,
-                               double *V) {
+                               double *V, double *Uo) {
     std::vector<uint4> P((size_t)n);
     std::vector<float4> W((size_t)n);
+    std::vector<float2> Uh;
+    if (s.U && Uo) {
+        Uh.resize((size_t)n);
+        if (cudaMemcpy(Uh.data(), s.U, (size_t)n * sizeof(float2), cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+            return MPCD_ERR_CUDA;
+    }
     if (cudaMemcpy(P.data(), s.P, (size_t)n * sizeof(uint4), cudaMemcpyDeviceToHost) !=
         cudaSuccess)
         return MPCD_ERR_CUDA;
@@ -204,6 +228,12 @@ static inline int mix_download(const MixState &s, const DevCfg &c, int n, double
         for (int d = 0; d < 3; d++) {
             if (Q) Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;
             if (V) V[3 * (size_t)pid + d] = d < c.dim ? (double)v[d] : 0.0;
+        }
+        if (Uo) {
+            bool has = !Uh.empty();
+            Uo[3 * (size_t)pid] = has ? (double)Uh[i].x : 0.0;
+            Uo[3 * (size_t)pid + 1] = has ? (double)Uh[i].y : 0.0;
+            Uo[3 * (size_t)pid + 2] = 0.0;
         }
     }
     return MPCD_OK;

@@ -629,6 +629,10 @@ __global__ void __launch_bounds__(256) k_scatter_f64v(Fp64State a, Fp64State b, 
         }
         b.pid[dst] = a.pid[i];
         if (a.sp) b.sp[dst] = a.sp[i];
+        if (a.u[0]) {
+            b.u[0][dst] = a.u[0][i];
+            b.u[1][dst] = a.u[1][i];
+        }
     }
 }
 

@@ -32,9 +32,11 @@ def test_fp64_matches_oracle(name):
         o.step(s)
         kg, ag = g.timestep(s)
         qo, vo, _ = o.particles()
-        qg, vg, _ = g.download()
+        qg, vg, ug = g.download()
         np.testing.assert_allclose(vg, vo, rtol=0, atol=1e-12 * 10)
         np.testing.assert_allclose(qg, qo, rtol=0, atol=1e-12 * max(cfg.L))
+        if cfg.lc:
+            np.testing.assert_allclose(ug, o.particles()[2], rtol=0, atol=1e-11)
         ko, ao = o.globals()
         assert kg == pytest.approx(ko, rel=1e-12)
         np.testing.assert_allclose(ag, ao, rtol=0, atol=1e-13)
@@ -52,9 +54,13 @@ def test_mixed_tracks_oracle(name):
     g.upload(Q, V, U, sp)
     o.step(1)
     kg, ag = g.timestep(1)
-    qo, vo, _ = o.particles()
-    qg, vg, _ = g.download()
+    qo, vo, uo = o.particles()
+    qg, vg, ug = g.download()
     L = np.array([cfg.L[d] if d < cfg.dim else 1 for d in range(3)], dtype=float)
+    if cfg.lc:
+        # nematic: orientation (sign-free) tracks to FP32 precision
+        du = np.minimum(np.abs(ug - uo).max(axis=1), np.abs(ug + uo).max(axis=1))
+        assert np.mean(du > 1e-4) < 2e-3, du.max()
     dv = np.abs(vg - vo).max(axis=1)
     dq = np.abs(_min_image(qg - qo, L)).max(axis=1)
     # a particle within ~1e-7 of a cell face may bin differently in FP32
@@ -178,3 +184,27 @@ def test_split_kernel_collides_any_cell_population():
     g.step(1, 1)
     np.testing.assert_allclose(g.download()[1], o.particles()[1], rtol=0, atol=1e-11)
     assert g.status().overflow == 0
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_nematic_multistep_conservation_and_order(prec):
+    # 2D active nematic: orientations stay unit vectors, the mean order
+    # parameter stays in [0, 1], and the FP64 form tracks the oracle over
+    # several steps
+    from mpcd_b200 import workloads as W
+    cfg = W.cfg_nematic2d((16, 16), precision=prec, seed=77)
+    cfg64 = W.cfg_nematic2d((16, 16), seed=77)
+    Q, V, U, sp = W.synthetic_state(cfg, 20, seed=78)
+    o = Oracle(cfg64, Q, V, U, sp)
+    g = Solver(cfg)
+    g.upload(Q, V, U, sp)
+    for s in range(1, 6):
+        o.step(s)
+        g.step(1, s)
+    _, vg, ug = g.download()
+    _, vo, uo = o.particles()
+    n = np.linalg.norm(ug[:, :2], axis=1)
+    assert np.abs(n - 1).max() < (1e-12 if prec == abi.PREC_FP64 else 1e-5)
+    if prec == abi.PREC_FP64:
+        np.testing.assert_allclose(vg, vo, rtol=0, atol=1e-10)
+        np.testing.assert_allclose(ug, uo, rtol=0, atol=1e-10)
