@@ -232,6 +232,29 @@ int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
 #define MPCD_KERNEL_SPLIT 3
 int mpcd_set_kernel(mpcd_handle *h, int kernel);
 
+/* One SRD timestep that allocates no memory, device or host (no
+ * counterpart in the reference, whose timestep works on host memory).  For
+ * callers that cannot allocate at step time: a program whose allocator owns
+ * all device memory, code running under CUDA stream capture (where cudaMalloc
+ * is not allowed), or a plugin that must not allocate behind its host
+ * framework's memory manager.  Q and V are the caller's DEVICE arrays of n
+ * particles (3 doubles each, AoS), updated in place in the caller's order;
+ * globals, if not NULL, is a device array of 4 doubles receiving
+ * KBTNOW and AVNOW[3] (TEMP and avVel).  cfg must select the SRD operator
+ * (MPCD_COLL_ARBAXIS) in FP64 form without phantom walls or nematic order.
+ * All scratch is one fixed device array of this library (11.6 MiB, held on
+ * every GPU that loads it until exit), so n is limited to
+ * MPCD_NOALLOC_MAX_PARTICLES and the (L+1)^D cell grid to
+ * MPCD_NOALLOC_MAX_CELLS; larger sizes return MPCD_ERR_SIZE.  The first call
+ * on a device looks up the array's device address; make that first call
+ * before any stream capture.  Calls share the array: work of two calls that
+ * overlaps on the GPU races and must be serialised by the caller.  stream is
+ * a cudaStream_t (NULL: the default stream); the call is asynchronous. */
+#define MPCD_NOALLOC_MAX_PARTICLES 65536
+#define MPCD_NOALLOC_MAX_CELLS 32768
+int mpcd_srd_step_noalloc(const mpcd_config *cfg, int n, double *Q, double *V,
+                          uint32_t step, double *globals, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

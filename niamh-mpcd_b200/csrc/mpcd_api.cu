@@ -188,6 +188,10 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     return MPCD_OK;
 }
 
+// Configuration check and device form, shared with the allocation-free
+// entry point (mpcd_noalloc.cu).
+int mpcd_build_devcfg(const mpcd_config *cfg, DevCfg *dc) { return build_devcfg(cfg, dc); }
+
 extern "C" int mpcd_abi_version(void) { return MPCD_ABI_VERSION; }
 
 extern "C" int mpcd_destroy(mpcd_handle *h) {

@@ -47,7 +47,7 @@ __device__ __forceinline__ int block_excl_scan256(int x, int &total) {
 }
 
 // Sum of each tile of counts.
-__global__ void __launch_bounds__(256) k_scan_partial(const int *count, int ncells,
+static __global__ void __launch_bounds__(256) k_scan_partial(const int *count, int ncells,
                                                       int *part) {
     int base = blockIdx.x * kScanTile;
     int local = 0;
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256) k_scan_partial(const int *count, int ncel
 // Exclusive scan of the counts into start[0..ncells]; zeroes the counts
 // (and the fill cursors, if given) for reuse, and the accumulators of the
 // step that will use these starts.
-__global__ void __launch_bounds__(256) k_scan_apply(int *count, int ncells,
+static __global__ void __launch_bounds__(256) k_scan_apply(int *count, int ncells,
                                                     const int *part, int *start,
                                                     int *fill, double *acc) {
     // offset of this block: sum of the partial sums of the blocks before it,

@@ -221,7 +221,7 @@ __device__ void lc_cell_moments(const DevCfg &c, const typename T::State &a, con
 }
 
 // bulk D2Q9 gradient of cells 1..L-1 in x and y
-__global__ void __launch_bounds__(256) k_lc_grad(const __grid_constant__ DevCfg c, LcCells lc) {
+static __global__ void __launch_bounds__(256) k_lc_grad(const __grid_constant__ DevCfg c, LcCells lc) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     const int nb = (c.L[0] - 1) * (c.L[1] - 1);
     if (id >= nb) return;
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256) k_lc_grad(const __grid_constant__ DevCfg 
 
 // edge copies: pass 0 the x-edges (a = 0 and a = L for b < L), pass 1 the
 // y-edges (b = 0 and b = L for a < L)
-__global__ void __launch_bounds__(256) k_lc_edges(const __grid_constant__ DevCfg c, LcCells lc,
+static __global__ void __launch_bounds__(256) k_lc_edges(const __grid_constant__ DevCfg c, LcCells lc,
                                                   int pass) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (pass == 0) {

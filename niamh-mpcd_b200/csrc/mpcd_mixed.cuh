@@ -143,7 +143,7 @@ __host__ __device__ __forceinline__ void fx_from_double(double q, int &ci, uint3
     f = (uint32_t)r;
 }
 
-__global__ void __launch_bounds__(256) k_scatter_mix(MixState a, MixState b, int n,
+static __global__ void __launch_bounds__(256) k_scatter_mix(MixState a, MixState b, int n,
                                                      const int *key, const int *rank,
                                                      const int *start) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

@@ -20,6 +20,7 @@ EXPORTS = [
     "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
+    "mpcd_srd_step_noalloc",
 ]
 
 _lib = None
@@ -54,6 +55,7 @@ def load():
         lib.mpcd_launches_per_step.argtypes = [vp]
         lib.mpcd_set_strategy.argtypes = [vp, C.c_int, C.c_int]
         lib.mpcd_set_kernel.argtypes = [vp, C.c_int]
+        lib.mpcd_srd_step_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_uint32, vp, vp]
         _lib = lib
     return _lib
 
@@ -65,6 +67,17 @@ def _check(r, what):
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def srd_step_noalloc(cfg, n, q_dev_ptr, v_dev_ptr, step, globals_dev_ptr=None, stream=None):
+    """One SRD timestep on caller-owned device arrays (AoS, 3 doubles per
+    particle) with no allocation (mpcd_srd_step_noalloc)."""
+    lib = load()
+    _check(lib.mpcd_srd_step_noalloc(C.byref(cfg), n, C.c_void_p(q_dev_ptr),
+                                     C.c_void_p(v_dev_ptr), step,
+                                     C.c_void_p(globals_dev_ptr) if globals_dev_ptr else None,
+                                     C.c_void_p(stream) if stream else None),
+           "mpcd_srd_step_noalloc")
 
 
 class Solver:
