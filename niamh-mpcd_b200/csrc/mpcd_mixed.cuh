@@ -103,6 +103,15 @@ __device__ __forceinline__ int fx_shift_axis(int ci, uint32_t f, uint32_t k, int
     return a;
 }
 
+// fx_shift_axis for a periodic axis and a cell index in [0, L): the shifted
+// cell is ci + carry, index L wrapping to 0 (both the gridShift wrap and
+// bin's L -> 0 rule reduce to this).
+__device__ __forceinline__ int fx_shift_axis_pbc(int ci, uint32_t f, uint32_t k, int L) {
+    const uint32_t t = f + k;
+    const int a = ci + (t < f ? 1 : 0);
+    return a == L ? 0 : a;
+}
+
 // Position of record p on the shifted grid relative to the origin of its
 // shifted cell, in cell units (exact in FP64).
 template <int DIM>
