@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define MPCD_ABI_VERSION 2
+#define MPCD_ABI_VERSION 1
 
 #define MPCD_MAX_SPECIES 10 /* reference MAXSPECI, definitions.h:66 */
 #define MPCD_MAX_WALLS 16
@@ -138,8 +138,6 @@ typedef struct mpcd_status {
     uint64_t nonfinite;     /* non-finite velocities seen by the step       */
     uint64_t overflow;      /* particles of cells too populous for one tile
                                (streamed without collision)                 */
-    uint64_t sync_timeout;  /* bounded inter-block waits that gave up (the
-                               step's cell starts are then invalid)         */
 } mpcd_status;
 
 typedef struct mpcd_handle mpcd_handle;

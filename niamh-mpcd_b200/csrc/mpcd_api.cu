@@ -35,13 +35,12 @@ struct mpcd_handle {
     MixState mx[2];  // mixed state, two buffers
     int cur;
     int *key, *rank, *count, *fill, *start[2], *part;
-    unsigned long long *scan_tiles;   // look-back words, one per scan tile
-    unsigned long long *scan_ticket;  // scan tile ticket counter (never reset)
     int scur;        // which start[] belongs to the current order
     double *acc;     // 2 x ACC_WORDS, by step parity
     unsigned long long *status;
     int nscan;
     int sm_count;
+    int smem_optin;  // largest dynamic shared memory a block may opt in to
     int launches;
     int strategy;    // MPCD_STRATEGY_*
     int tile_target; // expected particles per tile
@@ -219,8 +218,6 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->start[0]);
     cudaFree(h->start[1]);
     cudaFree(h->part);
-    cudaFree(h->scan_tiles);
-    cudaFree(h->scan_ticket);
     cudaFree(h->acc);
     cudaFree(h->status);
     cudaFree(h->crec);
@@ -251,6 +248,7 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     h->prec = cfg->precision;
     cudaGetDevice(&h->device);
     cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
+    cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
         return MPCD_ERR_CUDA;
@@ -263,8 +261,6 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     ALLOC(h->start[0], sizeof(int) * (nc + 1));
     ALLOC(h->start[1], sizeof(int) * (nc + 1));
     ALLOC(h->part, sizeof(int) * h->nscan);
-    ALLOC(h->scan_tiles, sizeof(unsigned long long) * h->nscan);
-    ALLOC(h->scan_ticket, sizeof(unsigned long long));
     ALLOC(h->acc, sizeof(double) * 2 * ACC_WORDS);
     ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
     ALLOC(h->crec, (size_t)nc * 128);
@@ -288,10 +284,6 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     h->strategy = -1;
     h->tile_target = 0;
     if (cudaMemsetAsync(h->count, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
-        cudaMemsetAsync(h->scan_tiles, 0, sizeof(unsigned long long) * h->nscan, h->stream) !=
-            cudaSuccess ||
-        cudaMemsetAsync(h->scan_ticket, 0, sizeof(unsigned long long), h->stream) !=
-            cudaSuccess ||
         cudaMemsetAsync(h->fill, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
         cudaMemsetAsync(h->status, 0, sizeof(unsigned long long) * ST_WORDS, h->stream) !=
             cudaSuccess ||
@@ -550,6 +542,11 @@ template <int DIM, class T>
 static int launch_group(mpcd_handle *h, int mode, const typename T::State &a,
                         const typename T::State &b, const TileBufs &tb, const StepArgs &sa) {
     int capw = group_capacity(h);
+    // clamp the staging capacity to what a block may hold (larger groups
+    // report overflow)
+    while (capw > 32 &&
+           GroupLayout<T>::kWarps * GroupLayout<T>::per_warp_bytes(capw) > h->smem_optin - 1024)
+        capw -= 32;
     int bytes = GroupLayout<T>::kWarps * GroupLayout<T>::per_warp_bytes(capw);
     int groups = (h->dc.ncells + 31) / 32;
     int grid = (groups + GroupLayout<T>::kWarps - 1) / GroupLayout<T>::kWarps;
@@ -585,17 +582,9 @@ static int kernel_family(const mpcd_handle *h) {
 template <int DIM, class T>
 static int launch_srd_cells(mpcd_handle *h, const typename T::State &a, const int *start,
                             const StepArgs &sa, double *acc) {
-    // warp per 32 cells with the group's velocities staged in shared memory
-    int capw = group_capacity(h);
-    int bytes = 8 * capw * (int)sizeof(typename CellStage<T>::S);
-    int groups = (h->dc.ncells + 31) / 32;
-    int grid = (groups + 7) / 8;
-    auto kfn = k_srd_cells_w<DIM, T>;
-    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-        cudaSuccess)
-        return MPCD_ERR_CUDA;
-    kfn<<<grid, 256, bytes, h->stream>>>(h->dc, a, start,
-                                         (typename SrdCell<T>::Rec *)h->crec, sa, acc, capw);
+    int grid = (h->dc.ncells + 255) / 256;
+    k_srd_cells<DIM, T><<<grid, 256, 0, h->stream>>>(
+        h->dc, a, start, (typename SrdCell<T>::Rec *)h->crec, sa, acc);
     return cudaGetLastError() == cudaSuccess ? MPCD_OK : MPCD_ERR_CUDA;
 }
 
@@ -652,9 +641,9 @@ static int launch_tile(mpcd_handle *h, int mode, const typename T::State &a,
 }
 
 static void launch_scan(mpcd_handle *h, int *start, int *fill, double *acc_zero) {
-    k_scan_lookback<<<h->nscan, 256, 0, h->stream>>>(h->count, h->dc.ncells, start, fill,
-                                                      acc_zero, h->scan_tiles, h->scan_ticket,
-                                                      h->status, ST_SCAN);
+    k_scan_partial<<<h->nscan, 256, 0, h->stream>>>(h->count, h->dc.ncells, h->part);
+    k_scan_apply<<<h->nscan, 256, 0, h->stream>>>(h->count, h->dc.ncells, h->part, start,
+                                                   fill, acc_zero);
 }
 
 template <int DIM, class T>
@@ -905,7 +894,6 @@ extern "C" int mpcd_get_status(mpcd_handle *h, mpcd_status *st) {
     st->bounce_limit = w[ST_BOUNCE];
     st->nonfinite = w[ST_NONFINITE];
     st->overflow = w[ST_OVERFLOW];
-    st->sync_timeout = w[ST_SCAN];
     return MPCD_OK;
 }
 

@@ -27,7 +27,7 @@ constexpr double kTol = 1e-8;  // reference TOL, definitions.h:56
 constexpr int kNBounce = 50;   // reference NBOUNCE, definitions.h:62
 
 // Status counters (device, uint64): index into DevStatus words.
-enum { ST_ESCAPED = 0, ST_BOUNCE = 1, ST_NONFINITE = 2, ST_SCAN = 4, ST_WORDS = 5 };
+enum { ST_ESCAPED = 0, ST_BOUNCE = 1, ST_NONFINITE = 2, ST_WORDS = 4 };
 
 // Per-step global accumulators: [0] sum m v^2 (TEMP), [1..3] sum VCM (avVel)
 enum { ACC_KE = 0, ACC_VCM = 1, ACC_WORDS = 4 };

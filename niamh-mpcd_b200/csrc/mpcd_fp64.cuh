@@ -8,8 +8,6 @@
 //   into the cell start offsets of the sorted order.
 #pragma once
 
-#include <cuda/atomic>
-
 #include "mpcd_device.cuh"
 
 namespace mpcd {
@@ -96,91 +94,6 @@ static __global__ void __launch_bounds__(256) k_scan_apply(int *count, int ncell
         pre += v[j];
     }
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 255) start[ncells] = pre;
-}
-
-// Single-pass exclusive scan of the counts (decoupled look-back).  Each block
-// takes the next tile from a 64-bit ticket counter that is never reset: the
-// ticket gives the tile (ticket mod tiles) and the launch's epoch (ticket div
-// tiles), so the kernel needs no host-side state and replays unchanged inside
-// a CUDA graph.  Tickets are handed out in the order blocks start, so every
-// tile's predecessors are already running.  A tile publishes its sum, walks
-// back over its predecessors' published words adding sums until it meets a
-// published inclusive prefix, publishes its own inclusive prefix and writes
-// its starts.  Word layout: bits 62-63 flag (1 sum, 2 prefix), 32-61 epoch,
-// 0-31 value.  Every wait is bounded: after kScanSpin polls the block records
-// the timeout in status[status_word] and carries on (the starts are then
-// wrong and the step is reported failed).
-constexpr unsigned long long kScanFlagA = 1ull << 62, kScanFlagP = 2ull << 62;
-constexpr int kScanSpin = 1 << 22;
-
-static __global__ void __launch_bounds__(256) k_scan_lookback(
-    int *count, int ncells, int *start, int *fill, double *acc, unsigned long long *tstat,
-    unsigned long long *ticket, unsigned long long *status, int status_word) {
-    __shared__ int s_tile, s_off;
-    __shared__ unsigned long long s_ep;
-    const unsigned ntiles = gridDim.x;
-    if (threadIdx.x == 0) {
-        const unsigned long long t = atomicAdd(ticket, 1ull);
-        s_tile = (int)(t % ntiles);
-        s_ep = ((t / ntiles) & 0x3FFFFFFFull) << 32;
-    }
-    __syncthreads();
-    const int tile = s_tile;
-    const int base = tile * kScanTile + threadIdx.x * 8;
-    int v[8], sum = 0;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-        const int idx = base + j;
-        v[j] = idx < ncells ? count[idx] : 0;
-        sum += v[j];
-    }
-    int agg;
-    int pre = block_excl_scan256(sum, agg);
-    if (threadIdx.x == 0) {
-        const unsigned long long ep = s_ep;
-        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me(tstat[tile]);
-        int prefix = 0;
-        if (tile == 0) {
-            me.store(kScanFlagP | ep | (unsigned)agg, cuda::memory_order_release);
-        } else {
-            me.store(kScanFlagA | ep | (unsigned)agg, cuda::memory_order_release);
-            bool timed_out = false;
-            for (int t = tile - 1; t >= 0; t--) {
-                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> w(tstat[t]);
-                unsigned long long x = w.load(cuda::memory_order_acquire);
-                int spins = 0;
-                while ((x & 0x3FFFFFFF00000000ull) != ep || (x >> 62) == 0) {
-                    if (++spins > kScanSpin) {
-                        timed_out = true;
-                        break;
-                    }
-                    __nanosleep(32);
-                    x = w.load(cuda::memory_order_acquire);
-                }
-                if (timed_out) break;
-                prefix += (int)(unsigned)(x & 0xFFFFFFFFull);
-                if ((x >> 62) == 2) break;
-            }
-            if (timed_out) atomicAdd(&status[status_word], 1ull);
-            me.store(kScanFlagP | ep | (unsigned)(prefix + agg), cuda::memory_order_release);
-        }
-        s_off = prefix;
-        if (acc && tile == 0)
-            for (int k = 0; k < ACC_WORDS; k++) acc[k] = 0.0;
-        if (tile == (int)ntiles - 1) start[ncells] = prefix + agg;
-    }
-    __syncthreads();
-    pre += s_off;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-        const int idx = base + j;
-        if (idx < ncells) {
-            start[idx] = pre;
-            count[idx] = 0;
-            if (fill) fill[idx] = 0;
-        }
-        pre += v[j];
-    }
 }
 
 }  // namespace mpcd

@@ -114,105 +114,6 @@ __global__ void __launch_bounds__(256) k_srd_cells(const __grid_constant__ DevCf
     }
 }
 
-// Warp-cooperative cell pass: one warp per group of 32 consecutive cells.
-// The group's velocities (contiguous in the sorted order) are loaded with
-// coalesced loads into the warp's shared memory, then lane l reduces cell l.
-// A group larger than the staging area is reduced from global memory.
-template <class T>
-struct CellStage;
-template <int DIM>
-struct CellStage<MixT<DIM>> {
-    using S = float4;
-    static __device__ __forceinline__ S load(const DevCfg &c, const MixState &st, int i) {
-        float4 w = st.W[i];
-        if (c.grav_flag) {
-            w.x += (float)(c.dt * c.grav[0]);
-            w.y += (float)(c.dt * c.grav[1]);
-            if (DIM == 3) w.z += (float)(c.dt * c.grav[2]);
-        }
-        return w;
-    }
-    static __device__ __forceinline__ void vel(const S &w, double v[3]) {
-        v[0] = w.x;
-        v[1] = w.y;
-        v[2] = DIM == 3 ? (double)w.z : 0.0;
-    }
-};
-template <int DIM>
-struct CellStage<F64T<DIM>> {
-    struct S {
-        double v[3];
-    };
-    static __device__ __forceinline__ S load(const DevCfg &c, const Fp64State &st, int i) {
-        S s;
-        SrdCell<F64T<DIM>>::vel(st, i, c, s.v);
-        return s;
-    }
-    static __device__ __forceinline__ void vel(const S &w, double v[3]) {
-        v[0] = w.v[0];
-        v[1] = w.v[1];
-        v[2] = w.v[2];
-    }
-};
-
-template <int DIM, class T>
-__global__ void __launch_bounds__(256) k_srd_cells_w(const __grid_constant__ DevCfg c,
-                                                     typename T::State a, const int *start,
-                                                     typename SrdCell<T>::Rec *crec,
-                                                     StepArgs sa, double *acc, int capw) {
-    using VT = typename T::VT;
-    using CS = CellStage<T>;
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double red[8];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    typename CS::S *sv = (typename CS::S *)smem + (size_t)wib * capw;
-    const int g0 = (blockIdx.x * (blockDim.x >> 5) + wib) * 32;
-    double av[3] = {0, 0, 0};
-    if (g0 < c.ncells) {
-        const int ncg = min(32, c.ncells - g0);
-        const int my_s = lane < ncg ? start[g0 + lane] : 0;
-        const int my_e = lane < ncg ? start[g0 + lane + 1] : 0;
-        const int base = __shfl_sync(0xffffffffu, my_s, 0);
-        const int pend = __shfl_sync(0xffffffffu, my_e, ncg - 1);
-        const int np = pend - base;
-        const bool staged = np <= capw;
-        if (staged)
-            for (int j = lane; j < np; j += 32) sv[j] = CS::load(c, a, base + j);
-        __syncwarp();
-        if (lane < ncg) {
-            const int cell = g0 + lane, pop = my_e - my_s;
-            double M = 0.0, pv[3] = {0, 0, 0};
-            for (int j = my_s; j < my_e; j++) {
-                double m = c.mass[T::sp(a, j)];
-                double v[3];
-                if (staged)
-                    CS::vel(sv[j - base], v);
-                else
-                    SrdCell<T>::vel(a, j, c, v);
-                M += m;
-                for (int d = 0; d < DIM; d++) pv[d] += v[d] * m;
-            }
-            double u[3] = {0, 0, 0};
-            if (M > 0.0) {
-                const double iM = 1.0 / M;
-                for (int d = 0; d < DIM; d++) u[d] = pv[d] * iM;
-            }
-            for (int d = 0; d < DIM; d++) av[d] = u[d];
-            VT R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            if (pop > 1) {
-                double Lx[3] = {0, 0, 1};
-                if (DIM == 3) mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
-                srd_matrix<DIM, VT>(c, Lx, R);
-            }
-            SrdCell<T>::put(crec, cell, u, pop, R);
-        }
-    }
-    for (int d = 0; d < DIM; d++) {
-        double t = block_sum256(av[d], red);
-        if (threadIdx.x == 0) atomicAdd(&acc[ACC_VCM + d], t);
-    }
-}
-
 // Current-step cell key of a particle from its stored position.
 template <int DIM>
 __device__ __forceinline__ int cur_key(const DevCfg &c, const MixRec &r, const StepArgs &sa) {
@@ -236,7 +137,7 @@ __device__ __forceinline__ int cur_key(const DevCfg &c, const F64Rec &r, const S
 }
 
 #ifndef MPCD_SPLIT_MINB
-#define MPCD_SPLIT_MINB 1  // minimum resident blocks per SM of the particle pass
+#define MPCD_SPLIT_MINB 4  // minimum resident blocks per SM of the particle pass
 #endif
 
 template <int DIM, class T, int MODE>
@@ -292,16 +193,30 @@ __global__ void __launch_bounds__(256, MPCD_SPLIT_MINB) k_srd_parts(const __grid
             }
         }
         const int k = T::finish(c, r, sp, sa, bounce, esc);
-        if (MODE == MODE_INPLACE) {
-            T::store(a, i, r);
-            tb.key[i] = k;
-            tb.rank[i] = atomicAdd(&tb.count_next[k], 1);
-        } else if (MODE == MODE_COUNT) {
-            atomicAdd(&tb.count_next[k], 1);
+        // warp-aggregated counting: lanes with the same next cell take one
+        // atomic (particles of a cell are adjacent and mostly move together)
+        const unsigned act = __activemask();
+        const unsigned peers = __match_any_sync(act, k);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        const int below = __popc(peers & ((1u << lane) - 1u));
+        if (MODE == MODE_COUNT) {
+            if (lane == leader) atomicAdd(&tb.count_next[k], __popc(peers));
         } else {
-            const int dst = tb.start_next[k] + atomicAdd(&tb.fill[k], 1);
-            T::store(b, dst, r);
-            T::store_sp(b, dst, sp);
+            int base = 0;
+            if (lane == leader)
+                base = atomicAdd(MODE == MODE_INPLACE ? &tb.count_next[k] : &tb.fill[k],
+                                 __popc(peers));
+            base = __shfl_sync(peers, base, leader) + below;
+            if (MODE == MODE_INPLACE) {
+                T::store(a, i, r);
+                tb.key[i] = k;
+                tb.rank[i] = base;
+            } else {
+                const int dst = tb.start_next[k] + base;
+                T::store(b, dst, r);
+                T::store_sp(b, dst, sp);
+            }
         }
     }
     if (MODE != MODE_COUNT) {

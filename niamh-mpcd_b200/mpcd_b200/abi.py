@@ -115,7 +115,6 @@ class Status(C.Structure):
         ("bounce_limit", C.c_uint64),
         ("nonfinite", C.c_uint64),
         ("overflow", C.c_uint64),
-        ("sync_timeout", C.c_uint64),
     ]
 
 

@@ -41,7 +41,7 @@ def test_fp64_matches_oracle(name):
         assert kg == pytest.approx(ko, rel=1e-12)
         np.testing.assert_allclose(ag, ao, rtol=0, atol=1e-13)
     st = g.status()
-    assert st.escaped == 0 and st.bounce_limit == 0 and st.sync_timeout == 0
+    assert st.escaped == 0 and st.bounce_limit == 0
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
