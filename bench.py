@@ -20,7 +20,7 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -39,7 +39,7 @@ WORKLOAD = "3D SRD fluid, periodic 64^3 cells, 10 particles/cell (2,621,440), ro
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--strategy", type=int, default=-1,
                     help="-1 default, 0 scatter, 1 recompute")
     ap.add_argument("--tile", type=int, default=0, help="particles per tile (0 default)")
+    ap.add_argument("--kernel", type=int, default=0,
+                    help="cell-kernel family: 0 auto, 1 tile, 2 group, 3 split, 4 resident")
+    ap.add_argument("--sort-interval", type=int, default=0,
+                    help="resident family: steps between re-sorts (0 = library default)")
     return ap.parse_args()
 
 
@@ -62,36 +66,52 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling (every 200 ms) around the timed region: a reader
+    thread stamps each sample with the host clock on arrival, and stop()
+    keeps the samples that arrived inside [t0, t1] (the nearest one if the
+    region was shorter than a sampling period)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
-        self.idx = gpu_index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.samples = []
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=self.f, stderr=subprocess.DEVNULL)
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
 
-    def stop(self):
+    def _read(self):
+        for line in self.p.stdout:
+            self.samples.append((time.time(), line))
+
+    def wait_ready(self, timeout=15.0):
+        t0 = time.time()
+        while self.p is not None and not self.samples and time.time() - t0 < timeout:
+            time.sleep(0.05)
+
+    def stop(self, t0, t1):
         if self.p is None:
             return None
+        time.sleep(0.25)  # let the sample that covers t1 arrive
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
-        self.f.flush()
-        self.f.seek(0)
+        inside = [s for s in self.samples if t0 <= s[0] <= t1 + 0.2]
+        if not inside and self.samples:
+            inside = [min(self.samples, key=lambda s: abs(s[0] - 0.5 * (t0 + t1)))]
         sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f.read().splitlines():
+        for _, line in inside:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -100,14 +120,14 @@ class Clocks:
                 smax = max(smax, float(parts[2]))
             except ValueError:
                 continue
-            for nm, val in zip(names, parts[5:9]):
+            for nm, val in zip(self.NAMES, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
-        os.unlink(self.f.name)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "timed_region_s": round(t1 - t0, 3)}
 
 
 def run_gpu(args, rank, world):
@@ -132,24 +152,31 @@ def run_gpu(args, rank, world):
         g = Solver(cfg)
         g.set_stream(stream.cuda_stream)
         g.set_strategy(args.strategy, args.tile)
+        g.set_kernel(args.kernel)
+        if args.sort_interval > 0:
+            g.set_sort_interval(args.sort_interval)
         g.upload(Q, V, U, sp)
         g.step(args.warmup, 1)
         torch.cuda.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
+        clk = Clocks(dev) if form == "mixed" else None
+        if clk:
+            clk.wait_ready()
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
-        clk = Clocks(dev) if form == "mixed" else None
+        t_begin = time.time()
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
             g.step(1, 1 + args.warmup + k)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
+        t_end = time.time()
         if world > 1:
             torch.distributed.barrier()
-        clocks = clk.stop() if clk else None
+        clocks = clk.stop(t_begin, t_end) if clk else None
         ms = [a.elapsed_time(b) for a, b in ev]
         total_ms = float(sum(ms))
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define MPCD_ABI_VERSION 1
+#define MPCD_ABI_VERSION 2
 
 #define MPCD_MAX_SPECIES 10 /* reference MAXSPECI, definitions.h:66 */
 #define MPCD_MAX_WALLS 16
@@ -138,6 +138,8 @@ typedef struct mpcd_status {
     uint64_t nonfinite;     /* non-finite velocities seen by the step       */
     uint64_t overflow;      /* particles of cells too populous for one tile
                                (streamed without collision)                 */
+    uint64_t sync_timeout;  /* bounded waits inside a kernel that gave up
+                               (the step's results are then invalid)       */
 } mpcd_status;
 
 typedef struct mpcd_handle mpcd_handle;
@@ -218,19 +220,33 @@ int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
 
 /* Cell-kernel family (no counterpart in the reference).  For the SRD
  * operator without phantom walls:
- *   MPCD_KERNEL_SPLIT  a thread-per-cell pass writes each cell's centre-of-
- *                      mass velocity and rotation, then a thread-per-particle
- *                      pass collides, streams and re-bins (the default);
+ *   MPCD_KERNEL_RESIDENT (mixed precision) the particles stay in place: a
+ *                      thread-per-cell pass turns the cell sums into each
+ *                      cell's centre-of-mass velocity and rotation, and a
+ *                      thread-per-particle pass collides, streams, writes the
+ *                      particle back and adds it, in 64-bit fixed point, to
+ *                      the next step's cell sums (the default for mixed;
+ *                      results do not depend on the particle order);
+ *   MPCD_KERNEL_SPLIT  the same two passes over a state kept sorted by cell,
+ *                      re-binned every step (the default for FP64);
  *   MPCD_KERNEL_GROUP  one warp per group of 32 cells does both, staging the
  *                      group in shared memory;
  *   MPCD_KERNEL_TILE   one block per tile of cells (the kernel every other
  *                      operator uses).
- * MPCD_KERNEL_AUTO picks SPLIT where it applies and TILE elsewhere. */
+ * MPCD_KERNEL_AUTO picks RESIDENT (mixed) or SPLIT (FP64) where they apply
+ * and TILE elsewhere; RESIDENT asked for in FP64 runs SPLIT. */
 #define MPCD_KERNEL_AUTO 0
 #define MPCD_KERNEL_TILE 1
 #define MPCD_KERNEL_GROUP 2
 #define MPCD_KERNEL_SPLIT 3
+#define MPCD_KERNEL_RESIDENT 4
 int mpcd_set_kernel(mpcd_handle *h, int kernel);
+
+/* MPCD_KERNEL_RESIDENT re-sorts the state by cell every 'steps' steps
+ * (default 20) to keep particles that are close in space close in memory;
+ * the sort changes no result, only the speed.  No counterpart in the
+ * reference. */
+int mpcd_set_sort_interval(mpcd_handle *h, int steps);
 
 /* One SRD timestep that allocates no memory, device or host (no
  * counterpart in the reference, whose timestep works on host memory).  For

@@ -5,6 +5,7 @@
 // count/start arrays and the per-step accumulators, all on one CUDA stream.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -18,6 +19,7 @@
 #include "mpcd_tile.cuh"
 #include "mpcd_group.cuh"
 #include "mpcd_split.cuh"
+#include "mpcd_resident.cuh"
 #include "mpcd_lc.cuh"
 
 using namespace mpcd;
@@ -49,6 +51,11 @@ struct mpcd_handle {
     LcCells lcc;     // per-cell nematic arrays (lc != 0)
     double *lcbuf;
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
+    ResSum *rsum;              // resident family: cell sums, two steps by parity
+    unsigned long long *rmsum;  // resident family: mass sums (several species)
+    int64_t sums_for;          // step whose cell sums rsum holds; -1 none
+    int sort_interval;         // resident family: steps between re-sorts
+    int sort_age;              // steps since the last sort; -1 unknown
     uint32_t last_step;
     uint64_t steps;
     double *host_acc;  // pinned
@@ -189,6 +196,34 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     dc->all_periodic = dc->n_solid == 0;
     for (int d = 0; d < cfg->dim; d++)
         if (!dc->pbc[d]) dc->all_periodic = 0;
+    {
+        // slot bit fields for the resident family's tables: the fastest
+        // axis of the linear cell order gets most bits, the next (3D) up to
+        // 3, the slowest the rest, so that the cells a block of particles
+        // (sorted by cell) lands in map to distinct, mostly consecutive
+        // slots (consecutive slots: distinct shared-memory banks)
+        auto clog2 = [](int x) {
+            int b = 0;
+            while ((1 << b) < x) b++;
+            return b;
+        };
+        int bits[3] = {0, 0, 0};
+        if (dc->dim == 3) {
+            bits[2] = std::min(clog2(dc->L[2]), kResBits - 4);
+            bits[1] = std::min(3, clog2(dc->L[1]));
+            bits[0] = kResBits - bits[2] - bits[1];
+            dc->res_shift[2] = 0;
+            dc->res_shift[1] = bits[2];
+            dc->res_shift[0] = bits[2] + bits[1];
+        } else {
+            bits[1] = std::min(clog2(dc->L[1]), kResBits - 2);
+            bits[0] = kResBits - bits[1];
+            dc->res_shift[1] = 0;
+            dc->res_shift[0] = bits[1];
+            dc->res_shift[2] = 0;
+        }
+        for (int d = 0; d < 3; d++) dc->res_mask[d] = (1 << bits[d]) - 1;
+    }
     return MPCD_OK;
 }
 
@@ -221,6 +256,8 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->acc);
     cudaFree(h->status);
     cudaFree(h->crec);
+    cudaFree(h->rsum);
+    cudaFree(h->rmsum);
     cudaFree(h->lcbuf);
     if (h->host_acc) cudaFreeHost(h->host_acc);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -264,6 +301,10 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     ALLOC(h->acc, sizeof(double) * 2 * ACC_WORDS);
     ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
     ALLOC(h->crec, (size_t)nc * 128);
+    if (cfg->precision == MPCD_PREC_MIXED && !dc.lc) {
+        ALLOC(h->rsum, sizeof(ResSum) * 2 * (size_t)nc);
+        if (dc.n_species > 1) ALLOC(h->rmsum, sizeof(unsigned long long) * 2 * (size_t)nc);
+    }
     if (dc.lc) {
         ALLOC(h->lcbuf, (size_t)nc * 13 * sizeof(double));
         if (cudaMemsetAsync(h->lcbuf, 0, (size_t)nc * 13 * sizeof(double), h->stream) !=
@@ -281,6 +322,9 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
         h->lcc.E = b + 9 * (size_t)nc;
     }
     h->sorted_for = -1;
+    h->sums_for = -1;
+    h->sort_interval = 20;
+    h->sort_age = -1;
     h->strategy = -1;
     h->tile_target = 0;
     if (cudaMemsetAsync(h->count, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
@@ -359,6 +403,8 @@ static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V
     h->n = n;
     h->cur = 0;
     h->sorted_for = -1;
+    h->sums_for = -1;
+    h->sort_age = -1;
     // global number density as globalDensities (init.c:1002-1018) unless given
     if (!(h->cfg.gndnst > 0.0)) {
         std::vector<int> pop((size_t)h->dc.ncells, 0);
@@ -574,9 +620,12 @@ static int launch_group(mpcd_handle *h, int mode, const typename T::State &a,
 }
 
 static int kernel_family(const mpcd_handle *h) {
-    bool srd_plain = h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom;
+    bool srd_plain = h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom && !h->dc.lc;
     if (!srd_plain) return MPCD_KERNEL_TILE;
-    return h->kernel == MPCD_KERNEL_AUTO ? MPCD_KERNEL_SPLIT : h->kernel;
+    const bool mixed = h->prec == MPCD_PREC_MIXED;
+    if (h->kernel == MPCD_KERNEL_AUTO) return mixed ? MPCD_KERNEL_RESIDENT : MPCD_KERNEL_SPLIT;
+    if (h->kernel == MPCD_KERNEL_RESIDENT && !mixed) return MPCD_KERNEL_SPLIT;
+    return h->kernel;
 }
 
 template <int DIM, class T>
@@ -746,6 +795,72 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
     h->cur = 1 - h->cur;
     h->scur = 1 - h->scur;
     h->sorted_for = (int64_t)step + 1;
+    h->sums_for = -1;
+    h->launches = launches;
+    return MPCD_OK;
+}
+
+// One SRD timestep with the particles resident in place (mixed precision):
+// an occasional re-sort for locality, the cell pass and the particle pass.
+template <int DIM>
+static int run_step_res(mpcd_handle *h, uint32_t step) {
+    StepArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.step = step;
+    host_shift(h, step, sa.s);
+    host_shift(h, step + 1u, sa.sn);
+    for (int d = 0; d < 3; d++) {
+        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0);
+        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0);
+    }
+    const DevCfg &c = h->dc;
+    const size_t nc = (size_t)c.ncells;
+    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
+    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    ResSum *sum_cur = h->rsum + (step & 1u) * nc;
+    ResSum *sum_nxt = h->rsum + ((step + 1u) & 1u) * nc;
+    unsigned long long *ms_cur = h->rmsum ? h->rmsum + (step & 1u) * nc : nullptr;
+    unsigned long long *ms_nxt = h->rmsum ? h->rmsum + ((step + 1u) & 1u) * nc : nullptr;
+    int launches = 0;
+    if (h->sorted_for == (int64_t)step) {
+        h->sort_age = 0;
+    } else if (h->sort_age < 0 || h->sort_age >= h->sort_interval) {
+        launch_key<DIM, MixT<DIM>>(h, h->mx[h->cur], sa);
+        launch_scan(h, h->start[h->scur], nullptr, nullptr);
+        launch_scatter(h, h->mx[h->cur], h->mx[1 - h->cur], h->start[h->scur]);
+        h->cur = 1 - h->cur;
+        h->sort_age = 0;
+        launches += 4;
+    }
+    const int pgrid = (int)((h->n + kResChunk - 1) / kResChunk);
+    const int pbytes = res_table_bytes(h->rmsum ? DIM + 1 : DIM);
+    typedef ResRec CRec;
+    if (h->sums_for != (int64_t)step) {
+        CK(cudaMemsetAsync(h->rsum, 0, sizeof(ResSum) * 2 * nc, h->stream));
+        if (h->rmsum)
+            CK(cudaMemsetAsync(h->rmsum, 0, sizeof(unsigned long long) * 2 * nc, h->stream));
+        CK(cudaMemsetAsync(acc_cur, 0, sizeof(double) * ACC_WORDS, h->stream));
+        auto ksum = k_res_parts<DIM, RES_SUM>;
+        CK(cudaFuncSetAttribute(ksum, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
+        CK(cudaFuncSetAttribute(ksum, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        ksum<<<pgrid, kResThreads, pbytes, h->stream>>>(c, h->mx[h->cur], h->n,
+                                                        (const CRec *)h->crec, sum_cur, ms_cur,
+                                                        acc_cur, h->status, sa);
+        launches += 1;
+    }
+    k_res_cells<DIM><<<(int)((nc + 255) / 256), 256, 0, h->stream>>>(
+        c, sum_cur, ms_cur, (CRec *)h->crec, sa, acc_cur, acc_nxt);
+    auto kstep = k_res_parts<DIM, RES_STEP>;
+    CK(cudaFuncSetAttribute(kstep, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
+    CK(cudaFuncSetAttribute(kstep, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    kstep<<<pgrid, kResThreads, pbytes, h->stream>>>(c, h->mx[h->cur], h->n,
+                                                     (const CRec *)h->crec, sum_nxt, ms_nxt,
+                                                     acc_cur, h->status, sa);
+    launches += 2;
+    CK(cudaGetLastError());
+    h->sums_for = (int64_t)step + 1;
+    h->sorted_for = -1;
+    h->sort_age++;
     h->launches = launches;
     return MPCD_OK;
 }
@@ -818,6 +933,7 @@ static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
     h->cur = 1 - h->cur;
     h->scur = 1 - h->scur;
     h->sorted_for = (int64_t)step + 1;
+    h->sums_for = -1;
     h->launches = launches;
     return MPCD_OK;
 }
@@ -836,6 +952,8 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
         else if (h->prec == MPCD_PREC_FP64)
             r = h->dc.dim == 3 ? run_step<3, F64T<3>>(h, h->f, step)
                                : run_step<2, F64T<2>>(h, h->f, step);
+        else if (kernel_family(h) == MPCD_KERNEL_RESIDENT)
+            r = h->dc.dim == 3 ? run_step_res<3>(h, step) : run_step_res<2>(h, step);
         else
             r = h->dc.dim == 3 ? run_step<3, MixT<3>>(h, h->mx, step)
                                : run_step<2, MixT<2>>(h, h->mx, step);
@@ -847,8 +965,14 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
 }
 
 extern "C" int mpcd_set_kernel(mpcd_handle *h, int kernel) {
-    if (!h || kernel < MPCD_KERNEL_AUTO || kernel > MPCD_KERNEL_SPLIT) return MPCD_ERR_ARG;
+    if (!h || kernel < MPCD_KERNEL_AUTO || kernel > MPCD_KERNEL_RESIDENT) return MPCD_ERR_ARG;
     h->kernel = kernel;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_set_sort_interval(mpcd_handle *h, int steps) {
+    if (!h || steps < 1) return MPCD_ERR_ARG;
+    h->sort_interval = steps;
     return MPCD_OK;
 }
 
@@ -894,6 +1018,7 @@ extern "C" int mpcd_get_status(mpcd_handle *h, mpcd_status *st) {
     st->bounce_limit = w[ST_BOUNCE];
     st->nonfinite = w[ST_NONFINITE];
     st->overflow = w[ST_OVERFLOW];
+    st->sync_timeout = w[ST_SYNC];
     return MPCD_OK;
 }
 

@@ -27,7 +27,9 @@ constexpr double kTol = 1e-8;  // reference TOL, definitions.h:56
 constexpr int kNBounce = 50;   // reference NBOUNCE, definitions.h:62
 
 // Status counters (device, uint64): index into DevStatus words.
-enum { ST_ESCAPED = 0, ST_BOUNCE = 1, ST_NONFINITE = 2, ST_WORDS = 4 };
+// status words (ST_OVERFLOW = 3 is defined with the tile kernels); ST_SYNC
+// counts bounded waits inside a kernel that gave up
+enum { ST_ESCAPED = 0, ST_BOUNCE = 1, ST_NONFINITE = 2, ST_SYNC = 4, ST_WORDS = 5 };
 
 // Per-step global accumulators: [0] sum m v^2 (TEMP), [1..3] sum VCM (avVel)
 enum { ACC_KE = 0, ACC_VCM = 1, ACC_WORDS = 4 };
@@ -49,6 +51,9 @@ struct DevCfg {
     int n_solid;  // walls that are not periodic (mixed mode loops only these)
     int all_periodic;  // every axis periodic and no solid wall
     int grav_flag;
+    // per-axis bit fields of a cell's slot in the resident family's
+    // per-block table: slot = sum_d ((idx[d] & res_mask[d]) << res_shift[d])
+    int res_shift[3], res_mask[3];
     double dt, kbt, gndnst, vol;
     double cosA, sinA;  // cos(RA) and the sine with the reference's sign (-sin RA)
     double grav[3];

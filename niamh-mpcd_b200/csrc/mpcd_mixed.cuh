@@ -131,9 +131,35 @@ __device__ __forceinline__ void mix_rel(const DevCfg &c, const uint4 &p, const u
     }
 }
 
-// Stream one axis by the FP32 displacement dx: exact fixed-point add.
+// rint(v * 2^32) as two signed limbs, hi * 2^20 + lo with |lo| <= 2^19,
+// for |v| < 1024, from FP32 adds and multiplies and integer operations only
+// (no conversion instructions).  a = v 2^12 is exact; adding 1.5 * 2^23
+// rounds it to the nearest integer hi (ties to even), which the sum holds
+// in its low mantissa bits; f = a - hi is exact (Sterbenz) and in
+// [-1/2, 1/2], g = f 2^20 is exact, and lo = rint(g) by the same addition.
+// Since hi 2^20 is an even integer, rint(v 2^32) = hi 2^20 + rint(g), ties
+// included.  Returns false (limbs undefined) for |v| >= 1024 or non-finite v.
+__device__ __forceinline__ bool fx_limbs(float v, int &hi, int &lo) {
+    const float kMagic = 12582912.0f;  // 1.5 * 2^23
+    const float a = __fmul_rn(v, 4096.0f);
+    if (!(fabsf(a) < 4194304.0f)) return false;  // 2^22
+    const float s = __fadd_rn(a, kMagic);
+    const float r = __fadd_rn(s, -kMagic);
+    const float g = __fmul_rn(__fadd_rn(a, -r), 1048576.0f);
+    hi = __float_as_int(s) - 0x4B400000;
+    lo = __float_as_int(__fadd_rn(g, kMagic)) - 0x4B400000;
+    return true;
+}
+
+// Stream one axis by the FP32 displacement dx: exact fixed-point add of
+// rint(dx * 2^32).
 __device__ __forceinline__ void fx_stream(uint32_t &f, int &ci, float dx) {
-    const long long disp = __float2ll_rn(dx * 4294967296.0f);
+    int hi, lo;
+    long long disp;
+    if (fx_limbs(dx, hi, lo))
+        disp = (long long)hi * (1ll << 20) + (long long)lo;
+    else
+        disp = __float2ll_rn(dx * 4294967296.0f);
     const long long nq = (long long)f + disp;
     ci += (int)(nq >> 32);
     f = (uint32_t)nq;

@@ -1,0 +1,377 @@
+// mpcd_resident.cuh -- SRD step with the particles resident in place.
+//
+// The sorted kernel families move every particle every step (the counting
+// sort by next cell).  For the stochastic-rotation operator the sort is not
+// needed for the physics: a particle's collision needs only its cell's
+// centre-of-mass velocity u and rotation R.  This family keeps the particle
+// arrays in place and computes the cell sums by accumulation instead:
+//   k_res_cells  one thread per cell: reads the cell's sums (accumulated by
+//                the previous particle pass), forms u, the random axis and R
+//                (localPROP + stochrotMPC + rotate, mpc.c:64-216,
+//                1181-1333), writes the 64-byte cell record and clears the
+//                sums for reuse; avVel term.
+//   k_res_parts  one thread per particle: v' = u + R (v - u) from its cell's
+//                record, TEMP term, shift back / stream / walls / wrap, the
+//                new state written back in place, and its mass and momentum
+//                (with the next step's gravity kick) added to its cell on the
+//                NEXT step's shifted grid.
+// One step therefore reads and writes each particle's 32 bytes once.
+//
+// Sums are 64-bit fixed point (value * 2^32): integer addition is exact and
+// order-independent, so the sums -- and the whole step -- are bitwise
+// reproducible whatever the order of the atomics and whatever the particle
+// order in memory.  Each block first aggregates its chunk of particles in a
+// shared-memory hash table keyed by cell (bounded linear probing; a particle
+// that finds no slot adds straight to global memory), then adds each table
+// entry to global memory once.  Aggregation works because particles that
+// are close in memory are close in space: the state is re-sorted by cell
+// every few steps (the sort changes no result).
+#pragma once
+
+#include "mpcd_split.cuh"
+
+namespace mpcd {
+
+// The resident family's cell record, one 32-byte sector: {u.x, u.y, u.z,
+// population (int bits)} and {axis x, y, z, 0}.  The particle pass applies
+// the rotation about the axis in its Rodrigues form,
+//   R w = cos(a) w + (1 - cos(a)) (L . w) L + s (L x w),
+// which is the matrix of stochrotMPC/rotate (mpc.c:1181-1333, the sine s
+// with the reference's sign) applied to w.
+struct ResRec {
+    float4 a, b;
+};
+
+// Fixed-point cell sums: p = sum w v * 2^32 with w = 1 for one species
+// (the cell's momentum is then m p) and w = m for several species; n =
+// population.
+struct ResSum {
+    long long p[3];
+    long long n;
+};
+constexpr double kSumFx = 4294967296.0;  // 2^32
+constexpr double kSumFxInv = 2.3283064365386963e-10;
+constexpr double kSumLimit = 36028797018963968.0;  // 2^55: per-particle bound
+
+#ifndef MPCD_RES_SLOTS
+#define MPCD_RES_SLOTS 2048  // table slots per block (power of two)
+#endif
+#ifndef MPCD_RES_PPT
+#define MPCD_RES_PPT 8  // particles per thread
+#endif
+#ifndef MPCD_RES_MINB
+#define MPCD_RES_MINB 3  // minimum resident blocks per SM of the particle pass
+#endif
+constexpr int kResSlots = MPCD_RES_SLOTS;
+constexpr int res_log2(int x) { return x <= 1 ? 0 : 1 + res_log2(x >> 1); }
+constexpr int kResBits = res_log2(kResSlots);
+static_assert((1 << kResBits) == kResSlots, "hash slots must be a power of two");
+constexpr int kResThreads = 256;
+constexpr int kResChunk = kResThreads * MPCD_RES_PPT;  // particles per block
+static_assert(kResChunk <= 2048, "limb sums are sized for at most 2048 particles");
+constexpr int kResProbe = 32;
+// Inside a block the fixed-point values are summed as two signed 32-bit
+// limbs, x = hi * 2^20 + lo with |lo| <= 2^19 (fx_limbs), so that the
+// shared-memory atomics are native 32-bit integer operations (64-bit and
+// floating-point shared atomics are compare-and-swap loops).  For at most
+// 2048 particles per entry the limb sums cannot overflow while |x| < 2^40
+// (|w v| < 256); a larger value goes straight to the 64-bit global sums.
+constexpr int kLimb = 20;
+constexpr float kResBigV = 256.0f;
+
+// Per-block accumulation table in dynamic shared memory: keys,
+// populations, and per component the momentum limbs (row DIM: the mass
+// sum, several species only).  ncomp = DIM for one species, DIM + 1 for
+// several.
+struct ResTable {
+    int *key;
+    unsigned *cnt;
+    int *hi;  // [ncomp][kResSlots]
+    int *lo;  // [ncomp][kResSlots]
+    __device__ void bind(unsigned char *base, int ncomp) {
+        key = (int *)base;
+        cnt = (unsigned *)(key + kResSlots);
+        hi = (int *)(cnt + kResSlots);
+        lo = hi + ncomp * kResSlots;
+    }
+};
+__host__ __device__ constexpr int res_table_bytes(int ncomp) {
+    return kResSlots * (8 + 8 * ncomp);
+}
+
+__device__ __forceinline__ long long res_fix(double x, int &bad) {
+    if (!(fabs(x) < kSumLimit)) {
+        bad = 1;
+        return 0ll;
+    }
+    return __double2ll_rn(x);
+}
+
+__device__ __forceinline__ void res_global_add(ResSum *gs, unsigned long long *gm, int k,
+                                               const long long x[4], unsigned cnt, bool multi) {
+    unsigned long long *g = (unsigned long long *)&gs[k];
+    for (int d = 0; d < 3; d++)
+        if (x[d]) atomicAdd(g + d, (unsigned long long)x[d]);
+    atomicAdd(g + 3, (unsigned long long)cnt);
+    if (multi) atomicAdd(&gm[k], (unsigned long long)x[3]);
+}
+
+// Slot of key k (per-axis indices idx) in the block's table, inserting it,
+// or -1 if the bounded probe found none.  The first slot tried packs the
+// low bits of the indices (DevCfg::res_shift/res_mask).
+__device__ __forceinline__ int res_slot(ResTable &t, const DevCfg &c, int k, const int idx[3]) {
+    unsigned h = (unsigned)(((idx[0] & c.res_mask[0]) << c.res_shift[0]) |
+                            ((idx[1] & c.res_mask[1]) << c.res_shift[1]) |
+                            ((idx[2] & c.res_mask[2]) << c.res_shift[2]));
+    for (int probe = 0; probe < kResProbe; probe++) {
+        const int cur = *(volatile int *)&t.key[h];
+        if (cur == k) return (int)h;
+        if (cur == -1) {
+            const int old = atomicCAS(&t.key[h], -1, k);
+            if (old == -1 || old == k) return (int)h;
+        }
+        h = (h + 1u) & (unsigned)(kResSlots - 1);
+    }
+    return -1;
+}
+
+// Add one particle (velocity v, weight w = 1 or its mass) to cell k.
+template <int DIM>
+__device__ __forceinline__ void res_add(ResTable &t, const DevCfg &c, ResSum *sums,
+                                        unsigned long long *msum, int k, const int idx[3],
+                                        const float v[3], double w, bool multi, int &bad) {
+    const int nc = multi ? DIM + 1 : DIM;
+    int hi[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0};
+    bool fast = !multi && fabsf(v[0]) < kResBigV && fabsf(v[1]) < kResBigV &&
+                (DIM == 2 || fabsf(v[2]) < kResBigV);
+    if (fast) {
+        fx_limbs(v[0], hi[0], lo[0]);
+        fx_limbs(v[1], hi[1], lo[1]);
+        if (DIM == 3) fx_limbs(v[2], hi[2], lo[2]);
+    } else {
+        // several species (w = m) or a large velocity: FP64 conversion
+        const double wf = w * kSumFx;
+        long long x[4];
+        for (int d = 0; d < 3; d++) x[d] = d < DIM ? res_fix((double)v[d] * wf, bad) : 0ll;
+        x[3] = multi ? res_fix(wf, bad) : 0ll;
+        bool fits = true;
+        for (int d = 0; d < 4; d++) fits &= (x[d] < (1ll << 40) && x[d] > -(1ll << 40));
+        if (!fits) {
+            res_global_add(sums, msum, k, x, 1u, multi);
+            return;
+        }
+        for (int d = 0; d < 4; d++) {
+            const long long q = (x[d] + (1ll << 19)) >> kLimb;  // nearest multiple of 2^20
+            hi[d] = (int)q;
+            lo[d] = (int)(x[d] - q * (1ll << kLimb));
+        }
+    }
+    const int slot = res_slot(t, c, k, idx);
+    if (slot >= 0) {
+        atomicAdd(&t.cnt[slot], 1u);
+        for (int d = 0; d < nc; d++) {
+            const int dd = d == DIM ? 3 : d;  // row DIM: the mass limbs
+            atomicAdd(&t.hi[d * kResSlots + slot], hi[dd]);
+            atomicAdd(&t.lo[d * kResSlots + slot], lo[dd]);
+        }
+    } else {
+        long long x[4];
+        for (int d = 0; d < 4; d++) x[d] = (long long)hi[d] * (1ll << kLimb) + lo[d];
+        res_global_add(sums, msum, k, x, 1u, multi);
+    }
+}
+
+// Add every used table entry to the global sums.
+template <int DIM>
+__device__ __forceinline__ void res_flush(const ResTable &t, ResSum *sums,
+                                          unsigned long long *msum, bool multi) {
+    const int nc = multi ? DIM + 1 : DIM;
+    for (int s = threadIdx.x; s < kResSlots; s += blockDim.x) {
+        const int k = t.key[s];
+        if (k < 0) continue;
+        long long x[4] = {0, 0, 0, 0};
+        for (int d = 0; d < nc; d++) {
+            const int dd = d == DIM ? 3 : d;
+            x[dd] = (long long)t.hi[d * kResSlots + s] * (1ll << kLimb) +
+                    (long long)t.lo[d * kResSlots + s];
+        }
+        res_global_add(sums, msum, k, x, t.cnt[s], multi);
+    }
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Cell pass: sums of this step -> u, R record; the sums are cleared.  Block
+// 0 also clears the next step's accumulators.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCfg c,
+                                                   ResSum *sums, unsigned long long *msum,
+                                                   ResRec *crec, StepArgs sa, double *acc,
+                                                   double *acc_next) {
+    __shared__ float4 srec[2 * 256];
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    double av[3] = {0, 0, 0};
+    if (blockIdx.x == 0 && threadIdx.x < ACC_WORDS) acc_next[threadIdx.x] = 0.0;
+    if (cell < c.ncells) {
+        const ResSum s = sums[cell];
+        sums[cell] = ResSum{{0, 0, 0}, 0};
+        const int pop = (int)s.n;
+        double W;  // divisor of the weighted sum: population or mass
+        if (msum) {
+            W = (double)(long long)msum[cell] * kSumFxInv;
+            msum[cell] = 0ull;
+        } else {
+            W = (double)pop;
+        }
+        double u[3] = {0, 0, 0};
+        if (pop > 0 && W > 0.0) {
+            const double iW = 1.0 / W;
+            for (int d = 0; d < DIM; d++) u[d] = ((double)s.p[d] * kSumFxInv) * iW;
+        }
+        for (int d = 0; d < DIM; d++) av[d] = u[d];
+        double Lx[3] = {0, 0, 1};
+        if (pop > 1 && DIM == 3) mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
+        float4 *my = srec + 2 * threadIdx.x;
+        my[0] = make_float4((float)u[0], (float)u[1], (float)u[2], __int_as_float(pop));
+        my[1] = make_float4((float)Lx[0], (float)Lx[1], (float)Lx[2], 0.f);
+    }
+    __syncthreads();
+    {
+        // the block's records leave as one contiguous, coalesced range
+        const int c0 = blockIdx.x * blockDim.x;
+        const int nrec = min((int)blockDim.x, c.ncells - c0);
+        float4 *dst = (float4 *)(crec + c0);
+        for (int j = threadIdx.x; j < 2 * nrec; j += blockDim.x) dst[j] = srec[j];
+    }
+    // block sum of the avVel terms: warp shuffles, then one thread per block
+    __shared__ double wsum[8][3];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int d = 0; d < DIM; d++) {
+        const double t = warp_sum_d(av[d]);
+        if (lane == 0) wsum[wid][d] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < DIM) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += wsum[w][threadIdx.x];
+        atomicAdd(&acc[ACC_VCM + threadIdx.x], t);
+    }
+}
+
+enum { RES_STEP = 0, RES_SUM = 1 };
+
+// Particle pass: block b owns particles [b * kResChunk, (b+1) * kResChunk),
+// one per thread at a time (coalesced loads and stores).
+//   RES_STEP: collide, stream, write the particle back in place, add it to
+//             the next step's sums.
+//   RES_SUM:  only add each particle to this step's sums (the first step,
+//             or after the state was replaced).
+// Accumulation: each particle adds its limbs to its cell's entry in the
+// block's table with native 32-bit shared-memory atomics (or, if the table
+// has no slot for it, straight to global memory); at the end every table
+// entry is added to the global sums once.
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
+    const __grid_constant__ DevCfg c, MixState a, int n,
+    const ResRec *__restrict__ crec, ResSum *sums, unsigned long long *msum, double *acc,
+    unsigned long long *status, StepArgs sa) {
+    extern __shared__ __align__(16) unsigned char res_smem[];
+    __shared__ double red[8];
+    const int tid = threadIdx.x;
+    const bool multi = msum != nullptr;
+    const int nc = multi ? DIM + 1 : DIM;
+    ResTable t;
+    t.bind(res_smem, nc);
+    for (int s = tid; s < kResSlots; s += kResThreads) {
+        t.key[s] = -1;
+        t.cnt[s] = 0u;
+    }
+    for (int s = tid; s < nc * kResSlots; s += kResThreads) {
+        t.hi[s] = 0;
+        t.lo[s] = 0;
+    }
+    __syncthreads();
+    float ke = 0.f;     // one species: sum of v^2 (times m at the end)
+    double ke_m = 0.0;  // several species: sum of m v^2
+    int bounce = 0, esc = 0, bad = 0;
+    const float gk[3] = {(float)(c.dt * c.grav[0]), (float)(c.dt * c.grav[1]),
+                         (float)(c.dt * c.grav[2])};
+    const float cosf_a = (float)c.cosA, sinf_a = (float)c.sinA;
+    const int base = blockIdx.x * kResChunk;
+    // the next particle's record is loaded one iteration ahead
+    MixRec nx;
+    if (base + tid < n) {
+        nx.P = a.P[base + tid];
+        nx.W = a.W[base + tid];
+    }
+#pragma unroll 1
+    for (int it = 0; it < MPCD_RES_PPT; it++) {
+        const int i = base + it * kResThreads + tid;
+        if (i >= n) break;
+        MixRec r = nx;
+        if (it + 1 < MPCD_RES_PPT && i + kResThreads < n) {
+            nx.P = a.P[i + kResThreads];
+            nx.W = a.W[i + kResThreads];
+        }
+        if (c.grav_flag) {
+            r.W.x += gk[0];
+            r.W.y += gk[1];
+            if (DIM == 3) r.W.z += gk[2];
+        }
+        const int sp = multi ? MixT<DIM>::sp(a, i) : 0;
+        int k, kidx[3];
+        if (MODE == RES_STEP) {
+            const int kc = cur_key<DIM>(c, r, sa);
+            const float4 *q = (const float4 *)(crec + kc);
+            const float4 ca = __ldg(q);
+            if (__float_as_int(ca.w) > 1) {
+                const float Cs = cosf_a, Sn = sinf_a;
+                const float w0 = r.W.x - ca.x, w1 = r.W.y - ca.y;
+                if (DIM == 3) {
+                    const float4 cb = __ldg(q + 1);
+                    const float w2 = r.W.z - ca.z;
+                    const float ld = (cb.x * w0 + cb.y * w1 + cb.z * w2) * (1.f - Cs);
+                    r.W.x = ca.x + (Cs * w0 + ld * cb.x + Sn * (cb.y * w2 - cb.z * w1));
+                    r.W.y = ca.y + (Cs * w1 + ld * cb.y + Sn * (cb.z * w0 - cb.x * w2));
+                    r.W.z = ca.z + (Cs * w2 + ld * cb.z + Sn * (cb.x * w1 - cb.y * w0));
+                } else {
+                    r.W.x = ca.x + (Cs * w0 - Sn * w1);
+                    r.W.y = ca.y + (Sn * w0 + Cs * w1);
+                }
+            }
+            float tt = r.W.x * r.W.x + r.W.y * r.W.y;
+            if (DIM == 3) tt += r.W.z * r.W.z;
+            if (multi)
+                ke_m += c.mass[sp] * (double)tt;
+            else
+                ke += tt;
+            k = MixT<DIM>::finish_idx(c, r, sp, sa, bounce, esc, kidx);
+            MixT<DIM>::store(a, i, r);
+            // the next step's load adds the same FP32 gravity kick
+            if (c.grav_flag) {
+                r.W.x += gk[0];
+                r.W.y += gk[1];
+                if (DIM == 3) r.W.z += gk[2];
+            }
+        } else {
+            k = cur_key_idx<DIM>(c, r, sa, kidx);
+        }
+        const float vs[3] = {r.W.x, r.W.y, DIM == 3 ? r.W.z : 0.f};
+        res_add<DIM>(t, c, sums, msum, k, kidx, vs, multi ? c.mass[sp] : 1.0, multi, bad);
+    }
+    __syncthreads();
+    res_flush<DIM>(t, sums, msum, multi);
+    if (MODE == RES_STEP) {
+        const double kt = multi ? ke_m : c.mass[0] * (double)ke;
+        const double tk = block_sum256(kt, red);
+        if (tid == 0) atomicAdd(&acc[ACC_KE], tk);
+        if (bounce) atomicAdd(&status[ST_BOUNCE], (unsigned long long)bounce);
+        if (esc) atomicAdd(&status[ST_ESCAPED], (unsigned long long)esc);
+    }
+    if (bad) atomicAdd(&status[ST_NONFINITE], (unsigned long long)bad);
+}
+
+}  // namespace mpcd

@@ -114,20 +114,29 @@ __global__ void __launch_bounds__(256) k_srd_cells(const __grid_constant__ DevCf
     }
 }
 
-// Current-step cell key of a particle from its stored position.
+// Current-step cell key of a particle from its stored position, and its
+// per-axis indices.
 template <int DIM>
-__device__ __forceinline__ int cur_key(const DevCfg &c, const MixRec &r, const StepArgs &sa) {
+__device__ __forceinline__ int cur_key_idx(const DevCfg &c, const MixRec &r,
+                                           const StepArgs &sa, int idx[3]) {
     int ca, cb, cz, e = 0;
     uint32_t t;
     unpack_cell((int)r.P.w, ca, cb, cz);
-    if (c.all_periodic)
-        return cell_lin(c, fx_shift_axis_pbc(ca, r.P.x, sa.ks[0], c.L[0]),
-                        fx_shift_axis_pbc(cb, r.P.y, sa.ks[1], c.L[1]),
-                        DIM == 3 ? fx_shift_axis_pbc(cz, r.P.z, sa.ks[2], c.L[2]) : 0);
-    int x = fx_shift_axis(ca, r.P.x, sa.ks[0], c.L[0], c.pbc[0], t, e);
-    int y = fx_shift_axis(cb, r.P.y, sa.ks[1], c.L[1], c.pbc[1], t, e);
-    int z = DIM == 3 ? fx_shift_axis(cz, r.P.z, sa.ks[2], c.L[2], c.pbc[2], t, e) : 0;
-    return cell_lin(c, x, y, z);
+    if (c.all_periodic) {
+        idx[0] = fx_shift_axis_pbc(ca, r.P.x, sa.ks[0], c.L[0]);
+        idx[1] = fx_shift_axis_pbc(cb, r.P.y, sa.ks[1], c.L[1]);
+        idx[2] = DIM == 3 ? fx_shift_axis_pbc(cz, r.P.z, sa.ks[2], c.L[2]) : 0;
+    } else {
+        idx[0] = fx_shift_axis(ca, r.P.x, sa.ks[0], c.L[0], c.pbc[0], t, e);
+        idx[1] = fx_shift_axis(cb, r.P.y, sa.ks[1], c.L[1], c.pbc[1], t, e);
+        idx[2] = DIM == 3 ? fx_shift_axis(cz, r.P.z, sa.ks[2], c.L[2], c.pbc[2], t, e) : 0;
+    }
+    return cell_lin(c, idx[0], idx[1], idx[2]);
+}
+template <int DIM>
+__device__ __forceinline__ int cur_key(const DevCfg &c, const MixRec &r, const StepArgs &sa) {
+    int idx[3];
+    return cur_key_idx<DIM>(c, r, sa, idx);
 }
 template <int DIM>
 __device__ __forceinline__ int cur_key(const DevCfg &c, const F64Rec &r, const StepArgs &sa) {

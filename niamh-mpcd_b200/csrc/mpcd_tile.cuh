@@ -114,6 +114,13 @@ struct MixT {
     // when the wall loop hit its limit.
     static __device__ __forceinline__ int finish(const DevCfg &c, Rec &r, int sp,
                                                  const StepArgs &sa, int &bounce, int &esc) {
+        int idx[3];
+        return finish_idx(c, r, sp, sa, bounce, esc, idx);
+    }
+    // finish(), also returning the next cell's per-axis indices
+    static __device__ __forceinline__ int finish_idx(const DevCfg &c, Rec &r, int sp,
+                                                     const StepArgs &sa, int &bounce, int &esc,
+                                                     int idx[3]) {
         int ci[3];
         unpack_cell((int)r.P.w, ci[0], ci[1], ci[2]);
         uint32_t f[3] = {r.P.x, r.P.y, r.P.z};
@@ -133,6 +140,7 @@ struct MixT {
             r.P.y = f[1];
             r.P.z = DIM == 3 ? f[2] : 0u;
             r.P.w = (unsigned)pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
+            for (int d = 0; d < 3; d++) idx[d] = a[d];
             return cell_lin(c, a[0], a[1], a[2]);
         }
         if (c.n_solid > 0) {
@@ -177,6 +185,9 @@ struct MixT {
         int b = fx_shift_axis(ci[1], f[1], sa.ksn[1], c.L[1], c.pbc[1], t, esc);
         int z = 0;
         if (DIM == 3) z = fx_shift_axis(ci[2], f[2], sa.ksn[2], c.L[2], c.pbc[2], t, esc);
+        idx[0] = a;
+        idx[1] = b;
+        idx[2] = z;
         return cell_lin(c, a, b, z);
     }
     static __device__ __forceinline__ void store(const State &st, int i, const Rec &r) {

@@ -32,6 +32,7 @@ KERNEL_AUTO = 0
 KERNEL_TILE = 1
 KERNEL_GROUP = 2
 KERNEL_SPLIT = 3
+KERNEL_RESIDENT = 4
 
 STRATEGY_SCATTER = 0
 STRATEGY_RECOMPUTE = 1
@@ -115,6 +116,7 @@ class Status(C.Structure):
         ("bounce_limit", C.c_uint64),
         ("nonfinite", C.c_uint64),
         ("overflow", C.c_uint64),
+        ("sync_timeout", C.c_uint64),
     ]
 
 

@@ -20,7 +20,7 @@ EXPORTS = [
     "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
-    "mpcd_srd_step_noalloc",
+    "mpcd_set_sort_interval", "mpcd_srd_step_noalloc",
 ]
 
 _lib = None
@@ -55,6 +55,7 @@ def load():
         lib.mpcd_launches_per_step.argtypes = [vp]
         lib.mpcd_set_strategy.argtypes = [vp, C.c_int, C.c_int]
         lib.mpcd_set_kernel.argtypes = [vp, C.c_int]
+        lib.mpcd_set_sort_interval.argtypes = [vp, C.c_int]
         lib.mpcd_srd_step_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_uint32, vp, vp]
         _lib = lib
     return _lib
@@ -137,6 +138,9 @@ class Solver:
 
     def set_kernel(self, kernel):
         _check(self.lib.mpcd_set_kernel(self.h, kernel), "mpcd_set_kernel")
+
+    def set_sort_interval(self, steps):
+        _check(self.lib.mpcd_set_sort_interval(self.h, steps), "mpcd_set_sort_interval")
 
     def set_stream(self, stream_ptr):
         _check(self.lib.mpcd_set_stream(self.h, C.c_void_p(stream_ptr)), "mpcd_set_stream")

@@ -1,0 +1,171 @@
+"""The resident SRD kernel family (mixed precision, particles kept in place,
+cell sums accumulated in 64-bit fixed point) against the CPU oracle and
+against the sorted kernel family of the same precision.
+
+Fixed-point sums are exact and order-independent, so the resident family's
+results must not depend on the particle order in memory: runs that re-sort
+the state at different intervals agree bit for bit.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from checkers import Oracle
+from mpcd_b200 import abi
+from mpcd_b200 import workloads as W
+from mpcd_b200.gpu import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _solid_channel(L):
+    """Periodic in x and z, bounce-back walls at y=0 and y=L[1] without
+    phantom particles (so the SRD operator stays on the resident path)."""
+    w = W.channel_walls(L)
+    for i in (2, 3):
+        w[i].phantom = 0
+    return w
+
+
+def _case(name, precision):
+    if name == "srd3d":
+        return W.cfg_srd3d((9, 7, 6), precision=precision, seed=101), 10
+    if name == "srd2d":
+        return W.base_config(2, (11, 9), coll_op=abi.COLL_ARBAXIS, rot_ang=math.radians(130.0),
+                             precision=precision, seed=102), 12
+    if name == "heavy":
+        return W.cfg_srd3d((6, 6, 6), species=[W._species(mass=2.5)], kbt=1.7, dt=0.25,
+                           precision=precision, seed=103), 10
+    if name == "species":
+        return W.cfg_srd3d((7, 6, 5), species=[W._species(mass=1.0), W._species(mass=3.0)],
+                           precision=precision, seed=104), 10
+    if name == "walls_grav":
+        L = (8, 6, 5)
+        return W.base_config(3, L, coll_op=abi.COLL_ARBAXIS, rot_ang=math.radians(130.0),
+                             walls=_solid_channel(L), grav=(1e-2, 0.0, 0.0),
+                             precision=precision, seed=105), 15
+    raise KeyError(name)
+
+
+def _state(cfg, ppc, seed):
+    Q, V, U, sp = W.synthetic_state(cfg, ppc, seed=seed)
+    if cfg.n_species > 1:
+        sp = (np.arange(len(Q)) % cfg.n_species).astype(np.int32)
+    if any(cfg.walls[i].phantom == 0 and cfg.walls[i].DN == 0.0 for i in range(cfg.n_walls)):
+        # keep particles off the walls' planes
+        Q[:, 1] = 0.02 + Q[:, 1] * (cfg.L[1] - 0.04) / cfg.L[1]
+    return Q, V, U, sp
+
+
+NAMES = ["srd3d", "srd2d", "heavy", "species", "walls_grav"]
+
+
+def _min_image(d, L):
+    return d - np.round(d / L) * L
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_resident_tracks_oracle_one_step(name):
+    cfg, ppc = _case(name, abi.PREC_FP64)
+    cfgm, _ = _case(name, abi.PREC_MIXED)
+    Q, V, U, sp = _state(cfg, ppc, 7)
+    o = Oracle(cfg, Q, V, U, sp)
+    g = Solver(cfgm)
+    g.set_kernel(abi.KERNEL_RESIDENT)
+    g.upload(Q, V, U, sp)
+    o.step(1)
+    kg, ag = g.timestep(1)
+    assert g.launches_per_step() >= 2
+    qo, vo, _ = o.particles()
+    qg, vg, _ = g.download()
+    L = np.array([cfg.L[d] if d < cfg.dim else 1 for d in range(3)], dtype=float)
+    dv = np.abs(vg - vo).max(axis=1)
+    dq = np.abs(_min_image(qg - qo, L)).max(axis=1)
+    bad = np.mean((dv > 1e-5) | (dq > 1e-5))
+    assert bad < 2e-3, (bad, dv.max(), dq.max())
+    ko, ao = o.globals()
+    assert kg == pytest.approx(ko, rel=1e-5)
+    np.testing.assert_allclose(ag, ao, rtol=0, atol=1e-6)
+    st = g.status()
+    assert st.escaped == 0 and st.bounce_limit == 0 and st.nonfinite == 0
+    assert st.sync_timeout == 0
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_resident_matches_sorted_family_multistep(name):
+    # same precision, same draws: the resident and the sorted (split) family
+    # differ only in how the FP64 cell sums are formed (~1e-10), so they
+    # agree to FP32 precision over many steps
+    cfgm, ppc = _case(name, abi.PREC_MIXED)
+    Q, V, U, sp = _state(cfgm, ppc, 8)
+    out = []
+    for kernel in (abi.KERNEL_RESIDENT, abi.KERNEL_SPLIT):
+        g = Solver(cfgm)
+        g.set_kernel(kernel)
+        g.upload(Q, V, U, sp)
+        glob = [g.timestep(s) for s in range(1, 11)]
+        out.append((g.download(), glob))
+    (qa, va, _), ga = out[0]
+    (qb, vb, _), gb = out[1]
+    L = np.array([cfgm.L[d] if d < cfgm.dim else 1 for d in range(3)], dtype=float)
+    dv = np.abs(va - vb).max(axis=1)
+    dq = np.abs(_min_image(qa - qb, L)).max(axis=1)
+    bad = np.mean((dv > 1e-4) | (dq > 1e-5))
+    assert bad < 5e-3, (bad, dv.max(), dq.max())
+    for (ka, aa), (kb, ab) in zip(ga, gb):
+        assert ka == pytest.approx(kb, rel=1e-5)
+
+
+@pytest.mark.parametrize("name", ["srd3d", "species", "walls_grav"])
+def test_resident_result_independent_of_sort_interval(name):
+    cfgm, ppc = _case(name, abi.PREC_MIXED)
+    Q, V, U, sp = _state(cfgm, ppc, 9)
+    res = []
+    for interval in (1, 3, 1000):
+        g = Solver(cfgm)
+        g.set_kernel(abi.KERNEL_RESIDENT)
+        g.set_sort_interval(interval)
+        g.upload(Q, V, U, sp)
+        g.step(12, 1)
+        q, v, _ = g.download()
+        res.append((q, v, g.globals()))
+    for q, v, gl in res[1:]:
+        assert np.array_equal(q, res[0][0])
+        assert np.array_equal(v, res[0][1])
+        # the global measures are floating-point reductions whose order
+        # follows the particle order: equal to rounding only
+        assert gl[0] == pytest.approx(res[0][2][0], rel=1e-7)
+
+
+def test_resident_switching_families_mid_run():
+    # resident -> split -> resident must continue the same trajectory as a
+    # run that stays on one family (to FP32 precision)
+    cfgm, ppc = _case("srd3d", abi.PREC_MIXED)
+    Q, V, U, sp = _state(cfgm, ppc, 10)
+    a = Solver(cfgm)
+    a.set_kernel(abi.KERNEL_SPLIT)
+    a.upload(Q, V, U, sp)
+    a.step(9, 1)
+    b = Solver(cfgm)
+    b.upload(Q, V, U, sp)
+    for s0, kern in ((1, abi.KERNEL_RESIDENT), (4, abi.KERNEL_SPLIT), (7, abi.KERNEL_RESIDENT)):
+        b.set_kernel(kern)
+        b.step(3, s0)
+    qa, va, _ = a.download()
+    qb, vb, _ = b.download()
+    dv = np.abs(va - vb).max(axis=1)
+    assert np.mean(dv > 1e-4) < 5e-3, dv.max()
+
+
+def test_resident_conserves_momentum_exactly_in_fixed_point():
+    # SRD conserves each cell's momentum; with exact fixed-point sums the
+    # total drifts only by the FP32 rounding of the rotated velocities
+    cfgm = W.cfg_srd3d((16, 16, 16), precision=abi.PREC_MIXED, seed=11)
+    Q, V, U, sp = W.synthetic_state(cfgm, 10, seed=12)
+    g = Solver(cfgm)
+    g.upload(Q, V, U, sp)
+    p0 = V.sum(axis=0)
+    g.step(50, 1)
+    _, v, _ = g.download()
+    assert np.abs(v.sum(axis=0) - p0).max() / np.abs(V).sum() < 1e-6
