@@ -51,9 +51,25 @@ def parse():
     ap.add_argument("--tile", type=int, default=0, help="particles per tile (0 default)")
     ap.add_argument("--kernel", type=int, default=0,
                     help="cell-kernel family: 0 auto, 1 tile, 2 group, 3 split, 4 resident")
+    ap.add_argument("--flush", default="write+read", choices=["write+read", "write"],
+                    help="L2 flush between timed steps")
     ap.add_argument("--sort-interval", type=int, default=0,
                     help="resident family: steps between re-sorts (0 = library default)")
     return ap.parse_args()
+
+
+def traffic_per_launch():
+    """DRAM bytes (read + write) of one particle-pass launch on this
+    workload, from the committed ncu summary of that kernel, or None."""
+    path = os.path.join(ROOT, "profiles", "k_res_parts_srd64_mixed.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
 
 
 def peaks():
@@ -141,6 +157,11 @@ def run_gpu(args, rank, world):
     dev = torch.cuda.current_device()
     stream = torch.cuda.current_stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    # the flush writes 256 MB, then reads another 256 MB so that the lines it
+    # leaves in L2 are clean (otherwise the timed step pays the write-back of
+    # the flush's own dirty lines); none of the step's data stays in L2
+    flush_rd = torch.ones(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    flush_sink = torch.empty(1, dtype=torch.float32, device="cuda")
     results = {}
     forms = [f for f in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED))
              if f[0] in args.forms.split(",")]
@@ -166,14 +187,21 @@ def run_gpu(args, rank, world):
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
+        g.set_timing(True)
+        launches = 0
         t_begin = time.time()
         for k in range(args.steps):
             flush.zero_()
+            if args.flush == "write+read":
+                torch.sum(flush_rd, dim=0, out=flush_sink[0])
             ev[k][0].record(stream)
             g.step(1, 1 + args.warmup + k)
             ev[k][1].record(stream)
+            launches += g.launches_per_step()
         torch.cuda.synchronize()
         t_end = time.time()
+        kern_ms, kern_n = g.kernel_time()
+        g.set_timing(False)
         if world > 1:
             torch.distributed.barrier()
         clocks = clk.stop(t_begin, t_end) if clk else None
@@ -185,10 +213,14 @@ def run_gpu(args, rank, world):
         total_ms = float(t.item())
         kb, av = g.globals()
         st = g.status()
+        kt = torch.tensor([kern_ms / max(kern_n, 1)], device="cuda", dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(kt, op=torch.distributed.ReduceOp.MAX)
         results[form] = {
             "n": n, "ms_total": total_ms, "ms_per_step": total_ms / args.steps,
-            "ms_min": min(ms), "launches": g.launches_per_step(), "clocks": clocks,
-            "kbt": kb, "escaped": int(st.escaped),
+            "ms_min": min(ms), "launches": launches, "clocks": clocks,
+            "kbt": kb, "escaped": int(st.escaped), "kernel_ms": float(kt.item()),
+            "kernel_launches": kern_n,
         }
         # e2e through the C ABI with host buffers: upload from pinned host
         # memory, K drop-in timestep() calls each returning the step's global
@@ -281,7 +313,9 @@ def main():
         value = n * world * args.steps / (mix["ms_total"] / 1e3)
         v64 = n * world * args.steps / (f64["ms_total"] / 1e3)
         peak, peak_kind = peaks()
-        ach = ALG_BYTES["mixed"] * n / (mix["ms_total"] / args.steps / 1e3) / 1e9
+        # dominant kernel: the particle pass (reads and writes every particle)
+        ach = ALG_BYTES["mixed"] * n / (mix["kernel_ms"] / 1e3) / 1e9
+        step_gbs = ALG_BYTES["mixed"] * n / (mix["ms_total"] / args.steps / 1e3) / 1e9
         ach64 = ALG_BYTES["fp64"] * n / (f64["ms_total"] / args.steps / 1e3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -291,15 +325,20 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "global_batch": n * world, "form": "mixed",
                        "parallelism": f"replicas x{world}",
-                       "l2": "flushed (256 MB write) between timed steps"},
+                       "l2": ("flushed between timed steps: 256 MB write, then 256 MB read "
+                              "(L2 left holding clean lines)") if args.flush == "write+read"
+                       else "flushed between timed steps: 256 MB write"},
             "fp64": {"value": v64, "ms_per_step": f64["ms_total"] / args.steps,
                      "achieved_gbs": ach64, "frac": ach64 / peak},
             "mixed_over_fp64": value / v64,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "traffic": None,
-                         "unit_of_work": "one timestep (all kernels of a step)",
+                         "frac": ach / peak, "traffic": traffic_per_launch(),
+                         "kernel": "k_res_parts<3, RES_STEP> (particle pass)",
+                         "kernel_ms": mix["kernel_ms"],
+                         "alg_bytes_per_launch": ALG_BYTES["mixed"] * n,
+                         "step_achieved": step_gbs, "step_frac": step_gbs / peak,
                          "peak_source": peak_kind},
-            "gpu_launches": mix["launches"] * args.steps,
+            "gpu_launches": mix["launches"],
             "clocks": mix["clocks"],
             "e2e": res["e2e"],
         }

@@ -204,6 +204,15 @@ int mpcd_set_stream(mpcd_handle *h, void *stream);
 /* Number of kernel launches the last mpcd_step issued per step. */
 int mpcd_launches_per_step(mpcd_handle *h);
 
+/* Timing of the step's particle pass (the kernel that reads and writes every
+ * particle; no counterpart in the reference): while enabled, each step
+ * records a CUDA event pair around that launch on the handle's stream.
+ * mpcd_kernel_time synchronizes, returns the summed duration (ms) and the
+ * number of timed launches since timing was enabled or last queried, and
+ * starts a new interval. */
+int mpcd_set_timing(mpcd_handle *h, int enable);
+int mpcd_kernel_time(mpcd_handle *h, double *ms_total, int *launches);
+
 /* Execution strategy of the per-step pipeline (no counterpart in the
  * reference, which has one serial path):
  *   MPCD_STRATEGY_SCATTER   fused cell kernel writes in place, a scatter

@@ -59,7 +59,34 @@ struct mpcd_handle {
     uint32_t last_step;
     uint64_t steps;
     double *host_acc;  // pinned
+    // optional timing of the step's particle pass (the dominant kernel):
+    // an event pair around each of its launches, summed on request
+    bool timing;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tev;
 };
+
+static void time_begin(mpcd_handle *h) {
+    if (!h->timing) return;
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return;
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return;
+    }
+    cudaEventRecord(a, h->stream);
+    h->tev.emplace_back(a, b);
+}
+static void time_end(mpcd_handle *h) {
+    if (!h->timing || h->tev.empty()) return;
+    cudaEventRecord(h->tev.back().second, h->stream);
+}
+static void time_clear(mpcd_handle *h) {
+    for (auto &p : h->tev) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    h->tev.clear();
+}
 
 #define CK(call)                                                        \
     do {                                                                \
@@ -260,6 +287,7 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->rmsum);
     cudaFree(h->lcbuf);
     if (h->host_acc) cudaFreeHost(h->host_acc);
+    time_clear(h);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MPCD_OK;
@@ -279,7 +307,6 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
         if (r != MPCD_OK) return r;
     }
     mpcd_handle *h = new mpcd_handle();
-    memset(h, 0, sizeof(*h));
     h->cfg = *cfg;
     h->dc = dc;
     h->prec = cfg->precision;
@@ -779,7 +806,9 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
         launches += 1;
     }
     if (h->strategy == MPCD_STRATEGY_SCATTER) {
+        time_begin(h);
         r = launch_tile<DIM, T>(h, MODE_INPLACE, st[h->cur], st[1 - h->cur], tb, sa);
+        time_end(h);
         if (r != MPCD_OK) return r;
         launch_scan(h, h->start[1 - h->scur], nullptr, acc_nxt);
         launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]);
@@ -787,7 +816,9 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
         r = launch_tile<DIM, T>(h, MODE_COUNT, st[h->cur], st[1 - h->cur], tb, sa);
         if (r != MPCD_OK) return r;
         launch_scan(h, h->start[1 - h->scur], h->fill, acc_nxt);
+        time_begin(h);
         r = launch_tile<DIM, T>(h, MODE_FINAL, st[h->cur], st[1 - h->cur], tb, sa);
+        time_end(h);
         if (r != MPCD_OK) return r;
     }
     launches += 4;
@@ -853,9 +884,11 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     auto kstep = k_res_parts<DIM, RES_STEP>;
     CK(cudaFuncSetAttribute(kstep, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
     CK(cudaFuncSetAttribute(kstep, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    time_begin(h);
     kstep<<<pgrid, kResThreads, pbytes, h->stream>>>(c, h->mx[h->cur], h->n,
                                                      (const CRec *)h->crec, sum_nxt, ms_nxt,
                                                      acc_cur, h->status, sa);
+    time_end(h);
     launches += 2;
     CK(cudaGetLastError());
     h->sums_for = (int64_t)step + 1;
@@ -924,8 +957,10 @@ static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
     tb.status = h->status;
     auto kfn = k_lc_tile<T>;
     CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.bytes));
+    time_begin(h);
     kfn<<<(c.ncells + ct - 1) / ct, 256, lay.bytes, h->stream>>>(c, st[h->cur], h->lcc, tb, sa,
                                                                  lay);
+    time_end(h);
     launch_scan(h, h->start[1 - h->scur], nullptr, acc_nxt);
     launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]);
     launches += 9;
@@ -1032,6 +1067,29 @@ extern "C" int mpcd_set_stream(mpcd_handle *h, void *stream) {
 }
 
 extern "C" int mpcd_launches_per_step(mpcd_handle *h) { return h ? h->launches : 0; }
+
+extern "C" int mpcd_set_timing(mpcd_handle *h, int enable) {
+    if (!h) return MPCD_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    time_clear(h);
+    h->timing = enable != 0;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_kernel_time(mpcd_handle *h, double *ms_total, int *launches) {
+    if (!h || !ms_total || !launches) return MPCD_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    double t = 0.0;
+    for (auto &p : h->tev) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, p.first, p.second));
+        t += ms;
+    }
+    *ms_total = t;
+    *launches = (int)h->tev.size();
+    time_clear(h);
+    return MPCD_OK;
+}
 
 extern "C" int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
                                double *cm) {

@@ -155,6 +155,13 @@ __device__ __forceinline__ bool fx_limbs(float v, int &hi, int &lo) {
 // rint(dx * 2^32).
 __device__ __forceinline__ void fx_stream(uint32_t &f, int &ci, float dx) {
     int hi, lo;
+    if (fabsf(dx) < 1.0f && fx_limbs(dx, hi, lo)) {
+        // |rint(dx 2^32)| < 2^32: 32-bit add, the carry from the wrap
+        const uint32_t nf = f + (((uint32_t)hi << 20) + (uint32_t)lo);
+        ci += dx >= 0.0f ? (nf < f ? 1 : 0) : (nf > f ? -1 : 0);
+        f = nf;
+        return;
+    }
     long long disp;
     if (fx_limbs(dx, hi, lo))
         disp = (long long)hi * (1ll << 20) + (long long)lo;

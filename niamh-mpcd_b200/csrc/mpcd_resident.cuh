@@ -118,11 +118,20 @@ __device__ __forceinline__ void res_global_add(ResSum *gs, unsigned long long *g
 
 // Slot of key k (per-axis indices idx) in the block's table, inserting it,
 // or -1 if the bounded probe found none.  The first slot tried packs the
-// low bits of the indices (DevCfg::res_shift/res_mask).
+// low bits of the indices (DevCfg::res_shift/res_mask), the fastest axis in
+// the lowest field, rotated by an offset of the other axes' indices so that
+// cells adjacent across rows or planes fall in different shared-memory
+// banks (a rotation within the field keeps the packing one-to-one).
+template <int DIM>
 __device__ __forceinline__ int res_slot(ResTable &t, const DevCfg &c, int k, const int idx[3]) {
-    unsigned h = (unsigned)(((idx[0] & c.res_mask[0]) << c.res_shift[0]) |
-                            ((idx[1] & c.res_mask[1]) << c.res_shift[1]) |
-                            ((idx[2] & c.res_mask[2]) << c.res_shift[2]));
+    unsigned h;
+    if (DIM == 3)
+        h = (unsigned)(((idx[2] + 5 * idx[1] + 11 * idx[0]) & c.res_mask[2]) |
+                       ((idx[1] & c.res_mask[1]) << c.res_shift[1]) |
+                       ((idx[0] & c.res_mask[0]) << c.res_shift[0]));
+    else
+        h = (unsigned)(((idx[1] + 5 * idx[0]) & c.res_mask[1]) |
+                       ((idx[0] & c.res_mask[0]) << c.res_shift[0]));
     for (int probe = 0; probe < kResProbe; probe++) {
         const int cur = *(volatile int *)&t.key[h];
         if (cur == k) return (int)h;
@@ -166,7 +175,7 @@ __device__ __forceinline__ void res_add(ResTable &t, const DevCfg &c, ResSum *su
             lo[d] = (int)(x[d] - q * (1ll << kLimb));
         }
     }
-    const int slot = res_slot(t, c, k, idx);
+    const int slot = res_slot<DIM>(t, c, k, idx);
     if (slot >= 0) {
         atomicAdd(&t.cnt[slot], 1u);
         for (int d = 0; d < nc; d++) {
@@ -285,13 +294,12 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     const int nc = multi ? DIM + 1 : DIM;
     ResTable t;
     t.bind(res_smem, nc);
-    for (int s = tid; s < kResSlots; s += kResThreads) {
-        t.key[s] = -1;
-        t.cnt[s] = 0u;
-    }
-    for (int s = tid; s < nc * kResSlots; s += kResThreads) {
-        t.hi[s] = 0;
-        t.lo[s] = 0;
+    {
+        // keys to -1, everything after them to 0, in 16-byte stores
+        uint4 *w = (uint4 *)res_smem;
+        const int nkey = kResSlots / 4, nall = res_table_bytes(nc) / 16;
+        for (int j = tid; j < nall; j += kResThreads)
+            w[j] = j < nkey ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
     float ke = 0.f;     // one species: sum of v^2 (times m at the end)

@@ -20,7 +20,8 @@ EXPORTS = [
     "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
-    "mpcd_set_sort_interval", "mpcd_srd_step_noalloc",
+    "mpcd_set_sort_interval", "mpcd_set_timing", "mpcd_kernel_time",
+    "mpcd_srd_step_noalloc",
 ]
 
 _lib = None
@@ -56,6 +57,8 @@ def load():
         lib.mpcd_set_strategy.argtypes = [vp, C.c_int, C.c_int]
         lib.mpcd_set_kernel.argtypes = [vp, C.c_int]
         lib.mpcd_set_sort_interval.argtypes = [vp, C.c_int]
+        lib.mpcd_set_timing.argtypes = [vp, C.c_int]
+        lib.mpcd_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         lib.mpcd_srd_step_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_uint32, vp, vp]
         _lib = lib
     return _lib
@@ -138,6 +141,16 @@ class Solver:
 
     def set_kernel(self, kernel):
         _check(self.lib.mpcd_set_kernel(self.h, kernel), "mpcd_set_kernel")
+
+    def set_timing(self, enable=True):
+        _check(self.lib.mpcd_set_timing(self.h, 1 if enable else 0), "mpcd_set_timing")
+
+    def kernel_time(self):
+        """(summed ms, launches) of the timed particle-pass launches."""
+        ms = C.c_double()
+        nl = C.c_int()
+        _check(self.lib.mpcd_kernel_time(self.h, C.byref(ms), C.byref(nl)), "mpcd_kernel_time")
+        return ms.value, nl.value
 
     def set_sort_interval(self, steps):
         _check(self.lib.mpcd_set_sort_interval(self.h, steps), "mpcd_set_sort_interval")

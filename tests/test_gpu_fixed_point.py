@@ -45,3 +45,22 @@ def test_isolated_particles_stream_exactly(kernel):
     disp = np.rint(dx * 2.0 ** 32)  # ties to even
     expect = (np.round(Q * 2.0 ** 32) + disp) * 2.0 ** -32
     np.testing.assert_array_equal(q, expect)
+
+
+@pytest.mark.parametrize("kernel", [abi.KERNEL_RESIDENT, abi.KERNEL_SPLIT])
+def test_fast_isolated_particles_stream_exactly(kernel):
+    # displacements of more than one cell per step take the 64-bit path
+    L = (16, 16, 16)
+    cfg = W.cfg_srd3d(L, precision=abi.PREC_MIXED, seed=7, dt=0.125)
+    Q = np.array([[2.25, 2.5, 2.75], [10.5, 3.25, 9.125], [5.5, 12.75, 4.25],
+                  [13.25, 9.5, 13.75]])
+    V = np.array([[12.5, -9.25, 15.75], [-14.125, 8.0, -11.5], [9.0625, -15.5, 13.25],
+                  [-10.75, 11.125, -8.5]])
+    g = Solver(cfg)
+    g.set_kernel(kernel)
+    g.upload(Q, V, None, np.zeros(len(Q), dtype=np.int32))
+    g.step(1, 1)
+    q, v, _ = g.download()
+    np.testing.assert_array_equal(v, V)
+    expect = np.mod(Q + 0.125 * V, 16.0)
+    np.testing.assert_array_equal(q, expect)
