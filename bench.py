@@ -58,6 +58,23 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The maximum of x over all ranks (every rank gets it): the job's time
+    is its slowest rank's."""
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(n_per_rank, world, steps, seconds):
+    """Whole-job particle-steps/s: every rank advances its own replica of
+    n_per_rank particles by `steps` steps; the job takes `seconds` (the max
+    over ranks)."""
+    return n_per_rank * world * steps / seconds
+
+
 def traffic_per_launch():
     """DRAM bytes (read + write) of one particle-pass launch on this
     workload, from the committed ncu summary of that kernel, or None."""
@@ -206,20 +223,14 @@ def run_gpu(args, rank, world):
             torch.distributed.barrier()
         clocks = clk.stop(t_begin, t_end) if clk else None
         ms = [a.elapsed_time(b) for a, b in ev]
-        total_ms = float(sum(ms))
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(float(sum(ms)), world)
         kb, av = g.globals()
         st = g.status()
-        kt = torch.tensor([kern_ms / max(kern_n, 1)], device="cuda", dtype=torch.float64)
-        if world > 1:
-            torch.distributed.all_reduce(kt, op=torch.distributed.ReduceOp.MAX)
+        kernel_ms = max_over_ranks(kern_ms / max(kern_n, 1), world)
         results[form] = {
             "n": n, "ms_total": total_ms, "ms_per_step": total_ms / args.steps,
             "ms_min": min(ms), "launches": launches, "clocks": clocks,
-            "kbt": kb, "escaped": int(st.escaped), "kernel_ms": float(kt.item()),
+            "kbt": kb, "escaped": int(st.escaped), "kernel_ms": kernel_ms,
             "kernel_launches": kern_n,
         }
         # e2e through the C ABI with host buffers: upload from pinned host
@@ -235,12 +246,9 @@ def run_gpu(args, rank, world):
                 g.timestep(1000 + k)
             q2, v2, _ = g.download()
             torch.cuda.synchronize()
-            e2e_s = time.perf_counter() - t0
-            te = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            if world > 1:
-                torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = max_over_ranks(time.perf_counter() - t0, world)
             results["e2e"] = {
-                "value": n * world * args.steps / float(te.item()), "unit": UNIT,
+                "value": job_rate(n, world, args.steps, e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": (Q.nbytes + V.nbytes + sp.nbytes) / args.steps,
                 "d2h_bytes_per_step": (q2.nbytes + v2.nbytes) / args.steps + 32,
             }
@@ -310,8 +318,8 @@ def main():
     elif rank == 0:
         mix, f64 = res["mixed"], res["fp64"]
         n = mix["n"]
-        value = n * world * args.steps / (mix["ms_total"] / 1e3)
-        v64 = n * world * args.steps / (f64["ms_total"] / 1e3)
+        value = job_rate(n, world, args.steps, mix["ms_total"] / 1e3)
+        v64 = job_rate(n, world, args.steps, f64["ms_total"] / 1e3)
         peak, peak_kind = peaks()
         # dominant kernel: the particle pass (reads and writes every particle)
         ach = ALG_BYTES["mixed"] * n / (mix["kernel_ms"] / 1e3) / 1e9
