@@ -37,6 +37,7 @@ struct mpcd_handle {
     MixState mx[2];  // mixed state, two buffers
     int cur;
     int *key, *rank, *count, *fill, *start[2], *part;
+    int *perm;  // destination -> source index of a reordering (mixed state)
     int scur;        // which start[] belongs to the current order
     double *acc;     // 2 x ACC_WORDS, by step parity
     unsigned long long *status;
@@ -275,6 +276,7 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     }
     cudaFree(h->key);
     cudaFree(h->rank);
+    cudaFree(h->perm);
     cudaFree(h->count);
     cudaFree(h->fill);
     cudaFree(h->start[0]);
@@ -391,7 +393,8 @@ static int ensure_capacity(mpcd_handle *h, int n) {
     }
     cudaFree(h->key);
     cudaFree(h->rank);
-    h->key = h->rank = nullptr;
+    cudaFree(h->perm);
+    h->key = h->rank = h->perm = nullptr;
     size_t N = (size_t)want;
     int r;
     for (int b = 0; b < 2; b++) {
@@ -412,6 +415,8 @@ static int ensure_capacity(mpcd_handle *h, int n) {
     }
     if ((r = dev_alloc((void **)&h->key, N * sizeof(int)))) return r;
     if ((r = dev_alloc((void **)&h->rank, N * sizeof(int)))) return r;
+    if (h->prec == MPCD_PREC_MIXED && (r = dev_alloc((void **)&h->perm, N * sizeof(int))))
+        return r;
     h->cap = want;
     return MPCD_OK;
 }
@@ -745,19 +750,22 @@ void launch_key<2, F64T<2>>(mpcd_handle *h, const Fp64State &a, const StepArgs &
                                                            h->count, sa, h->status);
 }
 
-static void launch_scatter(mpcd_handle *h, const MixState &a, const MixState &b,
-                           const int *start) {
-    k_scatter_mix<<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key, h->rank,
-                                                            start);
+// Reorder the state into counting-sort order; returns the launch count.
+static int launch_scatter(mpcd_handle *h, const MixState &a, const MixState &b,
+                          const int *start) {
+    k_perm<<<grid_for(h, h->n), 256, 0, h->stream>>>(h->n, h->key, h->rank, start, h->perm);
+    k_gather_mix<<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->perm);
+    return 2;
 }
-static void launch_scatter(mpcd_handle *h, const Fp64State &a, const Fp64State &b,
-                           const int *start) {
+static int launch_scatter(mpcd_handle *h, const Fp64State &a, const Fp64State &b,
+                          const int *start) {
     if (h->dc.dim == 3)
         k_scatter_f64v<3><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key,
                                                                     h->rank, start);
     else
         k_scatter_f64v<2><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key,
                                                                     h->rank, start);
+    return 1;
 }
 
 static void host_shift(const mpcd_handle *h, uint32_t step, double s[3]) {
@@ -785,9 +793,8 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
     if (h->sorted_for != (int64_t)step) {
         launch_key<DIM, T>(h, st[h->cur], sa);
         launch_scan(h, h->start[h->scur], nullptr, acc_cur);
-        launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[h->scur]);
+        launches += 3 + launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[h->scur]);
         h->cur = 1 - h->cur;
-        launches += 4;
     }
     TileBufs tb;
     memset(&tb, 0, sizeof(tb));
@@ -811,7 +818,7 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
         time_end(h);
         if (r != MPCD_OK) return r;
         launch_scan(h, h->start[1 - h->scur], nullptr, acc_nxt);
-        launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]);
+        launches += launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]) - 1;
     } else {
         r = launch_tile<DIM, T>(h, MODE_COUNT, st[h->cur], st[1 - h->cur], tb, sa);
         if (r != MPCD_OK) return r;
@@ -858,10 +865,9 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     } else if (h->sort_age < 0 || h->sort_age >= h->sort_interval) {
         launch_key<DIM, MixT<DIM>>(h, h->mx[h->cur], sa);
         launch_scan(h, h->start[h->scur], nullptr, nullptr);
-        launch_scatter(h, h->mx[h->cur], h->mx[1 - h->cur], h->start[h->scur]);
+        launches += 3 + launch_scatter(h, h->mx[h->cur], h->mx[1 - h->cur], h->start[h->scur]);
         h->cur = 1 - h->cur;
         h->sort_age = 0;
-        launches += 4;
     }
     const int pgrid = (int)((h->n + kResChunk - 1) / kResChunk);
     const int pbytes = res_table_bytes(h->rmsum ? DIM + 1 : DIM);
@@ -879,7 +885,8 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
                                                         acc_cur, h->status, sa);
         launches += 1;
     }
-    k_res_cells<DIM><<<(int)((nc + 255) / 256), 256, 0, h->stream>>>(
+    k_res_cells<DIM><<<(int)((nc + 256 * kResCellsPer - 1) / (256 * kResCellsPer)), 256, 0,
+                       h->stream>>>(
         c, sum_cur, ms_cur, (CRec *)h->crec, sa, acc_cur, acc_nxt);
     auto kstep = k_res_parts<DIM, RES_STEP>;
     CK(cudaFuncSetAttribute(kstep, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
@@ -922,9 +929,8 @@ static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
     if (h->sorted_for != (int64_t)step) {
         launch_key<2, T>(h, st[h->cur], sa);
         launch_scan(h, h->start[h->scur], nullptr, acc_cur);
-        launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[h->scur]);
+        launches += 3 + launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[h->scur]);
         h->cur = 1 - h->cur;
-        launches += 4;
     }
     const DevCfg &c = h->dc;
     const int *start = h->start[h->scur];
@@ -962,8 +968,7 @@ static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
                                                                  lay);
     time_end(h);
     launch_scan(h, h->start[1 - h->scur], nullptr, acc_nxt);
-    launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]);
-    launches += 9;
+    launches += 8 + launch_scatter(h, st[h->cur], st[1 - h->cur], h->start[1 - h->scur]);
     CK(cudaGetLastError());
     h->cur = 1 - h->cur;
     h->scur = 1 - h->scur;

@@ -139,6 +139,16 @@ __device__ __forceinline__ void mix_rel(const DevCfg &c, const uint4 &p, const u
 // [-1/2, 1/2], g = f 2^20 is exact, and lo = rint(g) by the same addition.
 // Since hi 2^20 is an even integer, rint(v 2^32) = hi 2^20 + rint(g), ties
 // included.  Returns false (limbs undefined) for |v| >= 1024 or non-finite v.
+// fx_limbs without the range check, for |v| < 1024 known to the caller.
+__device__ __forceinline__ void fx_limbs_unchecked(float v, int &hi, int &lo) {
+    const float kMagic = 12582912.0f;  // 1.5 * 2^23
+    const float a = __fmul_rn(v, 4096.0f);
+    const float s = __fadd_rn(a, kMagic);
+    const float r = __fadd_rn(s, -kMagic);
+    const float g = __fmul_rn(__fadd_rn(a, -r), 1048576.0f);
+    hi = __float_as_int(s) - 0x4B400000;
+    lo = __float_as_int(__fadd_rn(g, kMagic)) - 0x4B400000;
+}
 __device__ __forceinline__ bool fx_limbs(float v, int &hi, int &lo) {
     const float kMagic = 12582912.0f;  // 1.5 * 2^23
     const float a = __fmul_rn(v, 4096.0f);
@@ -155,7 +165,8 @@ __device__ __forceinline__ bool fx_limbs(float v, int &hi, int &lo) {
 // rint(dx * 2^32).
 __device__ __forceinline__ void fx_stream(uint32_t &f, int &ci, float dx) {
     int hi, lo;
-    if (fabsf(dx) < 1.0f && fx_limbs(dx, hi, lo)) {
+    if (fabsf(dx) < 1.0f) {
+        fx_limbs_unchecked(dx, hi, lo);
         // |rint(dx 2^32)| < 2^32: 32-bit add, the carry from the wrap
         const uint32_t nf = f + (((uint32_t)hi << 20) + (uint32_t)lo);
         ci += dx >= 0.0f ? (nf < f ? 1 : 0) : (nf > f ? -1 : 0);
@@ -185,15 +196,24 @@ __host__ __device__ __forceinline__ void fx_from_double(double q, int &ci, uint3
     f = (uint32_t)r;
 }
 
-static __global__ void __launch_bounds__(256) k_scatter_mix(MixState a, MixState b, int n,
-                                                     const int *key, const int *rank,
-                                                     const int *start) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int dst = start[key[i]] + rank[i];
-        b.P[dst] = a.P[i];
-        b.W[dst] = a.W[i];
-        if (a.sp) b.sp[dst] = a.sp[i];
-        if (a.U) b.U[dst] = a.U[i];
+
+// Reordering of the state into counting-sort order, as a gather: k_perm scatters only the 4-byte source
+// index of each destination slot, then k_gather_mix reads each destination's
+// record from its source and writes the new order with coalesced stores
+// (16-byte scattered writes would each touch a 32-byte sector).
+static __global__ void __launch_bounds__(256) k_perm(int n, const int *key, const int *rank,
+                                                     const int *start, int *perm) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        perm[start[key[i]] + rank[i]] = i;
+}
+static __global__ void __launch_bounds__(256) k_gather_mix(MixState a, MixState b, int n,
+                                                           const int *perm) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int i = __ldg(perm + j);
+        b.P[j] = a.P[i];
+        b.W[j] = a.W[i];
+        if (a.sp) b.sp[j] = a.sp[i];
+        if (a.U) b.U[j] = a.U[i];
     }
 }
 

@@ -45,7 +45,7 @@ struct ResRec {
 // Fixed-point cell sums: p = sum w v * 2^32 with w = 1 for one species
 // (the cell's momentum is then m p) and w = m for several species; n =
 // population.
-struct ResSum {
+struct __align__(16) ResSum {
     long long p[3];
     long long n;
 };
@@ -154,9 +154,9 @@ __device__ __forceinline__ void res_add(ResTable &t, const DevCfg &c, ResSum *su
     bool fast = !multi && fabsf(v[0]) < kResBigV && fabsf(v[1]) < kResBigV &&
                 (DIM == 2 || fabsf(v[2]) < kResBigV);
     if (fast) {
-        fx_limbs(v[0], hi[0], lo[0]);
-        fx_limbs(v[1], hi[1], lo[1]);
-        if (DIM == 3) fx_limbs(v[2], hi[2], lo[2]);
+        fx_limbs_unchecked(v[0], hi[0], lo[0]);
+        fx_limbs_unchecked(v[1], hi[1], lo[1]);
+        if (DIM == 3) fx_limbs_unchecked(v[2], hi[2], lo[2]);
     } else {
         // several species (w = m) or a large velocity: FP64 conversion
         const double wf = w * kSumFx;
@@ -213,50 +213,61 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-// Cell pass: sums of this step -> u, R record; the sums are cleared.  Block
-// 0 also clears the next step's accumulators.
+// Cell pass: sums of this step -> u, axis record; the sums are cleared.
+// Each thread takes kResCellsPer cells (their loads issued together); the
+// block's records leave through shared memory as one contiguous range.
+// Block 0 also clears the next step's accumulators.
+constexpr int kResCellsPer = 2;
 template <int DIM>
 __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCfg c,
                                                    ResSum *sums, unsigned long long *msum,
                                                    ResRec *crec, StepArgs sa, double *acc,
                                                    double *acc_next) {
-    __shared__ float4 srec[2 * 256];
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float4 srec[2 * 256 * kResCellsPer];
+    __shared__ double wsum[8][3];
+    const int c0 = blockIdx.x * 256 * kResCellsPer;
     double av[3] = {0, 0, 0};
     if (blockIdx.x == 0 && threadIdx.x < ACC_WORDS) acc_next[threadIdx.x] = 0.0;
-    if (cell < c.ncells) {
-        const ResSum s = sums[cell];
-        sums[cell] = ResSum{{0, 0, 0}, 0};
-        const int pop = (int)s.n;
-        double W;  // divisor of the weighted sum: population or mass
-        if (msum) {
-            W = (double)(long long)msum[cell] * kSumFxInv;
-            msum[cell] = 0ull;
-        } else {
-            W = (double)pop;
+    ResSum s[kResCellsPer];
+    unsigned long long ms[kResCellsPer];
+#pragma unroll
+    for (int q = 0; q < kResCellsPer; q++) {
+        const int cell = c0 + q * 256 + threadIdx.x;
+        s[q] = ResSum{{0, 0, 0}, 0};
+        ms[q] = 0ull;
+        if (cell < c.ncells) {
+            s[q] = sums[cell];
+            if (msum) ms[q] = msum[cell];
         }
+    }
+#pragma unroll
+    for (int q = 0; q < kResCellsPer; q++) {
+        const int cell = c0 + q * 256 + threadIdx.x;
+        if (cell >= c.ncells) continue;
+        sums[cell] = ResSum{{0, 0, 0}, 0};
+        if (msum) msum[cell] = 0ull;
+        const int pop = (int)s[q].n;
+        // divisor of the weighted sum: population (one species) or mass
+        const double W = msum ? (double)(long long)ms[q] * kSumFxInv : (double)pop;
         double u[3] = {0, 0, 0};
         if (pop > 0 && W > 0.0) {
             const double iW = 1.0 / W;
-            for (int d = 0; d < DIM; d++) u[d] = ((double)s.p[d] * kSumFxInv) * iW;
+            for (int d = 0; d < DIM; d++) u[d] = ((double)s[q].p[d] * kSumFxInv) * iW;
         }
-        for (int d = 0; d < DIM; d++) av[d] = u[d];
+        for (int d = 0; d < DIM; d++) av[d] += u[d];
         double Lx[3] = {0, 0, 1};
         if (pop > 1 && DIM == 3) mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
-        float4 *my = srec + 2 * threadIdx.x;
+        float4 *my = srec + 2 * (q * 256 + threadIdx.x);
         my[0] = make_float4((float)u[0], (float)u[1], (float)u[2], __int_as_float(pop));
         my[1] = make_float4((float)Lx[0], (float)Lx[1], (float)Lx[2], 0.f);
     }
     __syncthreads();
     {
-        // the block's records leave as one contiguous, coalesced range
-        const int c0 = blockIdx.x * blockDim.x;
-        const int nrec = min((int)blockDim.x, c.ncells - c0);
+        const int nrec = min(256 * kResCellsPer, c.ncells - c0);
         float4 *dst = (float4 *)(crec + c0);
-        for (int j = threadIdx.x; j < 2 * nrec; j += blockDim.x) dst[j] = srec[j];
+        for (int j = threadIdx.x; j < 2 * nrec; j += 256) dst[j] = srec[j];
     }
     // block sum of the avVel terms: warp shuffles, then one thread per block
-    __shared__ double wsum[8][3];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int d = 0; d < DIM; d++) {
         const double t = warp_sum_d(av[d]);

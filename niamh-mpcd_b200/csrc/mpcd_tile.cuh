@@ -131,9 +131,11 @@ struct MixT {
             // periodic box: exact wrap and the short form of the next key
             int a[3] = {0, 0, 0};
             for (int d = 0; d < DIM; d++) {
+                // one period at most, unless the particle moved more than a box
                 if (ci[d] < 0) ci[d] += c.L[d];
                 else if (ci[d] >= c.L[d]) ci[d] -= c.L[d];
-                if (ci[d] < 0 || ci[d] >= c.L[d]) ci[d] = ((ci[d] % c.L[d]) + c.L[d]) % c.L[d];
+                if ((unsigned)ci[d] >= (unsigned)c.L[d])
+                    ci[d] = ((ci[d] % c.L[d]) + c.L[d]) % c.L[d];
                 a[d] = fx_shift_axis_pbc(ci[d], f[d], sa.ksn[d], c.L[d]);
             }
             r.P.x = f[0];
