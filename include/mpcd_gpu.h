@@ -257,6 +257,35 @@ int mpcd_set_kernel(mpcd_handle *h, int kernel);
  * reference. */
 int mpcd_set_sort_interval(mpcd_handle *h, int steps);
 
+/* ---------------------------------------------------------------------
+ * Ensembles: many independent periodic 3D SRD boxes of different sizes
+ * stepped together (mixed precision).  No counterpart in the reference,
+ * which runs one box per process.  Every kernel of a step runs once for the
+ * whole ensemble, driven by per-box offset tables; the step counter lives in
+ * device memory and each step is one replay of a captured CUDA graph.  Box b
+ * uses the generator key (seeds[b], replica b): its trajectory equals, bit
+ * for bit, that of a single-box handle (MPCD_KERNEL_RESIDENT) created with
+ * seed = seeds[b] and replica = b.
+ * base: dim 3, MPCD_COLL_ARBAXIS, one species, no gravity, MPCD_PREC_MIXED;
+ * its L and walls are ignored (every box is periodic).  L holds 3 sizes per
+ * box; seeds may be NULL (base->seed for every box). */
+typedef struct mpcd_batch mpcd_batch;
+int mpcd_batch_create(const mpcd_config *base, int nboxes, const int *L,
+                      const uint64_t *seeds, mpcd_batch **out);
+int mpcd_batch_destroy(mpcd_batch *b);
+/* npart[b] particles per box; Q, V: the boxes' arrays concatenated in box
+ * order (3 doubles per particle); step0 numbers the first step. */
+int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *Q, const double *V,
+                      uint32_t step0);
+int mpcd_batch_step(mpcd_batch *b, int nsteps);
+int mpcd_batch_download(mpcd_batch *b, double *Q, double *V);
+/* per-box TEMP (kbt[b]) and avVel (avv[3b..3b+2]) of the last step */
+int mpcd_batch_globals(mpcd_batch *b, double *kbt, double *avv);
+int mpcd_batch_set_sort_interval(mpcd_batch *b, int steps);
+int mpcd_batch_set_stream(mpcd_batch *b, void *stream);
+/* particles, particle slots (with padding) and cells (with padding) */
+int mpcd_batch_info(mpcd_batch *b, int *n, int *slots, int *cells);
+
 /* One SRD timestep that allocates no memory, device or host (no
  * counterpart in the reference, whose timestep works on host memory).  For
  * callers that cannot allocate at step time: a program whose allocator owns

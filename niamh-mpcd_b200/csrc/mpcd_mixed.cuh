@@ -183,6 +183,44 @@ __device__ __forceinline__ void fx_stream(uint32_t &f, int &ci, float dx) {
     f = (uint32_t)nq;
 }
 
+// Streaming, exact periodic wrap and next-step cell indices of one record
+// in a fully periodic box of L cells per axis, the next grid shift ksn (as
+// 32-bit fractions).  Shared by every mixed-precision kernel family so that
+// they stream identically.
+template <int DIM>
+__device__ __forceinline__ void fx_finish_periodic(uint4 &P, const float4 &W, float dtf,
+                                                   const int L[3], const uint32_t ksn[3],
+                                                   int idx[3]) {
+    int ci[3];
+    unpack_cell((int)P.w, ci[0], ci[1], ci[2]);
+    uint32_t f[3] = {P.x, P.y, P.z};
+    const float vv[3] = {W.x, W.y, W.z};
+    idx[0] = idx[1] = idx[2] = 0;
+    for (int d = 0; d < DIM; d++) {
+        fx_stream(f[d], ci[d], dtf * vv[d]);
+        // one period at most, unless the particle moved more than a box
+        if (ci[d] < 0) ci[d] += L[d];
+        else if (ci[d] >= L[d]) ci[d] -= L[d];
+        if ((unsigned)ci[d] >= (unsigned)L[d]) ci[d] = ((ci[d] % L[d]) + L[d]) % L[d];
+        idx[d] = fx_shift_axis_pbc(ci[d], f[d], ksn[d], L[d]);
+    }
+    P.x = f[0];
+    P.y = f[1];
+    P.z = DIM == 3 ? f[2] : 0u;
+    P.w = (unsigned)pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
+}
+
+// Current-step cell indices of a record in a fully periodic box.
+template <int DIM>
+__device__ __forceinline__ void fx_cur_idx_periodic(const uint4 &P, const int L[3],
+                                                    const uint32_t ks[3], int idx[3]) {
+    int ca, cb, cz;
+    unpack_cell((int)P.w, ca, cb, cz);
+    idx[0] = fx_shift_axis_pbc(ca, P.x, ks[0], L[0]);
+    idx[1] = fx_shift_axis_pbc(cb, P.y, ks[1], L[1]);
+    idx[2] = DIM == 3 ? fx_shift_axis_pbc(cz, P.z, ks[2], L[2]) : 0;
+}
+
 // Fixed-point representation of a coordinate (host and device).
 __host__ __device__ __forceinline__ void fx_from_double(double q, int &ci, uint32_t &f) {
     double fl = floor(q);

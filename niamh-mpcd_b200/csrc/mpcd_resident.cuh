@@ -123,15 +123,14 @@ __device__ __forceinline__ void res_global_add(ResSum *gs, unsigned long long *g
 // cells adjacent across rows or planes fall in different shared-memory
 // banks (a rotation within the field keeps the packing one-to-one).
 template <int DIM>
-__device__ __forceinline__ int res_slot(ResTable &t, const DevCfg &c, int k, const int idx[3]) {
+__device__ __forceinline__ int res_slot(ResTable &t, const int *mask, const int *shift, int k,
+                                        const int idx[3]) {
     unsigned h;
     if (DIM == 3)
-        h = (unsigned)(((idx[2] + 5 * idx[1] + 11 * idx[0]) & c.res_mask[2]) |
-                       ((idx[1] & c.res_mask[1]) << c.res_shift[1]) |
-                       ((idx[0] & c.res_mask[0]) << c.res_shift[0]));
+        h = (unsigned)(((idx[2] + 5 * idx[1] + 11 * idx[0]) & mask[2]) |
+                       ((idx[1] & mask[1]) << shift[1]) | ((idx[0] & mask[0]) << shift[0]));
     else
-        h = (unsigned)(((idx[1] + 5 * idx[0]) & c.res_mask[1]) |
-                       ((idx[0] & c.res_mask[0]) << c.res_shift[0]));
+        h = (unsigned)(((idx[1] + 5 * idx[0]) & mask[1]) | ((idx[0] & mask[0]) << shift[0]));
     for (int probe = 0; probe < kResProbe; probe++) {
         const int cur = *(volatile int *)&t.key[h];
         if (cur == k) return (int)h;
@@ -146,9 +145,10 @@ __device__ __forceinline__ int res_slot(ResTable &t, const DevCfg &c, int k, con
 
 // Add one particle (velocity v, weight w = 1 or its mass) to cell k.
 template <int DIM>
-__device__ __forceinline__ void res_add(ResTable &t, const DevCfg &c, ResSum *sums,
-                                        unsigned long long *msum, int k, const int idx[3],
-                                        const float v[3], double w, bool multi, int &bad) {
+__device__ __forceinline__ void res_add(ResTable &t, const int *mask, const int *shift,
+                                        ResSum *sums, unsigned long long *msum, int k,
+                                        const int idx[3], const float v[3], double w, bool multi,
+                                        int &bad) {
     const int nc = multi ? DIM + 1 : DIM;
     int hi[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0};
     bool fast = !multi && fabsf(v[0]) < kResBigV && fabsf(v[1]) < kResBigV &&
@@ -175,7 +175,7 @@ __device__ __forceinline__ void res_add(ResTable &t, const DevCfg &c, ResSum *su
             lo[d] = (int)(x[d] - q * (1ll << kLimb));
         }
     }
-    const int slot = res_slot<DIM>(t, c, k, idx);
+    const int slot = res_slot<DIM>(t, mask, shift, k, idx);
     if (slot >= 0) {
         atomicAdd(&t.cnt[slot], 1u);
         for (int d = 0; d < nc; d++) {
@@ -205,6 +205,28 @@ __device__ __forceinline__ void res_flush(const ResTable &t, ResSum *sums,
                     (long long)t.lo[d * kResSlots + s];
         }
         res_global_add(sums, msum, k, x, t.cnt[s], multi);
+    }
+}
+
+// v' = u + R (v - u) from a cell's record (Rodrigues form, see ResRec);
+// cells of fewer than two particles leave v unchanged.
+template <int DIM>
+__device__ __forceinline__ void res_rotate(float4 &W, const ResRec *rec, float Cs, float Sn) {
+    const float4 *q = (const float4 *)rec;
+    const float4 ca = __ldg(q);
+    if (__float_as_int(ca.w) > 1) {
+        const float w0 = W.x - ca.x, w1 = W.y - ca.y;
+        if (DIM == 3) {
+            const float4 cb = __ldg(q + 1);
+            const float w2 = W.z - ca.z;
+            const float ld = (cb.x * w0 + cb.y * w1 + cb.z * w2) * (1.f - Cs);
+            W.x = ca.x + (Cs * w0 + ld * cb.x + Sn * (cb.y * w2 - cb.z * w1));
+            W.y = ca.y + (Cs * w1 + ld * cb.y + Sn * (cb.z * w0 - cb.x * w2));
+            W.z = ca.z + (Cs * w2 + ld * cb.z + Sn * (cb.x * w1 - cb.y * w0));
+        } else {
+            W.x = ca.x + (Cs * w0 - Sn * w1);
+            W.y = ca.y + (Sn * w0 + Cs * w1);
+        }
     }
 }
 
@@ -344,23 +366,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
         int k, kidx[3];
         if (MODE == RES_STEP) {
             const int kc = cur_key<DIM>(c, r, sa);
-            const float4 *q = (const float4 *)(crec + kc);
-            const float4 ca = __ldg(q);
-            if (__float_as_int(ca.w) > 1) {
-                const float Cs = cosf_a, Sn = sinf_a;
-                const float w0 = r.W.x - ca.x, w1 = r.W.y - ca.y;
-                if (DIM == 3) {
-                    const float4 cb = __ldg(q + 1);
-                    const float w2 = r.W.z - ca.z;
-                    const float ld = (cb.x * w0 + cb.y * w1 + cb.z * w2) * (1.f - Cs);
-                    r.W.x = ca.x + (Cs * w0 + ld * cb.x + Sn * (cb.y * w2 - cb.z * w1));
-                    r.W.y = ca.y + (Cs * w1 + ld * cb.y + Sn * (cb.z * w0 - cb.x * w2));
-                    r.W.z = ca.z + (Cs * w2 + ld * cb.z + Sn * (cb.x * w1 - cb.y * w0));
-                } else {
-                    r.W.x = ca.x + (Cs * w0 - Sn * w1);
-                    r.W.y = ca.y + (Sn * w0 + Cs * w1);
-                }
-            }
+            res_rotate<DIM>(r.W, crec + kc, cosf_a, sinf_a);
             float tt = r.W.x * r.W.x + r.W.y * r.W.y;
             if (DIM == 3) tt += r.W.z * r.W.z;
             if (multi)
@@ -379,7 +385,8 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
             k = cur_key_idx<DIM>(c, r, sa, kidx);
         }
         const float vs[3] = {r.W.x, r.W.y, DIM == 3 ? r.W.z : 0.f};
-        res_add<DIM>(t, c, sums, msum, k, kidx, vs, multi ? c.mass[sp] : 1.0, multi, bad);
+        res_add<DIM>(t, c.res_mask, c.res_shift, sums, msum, k, kidx, vs,
+                     multi ? c.mass[sp] : 1.0, multi, bad);
     }
     __syncthreads();
     res_flush<DIM>(t, sums, msum, multi);

@@ -123,9 +123,7 @@ __device__ __forceinline__ int cur_key_idx(const DevCfg &c, const MixRec &r,
     uint32_t t;
     unpack_cell((int)r.P.w, ca, cb, cz);
     if (c.all_periodic) {
-        idx[0] = fx_shift_axis_pbc(ca, r.P.x, sa.ks[0], c.L[0]);
-        idx[1] = fx_shift_axis_pbc(cb, r.P.y, sa.ks[1], c.L[1]);
-        idx[2] = DIM == 3 ? fx_shift_axis_pbc(cz, r.P.z, sa.ks[2], c.L[2]) : 0;
+        fx_cur_idx_periodic<DIM>(r.P, c.L, sa.ks, idx);
     } else {
         idx[0] = fx_shift_axis(ca, r.P.x, sa.ks[0], c.L[0], c.pbc[0], t, e);
         idx[1] = fx_shift_axis(cb, r.P.y, sa.ks[1], c.L[1], c.pbc[1], t, e);

@@ -121,30 +121,17 @@ struct MixT {
     static __device__ __forceinline__ int finish_idx(const DevCfg &c, Rec &r, int sp,
                                                      const StepArgs &sa, int &bounce, int &esc,
                                                      int idx[3]) {
+        const float dtf = (float)c.dt;
+        if (c.all_periodic) {
+            // periodic box: exact wrap and the short form of the next key
+            fx_finish_periodic<DIM>(r.P, r.W, dtf, c.L, sa.ksn, idx);
+            return cell_lin(c, idx[0], idx[1], idx[2]);
+        }
         int ci[3];
         unpack_cell((int)r.P.w, ci[0], ci[1], ci[2]);
         uint32_t f[3] = {r.P.x, r.P.y, r.P.z};
         float vv[3] = {r.W.x, r.W.y, r.W.z};
-        const float dtf = (float)c.dt;
         for (int d = 0; d < DIM; d++) fx_stream(f[d], ci[d], dtf * vv[d]);
-        if (c.all_periodic) {
-            // periodic box: exact wrap and the short form of the next key
-            int a[3] = {0, 0, 0};
-            for (int d = 0; d < DIM; d++) {
-                // one period at most, unless the particle moved more than a box
-                if (ci[d] < 0) ci[d] += c.L[d];
-                else if (ci[d] >= c.L[d]) ci[d] -= c.L[d];
-                if ((unsigned)ci[d] >= (unsigned)c.L[d])
-                    ci[d] = ((ci[d] % c.L[d]) + c.L[d]) % c.L[d];
-                a[d] = fx_shift_axis_pbc(ci[d], f[d], sa.ksn[d], c.L[d]);
-            }
-            r.P.x = f[0];
-            r.P.y = f[1];
-            r.P.z = DIM == 3 ? f[2] : 0u;
-            r.P.w = (unsigned)pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
-            for (int d = 0; d < 3; d++) idx[d] = a[d];
-            return cell_lin(c, a[0], a[1], a[2]);
-        }
         if (c.n_solid > 0) {
             double q[3] = {0, 0, 0}, v[3] = {0, 0, 0};
             for (int d = 0; d < DIM; d++) {

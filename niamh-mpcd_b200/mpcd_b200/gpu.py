@@ -21,7 +21,9 @@ EXPORTS = [
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
     "mpcd_set_sort_interval", "mpcd_set_timing", "mpcd_kernel_time",
-    "mpcd_srd_step_noalloc",
+    "mpcd_srd_step_noalloc", "mpcd_batch_create", "mpcd_batch_destroy", "mpcd_batch_upload",
+    "mpcd_batch_step", "mpcd_batch_download", "mpcd_batch_globals",
+    "mpcd_batch_set_sort_interval", "mpcd_batch_set_stream", "mpcd_batch_info",
 ]
 
 _lib = None
@@ -58,6 +60,15 @@ def load():
         lib.mpcd_set_kernel.argtypes = [vp, C.c_int]
         lib.mpcd_set_sort_interval.argtypes = [vp, C.c_int]
         lib.mpcd_set_timing.argtypes = [vp, C.c_int]
+        lib.mpcd_batch_create.argtypes = [vp, C.c_int, vp, vp, vp]
+        lib.mpcd_batch_destroy.argtypes = [vp]
+        lib.mpcd_batch_upload.argtypes = [vp, vp, vp, vp, C.c_uint32]
+        lib.mpcd_batch_step.argtypes = [vp, C.c_int]
+        lib.mpcd_batch_download.argtypes = [vp, vp, vp]
+        lib.mpcd_batch_globals.argtypes = [vp, vp, vp]
+        lib.mpcd_batch_set_sort_interval.argtypes = [vp, C.c_int]
+        lib.mpcd_batch_set_stream.argtypes = [vp, vp]
+        lib.mpcd_batch_info.argtypes = [vp, vp, vp, vp]
         lib.mpcd_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         lib.mpcd_srd_step_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_uint32, vp, vp]
         _lib = lib
@@ -162,6 +173,70 @@ class Solver:
         if self.h:
             self.lib.mpcd_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """An ensemble of periodic 3D SRD boxes stepped together (mpcd_batch_*)."""
+
+    def __init__(self, base_cfg, sizes, seeds=None):
+        self.lib = load()
+        self.sizes = np.ascontiguousarray(np.asarray(sizes, dtype=np.int32).reshape(-1, 3))
+        self.nb = len(self.sizes)
+        self.seeds = (None if seeds is None
+                      else np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64)))
+        self.h = C.c_void_p()
+        _check(self.lib.mpcd_batch_create(C.byref(base_cfg), self.nb, _p(self.sizes),
+                                          _p(self.seeds) if self.seeds is not None else None,
+                                          C.byref(self.h)), "mpcd_batch_create")
+        self.npart = None
+
+    def upload(self, npart, Q, V, step0=1):
+        self.npart = np.ascontiguousarray(np.asarray(npart, dtype=np.int32))
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        _check(self.lib.mpcd_batch_upload(self.h, _p(self.npart), _p(Q), _p(V), step0),
+               "mpcd_batch_upload")
+
+    def step(self, nsteps=1):
+        _check(self.lib.mpcd_batch_step(self.h, nsteps), "mpcd_batch_step")
+
+    def download(self):
+        n = int(self.npart.sum())
+        Q = np.zeros((n, 3))
+        V = np.zeros((n, 3))
+        _check(self.lib.mpcd_batch_download(self.h, _p(Q), _p(V)), "mpcd_batch_download")
+        return Q, V
+
+    def globals(self):
+        kb = np.zeros(self.nb)
+        av = np.zeros((self.nb, 3))
+        _check(self.lib.mpcd_batch_globals(self.h, _p(kb), _p(av)), "mpcd_batch_globals")
+        return kb, av
+
+    def set_sort_interval(self, steps):
+        _check(self.lib.mpcd_batch_set_sort_interval(self.h, steps),
+               "mpcd_batch_set_sort_interval")
+
+    def set_stream(self, stream_ptr):
+        _check(self.lib.mpcd_batch_set_stream(self.h, C.c_void_p(stream_ptr)),
+               "mpcd_batch_set_stream")
+
+    def info(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(self.lib.mpcd_batch_info(self.h, C.byref(a), C.byref(b), C.byref(c)),
+               "mpcd_batch_info")
+        return a.value, b.value, c.value
+
+    def close(self):
+        if self.h:
+            self.lib.mpcd_batch_destroy(self.h)
+            self.h = C.c_void_p()
 
     def __del__(self):
         try:
