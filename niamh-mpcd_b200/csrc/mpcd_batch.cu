@@ -249,7 +249,8 @@ struct mpcd_batch {
     ResRec *crec = nullptr;
     double *acc = nullptr;  // 2 x nb x ACC_WORDS, by step parity
     unsigned long long *status = nullptr;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // where the steps run
+    cudaStream_t cap_stream = nullptr;  // private stream the step graphs are captured on
     bool own_stream = true;
     // one captured step per (with re-sort, step parity, current state buffer)
     cudaGraphExec_t graph[2][2][2] = {};
@@ -358,7 +359,9 @@ extern "C" int mpcd_batch_create(const mpcd_config *base, int nboxes, const int 
     }
     b->ncells = cell0;
     b->ncblk = (int)b->hcblk_box.size();
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return MPCD_ERR_CUDA;
     }
@@ -371,6 +374,7 @@ extern "C" int mpcd_batch_destroy(mpcd_batch *b) {
     cudaStreamSynchronize(b->stream);
     batch_free(b);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     delete b;
     return MPCD_OK;
 }
@@ -480,29 +484,29 @@ static int record_step(mpcd_batch *b, bool sorted, int parity, int state_cur,
     double *acc_nxt = b->acc + (size_t)(1 - parity) * b->nb * ACC_WORDS;
     const int pbytes = res_table_bytes(3);
     int cur = state_cur;
-    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    k_bat_shift<<<(b->nb + 127) / 128, 128, 0, b->stream>>>(b->box, b->nb, b->st, b->counter,
+    BCK(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+    k_bat_shift<<<(b->nb + 127) / 128, 128, 0, b->cap_stream>>>(b->box, b->nb, b->st, b->counter,
                                                              b->dc.galinv);
     if (sorted) {
-        k_bat_key<<<grid_for(b, b->nslots), 256, 0, b->stream>>>(
+        k_bat_key<<<grid_for(b, b->nslots), 256, 0, b->cap_stream>>>(
             b->box, b->chunk_box, b->st, b->mx[cur], b->nslots, b->key, b->rank, b->count);
-        k_scan_partial<<<b->nscan, 256, 0, b->stream>>>(b->count, b->ncells, b->part);
-        k_scan_apply<<<b->nscan, 256, 0, b->stream>>>(b->count, b->ncells, b->part, b->start,
+        k_scan_partial<<<b->nscan, 256, 0, b->cap_stream>>>(b->count, b->ncells, b->part);
+        k_scan_apply<<<b->nscan, 256, 0, b->cap_stream>>>(b->count, b->ncells, b->part, b->start,
                                                       nullptr, nullptr);
-        k_perm<<<grid_for(b, b->nslots), 256, 0, b->stream>>>(b->nslots, b->key, b->rank,
+        k_perm<<<grid_for(b, b->nslots), 256, 0, b->cap_stream>>>(b->nslots, b->key, b->rank,
                                                                b->start, b->perm);
-        k_gather_mix<<<grid_for(b, b->nslots), 256, 0, b->stream>>>(b->mx[cur],
+        k_gather_mix<<<grid_for(b, b->nslots), 256, 0, b->cap_stream>>>(b->mx[cur],
                                                                       b->mx[1 - cur],
                                                                       b->nslots, b->perm);
         cur = 1 - cur;
     }
-    k_bat_cells<<<b->ncblk, 256, 0, b->stream>>>(b->dc, b->box, b->cblk_box, b->st, sum_cur,
+    k_bat_cells<<<b->ncblk, 256, 0, b->cap_stream>>>(b->dc, b->box, b->cblk_box, b->st, sum_cur,
                                                  b->crec, acc_cur, acc_nxt, b->nb);
-    k_bat_parts<RES_STEP><<<b->nchunks, kResThreads, pbytes, b->stream>>>(
+    k_bat_parts<RES_STEP><<<b->nchunks, kResThreads, pbytes, b->cap_stream>>>(
         b->dc, b->box, b->chunk_box, b->st, b->mx[cur], b->crec, sum_nxt, acc_cur, b->status);
-    k_bat_advance<<<1, 32, 0, b->stream>>>(b->counter);
+    k_bat_advance<<<1, 32, 0, b->cap_stream>>>(b->counter);
     cudaGraph_t g = nullptr;
-    const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
+    const cudaError_t ec = cudaStreamEndCapture(b->cap_stream, &g);
     if (ec != cudaSuccess) {
         fprintf(stderr, "mpcd batch: capture failed: %s\n", cudaGetErrorString(ec));
         return MPCD_ERR_CUDA;
@@ -615,7 +619,9 @@ extern "C" int mpcd_batch_info(mpcd_batch *b, int *n, int *slots, int *cells) {
     return MPCD_OK;
 }
 
-// Use the caller's CUDA stream from now on (graphs are re-captured).
+// Run the steps on the caller's CUDA stream from now on (the graphs are
+// captured on a private stream and launched on this one; any stream works,
+// the legacy default stream included).
 extern "C" int mpcd_batch_set_stream(mpcd_batch *b, void *stream) {
     if (!b) return MPCD_ERR_ARG;
     BCK(cudaStreamSynchronize(b->stream));

@@ -81,3 +81,22 @@ def test_batch_rejects_unsupported_configs():
     base = W.cfg_srd3d((8, 8, 8), precision=abi.PREC_FP64)
     with pytest.raises(Exception):
         Batch(base, [(8, 8, 8)])
+
+
+def test_batch_runs_on_the_legacy_default_stream():
+    # the step graphs are captured on a private stream, so any launch stream
+    # works, the legacy default stream (handle 0) included
+    states = _states()[:3]
+    base = W.cfg_srd3d(SIZES[0], precision=abi.PREC_MIXED, seed=3)
+    out = []
+    for use_default in (False, True):
+        bat = Batch(base, SIZES[:3], SEEDS[:3])
+        if use_default:
+            bat.set_stream(0)
+        bat.upload([len(Q) for _, Q, _ in states], np.concatenate([Q for _, Q, _ in states]),
+                   np.concatenate([V for _, _, V in states]), step0=5)
+        bat.step(4)
+        out.append(bat.download())
+        bat.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
