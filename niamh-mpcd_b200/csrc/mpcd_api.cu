@@ -877,7 +877,7 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
         if (h->rmsum)
             CK(cudaMemsetAsync(h->rmsum, 0, sizeof(unsigned long long) * 2 * nc, h->stream));
         CK(cudaMemsetAsync(acc_cur, 0, sizeof(double) * ACC_WORDS, h->stream));
-        auto ksum = k_res_parts<DIM, RES_SUM>;
+        auto ksum = k_res_parts<DIM, RES_SUM, false>;
         CK(cudaFuncSetAttribute(ksum, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
         CK(cudaFuncSetAttribute(ksum, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         ksum<<<pgrid, kResThreads, pbytes, h->stream>>>(c, h->mx[h->cur], h->n,
@@ -888,7 +888,8 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     k_res_cells<DIM><<<(int)((nc + 256 * kResCellsPer - 1) / (256 * kResCellsPer)), 256, 0,
                        h->stream>>>(
         c, sum_cur, ms_cur, (CRec *)h->crec, sa, acc_cur, acc_nxt);
-    auto kstep = k_res_parts<DIM, RES_STEP>;
+    const bool lean = c.all_periodic && !h->rmsum && !c.grav_flag;
+    auto kstep = lean ? k_res_parts<DIM, RES_STEP, true> : k_res_parts<DIM, RES_STEP, false>;
     CK(cudaFuncSetAttribute(kstep, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
     CK(cudaFuncSetAttribute(kstep, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     time_begin(h);

@@ -315,7 +315,9 @@ enum { RES_STEP = 0, RES_SUM = 1 };
 // block's table with native 32-bit shared-memory atomics (or, if the table
 // has no slot for it, straight to global memory); at the end every table
 // entry is added to the global sums once.
-template <int DIM, int MODE>
+// LEAN: the common case of a fully periodic box, one species and no
+// gravity, compiled without the general paths (walls, species, gravity).
+template <int DIM, int MODE, bool LEAN>
 __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     const __grid_constant__ DevCfg c, MixState a, int n,
     const ResRec *__restrict__ crec, ResSum *sums, unsigned long long *msum, double *acc,
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     extern __shared__ __align__(16) unsigned char res_smem[];
     __shared__ double red[8];
     const int tid = threadIdx.x;
-    const bool multi = msum != nullptr;
+    const bool multi = !LEAN && msum != nullptr;
     const int nc = multi ? DIM + 1 : DIM;
     ResTable t;
     t.bind(res_smem, nc);
@@ -357,7 +359,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
             nx.P = a.P[i + kResThreads];
             nx.W = a.W[i + kResThreads];
         }
-        if (c.grav_flag) {
+        if (!LEAN && c.grav_flag) {
             r.W.x += gk[0];
             r.W.y += gk[1];
             if (DIM == 3) r.W.z += gk[2];
@@ -365,7 +367,14 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
         const int sp = multi ? MixT<DIM>::sp(a, i) : 0;
         int k, kidx[3];
         if (MODE == RES_STEP) {
-            const int kc = cur_key<DIM>(c, r, sa);
+            int kc;
+            if (LEAN) {
+                int cidx[3];
+                fx_cur_idx_periodic<DIM>(r.P, c.L, sa.ks, cidx);
+                kc = cell_lin(c, cidx[0], cidx[1], cidx[2]);
+            } else {
+                kc = cur_key<DIM>(c, r, sa);
+            }
             res_rotate<DIM>(r.W, crec + kc, cosf_a, sinf_a);
             float tt = r.W.x * r.W.x + r.W.y * r.W.y;
             if (DIM == 3) tt += r.W.z * r.W.z;
@@ -373,10 +382,15 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
                 ke_m += c.mass[sp] * (double)tt;
             else
                 ke += tt;
-            k = MixT<DIM>::finish_idx(c, r, sp, sa, bounce, esc, kidx);
+            if (LEAN) {
+                fx_finish_periodic<DIM>(r.P, r.W, (float)c.dt, c.L, sa.ksn, kidx);
+                k = cell_lin(c, kidx[0], kidx[1], kidx[2]);
+            } else {
+                k = MixT<DIM>::finish_idx(c, r, sp, sa, bounce, esc, kidx);
+            }
             MixT<DIM>::store(a, i, r);
             // the next step's load adds the same FP32 gravity kick
-            if (c.grav_flag) {
+            if (!LEAN && c.grav_flag) {
                 r.W.x += gk[0];
                 r.W.y += gk[1];
                 if (DIM == 3) r.W.z += gk[2];
