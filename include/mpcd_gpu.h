@@ -195,6 +195,14 @@ int mpcd_globals(mpcd_handle *h, double *kbtnow, double avnow[3]);
 int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
                     double *cm);
 
+/* Transverse momentum modes of the smallest wavevectors (an analysis
+ * helper with no counterpart in the reference): for each ordered pair of
+ * axes (a, b), a != b (b outer, a inner), j = sum_i v_i,a exp(-2 pi i
+ * x_i,b / L_b), written as (Re, Im) pairs to out[0 .. 2*nmodes-1] (at most
+ * 12 doubles; nmodes = 6 in 3D, 2 in 2D).  Their decay measures the
+ * kinematic viscosity. */
+int mpcd_transverse_modes(mpcd_handle *h, double *out, int *nmodes);
+
 /* Error counters accumulated so far. */
 int mpcd_get_status(mpcd_handle *h, mpcd_status *st);
 

@@ -51,6 +51,7 @@ struct mpcd_handle {
     void *crec;      // per-cell SRD records (split kernel family)
     LcCells lcc;     // per-cell nematic arrays (lc != 0)
     double *lcbuf;
+    double *modes;   // transverse momentum modes (mpcd_transverse_modes)
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     ResSum *rsum;              // resident family: cell sums, two steps by parity
     unsigned long long *rmsum;  // resident family: mass sums (several species)
@@ -285,6 +286,7 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->acc);
     cudaFree(h->status);
     cudaFree(h->crec);
+    cudaFree(h->modes);
     cudaFree(h->rsum);
     cudaFree(h->rmsum);
     cudaFree(h->lcbuf);
@@ -1094,6 +1096,93 @@ extern "C" int mpcd_kernel_time(mpcd_handle *h, double *ms_total, int *launches)
     *ms_total = t;
     *launches = (int)h->tev.size();
     time_clear(h);
+    return MPCD_OK;
+}
+
+// Transverse momentum modes of the smallest wavevectors: for each ordered
+// pair (a, b), a != b, j = sum_i v_i,a exp(-2 pi i x_i,b / L_b), accumulated
+// as (Re, Im) in FP64 (phases in FP32).  Pair order: b outer, a inner.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_modes_mix(const __grid_constant__ DevCfg c, MixState s,
+                                                   int n, double *out) {
+    constexpr int NM = DIM * (DIM - 1);
+    double acc[2 * NM];
+    for (int j = 0; j < 2 * NM; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4 P = s.P[i];
+        const float4 W = s.W[i];
+        int ci[3];
+        unpack_cell((int)P.w, ci[0], ci[1], ci[2]);
+        const uint32_t f[3] = {P.x, P.y, P.z};
+        const float v[3] = {W.x, W.y, W.z};
+        int m = 0;
+        for (int b = 0; b < DIM; b++) {
+            const float x = (float)ci[b] + (float)((double)f[b] * kFxInv);
+            float sn, cs;
+            sincospif(2.0f * x / (float)c.L[b], &sn, &cs);
+            for (int a = 0; a < DIM; a++) {
+                if (a == b) continue;
+                acc[2 * m] += (double)(v[a] * cs);
+                acc[2 * m + 1] -= (double)(v[a] * sn);
+                m++;
+            }
+        }
+    }
+    for (int j = 0; j < 2 * NM; j++) {
+        double t = acc[j];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&out[j], t);
+    }
+}
+template <int DIM>
+__global__ void __launch_bounds__(256) k_modes_f64(const __grid_constant__ DevCfg c,
+                                                   Fp64State s, int n, double *out) {
+    constexpr int NM = DIM * (DIM - 1);
+    double acc[2 * NM];
+    for (int j = 0; j < 2 * NM; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int m = 0;
+        for (int b = 0; b < DIM; b++) {
+            double sn, cs;
+            sincospi(2.0 * s.q[b][i] / (double)c.L[b], &sn, &cs);
+            for (int a = 0; a < DIM; a++) {
+                if (a == b) continue;
+                acc[2 * m] += s.v[a][i] * cs;
+                acc[2 * m + 1] -= s.v[a][i] * sn;
+                m++;
+            }
+        }
+    }
+    for (int j = 0; j < 2 * NM; j++) {
+        double t = acc[j];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&out[j], t);
+    }
+}
+
+extern "C" int mpcd_transverse_modes(mpcd_handle *h, double *out, int *nmodes) {
+    if (!h || !out) return MPCD_ERR_ARG;
+    if (h->n <= 0) return MPCD_ERR_STATE;
+    const int dim = h->dc.dim, nm = dim * (dim - 1);
+    if (!h->modes) CK(cudaMalloc((void **)&h->modes, sizeof(double) * 12));
+    CK(cudaMemsetAsync(h->modes, 0, sizeof(double) * 12, h->stream));
+    const int grid = grid_for(h, h->n);
+    if (h->prec == MPCD_PREC_MIXED) {
+        if (dim == 3)
+            k_modes_mix<3><<<grid, 256, 0, h->stream>>>(h->dc, h->mx[h->cur], h->n, h->modes);
+        else
+            k_modes_mix<2><<<grid, 256, 0, h->stream>>>(h->dc, h->mx[h->cur], h->n, h->modes);
+    } else {
+        if (dim == 3)
+            k_modes_f64<3><<<grid, 256, 0, h->stream>>>(h->dc, h->f[h->cur], h->n, h->modes);
+        else
+            k_modes_f64<2><<<grid, 256, 0, h->stream>>>(h->dc, h->f[h->cur], h->n, h->modes);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, h->modes, sizeof(double) * 2 * nm, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (nmodes) *nmodes = nm;
     return MPCD_OK;
 }
 

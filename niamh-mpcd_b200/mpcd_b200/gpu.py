@@ -21,6 +21,7 @@ EXPORTS = [
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
     "mpcd_set_sort_interval", "mpcd_set_timing", "mpcd_kernel_time",
+    "mpcd_transverse_modes",
     "mpcd_srd_step_noalloc", "mpcd_batch_create", "mpcd_batch_destroy", "mpcd_batch_upload",
     "mpcd_batch_step", "mpcd_batch_download", "mpcd_batch_globals",
     "mpcd_batch_set_sort_interval", "mpcd_batch_set_stream", "mpcd_batch_info",
@@ -60,6 +61,7 @@ def load():
         lib.mpcd_set_kernel.argtypes = [vp, C.c_int]
         lib.mpcd_set_sort_interval.argtypes = [vp, C.c_int]
         lib.mpcd_set_timing.argtypes = [vp, C.c_int]
+        lib.mpcd_transverse_modes.argtypes = [vp, vp, C.POINTER(C.c_int)]
         lib.mpcd_batch_create.argtypes = [vp, C.c_int, vp, vp, vp]
         lib.mpcd_batch_destroy.argtypes = [vp]
         lib.mpcd_batch_upload.argtypes = [vp, vp, vp, vp, C.c_uint32]
@@ -152,6 +154,14 @@ class Solver:
 
     def set_kernel(self, kernel):
         _check(self.lib.mpcd_set_kernel(self.h, kernel), "mpcd_set_kernel")
+
+    def transverse_modes(self):
+        """The transverse momentum modes as complex numbers (6 in 3D)."""
+        out = np.zeros(12)
+        nm = C.c_int()
+        _check(self.lib.mpcd_transverse_modes(self.h, _p(out), C.byref(nm)),
+               "mpcd_transverse_modes")
+        return out[0:2 * nm.value:2] + 1j * out[1:2 * nm.value:2]
 
     def set_timing(self, enable=True):
         _check(self.lib.mpcd_set_timing(self.h, 1 if enable else 0), "mpcd_set_timing")

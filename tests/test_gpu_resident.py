@@ -169,3 +169,57 @@ def test_resident_conserves_momentum_exactly_in_fixed_point():
     g.step(50, 1)
     _, v, _ = g.download()
     assert np.abs(v.sum(axis=0) - p0).max() / np.abs(V).sum() < 1e-6
+
+
+def _cell_momenta(Q, V, L):
+    idx = np.floor(Q[:, :3]).astype(np.int64)
+    lin = (idx[:, 0] * L[1] + idx[:, 1]) * L[2] + idx[:, 2]
+    n = int(np.prod(L))
+    p = np.zeros((n, 3))
+    for d in range(3):
+        p[:, d] = np.bincount(lin, weights=V[:, d], minlength=n)
+    return p
+
+
+@pytest.mark.parametrize("prec,kernel,tol", [
+    (abi.PREC_FP64, abi.KERNEL_SPLIT, 1e-10),
+    (abi.PREC_MIXED, abi.KERNEL_SPLIT, 2e-6),
+    (abi.PREC_MIXED, abi.KERNEL_RESIDENT, 2e-6),
+])
+def test_collision_conserves_each_cells_momentum(prec, kernel, tol):
+    # no grid shift and no streaming to speak of (dt = 1e-30): the collision
+    # cells are the unshifted cells and positions do not move, so each
+    # cell's momentum before and after the step must agree (SRD conserves
+    # it per cell)
+    L = (10, 9, 8)
+    cfg = W.cfg_srd3d(L, precision=prec, seed=21, galinv=0, dt=1e-30)
+    Q, V, U, sp = W.synthetic_state(cfg, 10, seed=22)
+    g = Solver(cfg)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, sp)
+    q0, v0, _ = g.download()
+    g.step(1, 1)
+    q1, v1, _ = g.download()
+    np.testing.assert_allclose(q1, q0, rtol=0, atol=1e-12)
+    p0 = _cell_momenta(q0, v0, L)
+    p1 = _cell_momenta(q1, v1, L)
+    scale = np.abs(v0).sum() / len(p0)
+    assert np.abs(p1 - p0).max() / scale < tol
+    # and something did happen
+    assert np.abs(v1 - v0).max() > 0.1
+
+
+@pytest.mark.parametrize("prec,tol", [(abi.PREC_FP64, 1e-9), (abi.PREC_MIXED, 1e-4)])
+def test_transverse_modes_match_host_restatement(prec, tol):
+    from mpcd_b200.validate import transverse_modes
+    L = (12, 10, 8)
+    cfg = W.cfg_srd3d(L, precision=prec, seed=31)
+    Q, V, U, sp = W.synthetic_state(cfg, 10, seed=32)
+    g = Solver(cfg)
+    g.upload(Q, V, U, sp)
+    g.step(3, 1)
+    q, v, _ = g.download()
+    dev = g.transverse_modes()
+    host = transverse_modes(q, v, L)
+    scale = np.abs(v).sum()
+    assert np.abs(dev - host).max() / scale < tol
