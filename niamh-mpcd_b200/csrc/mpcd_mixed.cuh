@@ -194,15 +194,28 @@ __device__ __forceinline__ void fx_finish_periodic(uint4 &P, const float4 &W, fl
     int ci[3];
     unpack_cell((int)P.w, ci[0], ci[1], ci[2]);
     uint32_t f[3] = {P.x, P.y, P.z};
-    const float vv[3] = {W.x, W.y, W.z};
+    const float dx[3] = {dtf * W.x, dtf * W.y, dtf * W.z};
     idx[0] = idx[1] = idx[2] = 0;
-    for (int d = 0; d < DIM; d++) {
-        fx_stream(f[d], ci[d], dtf * vv[d]);
-        // one period at most, unless the particle moved more than a box
-        if (ci[d] < 0) ci[d] += L[d];
-        else if (ci[d] >= L[d]) ci[d] -= L[d];
-        if ((unsigned)ci[d] >= (unsigned)L[d]) ci[d] = ((ci[d] % L[d]) + L[d]) % L[d];
-        idx[d] = fx_shift_axis_pbc(ci[d], f[d], ksn[d], L[d]);
+    bool fast = fabsf(dx[0]) < 1.0f && fabsf(dx[1]) < 1.0f;
+    if (DIM == 3) fast = fast && fabsf(dx[2]) < 1.0f;
+    if (fast) {
+        // every displacement below one cell: 32-bit adds, one-period wrap
+        for (int d = 0; d < DIM; d++) {
+            int hi, lo;
+            fx_limbs_unchecked(dx[d], hi, lo);
+            const uint32_t nf = f[d] + (((uint32_t)hi << 20) + (uint32_t)lo);
+            int c = ci[d] + (dx[d] >= 0.0f ? (nf < f[d] ? 1 : 0) : (nf > f[d] ? -1 : 0));
+            c = c < 0 ? c + L[d] : (c >= L[d] ? c - L[d] : c);
+            f[d] = nf;
+            ci[d] = c;
+            idx[d] = fx_shift_axis_pbc(c, nf, ksn[d], L[d]);
+        }
+    } else {
+        for (int d = 0; d < DIM; d++) {
+            fx_stream(f[d], ci[d], dx[d]);
+            ci[d] = ((ci[d] % L[d]) + L[d]) % L[d];
+            idx[d] = fx_shift_axis_pbc(ci[d], f[d], ksn[d], L[d]);
+        }
     }
     P.x = f[0];
     P.y = f[1];
