@@ -238,8 +238,13 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         };
         int bits[3] = {0, 0, 0};
         if (dc->dim == 3) {
+            // a block's particles span one or two planes of the slowest
+            // axis and a few rows of the middle one; their next cells add
+            // one cell on each side: 2 bits for the slowest axis, up to 3
+            // for the middle one, the rest for the fastest
             bits[2] = std::min(clog2(dc->L[2]), kResBits - 4);
-            bits[1] = std::min(3, clog2(dc->L[1]));
+            bits[0] = std::min(2, clog2(dc->L[0]));
+            bits[1] = std::min(std::min(3, clog2(dc->L[1])), kResBits - bits[2] - bits[0]);
             bits[0] = kResBits - bits[2] - bits[1];
             dc->res_shift[2] = 0;
             dc->res_shift[1] = bits[2];
