@@ -791,8 +791,9 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
     host_shift(h, step, sa.s);
     host_shift(h, step + 1u, sa.sn);
     for (int d = 0; d < 3; d++) {  // s = k * 2^-32 exactly
-        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0);
-        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0);
+        // the mixed form's position words carry 22 fraction bits
+        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0) & kShiftMask;
+        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0) & kShiftMask;
     }
     double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
     double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
@@ -855,8 +856,9 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     host_shift(h, step, sa.s);
     host_shift(h, step + 1u, sa.sn);
     for (int d = 0; d < 3; d++) {
-        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0);
-        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0);
+        // the mixed form's position words carry 22 fraction bits
+        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0) & kShiftMask;
+        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0) & kShiftMask;
     }
     const DevCfg &c = h->dc;
     const size_t nc = (size_t)c.ncells;
@@ -928,8 +930,9 @@ static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
     host_shift(h, step, sa.s);
     host_shift(h, step + 1u, sa.sn);
     for (int d = 0; d < 3; d++) {
-        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0);
-        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0);
+        // the mixed form's position words carry 22 fraction bits
+        sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0) & kShiftMask;
+        sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0) & kShiftMask;
     }
     double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
     double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
@@ -1114,11 +1117,10 @@ __global__ void __launch_bounds__(256) k_modes_mix(const __grid_constant__ DevCf
     double acc[2 * NM];
     for (int j = 0; j < 2 * NM; j++) acc[j] = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint4 P = s.P[i];
         const float4 W = s.W[i];
         int ci[3];
-        unpack_cell((int)P.w, ci[0], ci[1], ci[2]);
-        const uint32_t f[3] = {P.x, P.y, P.z};
+        uint32_t f[3];
+        pos_unpack(s.P[i], ci, f);
         const float v[3] = {W.x, W.y, W.z};
         int m = 0;
         for (int b = 0; b < DIM; b++) {

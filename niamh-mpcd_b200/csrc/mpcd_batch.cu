@@ -72,12 +72,13 @@ __global__ void k_bat_shift(const BatchBox *box, int nb, BatchStep *st, const ui
         const mpcd_u4 r = mpcd_block(box[b].seed, box[b].replica, step, MPCD_STREAM_SHIFT, 0u, 0u);
         const mpcd_u4 q =
             mpcd_block(box[b].seed, box[b].replica, step + 1u, MPCD_STREAM_SHIFT, 0u, 0u);
-        o.ks[0] = r.x;
-        o.ks[1] = r.y;
-        o.ks[2] = r.z;
-        o.ksn[0] = q.x;
-        o.ksn[1] = q.y;
-        o.ksn[2] = q.z;
+        // position words carry 22 fraction bits (mpcd_mixed.cuh)
+        o.ks[0] = r.x & kShiftMask;
+        o.ks[1] = r.y & kShiftMask;
+        o.ks[2] = r.z & kShiftMask;
+        o.ksn[0] = q.x & kShiftMask;
+        o.ksn[1] = q.y & kShiftMask;
+        o.ksn[2] = q.z & kShiftMask;
     }
     st[b] = o;
 }
@@ -418,7 +419,7 @@ extern "C" int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *
                 fx_from_double(q, ci[d], f[d]);
                 if (ci[d] >= bx.L[d]) ci[d] -= bx.L[d];
             }
-            P[bx.part0 + j] = make_uint4(f[0], f[1], f[2], (unsigned)pack_cell(ci[0], ci[1], ci[2]));
+            P[bx.part0 + j] = pos_pack(ci, f);
             W[bx.part0 + j] = make_float4((float)V[3 * gi], (float)V[3 * gi + 1],
                                           (float)V[3 * gi + 2], __int_as_float_host((int)gi));
         }
@@ -578,8 +579,8 @@ extern "C" int mpcd_batch_download(mpcd_batch *b, double *Q, double *V) {
         if (pid < 0) continue;
         if (pid >= b->n) return MPCD_ERR_STATE;
         int ci[3];
-        unpack_cell((int)P[i].w, ci[0], ci[1], ci[2]);
-        const uint32_t f[3] = {P[i].x, P[i].y, P[i].z};
+        uint32_t f[3];
+        pos_unpack(P[i], ci, f);
         const float v[3] = {W[i].x, W[i].y, W[i].z};
         for (int d = 0; d < 3; d++) {
             Q[3 * (size_t)pid + d] = (double)ci[d] + (double)f[d] * kFxInv;

@@ -288,8 +288,8 @@ template <>
 __device__ int lc_finish<MixT<2>>(const DevCfg &c, MixRec &r, int sp, const StepArgs &sa,
                                   int &bounce, int &esc, double *U) {
     int ci[3];
-    unpack_cell((int)r.P.w, ci[0], ci[1], ci[2]);
-    uint32_t f[2] = {r.P.x, r.P.y};
+    uint32_t f[3];
+    pos_unpack(r.P, ci, f);
     float vv[2] = {r.W.x, r.W.y};
     const float dtf = (float)c.dt;
     for (int d = 0; d < 2; d++) fx_stream(f[d], ci[d], dtf * vv[d]);
@@ -318,10 +318,9 @@ __device__ int lc_finish<MixT<2>>(const DevCfg &c, MixRec &r, int sp, const Step
             ci[d] = c.L[d];
         }
     }
-    r.P.x = f[0];
-    r.P.y = f[1];
-    r.P.z = 0u;
-    r.P.w = (unsigned)pack_cell(ci[0], ci[1], 0);
+    ci[2] = 0;
+    f[2] = 0u;
+    r.P = pos_pack(ci, f);
     r.W.x = vv[0];
     r.W.y = vv[1];
     uint32_t t;

@@ -1,19 +1,24 @@
 // mpcd_mixed.cuh -- the mixed-precision form of the solvent timestep.
 //
 // Particle state, 32 bytes per particle in two 16-byte records:
-//   P = {fx, fy, fz, cell} (uint4)  position = integer cell (10 bits per
-//                          axis, packed) + 32-bit fixed-point offset within
-//                          the cell (value f * 2^-32 in [0,1))
-//   W = {vx, vy, vz, pid} (float4)  FP32 velocity + original particle index
-// The sub-cell offset has a uniform resolution of 2^-32 cell whatever the box
-// size, and the grid shift (a 32-bit uniform, s = k * 2^-32 exactly, as the
-// reference's genrand_real, rand.c:365-368) adds to it exactly in integer
-// arithmetic, so shifting, wrapping and binning follow the reference's
-// gridShift_all/bin rules (mpc.c:728-736, 958-968) without rounding.  The
-// periodic wrap is an exact integer wrap (the reference shifts by L(1-2e-8)
-// instead, bc.c:769).  Streaming adds the FP32 displacement dt*v converted
-// to fixed point.  Cell sums, the MPC-AT+a inertia tensor and its inverse
-// are FP64; the SRD rotation and streaming are FP32.
+//   P = {X, Y, Z, 0} (uint4)         per axis one 32-bit fixed-point word:
+//                                    the cell index in the top 10 bits and
+//                                    the offset within the cell in the low
+//                                    22 bits (X = cell * 2^22 + offset * 2^22)
+//   W = {vx, vy, vz, pid} (float4)   FP32 velocity + original particle index
+// The sub-cell offset has a uniform resolution of 2^-22 cell whatever the box
+// size (an FP32 offset in [0,1) has 2^-24 at best).  Grid shifts are taken
+// with 22 fraction bits (the reference draws a 32-bit uniform, rand.c:365-368,
+// whose low 10 bits are dropped here), and shifting, wrapping and binning are
+// exact integer operations following the reference's gridShift_all/bin rules
+// (mpc.c:728-736, 958-968).  The periodic wrap is an exact integer wrap (the
+// reference shifts by L(1-2e-8) instead, bc.c:769).  Streaming adds the FP32
+// displacement dt*v rounded to the nearest 2^-22.  Cell sums, the MPC-AT+a
+// inertia tensor and its inverse are FP64 or exact fixed point; the SRD
+// rotation and streaming are FP32.
+//
+// Helpers that take a (cell index, 32-bit offset f) pair use f = offset word
+// << 10, so f always has its low 10 bits zero, as do the shift words.
 #pragma once
 
 #include "mpcd_device.cuh"
@@ -29,17 +34,27 @@ struct MixState {
 };
 
 constexpr int kCellBits = 10;
-constexpr int kCellMask = (1 << kCellBits) - 1;
+constexpr int kFracBits = 22;                      // offset bits of a position word
+constexpr uint32_t kShiftMask = 0xFFFFFC00u;       // 32-bit shift words keep 22 bits
 constexpr double kFx = 4294967296.0;               // 2^32
 constexpr double kFxInv = 2.3283064365386963e-10;  // 2^-32
 
-__host__ __device__ __forceinline__ int pack_cell(int a, int b, int z) {
-    return a | (b << kCellBits) | (z << (2 * kCellBits));
+// (cell index, 32-bit offset) per axis of a position record, and back.
+__host__ __device__ __forceinline__ void pos_unpack(const uint4 &P, int ci[3], uint32_t f[3]) {
+    ci[0] = (int)(P.x >> kFracBits);
+    ci[1] = (int)(P.y >> kFracBits);
+    ci[2] = (int)(P.z >> kFracBits);
+    f[0] = P.x << kCellBits;
+    f[1] = P.y << kCellBits;
+    f[2] = P.z << kCellBits;
 }
-__host__ __device__ __forceinline__ void unpack_cell(int p, int &a, int &b, int &z) {
-    a = p & kCellMask;
-    b = (p >> kCellBits) & kCellMask;
-    z = (p >> (2 * kCellBits)) & kCellMask;
+__host__ __device__ __forceinline__ uint4 pos_pack(const int ci[3], const uint32_t f[3]) {
+    uint4 P;
+    P.x = ((uint32_t)ci[0] << kFracBits) | (f[0] >> kCellBits);
+    P.y = ((uint32_t)ci[1] << kFracBits) | (f[1] >> kCellBits);
+    P.z = ((uint32_t)ci[2] << kFracBits) | (f[2] >> kCellBits);
+    P.w = 0u;
+    return P;
 }
 
 static inline int mix_check(const DevCfg &c) {
@@ -117,16 +132,16 @@ __device__ __forceinline__ int fx_shift_axis_pbc(int ci, uint32_t f, uint32_t k,
 template <int DIM>
 __device__ __forceinline__ void mix_rel(const DevCfg &c, const uint4 &p, const uint32_t *k,
                                         double *r) {
-    int ca, cb, cz, e = 0;
-    uint32_t t;
-    unpack_cell((int)p.w, ca, cb, cz);
-    fx_shift_axis(ca, p.x, k[0], c.L[0], c.pbc[0], t, e);
+    int ci[3], e = 0;
+    uint32_t f[3], t;
+    pos_unpack(p, ci, f);
+    fx_shift_axis(ci[0], f[0], k[0], c.L[0], c.pbc[0], t, e);
     r[0] = (double)t * kFxInv;
-    fx_shift_axis(cb, p.y, k[1], c.L[1], c.pbc[1], t, e);
+    fx_shift_axis(ci[1], f[1], k[1], c.L[1], c.pbc[1], t, e);
     r[1] = (double)t * kFxInv;
     r[2] = 0.0;
     if (DIM == 3) {
-        fx_shift_axis(cz, p.z, k[2], c.L[2], c.pbc[2], t, e);
+        fx_shift_axis(ci[2], f[2], k[2], c.L[2], c.pbc[2], t, e);
         r[2] = (double)t * kFxInv;
     }
 }
@@ -161,23 +176,23 @@ __device__ __forceinline__ bool fx_limbs(float v, int &hi, int &lo) {
     return true;
 }
 
+// rint(dx * 2^22) for |dx| < 0.999, from one FP32 multiply and one add of
+// 1.5 * 2^23 (ties to even), read back from the sum's mantissa bits.
+__device__ __forceinline__ int fx_rint22(float dx) {
+    return __float_as_int(__fadd_rn(__fmul_rn(dx, 4194304.0f), 12582912.0f)) - 0x4B400000;
+}
+constexpr float kStreamFast = 0.999f;  // |dx| below this: |rint(dx 2^22)| < 2^22
+
 // Stream one axis by the FP32 displacement dx: exact fixed-point add of
-// rint(dx * 2^32).
+// rint(dx * 2^22) units of 2^-22 cell.
 __device__ __forceinline__ void fx_stream(uint32_t &f, int &ci, float dx) {
-    int hi, lo;
-    if (fabsf(dx) < 1.0f) {
-        fx_limbs_unchecked(dx, hi, lo);
-        // |rint(dx 2^32)| < 2^32: 32-bit add, the carry from the wrap
-        const uint32_t nf = f + (((uint32_t)hi << 20) + (uint32_t)lo);
+    if (fabsf(dx) < kStreamFast) {
+        const uint32_t nf = f + ((uint32_t)fx_rint22(dx) << kCellBits);
         ci += dx >= 0.0f ? (nf < f ? 1 : 0) : (nf > f ? -1 : 0);
         f = nf;
         return;
     }
-    long long disp;
-    if (fx_limbs(dx, hi, lo))
-        disp = (long long)hi * (1ll << 20) + (long long)lo;
-    else
-        disp = __float2ll_rn(dx * 4294967296.0f);
+    const long long disp = __float2ll_rn(dx * 4194304.0f) * (1ll << kCellBits);
     const long long nq = (long long)f + disp;
     ci += (int)(nq >> 32);
     f = (uint32_t)nq;
@@ -191,60 +206,67 @@ template <int DIM>
 __device__ __forceinline__ void fx_finish_periodic(uint4 &P, const float4 &W, float dtf,
                                                    const int L[3], const uint32_t ksn[3],
                                                    int idx[3]) {
-    int ci[3];
-    unpack_cell((int)P.w, ci[0], ci[1], ci[2]);
-    uint32_t f[3] = {P.x, P.y, P.z};
     const float dx[3] = {dtf * W.x, dtf * W.y, dtf * W.z};
     idx[0] = idx[1] = idx[2] = 0;
-    bool fast = fabsf(dx[0]) < 1.0f && fabsf(dx[1]) < 1.0f;
-    if (DIM == 3) fast = fast && fabsf(dx[2]) < 1.0f;
+    bool fast = fabsf(dx[0]) < kStreamFast && fabsf(dx[1]) < kStreamFast;
+    if (DIM == 3) fast = fast && fabsf(dx[2]) < kStreamFast;
     if (fast) {
-        // every displacement below one cell: 32-bit adds, one-period wrap
+        // directly on the position words: add, one-period wrap (a word at
+        // or above L 2^22 either crossed the top face or, for a negative
+        // step, wrapped below zero), next cell from the shifted word
+        uint32_t X[3] = {P.x, P.y, P.z};
         for (int d = 0; d < DIM; d++) {
-            int hi, lo;
-            fx_limbs_unchecked(dx[d], hi, lo);
-            const uint32_t nf = f[d] + (((uint32_t)hi << 20) + (uint32_t)lo);
-            int c = ci[d] + (dx[d] >= 0.0f ? (nf < f[d] ? 1 : 0) : (nf > f[d] ? -1 : 0));
-            c = c < 0 ? c + L[d] : (c >= L[d] ? c - L[d] : c);
-            f[d] = nf;
-            ci[d] = c;
-            idx[d] = fx_shift_axis_pbc(c, nf, ksn[d], L[d]);
+            const int st = fx_rint22(dx[d]);
+            const uint32_t Lw = (uint32_t)L[d] << kFracBits;
+            uint32_t x = X[d] + (uint32_t)st;
+            if (x >= Lw) x = st < 0 ? x + Lw : x - Lw;
+            X[d] = x;
+            const int a = (int)((x + (ksn[d] >> kCellBits)) >> kFracBits);
+            idx[d] = a == L[d] ? 0 : a;
         }
-    } else {
-        for (int d = 0; d < DIM; d++) {
-            fx_stream(f[d], ci[d], dx[d]);
-            ci[d] = ((ci[d] % L[d]) + L[d]) % L[d];
-            idx[d] = fx_shift_axis_pbc(ci[d], f[d], ksn[d], L[d]);
-        }
+        P.x = X[0];
+        P.y = X[1];
+        P.z = DIM == 3 ? X[2] : 0u;
+        return;
     }
-    P.x = f[0];
-    P.y = f[1];
-    P.z = DIM == 3 ? f[2] : 0u;
-    P.w = (unsigned)pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
+    int ci[3];
+    uint32_t f[3];
+    pos_unpack(P, ci, f);
+    for (int d = 0; d < DIM; d++) {
+        fx_stream(f[d], ci[d], dx[d]);
+        ci[d] = ((ci[d] % L[d]) + L[d]) % L[d];
+        idx[d] = fx_shift_axis_pbc(ci[d], f[d], ksn[d], L[d]);
+    }
+    if (DIM == 2) {
+        ci[2] = 0;
+        f[2] = 0u;
+    }
+    P = pos_pack(ci, f);
 }
 
 // Current-step cell indices of a record in a fully periodic box.
 template <int DIM>
 __device__ __forceinline__ void fx_cur_idx_periodic(const uint4 &P, const int L[3],
                                                     const uint32_t ks[3], int idx[3]) {
-    int ca, cb, cz;
-    unpack_cell((int)P.w, ca, cb, cz);
-    idx[0] = fx_shift_axis_pbc(ca, P.x, ks[0], L[0]);
-    idx[1] = fx_shift_axis_pbc(cb, P.y, ks[1], L[1]);
-    idx[2] = DIM == 3 ? fx_shift_axis_pbc(cz, P.z, ks[2], L[2]) : 0;
+    const uint32_t X[3] = {P.x, P.y, P.z};
+    idx[2] = 0;
+    for (int d = 0; d < DIM; d++) {
+        const int a = (int)((X[d] + (ks[d] >> kCellBits)) >> kFracBits);
+        idx[d] = a == L[d] ? 0 : a;
+    }
 }
 
 // Fixed-point representation of a coordinate (host and device).
 __host__ __device__ __forceinline__ void fx_from_double(double q, int &ci, uint32_t &f) {
     double fl = floor(q);
-    double fr = (q - fl) * kFx;
+    double fr = (q - fl) * 4194304.0;  // 2^22
     long long r = (long long)(fr + 0.5);
     ci = (int)fl;
-    if (r >= (1LL << 32)) {
+    if (r >= (1LL << kFracBits)) {
         ci += 1;
         r = 0;
     }
-    f = (uint32_t)r;
+    f = (uint32_t)r << kCellBits;
 }
 
 
@@ -281,7 +303,7 @@ static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *
             fx_from_double(Q[3 * (size_t)i + d], ci[d], f[d]);
             if (ci[d] < 0 || ci[d] > c.L[d]) return MPCD_ERR_ARG;
         }
-        P[i] = make_uint4(f[0], f[1], f[2], (unsigned)pack_cell(ci[0], ci[1], ci[2]));
+        P[i] = pos_pack(ci, f);
         W[i] = make_float4((float)V[3 * (size_t)i], (float)V[3 * (size_t)i + 1],
                            c.dim == 3 ? (float)V[3 * (size_t)i + 2] : 0.f,
                            __int_as_float_host(i));
@@ -335,8 +357,8 @@ static inline int mix_download(const MixState &s, const DevCfg &c, int n, double
         int pid = __float_as_int_host(W[i].w);
         if (pid < 0 || pid >= n) return MPCD_ERR_STATE;
         int ci[3];
-        unpack_cell((int)P[i].w, ci[0], ci[1], ci[2]);
-        uint32_t f[3] = {P[i].x, P[i].y, P[i].z};
+        uint32_t f[3];
+        pos_unpack(P[i], ci, f);
         float v[3] = {W[i].x, W[i].y, W[i].z};
         for (int d = 0; d < 3; d++) {
             if (Q) Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;

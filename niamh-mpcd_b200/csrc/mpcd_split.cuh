@@ -119,15 +119,15 @@ __global__ void __launch_bounds__(256) k_srd_cells(const __grid_constant__ DevCf
 template <int DIM>
 __device__ __forceinline__ int cur_key_idx(const DevCfg &c, const MixRec &r,
                                            const StepArgs &sa, int idx[3]) {
-    int ca, cb, cz, e = 0;
-    uint32_t t;
-    unpack_cell((int)r.P.w, ca, cb, cz);
     if (c.all_periodic) {
         fx_cur_idx_periodic<DIM>(r.P, c.L, sa.ks, idx);
     } else {
-        idx[0] = fx_shift_axis(ca, r.P.x, sa.ks[0], c.L[0], c.pbc[0], t, e);
-        idx[1] = fx_shift_axis(cb, r.P.y, sa.ks[1], c.L[1], c.pbc[1], t, e);
-        idx[2] = DIM == 3 ? fx_shift_axis(cz, r.P.z, sa.ks[2], c.L[2], c.pbc[2], t, e) : 0;
+        int ci[3], e = 0;
+        uint32_t f[3], t;
+        pos_unpack(r.P, ci, f);
+        idx[0] = fx_shift_axis(ci[0], f[0], sa.ks[0], c.L[0], c.pbc[0], t, e);
+        idx[1] = fx_shift_axis(ci[1], f[1], sa.ks[1], c.L[1], c.pbc[1], t, e);
+        idx[2] = DIM == 3 ? fx_shift_axis(ci[2], f[2], sa.ks[2], c.L[2], c.pbc[2], t, e) : 0;
     }
     return cell_lin(c, idx[0], idx[1], idx[2]);
 }

@@ -128,8 +128,8 @@ struct MixT {
             return cell_lin(c, idx[0], idx[1], idx[2]);
         }
         int ci[3];
-        unpack_cell((int)r.P.w, ci[0], ci[1], ci[2]);
-        uint32_t f[3] = {r.P.x, r.P.y, r.P.z};
+        uint32_t f[3];
+        pos_unpack(r.P, ci, f);
         float vv[3] = {r.W.x, r.W.y, r.W.z};
         for (int d = 0; d < DIM; d++) fx_stream(f[d], ci[d], dtf * vv[d]);
         if (c.n_solid > 0) {
@@ -162,10 +162,11 @@ struct MixT {
                 ci[d] = c.L[d];
             }
         }
-        r.P.x = f[0];
-        r.P.y = f[1];
-        r.P.z = DIM == 3 ? f[2] : 0u;
-        r.P.w = (unsigned)pack_cell(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
+        if (DIM == 2) {
+            ci[2] = 0;
+            f[2] = 0u;
+        }
+        r.P = pos_pack(ci, f);
         r.W.x = vv[0];
         r.W.y = vv[1];
         if (DIM == 3) r.W.z = vv[2];
@@ -597,13 +598,12 @@ __global__ void __launch_bounds__(256) k_key_mix(const __grid_constant__ DevCfg 
                                                  StepArgs sa, unsigned long long *status) {
     int esc_local = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint4 p = a.P[i];
-        int ca, cb, cz, e = 0;
-        uint32_t t;
-        unpack_cell((int)p.w, ca, cb, cz);
-        int x = fx_shift_axis(ca, p.x, sa.ks[0], c.L[0], c.pbc[0], t, e);
-        int y = fx_shift_axis(cb, p.y, sa.ks[1], c.L[1], c.pbc[1], t, e);
-        int z = DIM == 3 ? fx_shift_axis(cz, p.z, sa.ks[2], c.L[2], c.pbc[2], t, e) : 0;
+        int ci[3], e = 0;
+        uint32_t f[3], t;
+        pos_unpack(a.P[i], ci, f);
+        int x = fx_shift_axis(ci[0], f[0], sa.ks[0], c.L[0], c.pbc[0], t, e);
+        int y = fx_shift_axis(ci[1], f[1], sa.ks[1], c.L[1], c.pbc[1], t, e);
+        int z = DIM == 3 ? fx_shift_axis(ci[2], f[2], sa.ks[2], c.L[2], c.pbc[2], t, e) : 0;
         esc_local += e;
         int k = cell_lin(c, x, y, z);
         key[i] = k;

@@ -1,13 +1,13 @@
 """The conversion-free fixed-point rounding used by the mixed form.
 
-Streaming adds rint(dx * 2^32) to a 32-bit fixed-point offset, and the
-resident kernel family sums rint(v * 2^32) per cell.  Both form that value
-as two signed limbs, hi * 2^20 + lo, from FP32 adds and multiplies only
-(fx_limbs in mpcd_mixed.cuh).  This file restates those steps in numpy
-float32 arithmetic (IEEE round-to-nearest-even, as the __fadd_rn/__fmul_rn
-intrinsics) and checks them against the exact value rint(float64(v) * 2^32)
-over random and adversarial inputs; the GPU test of the same rounding is in
-test_gpu_fixed_point.py.
+The resident kernel family sums rint(v * 2^32) per cell, formed as two
+signed limbs, hi * 2^20 + lo, from FP32 adds and multiplies only (fx_limbs
+in mpcd_mixed.cuh); streaming adds rint(dx * 2^22) to the 22-bit offsets of
+the position words, from one multiply and one add (fx_rint22).  This file
+restates those steps in numpy float32 arithmetic (IEEE round-to-nearest-even,
+as the __fadd_rn/__fmul_rn intrinsics) and checks them against exact float64
+rounding over random and adversarial inputs; the GPU test of the streaming
+rounding is in test_gpu_fixed_point.py.
 """
 import numpy as np
 
@@ -70,3 +70,17 @@ def test_out_of_range_is_refused():
     assert limbs(F(-5000.0)) is None
     assert limbs(F(np.inf)) is None
     assert limbs(F(np.nan)) is None
+
+
+def rint22(dx):
+    s = F(F(F(dx) * F(4194304.0)) + MAGIC)
+    return _bits(s) - 0x4B400000
+
+
+def test_stream_rounding_rint22():
+    rng = np.random.default_rng(5)
+    vals = (rng.random(20000) * 1.998 - 0.999).astype(np.float32)
+    vals = np.concatenate([vals, np.array([k * 2.0 ** -23 for k in range(-41, 42, 2)],
+                                          dtype=np.float32)])  # exact ties
+    for dx in vals:
+        assert rint22(dx) == int(np.rint(float(dx) * 2.0 ** 22)), float(dx)

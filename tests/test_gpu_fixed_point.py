@@ -1,7 +1,7 @@
 """Exact streaming in the mixed form, on the GPU, through both SRD kernel
 families: particles alone in their cells (no collision partner, so their
-velocity is unchanged) must move by exactly rint(float32(dt * v) * 2^32)
-units of 2^-32 cell."""
+velocity is unchanged) must move by exactly rint(float32(dt * v) * 2^22)
+units of 2^-22 cell, the resolution of the mixed form's position words."""
 import numpy as np
 import pytest
 
@@ -14,19 +14,19 @@ pytestmark = pytest.mark.gpu
 
 def _isolated_state(L, seed):
     """One particle in every second cell along each axis (so no shifted cell
-    ever holds two), at positions that are exact multiples of 2^-32, with
+    ever holds two), at positions that are exact multiples of 2^-22, with
     velocities spanning many magnitudes, both signs and exact ties."""
     rng = np.random.default_rng(seed)
     idx = np.stack(np.meshgrid(*[np.arange(0, l - 1, 2) for l in L], indexing="ij"), -1)
     idx = idx.reshape(-1, 3)
     n = len(idx)
-    frac = np.floor(rng.random((n, 3)) * 2.0 ** 32) * 2.0 ** -32
+    frac = np.floor(rng.random((n, 3)) * 2.0 ** 22) * 2.0 ** -22
     frac = 0.25 + 0.5 * frac  # away from the cell faces
-    frac = np.round(frac * 2.0 ** 32) * 2.0 ** -32
+    frac = np.round(frac * 2.0 ** 22) * 2.0 ** -22
     Q = idx + frac
     mag = np.exp2(rng.integers(-30, 1, size=(n, 3))) * (1.0 + rng.random((n, 3)))
     V = (np.where(rng.random((n, 3)) < 0.5, -1.0, 1.0) * mag).astype(np.float32)
-    V[: n // 4] = (rng.integers(-99, 100, size=(n // 4, 3)) * 2 + 1) * 2.0 ** -30  # ties at dt=1/8
+    V[: n // 4] = (rng.integers(-99, 100, size=(n // 4, 3)) * 2 + 1) * 2.0 ** -20  # ties at dt=1/8
     return Q, V.astype(np.float64)
 
 
@@ -42,8 +42,8 @@ def test_isolated_particles_stream_exactly(kernel):
     q, v, _ = g.download()
     np.testing.assert_array_equal(v, V)
     dx = (np.float32(0.125) * V.astype(np.float32)).astype(np.float64)
-    disp = np.rint(dx * 2.0 ** 32)  # ties to even
-    expect = (np.round(Q * 2.0 ** 32) + disp) * 2.0 ** -32
+    disp = np.rint(dx * 2.0 ** 22)  # ties to even
+    expect = (np.round(Q * 2.0 ** 22) + disp) * 2.0 ** -22
     np.testing.assert_array_equal(q, expect)
 
 
