@@ -140,6 +140,21 @@ class Solver:
                "mpcd_download_state")
         return Q, V, U
 
+    def cell_props(self):
+        """Per-cell population, mass, centre-of-mass velocity and centre of
+        mass on the unshifted (L+1)^D grid, as arrays shaped (L0+1, L1+1,
+        L2+1) (the last two with a trailing axis of 3)."""
+        shp = tuple(int(self.cfg.L[d]) + 1 for d in range(3))
+        nc = shp[0] * shp[1] * shp[2]
+        pop = np.zeros(nc, dtype=np.int32)
+        mass = np.zeros(nc)
+        vcm = np.zeros((nc, 3))
+        cm = np.zeros((nc, 3))
+        _check(self.lib.mpcd_cell_props(self.h, _p(pop), _p(mass), _p(vcm), _p(cm)),
+               "mpcd_cell_props")
+        return (pop.reshape(shp), mass.reshape(shp), vcm.reshape(shp + (3,)),
+                cm.reshape(shp + (3,)))
+
     def status(self):
         st = abi.Status()
         _check(self.lib.mpcd_get_status(self.h, C.byref(st)), "mpcd_get_status")

@@ -1,5 +1,6 @@
-"""Transport validation: kinematic viscosity of an SRD fluid from the decay
-of transverse momentum modes.
+"""Transport validation: kinematic viscosity (1) of an SRD fluid from the
+decay of transverse momentum modes, (2) of a walled channel from the
+curvature of its steady Poiseuille profile.
 
 A transverse momentum mode of the smallest wavevector of a periodic box,
 j_a(k e_b) = sum_i v_i,a exp(-i k x_i,b) with a != b and k = 2 pi / L,
@@ -11,7 +12,16 @@ such analysis tool; `theory_nu_srd3d` gives the analytic values it is
 compared with (Gompper, Ihle, Kroll and Winkler, Adv. Polym. Sci. 221
 (2009), random-axis SRD in 3D: kinetic and collisional parts).
 
+A channel between two no-slip walls at y = 0 and y = H, driven by the body
+force g along x, reaches the profile v_x(y) = g y (H - y) / (2 nu); the
+fit of a parabola to the time-averaged, mass-weighted layer velocities gives
+nu = -g / (2 c2) from its curvature c2 alone (a slip length moves the
+parabola, not its curvature).  `theory_nu_reference` restates the analytic
+kinematic viscosity the reference prints to synopsis.dat (theory_trans,
+init.c:800-942; Noguchi and Gompper, PRE 78, 016706 (2008)).
+
     python -m mpcd_b200.validate --L 32 --steps 40000 --every 10 --form mixed
+    python -m mpcd_b200.validate --channel --form fp64
 """
 import argparse
 import json
@@ -30,6 +40,85 @@ def theory_nu_srd3d(n, alpha, dt, kbt=1.0, m=1.0, a=1.0):
     kin = kbt * dt / (2.0 * m) * (5.0 * n / (en * (2.0 - math.cos(alpha) - math.cos(2 * alpha))) - 1.0)
     col = a * a / (18.0 * dt) * en / n * (1.0 - math.cos(alpha))
     return kin, col
+
+
+def theory_nu_reference(coll_op, dim, n, rot_ang=math.pi / 2, dt=0.1, kbt=1.0, m=1.0):
+    """Kinematic viscosity (kinetic, collisional) of theory_trans
+    (init.c:800-942) for one species of mass m at number density n, a = 1:
+    the correlation factors A, B of the operator (ARBAXIS, MPC-AT, MPC-AT+a),
+    then the kinetic and collisional dynamic viscosities divided by n m."""
+    en = math.exp(-n)
+    Mf = n / (n - 1.0 + en)
+    if coll_op == abi.COLL_ARBAXIS:
+        A = 2.0 / dim * (1.0 - math.sin(rot_ang) / rot_ang)
+        if dim == 2:
+            B = 1.0 - 0.5 * math.sin(2.0 * rot_ang) / rot_ang
+        else:
+            B = 0.4 * (2.0 - 1.5 * math.sin(rot_ang) / rot_ang)
+    elif coll_op in (abi.COLL_MPCAT, abi.COLL_RAT):
+        A = B = 1.0
+    else:
+        raise ValueError("no analytic viscosity for this operator")
+    if coll_op == abi.COLL_RAT:
+        cm = B * (1.0 - en * (1.0 + n)) + (A + B / dim) * n * en / (dim + 2.0)
+        cm += 0.5 * (A * dim - 0.5 * B * (3.0 * dim + 2.0)) * \
+            (1.0 - en * (1.0 + n + 0.5 * n * n)) / n
+        col = A * m / (24.0 * dt) * (n - 1.4 + en * (1.4 + 0.4 * n + (1.0 / dim - 0.3) * n * n))
+    else:
+        cm = B / Mf
+        col = A * n / Mf * m / (12.0 * dt)
+    kin = n * kbt * dt * (1.0 / cm - 0.5)
+    return kin / (n * m), col / (n * m)
+
+
+def channel_viscosity(L=(32, 32, 16), ppc=20, g=5e-4, warm=12000, steps=24000, every=10,
+                      precision=abi.PREC_MIXED, seed=21, edge=2, nblk=8):
+    """Kinematic viscosity from the steady profile of the MPC-AT+a channel
+    (phantom no-slip walls at y = 0 and y = L1, periodic x and z, body force
+    g along x): mass-weighted x velocity per y layer, averaged over time,
+    fitted by a parabola over the layers at least `edge` cells from a wall."""
+    cfg = W.cfg_channel3d(tuple(L), g=g, precision=precision, seed=seed)
+    Q, V, U, sp = W.synthetic_state(cfg, ppc, seed=seed + 1)
+    s = Solver(cfg)
+    s.upload(Q, V, U, sp)
+    s.step(warm, 1)
+    step = warm + 1
+    H = int(L[1])
+    mv, mm = [], []
+    for _ in range(steps // every):
+        s.step(every, step)
+        step += every
+        _, mass, vcm, _ = s.cell_props()
+        mv.append((mass * vcm[..., 0])[:L[0], :H, :L[2]].sum(axis=(0, 2)))
+        mm.append(mass[:L[0], :H, :L[2]].sum(axis=(0, 2)))
+    s.close()
+    res = fit_channel(np.array(mv), np.array(mm), g, edge=edge, nblk=nblk)
+    res.update(L=list(L), g=g, warm=warm, steps=steps, every=every,
+               precision="fp64" if precision == abi.PREC_FP64 else "mixed")
+    return res
+
+
+def fit_channel(mv, mm, g, edge=2, nblk=8):
+    """nu from per-sample layer sums mv[t, y] (mass times x velocity) and
+    mm[t, y] (mass): the time-averaged profile v = sum mv / sum mm is fitted
+    by c0 + c1 y + c2 y^2 at the layer centres y + 1/2 at least `edge` layers
+    from a wall, nu = -g / (2 c2); the error is the scatter of the fits of
+    nblk consecutive blocks of samples."""
+    H = mv.shape[1]
+    y = np.arange(H) + 0.5
+    use = slice(edge, H - edge)
+
+    def fit(a, b):
+        v = a.sum(axis=0) / b.sum(axis=0)
+        c2, c1, c0 = np.polyfit(y[use], v[use], 2)
+        return -g / (2.0 * c2), v, np.array([c2, c1, c0])
+
+    nu, v, coef = fit(mv, mm)
+    nus = [fit(a, b)[0] for a, b in zip(np.array_split(mv, nblk), np.array_split(mm, nblk))]
+    err = float(np.std(nus) / math.sqrt(len(nus)))
+    resid = v[use] - np.polyval(coef, y[use])
+    return {"nu": float(nu), "nu_err": err, "v_max": float(v.max()),
+            "fit_rms": float(np.sqrt(np.mean(resid ** 2))), "profile": v.tolist()}
 
 
 def transverse_modes(Q, V, L):
@@ -95,8 +184,19 @@ def main():
     ap.add_argument("--steps", type=int, default=40000)
     ap.add_argument("--every", type=int, default=10)
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--channel", action="store_true",
+                    help="Poiseuille channel (MPC-AT+a, phantom walls) instead of SRD modes")
+    ap.add_argument("--warm", type=int, default=12000)
     args = ap.parse_args()
     prec = abi.PREC_MIXED if args.form == "mixed" else abi.PREC_FP64
+    if args.channel:
+        res = channel_viscosity(warm=args.warm, steps=args.steps if args.steps != 40000 else 24000,
+                                every=args.every, precision=prec)
+        kin, col = theory_nu_reference(abi.COLL_RAT, 3, 20.0)
+        res.update(theory_kinetic=kin, theory_collisional=col, theory_total=kin + col)
+        res.pop("profile")
+        print(json.dumps(res))
+        return
     res = measure_viscosity(L=args.L, steps=args.steps, every=args.every, precision=prec)
     kin, col = theory_nu_srd3d(10.0, math.radians(130.0), 0.1)
     res["theory_kinetic"] = kin
