@@ -133,17 +133,18 @@ __global__ void __launch_bounds__(256) k_bat_cells(const __grid_constant__ DevCf
         const int local = cell - bx.cell0;
         sums[cell] = ResSum{{0, 0, 0}, 0};
         const int pop = local < bx.ncells ? (int)s[q].n : 0;
-        double u[3] = {0, 0, 0};
+        // the record of k_res_cells (one species): u in FP32, the FP32 axis
+        float u[3] = {0.f, 0.f, 0.f};
         if (pop > 0) {
-            const double iW = 1.0 / (double)pop;
-            for (int d = 0; d < 3; d++) u[d] = ((double)s[q].p[d] * kSumFxInv) * iW;
+            const float ip = __frcp_rn((float)pop);
+            for (int d = 0; d < 3; d++) u[d] = (float)((double)s[q].p[d] * kSumFxInv) * ip;
         }
-        for (int d = 0; d < 3; d++) av[d] += u[d];
-        double Lx[3] = {0, 0, 1};
-        if (pop > 1) mpcd_rng_axis3(bx.seed, bx.replica, step, (uint32_t)local, Lx);
+        for (int d = 0; d < 3; d++) av[d] += (double)u[d];
+        float Lx[3] = {0.f, 0.f, 1.f};
+        if (pop > 1) res_axis3(bx.seed, bx.replica, step, (uint32_t)local, Lx);
         float4 *my = srec + 2 * (q * 256 + threadIdx.x);
-        my[0] = make_float4((float)u[0], (float)u[1], (float)u[2], __int_as_float(pop));
-        my[1] = make_float4((float)Lx[0], (float)Lx[1], (float)Lx[2], 0.f);
+        my[0] = make_float4(u[0], u[1], u[2], __int_as_float(pop));
+        my[1] = make_float4(Lx[0], Lx[1], Lx[2], 0.f);
     }
     __syncthreads();
     float4 *dst = (float4 *)(crec + c0);
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_bat_parts(
     t.bind(res_smem, 3);
     {
         uint4 *w = (uint4 *)res_smem;
-        const int nkey = kResSlots / 4, nall = res_table_bytes(3) / 16;
+        const int nkey = kResSlots / 4, nall = res_table_init_bytes(3) / 16;
         for (int j = tid; j < nall; j += kResThreads)
             w[j] = j < nkey ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0u, 0u, 0u, 0u);
     }
@@ -196,27 +197,47 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_bat_parts(
     const float cosf_a = (float)c.cosA, sinf_a = (float)c.sinA;
     const int base = blockIdx.x * kResChunk;
     const int end = bx.part0 + bx.npart;
+    // the same software pipeline as k_res_parts: next particle loaded at the
+    // top of an iteration, its record requested halfway through; the cell a
+    // particle was added to at the end of the previous step is in P.w
+    // (clamped to its box as a guard)
+    const int clast = bx.cell0 + (L[0] + 1) * N1y * N1z - 1;
+    auto cur_cell = [&](const MixRec &q) { return (int)min(q.P.w, (unsigned)clast); };
+    MixRec nx;
+    float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
+    if (base + tid < end) {
+        nx.P = a.P[base + tid];
+        nx.W = a.W[base + tid];
+        if (MODE == RES_STEP) res_load(crec + cur_cell(nx), na, nb);
+    }
 #pragma unroll 1
     for (int it = 0; it < MPCD_RES_PPT; it++) {
         const int i = base + it * kResThreads + tid;
         if (i >= end) break;
-        MixRec r;
-        r.P = a.P[i];
-        r.W = a.W[i];
+        MixRec r = nx;
+        const float4 ca = na, cb = nb;
+        const bool more = it + 1 < MPCD_RES_PPT && i + kResThreads < end;
+        if (more) {
+            nx.P = a.P[i + kResThreads];
+            nx.W = a.W[i + kResThreads];
+        }
         int kidx[3];
         if (MODE == RES_STEP) {
-            int cidx[3];
-            fx_cur_idx_periodic<3>(r.P, L, sp.ks, cidx);
-            const int kc = bx.cell0 + (cidx[0] * N1y + cidx[1]) * N1z + cidx[2];
-            res_rotate<3>(r.W, crec + kc, cosf_a, sinf_a);
+            res_apply<3>(r.W, ca, cb, cosf_a, sinf_a);
             ke += r.W.x * r.W.x + r.W.y * r.W.y + r.W.z * r.W.z;
             fx_finish_periodic<3>(r.P, r.W, dtf, L, sp.ksn, kidx);
-            a.P[i] = r.P;
-            a.W[i] = r.W;
         } else {
             fx_cur_idx_periodic<3>(r.P, L, sp.ks, kidx);
         }
         const int k = bx.cell0 + (kidx[0] * N1y + kidx[1]) * N1z + kidx[2];
+        // the cell of the next step (RES_STEP) or of this one (RES_SUM),
+        // read back by cur_cell
+        r.P.w = (unsigned)k;
+        a.P[i] = r.P;
+        if (MODE == RES_STEP) {
+            a.W[i] = r.W;
+            if (more) res_load(crec + cur_cell(nx), na, nb);
+        }
         const float vs[3] = {r.W.x, r.W.y, r.W.z};
         res_add<3>(t, mask, shift, sums, nullptr, k, kidx, vs, 1.0, false, bad);
     }

@@ -82,21 +82,29 @@ constexpr float kResBigV = 256.0f;
 // Per-block accumulation table in dynamic shared memory: keys,
 // populations, and per component the momentum limbs (row DIM: the mass
 // sum, several species only).  ncomp = DIM for one species, DIM + 1 for
-// several.
+// several.  After them, scratch for the flush's list of used slots (not
+// initialised).
 struct ResTable {
     int *key;
     unsigned *cnt;
     int *hi;  // [ncomp][kResSlots]
     int *lo;  // [ncomp][kResSlots]
+    unsigned short *list;
     __device__ void bind(unsigned char *base, int ncomp) {
         key = (int *)base;
         cnt = (unsigned *)(key + kResSlots);
         hi = (int *)(cnt + kResSlots);
         lo = hi + ncomp * kResSlots;
+        list = (unsigned short *)(lo + ncomp * kResSlots);
     }
 };
-__host__ __device__ constexpr int res_table_bytes(int ncomp) {
+static_assert(kResSlots <= 65536, "slot indices are 16-bit");
+// bytes the particle pass sets before use (keys to -1, the rest to 0)
+__host__ __device__ constexpr int res_table_init_bytes(int ncomp) {
     return kResSlots * (8 + 8 * ncomp);
+}
+__host__ __device__ constexpr int res_table_bytes(int ncomp) {
+    return res_table_init_bytes(ncomp) + kResSlots * 2;
 }
 
 __device__ __forceinline__ long long res_fix(double x, int &bad) {
@@ -190,34 +198,57 @@ __device__ __forceinline__ void res_add(ResTable &t, const int *mask, const int 
     }
 }
 
-// Add every used table entry to the global sums.
+// Add every used table entry to the global sums.  Each warp first lists
+// the used slots of its share of the table (ballot + prefix count), then
+// adds them with all its lanes busy; most slots of a table are unused.
+// Requires kResThreads threads.
 template <int DIM>
 __device__ __forceinline__ void res_flush(const ResTable &t, ResSum *sums,
                                           unsigned long long *msum, bool multi) {
     const int nc = multi ? DIM + 1 : DIM;
-    for (int s = threadIdx.x; s < kResSlots; s += blockDim.x) {
-        const int k = t.key[s];
-        if (k < 0) continue;
+    constexpr int kPer = kResSlots / (kResThreads / 32);
+    static_assert(kPer % 32 == 0, "each warp lists whole 32-slot groups");
+    const int lane = threadIdx.x & 31;
+    const int s0 = (threadIdx.x >> 5) * kPer;
+    unsigned short *list = t.list + s0;
+    int total = 0;
+    for (int j = 0; j < kPer; j += 32) {
+        const int s = s0 + j + lane;
+        const bool used = t.key[s] >= 0;
+        const unsigned m = __ballot_sync(0xffffffffu, used);
+        if (used) list[total + __popc(m & ((1u << lane) - 1u))] = (unsigned short)s;
+        total += __popc(m);
+    }
+    __syncwarp();
+    for (int j = lane; j < total; j += 32) {
+        const int s = list[j];
         long long x[4] = {0, 0, 0, 0};
         for (int d = 0; d < nc; d++) {
             const int dd = d == DIM ? 3 : d;
             x[dd] = (long long)t.hi[d * kResSlots + s] * (1ll << kLimb) +
                     (long long)t.lo[d * kResSlots + s];
         }
-        res_global_add(sums, msum, k, x, t.cnt[s], multi);
+        res_global_add(sums, msum, t.key[s], x, t.cnt[s], multi);
     }
+}
+
+// A cell's record, both halves: one 32-byte sector, two loads issued
+// together (the axis half is loaded whatever the population, so that the
+// rotation never waits for a second round trip).
+__device__ __forceinline__ void res_load(const ResRec *rec, float4 &ca, float4 &cb) {
+    const float4 *q = (const float4 *)rec;
+    ca = __ldg(q);
+    cb = __ldg(q + 1);
 }
 
 // v' = u + R (v - u) from a cell's record (Rodrigues form, see ResRec);
 // cells of fewer than two particles leave v unchanged.
 template <int DIM>
-__device__ __forceinline__ void res_rotate(float4 &W, const ResRec *rec, float Cs, float Sn) {
-    const float4 *q = (const float4 *)rec;
-    const float4 ca = __ldg(q);
+__device__ __forceinline__ void res_apply(float4 &W, const float4 ca, const float4 cb, float Cs,
+                                          float Sn) {
     if (__float_as_int(ca.w) > 1) {
         const float w0 = W.x - ca.x, w1 = W.y - ca.y;
         if (DIM == 3) {
-            const float4 cb = __ldg(q + 1);
             const float w2 = W.z - ca.z;
             const float ld = (cb.x * w0 + cb.y * w1 + cb.z * w2) * (1.f - Cs);
             W.x = ca.x + (Cs * w0 + ld * cb.x + Sn * (cb.y * w2 - cb.z * w1));
@@ -233,6 +264,32 @@ __device__ __forceinline__ void res_rotate(float4 &W, const ResRec *rec, float C
 __device__ __forceinline__ double warp_sum_d(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// The SRD axis of mpcd_rng_axis3 (same Philox draws, same FP64
+// acceptance test of the Marsaglia pair, so the same pair is taken), with
+// the square root and the products in FP32: the record holds the axis in
+// FP32 anyway.
+__device__ __forceinline__ void res_axis3(uint64_t seed, uint32_t replica, uint32_t step,
+                                          uint32_t cell, float v[3]) {
+    for (uint32_t blk = 0; blk < MPCD_RNG_MAX_BLOCKS; ++blk) {
+        const mpcd_u4 r = mpcd_block(seed, replica, step, MPCD_STREAM_AXIS, cell, blk);
+        for (int a = 0; a < 2; ++a) {
+            const double x = MPCD_DSUB(MPCD_DMUL(2.0, mpcd_u01(a ? r.z : r.x)), 1.0);
+            const double y = MPCD_DSUB(MPCD_DMUL(2.0, mpcd_u01(a ? r.w : r.y)), 1.0);
+            const double q = MPCD_DADD(MPCD_DMUL(x, x), MPCD_DMUL(y, y));
+            if (q <= 1.0) {
+                const float f = 2.0f * sqrtf((float)MPCD_DSUB(1.0, q));
+                v[0] = f * (float)x;
+                v[1] = f * (float)y;
+                v[2] = (float)MPCD_DSUB(1.0, MPCD_DMUL(2.0, q));
+                return;
+            }
+        }
+    }
+    v[0] = 0.f;
+    v[1] = 0.f;
+    v[2] = 1.f;
 }
 
 // Cell pass: sums of this step -> u, axis record; the sums are cleared.
@@ -269,19 +326,25 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
         sums[cell] = ResSum{{0, 0, 0}, 0};
         if (msum) msum[cell] = 0ull;
         const int pop = (int)s[q].n;
-        // divisor of the weighted sum: population (one species) or mass
-        const double W = msum ? (double)(long long)ms[q] * kSumFxInv : (double)pop;
-        double u[3] = {0, 0, 0};
-        if (pop > 0 && W > 0.0) {
-            const double iW = 1.0 / W;
-            for (int d = 0; d < DIM; d++) u[d] = ((double)s[q].p[d] * kSumFxInv) * iW;
+        // u = weighted sum / divisor: the population (one species, in FP32:
+        // the record is FP32) or the mass sum (several species, in FP64)
+        float u[3] = {0.f, 0.f, 0.f};
+        if (msum) {
+            const double W = (double)(long long)ms[q] * kSumFxInv;
+            if (pop > 0 && W > 0.0) {
+                const double iW = 1.0 / W;
+                for (int d = 0; d < DIM; d++) u[d] = (float)(((double)s[q].p[d] * kSumFxInv) * iW);
+            }
+        } else if (pop > 0) {
+            const float ip = __frcp_rn((float)pop);
+            for (int d = 0; d < DIM; d++) u[d] = (float)((double)s[q].p[d] * kSumFxInv) * ip;
         }
-        for (int d = 0; d < DIM; d++) av[d] += u[d];
-        double Lx[3] = {0, 0, 1};
-        if (pop > 1 && DIM == 3) mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
+        for (int d = 0; d < DIM; d++) av[d] += (double)u[d];
+        float Lx[3] = {0.f, 0.f, 1.f};
+        if (pop > 1 && DIM == 3) res_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
         float4 *my = srec + 2 * (q * 256 + threadIdx.x);
-        my[0] = make_float4((float)u[0], (float)u[1], (float)u[2], __int_as_float(pop));
-        my[1] = make_float4((float)Lx[0], (float)Lx[1], (float)Lx[2], 0.f);
+        my[0] = make_float4(u[0], u[1], u[2], __int_as_float(pop));
+        my[1] = make_float4(Lx[0], Lx[1], Lx[2], 0.f);
     }
     __syncthreads();
     {
@@ -311,6 +374,9 @@ enum { RES_STEP = 0, RES_SUM = 1 };
 //             the next step's sums.
 //   RES_SUM:  only add each particle to this step's sums (the first step,
 //             or after the state was replaced).
+// Both leave in P.w the linear index of the cell each particle was added
+// to: the cell whose record it reads at the next RES_STEP (the re-sort
+// moves P.w with the particle).
 // Accumulation: each particle adds its limbs to its cell's entry in the
 // block's table with native 32-bit shared-memory atomics (or, if the table
 // has no slot for it, straight to global memory); at the end every table
@@ -332,7 +398,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     {
         // keys to -1, everything after them to 0, in 16-byte stores
         uint4 *w = (uint4 *)res_smem;
-        const int nkey = kResSlots / 4, nall = res_table_bytes(nc) / 16;
+        const int nkey = kResSlots / 4, nall = res_table_init_bytes(nc) / 16;
         for (int j = tid; j < nall; j += kResThreads)
             w[j] = j < nkey ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0u, 0u, 0u, 0u);
     }
@@ -344,18 +410,27 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
                          (float)(c.dt * c.grav[2])};
     const float cosf_a = (float)c.cosA, sinf_a = (float)c.sinA;
     const int base = blockIdx.x * kResChunk;
-    // the next particle's record is loaded one iteration ahead
+    // Software pipeline: the next particle is loaded at the top of an
+    // iteration, and its cell's record is requested halfway through it
+    // (before the accumulation), so neither load is waited for.  The cell
+    // is the one the particle was added to at the end of the previous step,
+    // which that step left in P.w (clamped only as a guard).
+    auto cur_cell = [&](const MixRec &q) { return (int)min(q.P.w, (unsigned)(c.ncells - 1)); };
     MixRec nx;
+    float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
     if (base + tid < n) {
         nx.P = a.P[base + tid];
         nx.W = a.W[base + tid];
+        if (MODE == RES_STEP) res_load(crec + cur_cell(nx), na, nb);
     }
 #pragma unroll 1
     for (int it = 0; it < MPCD_RES_PPT; it++) {
         const int i = base + it * kResThreads + tid;
         if (i >= n) break;
         MixRec r = nx;
-        if (it + 1 < MPCD_RES_PPT && i + kResThreads < n) {
+        const float4 ca = na, cb = nb;
+        const bool more = it + 1 < MPCD_RES_PPT && i + kResThreads < n;
+        if (more) {
             nx.P = a.P[i + kResThreads];
             nx.W = a.W[i + kResThreads];
         }
@@ -367,15 +442,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
         const int sp = multi ? MixT<DIM>::sp(a, i) : 0;
         int k, kidx[3];
         if (MODE == RES_STEP) {
-            int kc;
-            if (LEAN) {
-                int cidx[3];
-                fx_cur_idx_periodic<DIM>(r.P, c.L, sa.ks, cidx);
-                kc = cell_lin(c, cidx[0], cidx[1], cidx[2]);
-            } else {
-                kc = cur_key<DIM>(c, r, sa);
-            }
-            res_rotate<DIM>(r.W, crec + kc, cosf_a, sinf_a);
+            res_apply<DIM>(r.W, ca, cb, cosf_a, sinf_a);
             float tt = r.W.x * r.W.x + r.W.y * r.W.y;
             if (DIM == 3) tt += r.W.z * r.W.z;
             if (multi)
@@ -388,7 +455,9 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
             } else {
                 k = MixT<DIM>::finish_idx(c, r, sp, sa, bounce, esc, kidx);
             }
+            r.P.w = (unsigned)k;  // next step's cell, read back by cur_cell
             MixT<DIM>::store(a, i, r);
+            if (more) res_load(crec + cur_cell(nx), na, nb);
             // the next step's load adds the same FP32 gravity kick
             if (!LEAN && c.grav_flag) {
                 r.W.x += gk[0];
@@ -397,6 +466,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
             }
         } else {
             k = cur_key_idx<DIM>(c, r, sa, kidx);
+            a.P[i] = make_uint4(r.P.x, r.P.y, r.P.z, (unsigned)k);
         }
         const float vs[3] = {r.W.x, r.W.y, DIM == 3 ? r.W.z : 0.f};
         res_add<DIM>(t, c.res_mask, c.res_shift, sums, msum, k, kidx, vs,

@@ -15,10 +15,12 @@
  *               species, walls, globals), create a handle and upload the
  *               particles (mpcd_upload_particles_strided, reading the
  *               reference's particleMPC array in place);
- *   each call   mpcd_timestep (AVNOW, KBTNOW), download the particles into
- *               the reference's array, then the end of the reference's
- *               timestep for the output writers: re-bin, localPROP and the
- *               flow sums (mpc.c:4936-4958).
+ *   each call   mpcd_timestep (AVNOW, KBTNOW); on the steps whose output
+ *               or checkpoint reads the particles (need_host_state), the
+ *               particles are downloaded into the reference's array and the
+ *               end of the reference's timestep runs for the output
+ *               writers: re-bin, localPROP and the flow sums
+ *               (mpc.c:4936-4958).
  *
  * Configurations outside the GPU path (MD coupling, swimmers, moving or
  * non-planar walls, thermostats, other collision operators, nematics) make
@@ -27,6 +29,7 @@
  * with dlsym(RTLD_NEXT)), and the run is the reference's.
  *
  * Environment: MPCD_DROPIN_PRECISION = fp64 (default) or mixed;
+ * MPCD_DROPIN_SYNC set downloads on every step;
  * MPCD_DROPIN_OFF set runs the reference's own timestep throughout (the same
  * executable as its CPU control).
  */
@@ -46,6 +49,7 @@
 #include "SRDclss.h"
 #include "mpc.h"
 #include "therm.h"
+#include "pout.h"
 
 extern int DIM, GPOP, NSPECI, NBC, NS, MDmode;
 extern double GnDNST;
@@ -151,6 +155,22 @@ static int setup(particleMPC *pp, spec SP[], bc WALL[], inputList in) {
     return 1;
 }
 
+/* Whether the caller reads the particles or the cell lists after this step:
+ * on the main loop's output and histogram steps (writeOutput,
+ * writeHistograms: mpcd.c:302-307), on checkpoint steps of either loop
+ * (mpcd.c:272, 310), on the last step, and on every step while the flow
+ * field is averaged (the per-step flow sums, mpc.c:4950-4958).  On the other
+ * steps the state stays on the GPU.  MPCD_DROPIN_SYNC set downloads on every
+ * step (the device state evolves the same either way). */
+static int need_host_state(int runtime, inputList in, outputFlagsList f) {
+    if (getenv("MPCD_DROPIN_SYNC")) return 1;
+    if (f.FLOWOUT >= OUT || f.SWFLOWOUT >= OUT) return 1;
+    if (f.CHCKPNT >= OUT && runtime % f.CHCKPNT == 0) return 1;
+    if (in.warmupSteps) return 0;
+    return writeOutput(runtime, f, in.RFRAME, in.zeroNetMom) || writeHistograms(runtime, f) ||
+           runtime >= in.simSteps;
+}
+
 void timestep(cell ***CL, particleMPC *SRDparticles, spec SP[], bc WALL[], simptr simMD,
               specSwimmer *SS, swimmer swimmers[], double AVNOW[_3D], double AVV[_3D],
               double avDIR[_3D], inputList in, double *KBTNOW, double *AVS, int runtime,
@@ -168,11 +188,15 @@ void timestep(cell ***CL, particleMPC *SRDparticles, spec SP[], bc WALL[], simpt
     }
     /* one monotonically increasing step number keys the draws (warm-up and
      * main loop both count runtime from zero) */
-    if (mpcd_timestep(g_h, g_step++, AVNOW, KBTNOW) != MPCD_OK ||
-        mpcd_download_particles_strided(g_h, SRDparticles, sizeof(particleMPC),
+    if (mpcd_timestep(g_h, g_step++, AVNOW, KBTNOW) != MPCD_OK) {
+        fprintf(stderr, "dropin: GPU timestep failed\n");
+        exit(1);
+    }
+    if (!need_host_state(runtime, in, outFlags)) return;
+    if (mpcd_download_particles_strided(g_h, SRDparticles, sizeof(particleMPC),
                                         offsetof(particleMPC, Q), offsetof(particleMPC, V),
                                         offsetof(particleMPC, U)) != MPCD_OK) {
-        fprintf(stderr, "dropin: GPU timestep failed\n");
+        fprintf(stderr, "dropin: GPU download failed\n");
         exit(1);
     }
     /* the end of the reference's timestep, for its output writers */

@@ -93,6 +93,21 @@ def test_dropin_srd_conserves_energy(tmp_path, prec):
 
 
 @pytest.mark.gpu
+def test_dropin_downloads_only_for_output(tmp_path):
+    """The particles come back to the host only on output and checkpoint
+    steps; the device state evolves the same whether or not they do, so the
+    reference's writers produce the same files as with a download on every
+    step (MPCD_DROPIN_SYNC)."""
+    inp = periodic2d(steps=60)
+    run(tmp_path, "sparse", inp, env={"MPCD_DROPIN_PRECISION": "mixed"})
+    run(tmp_path, "sync", inp, env={"MPCD_DROPIN_PRECISION": "mixed", "MPCD_DROPIN_SYNC": "1"})
+    for f in ("avVel.dat", "energy.dat"):
+        a = (tmp_path / "sparse" / "out" / f).read_text()
+        b = (tmp_path / "sync" / "out" / f).read_text()
+        assert a == b, f
+
+
+@pytest.mark.gpu
 def test_dropin_channel_matches_reference_run(tmp_path):
     """2D gravity-driven channel between phantom no-slip walls (the layout of
     the reference's channelFlow sample, smaller): the GPU run and the
