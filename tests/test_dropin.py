@@ -36,21 +36,24 @@ def run(tmp_path, name, inp, env=None):
     return p, rows
 
 
-def periodic2d(steps=100, coll=2, L=(24, 24), dens=20):
-    return {"domain": list(L), "simSteps": steps, "collOp": coll, "species": [{"dens": dens}],
+# a fixed "seed" (read.c:1114): 0 would seed the reference's generator, and so
+# its initial state and the GPU's draws, from the clock
+def periodic2d(steps=100, coll=2, L=(24, 24), dens=20, seed=4711):
+    return {"domain": list(L), "simSteps": steps, "collOp": coll, "seed": seed,
+            "species": [{"dens": dens}],
             "domainWalls": 1, "checkpointOut": 0, "avVelOut": 10, "energyOut": 10}
 
 
-def srd3d(steps=100, L=(12, 12, 12), dens=10):
-    return {"domain": list(L), "simSteps": steps, "collOp": 0, "rotAng": 2.2689280,
+def srd3d(steps=100, L=(12, 12, 12), dens=10, seed=4712):
+    return {"domain": list(L), "simSteps": steps, "collOp": 0, "rotAng": 2.2689280, "seed": seed,
             "species": [{"dens": dens}], "domainWalls": 1, "checkpointOut": 0, "avVelOut": 10}
 
 
-def channel2d(steps=400, L=(60, 20), g=0.003):
+def channel2d(steps=400, L=(60, 20), g=0.003, seed=4713):
     def wall(q, a, phantom, dn, mv):
         return {"phantom": phantom, "Q": q, "aInv": a, "P": [1, 1, 1, 1], "R": 0,
                 "DN": dn, "MVN": mv, "MVT": mv}
-    return {"domain": list(L), "simSteps": steps, "collOp": 2, "grav": [g, 0, 0],
+    return {"domain": list(L), "simSteps": steps, "collOp": 2, "grav": [g, 0, 0], "seed": seed,
             "species": [{"dens": 20}], "checkpointOut": 0, "avVelOut": 20,
             "BC": [wall([0, 0, 0], [1, 0, 0], 0, L[0], 1),
                    wall([L[0], 0, 0], [-1, 0, 0], 0, L[0], 1),
