@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -848,6 +849,26 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
 
 // One SRD timestep with the particles resident in place (mixed precision):
 // an occasional re-sort for locality, the cell pass and the particle pass.
+// The cell and particle passes are launched as programmatic dependents
+// (launch_pdl): each may start while the kernel before it finishes, doing the
+// work that reads nothing that kernel writes (the cell pass's axis draws, the
+// particle pass's table set-up) before it waits for it.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem,
+                              cudaStream_t stream, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <int DIM>
 static int run_step_res(mpcd_handle *h, uint32_t step) {
     StepArgs sa;
@@ -894,17 +915,15 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
                                                         acc_cur, h->status, sa);
         launches += 1;
     }
-    k_res_cells<DIM><<<(int)((nc + 256 * kResCellsPer - 1) / (256 * kResCellsPer)), 256, 0,
-                       h->stream>>>(
-        c, sum_cur, ms_cur, (CRec *)h->crec, sa, acc_cur, acc_nxt);
+    CK(launch_pdl(k_res_cells<DIM>, (int)((nc + 256 * kResCellsPer - 1) / (256 * kResCellsPer)),
+                  256, 0, h->stream, c, sum_cur, ms_cur, (CRec *)h->crec, sa, acc_cur, acc_nxt));
     const bool lean = c.all_periodic && !h->rmsum && !c.grav_flag;
     auto kstep = lean ? k_res_parts<DIM, RES_STEP, true> : k_res_parts<DIM, RES_STEP, false>;
     CK(cudaFuncSetAttribute(kstep, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
     CK(cudaFuncSetAttribute(kstep, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     time_begin(h);
-    kstep<<<pgrid, kResThreads, pbytes, h->stream>>>(c, h->mx[h->cur], h->n,
-                                                     (const CRec *)h->crec, sum_nxt, ms_nxt,
-                                                     acc_cur, h->status, sa);
+    CK(launch_pdl(kstep, pgrid, kResThreads, pbytes, h->stream, c, h->mx[h->cur], h->n,
+                  (const CRec *)h->crec, sum_nxt, ms_nxt, acc_cur, h->status, sa));
     time_end(h);
     launches += 2;
     CK(cudaGetLastError());

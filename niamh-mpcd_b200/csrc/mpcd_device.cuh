@@ -12,6 +12,18 @@
 
 namespace mpcd {
 
+// Programmatic dependent launch (griddepcontrol, sm_90 and later).  A kernel
+// launched with cudaLaunchAttributeProgrammaticStreamSerialization may begin
+// while the kernel before it in the stream is still running: pdl_wait()
+// returns once that kernel has completed and its memory operations are
+// visible (at once for a kernel launched without the attribute), so a kernel
+// touches no global memory the previous one uses before it; pdl_trigger()
+// lets the next kernel of the stream begin launching.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 static inline float __int_as_float_host(int i) {
     float f;
     std::memcpy(&f, &i, 4);

@@ -305,6 +305,20 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
     __shared__ float4 srec[2 * 256 * kResCellsPer];
     __shared__ double wsum[8][3];
     const int c0 = blockIdx.x * 256 * kResCellsPer;
+    pdl_trigger();
+    // The axes depend on the step and the cell only: they are drawn while
+    // the particle pass before this kernel may still be running (for every
+    // cell; cells of fewer than two particles then ignore theirs).
+    float Lx[kResCellsPer][3];
+#pragma unroll
+    for (int q = 0; q < kResCellsPer; q++) {
+        const int cell = c0 + q * 256 + threadIdx.x;
+        Lx[q][0] = 0.f;
+        Lx[q][1] = 0.f;
+        Lx[q][2] = 1.f;
+        if (DIM == 3 && cell < c.ncells) res_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx[q]);
+    }
+    pdl_wait();  // the sums are complete from here on
     double av[3] = {0, 0, 0};
     if (blockIdx.x == 0 && threadIdx.x < ACC_WORDS) acc_next[threadIdx.x] = 0.0;
     ResSum s[kResCellsPer];
@@ -340,11 +354,10 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
             for (int d = 0; d < DIM; d++) u[d] = (float)((double)s[q].p[d] * kSumFxInv) * ip;
         }
         for (int d = 0; d < DIM; d++) av[d] += (double)u[d];
-        float Lx[3] = {0.f, 0.f, 1.f};
-        if (pop > 1 && DIM == 3) res_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
+        const bool rot = pop > 1 && DIM == 3;
         float4 *my = srec + 2 * (q * 256 + threadIdx.x);
         my[0] = make_float4(u[0], u[1], u[2], __int_as_float(pop));
-        my[1] = make_float4(Lx[0], Lx[1], Lx[2], 0.f);
+        my[1] = make_float4(rot ? Lx[q][0] : 0.f, rot ? Lx[q][1] : 0.f, rot ? Lx[q][2] : 1.f, 0.f);
     }
     __syncthreads();
     {
@@ -395,14 +408,17 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     const int nc = multi ? DIM + 1 : DIM;
     ResTable t;
     t.bind(res_smem, nc);
+    pdl_trigger();
     {
-        // keys to -1, everything after them to 0, in 16-byte stores
+        // keys to -1, everything after them to 0, in 16-byte stores (while
+        // the kernel before this one may still be running)
         uint4 *w = (uint4 *)res_smem;
         const int nkey = kResSlots / 4, nall = res_table_init_bytes(nc) / 16;
         for (int j = tid; j < nall; j += kResThreads)
             w[j] = j < nkey ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
+    pdl_wait();  // records, sums and particles are complete from here on
     float ke = 0.f;     // one species: sum of v^2 (times m at the end)
     double ke_m = 0.0;  // several species: sum of m v^2
     int bounce = 0, esc = 0, bad = 0;
