@@ -42,7 +42,8 @@ struct mpcd_handle {
     int scur;        // which start[] belongs to the current order
     double *acc;     // 2 x ACC_WORDS, by step parity
     unsigned long long *status;
-    int nscan;
+    int nscan;       // scan tiles of the largest key space
+    int nkeys;       // keys the counting sort may use: cells, or the bricks' slots
     int sm_count;
     int smem_optin;  // largest dynamic shared memory a block may opt in to
     int launches;
@@ -239,14 +240,13 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         };
         int bits[3] = {0, 0, 0};
         if (dc->dim == 3) {
-            // a block's particles span one or two planes of the slowest
-            // axis and a few rows of the middle one; their next cells add
-            // one cell on each side: 2 bits for the slowest axis, up to 3
-            // for the middle one, the rest for the fastest
-            bits[2] = std::min(clog2(dc->L[2]), kResBits - 4);
-            bits[0] = std::min(2, clog2(dc->L[0]));
-            bits[1] = std::min(std::min(3, clog2(dc->L[1])), kResBits - bits[2] - bits[0]);
-            bits[0] = kResBits - bits[2] - bits[1];
+            // a block's particles (brick order, k_key_res3) span about one
+            // brick, 4 cells, of the two slower axes and about three bricks
+            // of the fastest; their next cells add one on each side: 3 bits
+            // for each slower axis, the rest (5) for the fastest
+            bits[0] = std::min(3, clog2(dc->L[0]));
+            bits[1] = std::min(3, clog2(dc->L[1]));
+            bits[2] = kResBits - bits[0] - bits[1];
             dc->res_shift[2] = 0;
             dc->res_shift[1] = bits[2];
             dc->res_shift[0] = bits[2] + bits[1];
@@ -329,11 +329,16 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     }
     h->own_stream = true;
     int nc = dc.ncells;
-    h->nscan = (nc + kScanTile - 1) / kScanTile;
-    ALLOC(h->count, sizeof(int) * nc);
-    ALLOC(h->fill, sizeof(int) * nc);
-    ALLOC(h->start[0], sizeof(int) * (nc + 1));
-    ALLOC(h->start[1], sizeof(int) * (nc + 1));
+    // the 3D resident family sorts by brick (k_key_res3): its key space
+    h->nkeys = nc;
+    if (cfg->precision == MPCD_PREC_MIXED && !dc.lc && dc.dim == 3)
+        h->nkeys = std::max(nc, res_brick_keys(dc.N1));
+    const int nk = h->nkeys;
+    h->nscan = (nk + kScanTile - 1) / kScanTile;
+    ALLOC(h->count, sizeof(int) * nk);
+    ALLOC(h->fill, sizeof(int) * nk);
+    ALLOC(h->start[0], sizeof(int) * (nk + 1));
+    ALLOC(h->start[1], sizeof(int) * (nk + 1));
     ALLOC(h->part, sizeof(int) * h->nscan);
     ALLOC(h->acc, sizeof(double) * 2 * ACC_WORDS);
     ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
@@ -364,8 +369,8 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     h->sort_age = -1;
     h->strategy = -1;
     h->tile_target = 0;
-    if (cudaMemsetAsync(h->count, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
-        cudaMemsetAsync(h->fill, 0, sizeof(int) * nc, h->stream) != cudaSuccess ||
+    if (cudaMemsetAsync(h->count, 0, sizeof(int) * nk, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->fill, 0, sizeof(int) * nk, h->stream) != cudaSuccess ||
         cudaMemsetAsync(h->status, 0, sizeof(unsigned long long) * ST_WORDS, h->stream) !=
             cudaSuccess ||
         cudaMemsetAsync(h->acc, 0, sizeof(double) * 2 * ACC_WORDS, h->stream) != cudaSuccess) {
@@ -729,10 +734,13 @@ static int launch_tile(mpcd_handle *h, int mode, const typename T::State &a,
     return MPCD_OK;
 }
 
-static void launch_scan(mpcd_handle *h, int *start, int *fill, double *acc_zero) {
-    k_scan_partial<<<h->nscan, 256, 0, h->stream>>>(h->count, h->dc.ncells, h->part);
-    k_scan_apply<<<h->nscan, 256, 0, h->stream>>>(h->count, h->dc.ncells, h->part, start,
-                                                   fill, acc_zero);
+// Exclusive scan of the first nkeys counts (default: one per cell).
+static void launch_scan(mpcd_handle *h, int *start, int *fill, double *acc_zero,
+                        int nkeys = -1) {
+    if (nkeys < 0) nkeys = h->dc.ncells;
+    const int tiles = (nkeys + kScanTile - 1) / kScanTile;
+    k_scan_partial<<<tiles, 256, 0, h->stream>>>(h->count, nkeys, h->part);
+    k_scan_apply<<<tiles, 256, 0, h->stream>>>(h->count, nkeys, h->part, start, fill, acc_zero);
 }
 
 template <int DIM, class T>
@@ -893,8 +901,14 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     if (h->sorted_for == (int64_t)step) {
         h->sort_age = 0;
     } else if (h->sort_age < 0 || h->sort_age >= h->sort_interval) {
-        launch_key<DIM, MixT<DIM>>(h, h->mx[h->cur], sa);
-        launch_scan(h, h->start[h->scur], nullptr, nullptr);
+        if (DIM == 3) {
+            k_key_res3<<<grid_for(h, h->n), 256, 0, h->stream>>>(
+                h->dc, h->mx[h->cur], h->n, h->key, h->rank, h->count, sa, h->status);
+            launch_scan(h, h->start[h->scur], nullptr, nullptr, res_brick_keys(h->dc.N1));
+        } else {
+            launch_key<DIM, MixT<DIM>>(h, h->mx[h->cur], sa);
+            launch_scan(h, h->start[h->scur], nullptr, nullptr);
+        }
         launches += 3 + launch_scatter(h, h->mx[h->cur], h->mx[1 - h->cur], h->start[h->scur]);
         h->cur = 1 - h->cur;
         h->sort_age = 0;
