@@ -34,6 +34,13 @@ PPC = 10
 # written+read once per ppc particles): 3D SRD mixed 62.4 B, FP64 102.4 B
 ALG_BYTES = {"mixed": 62.4, "fp64": 102.4}
 WORKLOAD = "3D SRD fluid, periodic 64^3 cells, 10 particles/cell (2,621,440), rot 130 deg"
+L2_NOTE = {
+    "none": ("not flushed: steps run back to back; each step reads and writes 2 x 84 MB of "
+             "particle state plus 26 MB of cell sums and records, more than the 126 MB L2; "
+             "ms_per_step_l2_flushed gives steps with L2 flushed before each"),
+    "write+read": "flushed between timed steps: 256 MB write, then 256 MB read (L2 left holding clean lines)",
+    "write": "flushed between timed steps: 256 MB write",
+}
 
 
 def parse():
@@ -55,8 +62,9 @@ def parse():
                     help="srd64: the 64^3 SRD fluid (default); ensemble: 512 periodic SRD "
                          "boxes of sides 8-32 stepped together")
     ap.add_argument("--boxes", type=int, default=512, help="ensemble: number of boxes")
-    ap.add_argument("--flush", default="write+read", choices=["write+read", "write"],
-                    help="L2 flush between timed steps")
+    ap.add_argument("--flush", default="none", choices=["none", "write+read", "write"],
+                    help="L2 between timed steps: none (the step's working set is larger "
+                         "than L2), or a flush before each step")
     ap.add_argument("--sort-interval", type=int, default=0,
                     help="resident family: steps between re-sorts (0 = library default)")
     return ap.parse_args()
@@ -184,6 +192,12 @@ def run_gpu(args, rank, world):
     flush_rd = torch.ones(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     flush_sink = torch.empty(1, dtype=torch.float32, device="cuda")
     results = {}
+
+    def flush_l2(kind):
+        flush.zero_()
+        if kind == "write+read":
+            torch.sum(flush_rd, dim=0, out=flush_sink[0])
+
     forms = [f for f in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED))
              if f[0] in args.forms.split(",")]
     for form, prec in forms:
@@ -200,8 +214,6 @@ def run_gpu(args, rank, world):
         g.upload(Q, V, U, sp)
         g.step(args.warmup, 1)
         torch.cuda.synchronize()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
         clk = Clocks(dev) if form == "mixed" else None
         if clk:
             clk.wait_ready()
@@ -209,41 +221,71 @@ def run_gpu(args, rank, world):
             torch.distributed.barrier()
         torch.cuda.synchronize()
         launches = 0
+        step0 = 1 + args.warmup
         t_begin = time.time()
-        for k in range(args.steps):
-            flush.zero_()
-            if args.flush == "write+read":
-                torch.sum(flush_rd, dim=0, out=flush_sink[0])
-            ev[k][0].record(stream)
-            g.step(1, 1 + args.warmup + k)
-            ev[k][1].record(stream)
-            launches += g.launches_per_step()
-        torch.cuda.synchronize()
+        if args.flush == "none":
+            # back to back: the step's working set (state 2 x 84 MB, cell
+            # sums and records 26 MB at 64^3) is larger than L2, so no step
+            # finds the previous one's data there
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for k in range(args.steps):
+                g.step(1, step0 + k)
+                launches += g.launches_per_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = [e0.elapsed_time(e1) / args.steps]
+            total = e0.elapsed_time(e1)
+        else:
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
+            for k in range(args.steps):
+                flush_l2(args.flush)
+                ev[k][0].record(stream)
+                g.step(1, step0 + k)
+                ev[k][1].record(stream)
+                launches += g.launches_per_step()
+            torch.cuda.synchronize()
+            ms = [a.elapsed_time(b) for a, b in ev]
+            total = float(sum(ms))
         t_end = time.time()
         clocks = clk.stop(t_begin, t_end) if clk else None
-        # The particle pass alone: a second run of the same kind of steps with
-        # the library's CUDA events around each particle-pass launch (kept
-        # out of the timed steps above, where an event between the cell and
-        # particle passes would hold back the particle pass's early start).
+        step0 += args.steps
+        # For comparison, steps with L2 flushed before each one (256 MB
+        # write, then 256 MB read), each timed on its own.
+        nf = min(args.steps, 200)
+        evf = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(nf)]
+        for k in range(nf):
+            flush_l2("write+read")
+            evf[k][0].record(stream)
+            g.step(1, step0 + k)
+            evf[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms_flushed = sum(a.elapsed_time(b) for a, b in evf) / nf
+        step0 += nf
+        # The particle pass alone: a run of flushed steps with the library's
+        # CUDA events around each particle-pass launch (kept out of the
+        # timed steps above, where an event between the cell and particle
+        # passes would hold back the particle pass's early start).
         g.set_timing(True)
-        for k in range(min(args.steps, 200)):
-            flush.zero_()
-            if args.flush == "write+read":
-                torch.sum(flush_rd, dim=0, out=flush_sink[0])
-            g.step(1, 1 + args.warmup + args.steps + k)
+        for k in range(nf):
+            flush_l2("write+read")
+            g.step(1, step0 + k)
         torch.cuda.synchronize()
         kern_ms, kern_n = g.kernel_time()
         g.set_timing(False)
         if world > 1:
             torch.distributed.barrier()
-        ms = [a.elapsed_time(b) for a, b in ev]
-        total_ms = max_over_ranks(float(sum(ms)), world)
+        total_ms = max_over_ranks(total, world)
         kb, av = g.globals()
         st = g.status()
         kernel_ms = max_over_ranks(kern_ms / max(kern_n, 1), world)
         results[form] = {
             "n": n, "ms_total": total_ms, "ms_per_step": total_ms / args.steps,
-            "ms_min": min(ms), "launches": launches, "clocks": clocks,
+            "ms_min": min(ms), "ms_per_step_l2_flushed": max_over_ranks(ms_flushed, world),
+            "launches": launches, "clocks": clocks,
             "kbt": kb, "escaped": int(st.escaped), "kernel_ms": kernel_ms,
             "kernel_launches": kern_n,
         }
@@ -442,12 +484,11 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "global_batch": n * world, "form": "mixed",
                        "parallelism": f"replicas x{world}",
-                       "l2": ("flushed between timed steps: 256 MB write, then 256 MB read "
-                              "(L2 left holding clean lines)") if args.flush == "write+read"
-                       else "flushed between timed steps: 256 MB write"},
+                       "l2": L2_NOTE[args.flush]},
             "fp64": {"value": v64, "ms_per_step": f64["ms_total"] / args.steps,
                      "achieved_gbs": ach64, "frac": ach64 / peak},
             "mixed_over_fp64": value / v64,
+            "ms_per_step_l2_flushed": mix["ms_per_step_l2_flushed"],
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "traffic": traffic_per_launch(),
                          "kernel": "k_res_parts<3, RES_STEP> (particle pass)",

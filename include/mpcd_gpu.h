@@ -260,7 +260,7 @@ int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
 int mpcd_set_kernel(mpcd_handle *h, int kernel);
 
 /* MPCD_KERNEL_RESIDENT re-sorts the state by cell every 'steps' steps
- * (default 20) to keep particles that are close in space close in memory;
+ * (default 30) to keep particles that are close in space close in memory;
  * the sort changes no result, only the speed.  No counterpart in the
  * reference. */
 int mpcd_set_sort_interval(mpcd_handle *h, int steps);

@@ -365,7 +365,7 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     }
     h->sorted_for = -1;
     h->sums_for = -1;
-    h->sort_interval = 20;
+    h->sort_interval = 30;
     h->sort_age = -1;
     h->strategy = -1;
     h->tile_target = 0;

@@ -48,7 +48,7 @@ struct BatchBox {
     int res_shift[3], res_mask[3];
     uint64_t seed;
     uint32_t replica;
-    int pad_;
+    int key0;  // first sort key: the box's cells in brick order, then its padding key
 };
 
 struct BatchStep {
@@ -87,8 +87,10 @@ __global__ void k_bat_advance(uint32_t *counter) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *counter += 1u;
 }
 
-// Cell key of every slot on the current grid (padding slots: the box's
-// padding cell) and its rank, for the locality re-sort.
+// Sort key of every slot on the current grid and its rank, for the
+// locality re-sort: the cell in the brick order of the single-box resident
+// family (res_brick_key) after the box's first key; padding slots take the
+// box's last key.
 __global__ void __launch_bounds__(256) k_bat_key(const BatchBox *box, const int *chunk_box,
                                                  const BatchStep *st, MixState a, int nslots,
                                                  int *key, int *rank, int *count) {
@@ -96,13 +98,14 @@ __global__ void __launch_bounds__(256) k_bat_key(const BatchBox *box, const int 
          i += gridDim.x * blockDim.x) {
         const int b = chunk_box[i / kResChunk];
         const BatchBox &bx = box[b];
+        const int N1[3] = {bx.L[0] + 1, bx.L[1] + 1, bx.L[2] + 1};
         int k;
         if (i - bx.part0 < bx.npart) {
             int idx[3];
             fx_cur_idx_periodic<3>(a.P[i], bx.L, st[b].ks, idx);
-            k = bx.cell0 + (idx[0] * (bx.L[1] + 1) + idx[1]) * (bx.L[2] + 1) + idx[2];
+            k = bx.key0 + res_brick_key(N1, idx);
         } else {
-            k = bx.cell0 + bx.ncells;
+            k = bx.key0 + res_brick_keys(N1);
         }
         key[i] = k;
         rank[i] = atomicAdd(&count[k], 1);
@@ -259,6 +262,7 @@ struct mpcd_batch {
     std::vector<BatchBox> hbox;
     std::vector<int> hchunk_box, hcblk_box;
     int nslots = 0, ncells = 0, nchunks = 0, ncblk = 0, n = 0, nscan = 0;
+    int nkeys = 0;  // sort keys of all boxes (brick order, one padding key each)
     BatchBox *box = nullptr;
     BatchStep *st = nullptr;
     int *chunk_box = nullptr, *cblk_box = nullptr;
@@ -348,7 +352,7 @@ extern "C" int mpcd_batch_create(const mpcd_config *base, int nboxes, const int 
         delete b;
         return r;
     }
-    int cell0 = 0;
+    int cell0 = 0, key0 = 0;
     for (int k = 0; k < nboxes; k++) {
         BatchBox bx;
         memset(&bx, 0, sizeof(bx));
@@ -372,6 +376,8 @@ extern "C" int mpcd_batch_create(const mpcd_config *base, int nboxes, const int 
         }
         bx.ncells = (bx.L[0] + 1) * (bx.L[1] + 1) * (bx.L[2] + 1);
         bx.cell0 = cell0;
+        bx.key0 = key0;
+        key0 += res_brick_keys(dk.N1) + 1;
         const int span = (bx.ncells + 1 + kCellsPerBlock - 1) / kCellsPerBlock;
         for (int j = 0; j < span; j++) b->hcblk_box.push_back(k);
         cell0 += span * kCellsPerBlock;
@@ -380,6 +386,7 @@ extern "C" int mpcd_batch_create(const mpcd_config *base, int nboxes, const int 
         b->hbox.push_back(bx);
     }
     b->ncells = cell0;
+    b->nkeys = key0;
     b->ncblk = (int)b->hcblk_box.size();
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -424,7 +431,7 @@ extern "C" int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *
     b->nslots = slot0;
     b->n = n;
     b->nchunks = (int)b->hchunk_box.size();
-    b->nscan = (b->ncells + kScanTile - 1) / kScanTile;
+    b->nscan = (b->nkeys + kScanTile - 1) / kScanTile;
     // host conversion into the slot layout (padding slots: pid -1)
     std::vector<uint4> P((size_t)slot0, make_uint4(0u, 0u, 0u, 0u));
     std::vector<float4> W((size_t)slot0, make_float4(0.f, 0.f, 0.f, __int_as_float_host(-1)));
@@ -463,8 +470,8 @@ extern "C" int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *
     BALLOC(b->key, sizeof(int) * S);
     BALLOC(b->rank, sizeof(int) * S);
     BALLOC(b->perm, sizeof(int) * S);
-    BALLOC(b->count, sizeof(int) * C);
-    BALLOC(b->start, sizeof(int) * (C + 1));
+    BALLOC(b->count, sizeof(int) * (size_t)b->nkeys);
+    BALLOC(b->start, sizeof(int) * ((size_t)b->nkeys + 1));
     BALLOC(b->part, sizeof(int) * b->nscan);
     BALLOC(b->rsum, sizeof(ResSum) * 2 * C);
     BALLOC(b->crec, sizeof(ResRec) * C);
@@ -483,7 +490,7 @@ extern "C" int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *
                         cudaMemcpyHostToDevice, b->stream));
     BCK(cudaMemcpyAsync(b->counter, &step0, sizeof(uint32_t), cudaMemcpyHostToDevice,
                         b->stream));
-    BCK(cudaMemsetAsync(b->count, 0, sizeof(int) * C, b->stream));
+    BCK(cudaMemsetAsync(b->count, 0, sizeof(int) * (size_t)b->nkeys, b->stream));
     BCK(cudaMemsetAsync(b->rsum, 0, sizeof(ResSum) * 2 * C, b->stream));
     BCK(cudaMemsetAsync(b->acc, 0, sizeof(double) * 2 * b->nb * ACC_WORDS, b->stream));
     BCK(cudaMemsetAsync(b->status, 0, sizeof(unsigned long long) * ST_WORDS, b->stream));
@@ -512,8 +519,8 @@ static int record_step(mpcd_batch *b, bool sorted, int parity, int state_cur,
     if (sorted) {
         k_bat_key<<<grid_for(b, b->nslots), 256, 0, b->cap_stream>>>(
             b->box, b->chunk_box, b->st, b->mx[cur], b->nslots, b->key, b->rank, b->count);
-        k_scan_partial<<<b->nscan, 256, 0, b->cap_stream>>>(b->count, b->ncells, b->part);
-        k_scan_apply<<<b->nscan, 256, 0, b->cap_stream>>>(b->count, b->ncells, b->part, b->start,
+        k_scan_partial<<<b->nscan, 256, 0, b->cap_stream>>>(b->count, b->nkeys, b->part);
+        k_scan_apply<<<b->nscan, 256, 0, b->cap_stream>>>(b->count, b->nkeys, b->part, b->start,
                                                       nullptr, nullptr);
         k_perm<<<grid_for(b, b->nslots), 256, 0, b->cap_stream>>>(b->nslots, b->key, b->rank,
                                                                b->start, b->perm);

@@ -394,10 +394,10 @@ __host__ __device__ __forceinline__ int res_brick_dim(int n1) {
 __host__ __device__ __forceinline__ int res_brick_keys(const int N1[3]) {
     return res_brick_dim(N1[0]) * res_brick_dim(N1[1]) * res_brick_dim(N1[2]) << (3 * kBrickBits);
 }
-__device__ __forceinline__ int res_brick_key(const DevCfg &c, const int idx[3]) {
+__host__ __device__ __forceinline__ int res_brick_key(const int N1[3], const int idx[3]) {
     constexpr int m = (1 << kBrickBits) - 1;
-    const int b = ((idx[0] >> kBrickBits) * res_brick_dim(c.N1[1]) + (idx[1] >> kBrickBits)) *
-                      res_brick_dim(c.N1[2]) +
+    const int b = ((idx[0] >> kBrickBits) * res_brick_dim(N1[1]) + (idx[1] >> kBrickBits)) *
+                      res_brick_dim(N1[2]) +
                   (idx[2] >> kBrickBits);
     return (b << (3 * kBrickBits)) | ((idx[0] & m) << (2 * kBrickBits)) |
            ((idx[1] & m) << kBrickBits) | (idx[2] & m);
@@ -415,7 +415,7 @@ static __global__ void __launch_bounds__(256)
         for (int d = 0; d < 3; d++)
             idx[d] = fx_shift_axis(ci[d], f[d], sa.ks[d], c.L[d], c.pbc[d], t, e);
         esc_local += e;
-        const int k = res_brick_key(c, idx);
+        const int k = res_brick_key(c.N1, idx);
         key[i] = k;
         rank[i] = atomicAdd(&count[k], 1);
     }
