@@ -227,38 +227,7 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     dc->all_periodic = dc->n_solid == 0;
     for (int d = 0; d < cfg->dim; d++)
         if (!dc->pbc[d]) dc->all_periodic = 0;
-    {
-        // slot bit fields for the resident family's tables: the fastest
-        // axis of the linear cell order gets most bits, the next (3D) up to
-        // 3, the slowest the rest, so that the cells a block of particles
-        // (sorted by cell) lands in map to distinct, mostly consecutive
-        // slots (consecutive slots: distinct shared-memory banks)
-        auto clog2 = [](int x) {
-            int b = 0;
-            while ((1 << b) < x) b++;
-            return b;
-        };
-        int bits[3] = {0, 0, 0};
-        if (dc->dim == 3) {
-            // a block's particles (brick order, k_key_res3) span about one
-            // brick, 4 cells, of the two slower axes and about three bricks
-            // of the fastest; their next cells add one on each side: 3 bits
-            // for each slower axis, the rest (5) for the fastest
-            bits[0] = std::min(3, clog2(dc->L[0]));
-            bits[1] = std::min(3, clog2(dc->L[1]));
-            bits[2] = kResBits - bits[0] - bits[1];
-            dc->res_shift[2] = 0;
-            dc->res_shift[1] = bits[2];
-            dc->res_shift[0] = bits[2] + bits[1];
-        } else {
-            bits[1] = std::min(clog2(dc->L[1]), kResBits - 2);
-            bits[0] = kResBits - bits[1];
-            dc->res_shift[1] = 0;
-            dc->res_shift[0] = bits[1];
-            dc->res_shift[2] = 0;
-        }
-        for (int d = 0; d < 3; d++) dc->res_mask[d] = (1 << bits[d]) - 1;
-    }
+    res_slot_bits(dc->dim, dc->L, dc->res_shift, dc->res_mask);
     return MPCD_OK;
 }
 

@@ -16,6 +16,12 @@
 // identical, bit for bit, to that of a single-box handle created with the
 // same seed and replica (the resident family's sums are exact and
 // order-independent).
+// The ensemble's boxes are small (sides 8 to 32 in the ensemble benchmark):
+// a 1024-slot table per block, so that four blocks fit on an SM.
+#define MPCD_RES_SLOTS 1024
+#define MPCD_RES_MINB 4
+#define MPCD_RES_NS res_s1024_b4
+
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -370,10 +376,7 @@ extern "C" int mpcd_batch_create(const mpcd_config *base, int nboxes, const int 
             delete b;
             return MPCD_ERR_ARG;
         }
-        for (int d = 0; d < 3; d++) {
-            bx.res_shift[d] = dk.res_shift[d];
-            bx.res_mask[d] = dk.res_mask[d];
-        }
+        res_slot_bits(3, bx.L, bx.res_shift, bx.res_mask);
         bx.ncells = (bx.L[0] + 1) * (bx.L[1] + 1) * (bx.L[2] + 1);
         bx.cell0 = cell0;
         bx.key0 = key0;

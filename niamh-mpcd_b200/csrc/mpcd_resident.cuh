@@ -30,7 +30,15 @@
 
 #include "mpcd_split.cuh"
 
+// The table size and occupancy below are compile-time choices of the file
+// that includes this header; each such choice gets its own inline
+// namespace, so translation units with different choices link together.
+#ifndef MPCD_RES_NS
+#define MPCD_RES_NS res_s2048_b3
+#endif
+
 namespace mpcd {
+inline namespace MPCD_RES_NS {
 
 // The resident family's cell record, one 32-byte sector: {u.x, u.y, u.z,
 // population (int bits)} and {axis x, y, z, 0}.  The particle pass applies
@@ -543,4 +551,36 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     if (bad) atomicAdd(&status[ST_NONFINITE], (unsigned long long)bad);
 }
 
+// Slot bit fields of the tables for a box of sides L: per-axis low bits of
+// the cell indices, so that the cells a block of particles lands in map to
+// distinct, mostly consecutive slots (consecutive slots: distinct banks).
+// 3D (brick order, k_key_res3): a block's particles span about one brick,
+// 4 cells, of the two slower axes and a few bricks of the fastest, and their
+// next cells add one on each side: 3 bits for each slower axis, the rest for
+// the fastest.  2D (row order): the fastest axis gets up to all but 2 bits.
+static inline void res_slot_bits(int dim, const int L[3], int shift[3], int mask[3]) {
+    auto clog2 = [](int x) {
+        int b = 0;
+        while ((1 << b) < x) b++;
+        return b;
+    };
+    int bits[3] = {0, 0, 0};
+    if (dim == 3) {
+        bits[0] = clog2(L[0]) < 3 ? clog2(L[0]) : 3;
+        bits[1] = clog2(L[1]) < 3 ? clog2(L[1]) : 3;
+        bits[2] = kResBits - bits[0] - bits[1];
+        shift[2] = 0;
+        shift[1] = bits[2];
+        shift[0] = bits[2] + bits[1];
+    } else {
+        bits[1] = clog2(L[1]) < kResBits - 2 ? clog2(L[1]) : kResBits - 2;
+        bits[0] = kResBits - bits[1];
+        shift[1] = 0;
+        shift[0] = bits[1];
+        shift[2] = 0;
+    }
+    for (int d = 0; d < 3; d++) mask[d] = (1 << bits[d]) - 1;
+}
+
+}  // namespace MPCD_RES_NS
 }  // namespace mpcd
