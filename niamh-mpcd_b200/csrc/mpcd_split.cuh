@@ -200,21 +200,14 @@ __global__ void __launch_bounds__(256, MPCD_SPLIT_MINB) k_srd_parts(const __grid
             }
         }
         const int k = T::finish(c, r, sp, sa, bounce, esc);
-        // warp-aggregated counting: lanes with the same next cell take one
-        // atomic (particles of a cell are adjacent and mostly move together)
-        const unsigned act = __activemask();
-        const unsigned peers = __match_any_sync(act, k);
-        const int lane = threadIdx.x & 31;
-        const int leader = __ffs(peers) - 1;
-        const int below = __popc(peers & ((1u << lane) - 1u));
+        // one atomic per particle on its next cell's counter (L2 resolves
+        // same-cell contention; a warp-level match of equal cells first
+        // measured far slower on this GPU)
         if (MODE == MODE_COUNT) {
-            if (lane == leader) atomicAdd(&tb.count_next[k], __popc(peers));
+            atomicAdd(&tb.count_next[k], 1);
         } else {
-            int base = 0;
-            if (lane == leader)
-                base = atomicAdd(MODE == MODE_INPLACE ? &tb.count_next[k] : &tb.fill[k],
-                                 __popc(peers));
-            base = __shfl_sync(peers, base, leader) + below;
+            const int base =
+                atomicAdd(MODE == MODE_INPLACE ? &tb.count_next[k] : &tb.fill[k], 1);
             if (MODE == MODE_INPLACE) {
                 T::store(a, i, r);
                 tb.key[i] = k;
