@@ -21,6 +21,7 @@
 #include "mpcd_group.cuh"
 #include "mpcd_split.cuh"
 #include "mpcd_resident.cuh"
+#include "mpcd_resident64.cuh"
 #include "mpcd_lc.cuh"
 
 using namespace mpcd;
@@ -56,6 +57,8 @@ struct mpcd_handle {
     double *modes;   // transverse momentum modes (mpcd_transverse_modes)
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     ResSum *rsum;              // resident family: cell sums, two steps by parity
+    R64Sum *r64sum;            // FP64 resident family: cell sums, two steps by parity
+    int *r64pop;               // FP64 resident family: populations, two steps by parity
     unsigned long long *rmsum;  // resident family: mass sums (several species)
     int64_t sums_for;          // step whose cell sums rsum holds; -1 none
     int sort_interval;         // resident family: steps between re-sorts
@@ -264,6 +267,8 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->modes);
     cudaFree(h->rsum);
     cudaFree(h->rmsum);
+    cudaFree(h->r64sum);
+    cudaFree(h->r64pop);
     cudaFree(h->lcbuf);
     if (h->host_acc) cudaFreeHost(h->host_acc);
     time_clear(h);
@@ -315,6 +320,10 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     if (cfg->precision == MPCD_PREC_MIXED && !dc.lc) {
         ALLOC(h->rsum, sizeof(ResSum) * 2 * (size_t)nc);
         if (dc.n_species > 1) ALLOC(h->rmsum, sizeof(unsigned long long) * 2 * (size_t)nc);
+    }
+    if (cfg->precision == MPCD_PREC_FP64 && !dc.lc) {
+        ALLOC(h->r64sum, sizeof(R64Sum) * 2 * (size_t)nc);
+        ALLOC(h->r64pop, sizeof(int) * 2 * (size_t)nc);
     }
     if (dc.lc) {
         ALLOC(h->lcbuf, (size_t)nc * 13 * sizeof(double));
@@ -638,7 +647,6 @@ static int kernel_family(const mpcd_handle *h) {
     if (!srd_plain) return MPCD_KERNEL_TILE;
     const bool mixed = h->prec == MPCD_PREC_MIXED;
     if (h->kernel == MPCD_KERNEL_AUTO) return mixed ? MPCD_KERNEL_RESIDENT : MPCD_KERNEL_SPLIT;
-    if (h->kernel == MPCD_KERNEL_RESIDENT && !mixed) return MPCD_KERNEL_SPLIT;
     return h->kernel;
 }
 
@@ -917,6 +925,59 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     return MPCD_OK;
 }
 
+// One step of the FP64 resident family (mpcd_resident64.cuh): an occasional
+// re-sort for locality (the FP64 counting sort), the cell pass and the
+// particle pass, both launched as programmatic dependents.
+template <int DIM>
+static int run_step_r64(mpcd_handle *h, uint32_t step) {
+    StepArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.step = step;
+    host_shift(h, step, sa.s);
+    host_shift(h, step + 1u, sa.sn);
+    const DevCfg &c = h->dc;
+    const size_t nc = (size_t)c.ncells;
+    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
+    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    R64Sum *sum_cur = h->r64sum + (step & 1u) * nc;
+    R64Sum *sum_nxt = h->r64sum + ((step + 1u) & 1u) * nc;
+    int *pop_cur = h->r64pop + (step & 1u) * nc;
+    int *pop_nxt = h->r64pop + ((step + 1u) & 1u) * nc;
+    using Rec = typename SrdCell<F64T<DIM>>::Rec;
+    int launches = 0;
+    if (h->sorted_for == (int64_t)step) {
+        h->sort_age = 0;
+    } else if (h->sort_age < 0 || h->sort_age >= h->sort_interval) {
+        launch_key<DIM, F64T<DIM>>(h, h->f[h->cur], sa);
+        launch_scan(h, h->start[h->scur], nullptr, nullptr);
+        launches += 3 + launch_scatter(h, h->f[h->cur], h->f[1 - h->cur], h->start[h->scur]);
+        h->cur = 1 - h->cur;
+        h->sort_age = 0;
+    }
+    const int pgrid = (int)((h->n + 255) / 256);
+    if (h->sums_for != (int64_t)step) {
+        CK(cudaMemsetAsync(h->r64sum, 0, sizeof(R64Sum) * 2 * nc, h->stream));
+        CK(cudaMemsetAsync(h->r64pop, 0, sizeof(int) * 2 * nc, h->stream));
+        CK(cudaMemsetAsync(acc_cur, 0, sizeof(double) * ACC_WORDS, h->stream));
+        k_r64_parts<DIM, RES_SUM><<<pgrid, 256, 0, h->stream>>>(
+            c, h->f[h->cur], h->n, (const Rec *)h->crec, sum_cur, pop_cur, acc_cur, h->status, sa);
+        launches += 1;
+    }
+    CK(launch_pdl(k_r64_cells<DIM>, (int)((nc + 255) / 256), 256, 0, h->stream, c, sum_cur,
+                  pop_cur, (Rec *)h->crec, sa, acc_cur, acc_nxt));
+    time_begin(h);
+    CK(launch_pdl(k_r64_parts<DIM, RES_STEP>, pgrid, 256, 0, h->stream, c, h->f[h->cur], h->n,
+                  (const Rec *)h->crec, sum_nxt, pop_nxt, acc_cur, h->status, sa));
+    time_end(h);
+    launches += 2;
+    CK(cudaGetLastError());
+    h->sums_for = (int64_t)step + 1;
+    h->sorted_for = -1;
+    h->sort_age++;
+    h->launches = launches;
+    return MPCD_OK;
+}
+
 static int default_strategy(const mpcd_handle *h) {
     // recompute (96 B/particle) wins when the collision is cheap to redo
     return h->dc.op == MPCD_COLL_ARBAXIS ? MPCD_STRATEGY_RECOMPUTE : MPCD_STRATEGY_SCATTER;
@@ -1002,6 +1063,8 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
         if (h->dc.lc)
             r = h->prec == MPCD_PREC_FP64 ? run_step_lc<F64T<2>>(h, h->f, step)
                                           : run_step_lc<MixT<2>>(h, h->mx, step);
+        else if (h->prec == MPCD_PREC_FP64 && kernel_family(h) == MPCD_KERNEL_RESIDENT)
+            r = h->dc.dim == 3 ? run_step_r64<3>(h, step) : run_step_r64<2>(h, step);
         else if (h->prec == MPCD_PREC_FP64)
             r = h->dc.dim == 3 ? run_step<3, F64T<3>>(h, h->f, step)
                                : run_step<2, F64T<2>>(h, h->f, step);

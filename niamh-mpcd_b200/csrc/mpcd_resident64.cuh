@@ -1,0 +1,127 @@
+// mpcd_resident64.cuh -- SRD step of the FP64 form with the particles
+// resident in place (MPCD_KERNEL_RESIDENT for MPCD_PREC_FP64).
+//
+// The same two-pass structure as the mixed resident family
+// (mpcd_resident.cuh), with the FP64 form's arithmetic:
+//   k_r64_cells  one thread per cell: u = (sum m v) / (sum m) from the FP64
+//                sums of the previous particle pass, the random axis and the
+//                rotation matrix (stochrotMPC + rotate, mpc.c:1181-1333), the
+//                avVel term; writes the FP64 record of the split family
+//                (SrdCell<F64T>) and clears the sums.
+//   k_r64_parts  one thread per particle: its cell on this step's grid
+//                (recomputed from its position exactly as the split family
+//                does), v' = u + R (v - u), TEMP term, finish() (shift back,
+//                stream, walls, next step's cell), the particle written back
+//                in place, and its mass and momentum (with the next step's
+//                gravity kick) added to its cell of the next step with FP64
+//                atomics.
+// The sums are FP64 additions in the order the atomics arrive, so they
+// agree with the split family's sorted-order sums to rounding (about 1e-16
+// relative); the state is re-sorted every few steps for locality only.
+#pragma once
+
+#include "mpcd_split.cuh"
+
+namespace mpcd {
+
+// FP64 cell sums: mass and mass-weighted momentum (with the step's gravity
+// kick); the population is a separate int array.
+struct __align__(32) R64Sum {
+    double M;
+    double p[3];
+};
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCfg c,
+                                                   R64Sum *sums, int *pops,
+                                                   typename SrdCell<F64T<DIM>>::Rec *crec,
+                                                   StepArgs sa, double *acc, double *acc_next) {
+    __shared__ double red[8];
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    pdl_trigger();
+    // the axis depends on the step and the cell only: drawn while the
+    // particle pass before this kernel may still be running
+    double Lx[3] = {0.0, 0.0, 1.0};
+    if (DIM == 3 && cell < c.ncells) mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
+    pdl_wait();  // the sums are complete from here on
+    if (blockIdx.x == 0 && threadIdx.x < ACC_WORDS) acc_next[threadIdx.x] = 0.0;
+    double av[3] = {0.0, 0.0, 0.0};
+    if (cell < c.ncells) {
+        const R64Sum s = sums[cell];
+        const int pop = pops[cell];
+        sums[cell] = R64Sum{0.0, {0.0, 0.0, 0.0}};
+        pops[cell] = 0;
+        double u[3] = {0.0, 0.0, 0.0};
+        if (s.M > 0.0) {
+            const double iM = 1.0 / s.M;
+            for (int d = 0; d < DIM; d++) u[d] = s.p[d] * iM;
+        }
+        for (int d = 0; d < DIM; d++) av[d] = u[d];
+        double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (pop > 1) srd_matrix<DIM, double>(c, Lx, R);
+        SrdCell<F64T<DIM>>::put(crec, cell, u, pop, R);
+    }
+    for (int d = 0; d < DIM; d++) {
+        const double t = block_sum256(av[d], red);
+        if (threadIdx.x == 0) atomicAdd(&acc[ACC_VCM + d], t);
+    }
+}
+
+// RES_STEP: collide, stream, write back, add to the next step's sums.
+// RES_SUM:  only add each particle to this step's sums (bootstrap).
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCfg c,
+                                                   Fp64State a, int n,
+                                                   const typename SrdCell<F64T<DIM>>::Rec *crec,
+                                                   R64Sum *sums, int *pops, double *acc,
+                                                   unsigned long long *status, StepArgs sa) {
+    __shared__ double red[8];
+    pdl_trigger();
+    pdl_wait();  // records, sums and particles are complete from here on
+    double ke = 0.0;
+    int bounce = 0, esc = 0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        F64Rec r;
+        F64T<DIM>::load(c, a, i, sa, r);  // shifted position, velocity with this step's kick
+        const int sp = F64T<DIM>::sp(a, i);
+        int k;
+        double v[3] = {0.0, 0.0, 0.0};
+        if (MODE == RES_STEP) {
+            const int kc = cur_key<DIM>(c, r, sa);
+            const typename SrdCell<F64T<DIM>>::Rec &cr = crec[kc];
+            if (cr.pop > 1.0) {
+                double w[3] = {0, 0, 0}, tt[3] = {0, 0, 0};
+                for (int d = 0; d < DIM; d++) w[d] = r.v[d] - cr.u[d];
+                for (int x = 0; x < DIM; x++)
+                    for (int y = 0; y < DIM; y++) tt[x] += cr.R[x * 3 + y] * w[y];
+                for (int d = 0; d < DIM; d++) r.v[d] = cr.u[d] + tt[d];
+            }
+            double t = r.v[0] * r.v[0];
+            t += r.v[1] * r.v[1];
+            t += r.v[2] * r.v[2];
+            ke = c.mass[sp] * t;
+            k = F64T<DIM>::finish(c, r, sp, sa, bounce, esc);
+            F64T<DIM>::store(a, i, r);
+            // the next step's cell pass sees the velocity with its kick
+            for (int d = 0; d < DIM; d++)
+                v[d] = c.grav_flag ? r.v[d] + c.dt * c.grav[d] : r.v[d];
+        } else {
+            k = cur_key<DIM>(c, r, sa);
+            for (int d = 0; d < DIM; d++) v[d] = r.v[d];
+        }
+        const double m = c.mass[sp];
+        R64Sum *s = sums + k;
+        atomicAdd(&s->M, m);
+        for (int d = 0; d < DIM; d++) atomicAdd(&s->p[d], v[d] * m);
+        atomicAdd(pops + k, 1);
+    }
+    if (MODE == RES_STEP) {
+        const double t = block_sum256(ke, red);
+        if (threadIdx.x == 0) atomicAdd(&acc[ACC_KE], t);
+        if (bounce) atomicAdd(&status[ST_BOUNCE], (unsigned long long)bounce);
+    }
+    if (esc) atomicAdd(&status[ST_ESCAPED], (unsigned long long)esc);
+}
+
+}  // namespace mpcd
