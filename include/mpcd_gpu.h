@@ -237,13 +237,15 @@ int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
 
 /* Cell-kernel family (no counterpart in the reference).  For the SRD
  * operator without phantom walls:
- *   MPCD_KERNEL_RESIDENT (mixed precision) the particles stay in place: a
- *                      thread-per-cell pass turns the cell sums into each
- *                      cell's centre-of-mass velocity and rotation, and a
+ *   MPCD_KERNEL_RESIDENT the particles stay in place: a thread-per-cell
+ *                      pass turns the cell sums into each cell's
+ *                      centre-of-mass velocity and rotation, and a
  *                      thread-per-particle pass collides, streams, writes the
- *                      particle back and adds it, in 64-bit fixed point, to
- *                      the next step's cell sums (the default for mixed;
- *                      results do not depend on the particle order);
+ *                      particle back and adds it to the next step's cell
+ *                      sums.  Mixed precision (the default there): sums in
+ *                      64-bit fixed point, results independent of the
+ *                      particle order.  FP64: FP64 atomic sums, which agree
+ *                      with the sorted-order sums to rounding;
  *   MPCD_KERNEL_SPLIT  the same two passes over a state kept sorted by cell,
  *                      re-binned every step (the default for FP64);
  *   MPCD_KERNEL_GROUP  one warp per group of 32 cells does both, staging the
@@ -251,7 +253,7 @@ int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
  *   MPCD_KERNEL_TILE   one block per tile of cells (the kernel every other
  *                      operator uses).
  * MPCD_KERNEL_AUTO picks RESIDENT (mixed) or SPLIT (FP64) where they apply
- * and TILE elsewhere; RESIDENT asked for in FP64 runs SPLIT. */
+ * and TILE elsewhere. */
 #define MPCD_KERNEL_AUTO 0
 #define MPCD_KERNEL_TILE 1
 #define MPCD_KERNEL_GROUP 2

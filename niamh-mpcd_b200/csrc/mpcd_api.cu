@@ -57,7 +57,7 @@ struct mpcd_handle {
     double *modes;   // transverse momentum modes (mpcd_transverse_modes)
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     ResSum *rsum;              // resident family: cell sums, two steps by parity
-    R64Sum *r64sum;            // FP64 resident family: cell sums, two steps by parity
+    double *r64sum;            // FP64 resident family: M, p[3] sums (4 x nc), two steps by parity
     int *r64pop;               // FP64 resident family: populations, two steps by parity
     unsigned long long *rmsum;  // resident family: mass sums (several species)
     int64_t sums_for;          // step whose cell sums rsum holds; -1 none
@@ -322,7 +322,7 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
         if (dc.n_species > 1) ALLOC(h->rmsum, sizeof(unsigned long long) * 2 * (size_t)nc);
     }
     if (cfg->precision == MPCD_PREC_FP64 && !dc.lc) {
-        ALLOC(h->r64sum, sizeof(R64Sum) * 2 * (size_t)nc);
+        ALLOC(h->r64sum, sizeof(double) * 8 * (size_t)nc);
         ALLOC(h->r64pop, sizeof(int) * 2 * (size_t)nc);
     }
     if (dc.lc) {
@@ -939,10 +939,15 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
     const size_t nc = (size_t)c.ncells;
     double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
     double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
-    R64Sum *sum_cur = h->r64sum + (step & 1u) * nc;
-    R64Sum *sum_nxt = h->r64sum + ((step + 1u) & 1u) * nc;
-    int *pop_cur = h->r64pop + (step & 1u) * nc;
-    int *pop_nxt = h->r64pop + ((step + 1u) & 1u) * nc;
+    auto sums_of = [&](uint32_t parity) {
+        R64Sums r;
+        double *b = h->r64sum + (size_t)(parity & 1u) * 4 * nc;
+        r.M = b;
+        for (int d = 0; d < 3; d++) r.p[d] = b + (size_t)(d + 1) * nc;
+        r.pop = h->r64pop + (size_t)(parity & 1u) * nc;
+        return r;
+    };
+    const R64Sums sum_cur = sums_of(step), sum_nxt = sums_of(step + 1u);
     using Rec = typename SrdCell<F64T<DIM>>::Rec;
     int launches = 0;
     if (h->sorted_for == (int64_t)step) {
@@ -956,18 +961,18 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
     }
     const int pgrid = (int)((h->n + 255) / 256);
     if (h->sums_for != (int64_t)step) {
-        CK(cudaMemsetAsync(h->r64sum, 0, sizeof(R64Sum) * 2 * nc, h->stream));
+        CK(cudaMemsetAsync(h->r64sum, 0, sizeof(double) * 8 * nc, h->stream));
         CK(cudaMemsetAsync(h->r64pop, 0, sizeof(int) * 2 * nc, h->stream));
         CK(cudaMemsetAsync(acc_cur, 0, sizeof(double) * ACC_WORDS, h->stream));
         k_r64_parts<DIM, RES_SUM><<<pgrid, 256, 0, h->stream>>>(
-            c, h->f[h->cur], h->n, (const Rec *)h->crec, sum_cur, pop_cur, acc_cur, h->status, sa);
+            c, h->f[h->cur], h->n, (const Rec *)h->crec, sum_cur, acc_cur, h->status, sa);
         launches += 1;
     }
     CK(launch_pdl(k_r64_cells<DIM>, (int)((nc + 255) / 256), 256, 0, h->stream, c, sum_cur,
-                  pop_cur, (Rec *)h->crec, sa, acc_cur, acc_nxt));
+                  (Rec *)h->crec, sa, acc_cur, acc_nxt));
     time_begin(h);
     CK(launch_pdl(k_r64_parts<DIM, RES_STEP>, pgrid, 256, 0, h->stream, c, h->f[h->cur], h->n,
-                  (const Rec *)h->crec, sum_nxt, pop_nxt, acc_cur, h->status, sa));
+                  (const Rec *)h->crec, sum_nxt, acc_cur, h->status, sa));
     time_end(h);
     launches += 2;
     CK(cudaGetLastError());

@@ -24,16 +24,18 @@
 
 namespace mpcd {
 
-// FP64 cell sums: mass and mass-weighted momentum (with the step's gravity
-// kick); the population is a separate int array.
-struct __align__(32) R64Sum {
-    double M;
-    double p[3];
+// FP64 cell sums: mass, mass-weighted momentum (with the step's gravity
+// kick) and population, one array each, so that the atomics of one cell's
+// particles fall on different sectors (the L2 serialises atomics on one
+// sector).  Each array holds nc entries.
+struct R64Sums {
+    double *M, *p[3];
+    int *pop;
 };
 
 template <int DIM>
 __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCfg c,
-                                                   R64Sum *sums, int *pops,
+                                                   R64Sums sums,
                                                    typename SrdCell<F64T<DIM>>::Rec *crec,
                                                    StepArgs sa, double *acc, double *acc_next) {
     __shared__ double red[8];
@@ -47,14 +49,17 @@ __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCf
     if (blockIdx.x == 0 && threadIdx.x < ACC_WORDS) acc_next[threadIdx.x] = 0.0;
     double av[3] = {0.0, 0.0, 0.0};
     if (cell < c.ncells) {
-        const R64Sum s = sums[cell];
-        const int pop = pops[cell];
-        sums[cell] = R64Sum{0.0, {0.0, 0.0, 0.0}};
-        pops[cell] = 0;
+        const double M = sums.M[cell];
+        double p[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < DIM; d++) p[d] = sums.p[d][cell];
+        const int pop = sums.pop[cell];
+        sums.M[cell] = 0.0;
+        for (int d = 0; d < DIM; d++) sums.p[d][cell] = 0.0;
+        sums.pop[cell] = 0;
         double u[3] = {0.0, 0.0, 0.0};
-        if (s.M > 0.0) {
-            const double iM = 1.0 / s.M;
-            for (int d = 0; d < DIM; d++) u[d] = s.p[d] * iM;
+        if (M > 0.0) {
+            const double iM = 1.0 / M;
+            for (int d = 0; d < DIM; d++) u[d] = p[d] * iM;
         }
         for (int d = 0; d < DIM; d++) av[d] = u[d];
         double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -73,7 +78,7 @@ template <int DIM, int MODE>
 __global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCfg c,
                                                    Fp64State a, int n,
                                                    const typename SrdCell<F64T<DIM>>::Rec *crec,
-                                                   R64Sum *sums, int *pops, double *acc,
+                                                   R64Sums sums, double *acc,
                                                    unsigned long long *status, StepArgs sa) {
     __shared__ double red[8];
     pdl_trigger();
@@ -111,10 +116,9 @@ __global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCf
             for (int d = 0; d < DIM; d++) v[d] = r.v[d];
         }
         const double m = c.mass[sp];
-        R64Sum *s = sums + k;
-        atomicAdd(&s->M, m);
-        for (int d = 0; d < DIM; d++) atomicAdd(&s->p[d], v[d] * m);
-        atomicAdd(pops + k, 1);
+        atomicAdd(sums.M + k, m);
+        for (int d = 0; d < DIM; d++) atomicAdd(sums.p[d] + k, v[d] * m);
+        atomicAdd(sums.pop + k, 1);
     }
     if (MODE == RES_STEP) {
         const double t = block_sum256(ke, red);
