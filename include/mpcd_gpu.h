@@ -247,13 +247,12 @@ int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
  *                      particle order.  FP64: FP64 atomic sums, which agree
  *                      with the sorted-order sums to rounding;
  *   MPCD_KERNEL_SPLIT  the same two passes over a state kept sorted by cell,
- *                      re-binned every step (the default for FP64);
+ *                      re-binned every step;
  *   MPCD_KERNEL_GROUP  one warp per group of 32 cells does both, staging the
  *                      group in shared memory;
  *   MPCD_KERNEL_TILE   one block per tile of cells (the kernel every other
  *                      operator uses).
- * MPCD_KERNEL_AUTO picks RESIDENT (mixed) or SPLIT (FP64) where they apply
- * and TILE elsewhere. */
+ * MPCD_KERNEL_AUTO picks RESIDENT where it applies and TILE elsewhere. */
 #define MPCD_KERNEL_AUTO 0
 #define MPCD_KERNEL_TILE 1
 #define MPCD_KERNEL_GROUP 2

@@ -646,7 +646,8 @@ static int kernel_family(const mpcd_handle *h) {
     bool srd_plain = h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom && !h->dc.lc;
     if (!srd_plain) return MPCD_KERNEL_TILE;
     const bool mixed = h->prec == MPCD_PREC_MIXED;
-    if (h->kernel == MPCD_KERNEL_AUTO) return mixed ? MPCD_KERNEL_RESIDENT : MPCD_KERNEL_SPLIT;
+    (void)mixed;
+    if (h->kernel == MPCD_KERNEL_AUTO) return MPCD_KERNEL_RESIDENT;
     return h->kernel;
 }
 

@@ -28,13 +28,21 @@ def _walled_srd(seed=777):
                          seed=seed)
 
 
-@pytest.mark.parametrize("name", ["srd3d", "srd2d", "srd3d_heavy", "walled"])
+@pytest.mark.parametrize("name", ["srd3d", "srd2d", "srd3d_heavy", "walled", "two_species"])
 def test_fp64_resident_matches_oracle(name):
     if name == "walled":
         cfg, ppc, sseed, nsteps = _walled_srd(), 10, 31, 5
+    elif name == "two_species":
+        cfg = W.cfg_srd3d((7, 6, 5), species=[W._species(mass=1.0), W._species(mass=3.0)],
+                          seed=778)
+        ppc, sseed, nsteps = 10, 32, 4
     else:
         cfg, ppc, sseed, nsteps = build(name)
     Q, V, U, sp = state(cfg, ppc, sseed)
+    if cfg.n_species > 1:
+        sp = (np.arange(len(Q)) % cfg.n_species).astype(np.int32)
+    if name == "walled":
+        Q[:, 1] = 0.02 + Q[:, 1] * (cfg.L[1] - 0.04) / cfg.L[1]  # off the walls' planes
     o = Oracle(cfg, Q, V, U, sp)
     g = Solver(cfg)
     g.set_kernel(abi.KERNEL_RESIDENT)
