@@ -949,7 +949,7 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
         return r;
     };
     const R64Sums sum_cur = sums_of(step), sum_nxt = sums_of(step + 1u);
-    using Rec = typename SrdCell<F64T<DIM>>::Rec;
+    using Rec = R64Rec;
     int launches = 0;
     if (h->sorted_for == (int64_t)step) {
         h->sort_age = 0;

@@ -4,13 +4,14 @@
 // The same two-pass structure as the mixed resident family
 // (mpcd_resident.cuh), with the FP64 form's arithmetic:
 //   k_r64_cells  one thread per cell: u = (sum m v) / (sum m) from the FP64
-//                sums of the previous particle pass, the random axis and the
-//                rotation matrix (stochrotMPC + rotate, mpc.c:1181-1333), the
-//                avVel term; writes the FP64 record of the split family
-//                (SrdCell<F64T>) and clears the sums.
+//                sums of the previous particle pass, the random axis
+//                (stochrotMPC, mpc.c:1275-1333), the avVel term; writes a
+//                64-byte record {u, pop, axis} and clears the sums.
 //   k_r64_parts  one thread per particle: its cell on this step's grid
 //                (recomputed from its position exactly as the split family
-//                does), v' = u + R (v - u), TEMP term, finish() (shift back,
+//                does), the rotation matrix from the record's axis (rotate,
+//                mpc.c:1181-1257, the split family's srd_matrix), v' = u +
+//                R (v - u), TEMP term, finish() (shift back,
 //                stream, walls, next step's cell), the particle written back
 //                in place, and its mass and momentum (with the next step's
 //                gravity kick) added to its cell of the next step with FP64
@@ -33,11 +34,20 @@ struct R64Sums {
     int *pop;
 };
 
+// A cell's record: two 32-byte sectors.  The particle pass builds the
+// rotation matrix from the axis (the 9 doubles of the matrix would double
+// the bytes every particle gathers).
+struct __align__(64) R64Rec {
+    double u[3];
+    double pop;
+    double L[3];
+    double pad_;
+};
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCfg c,
-                                                   R64Sums sums,
-                                                   typename SrdCell<F64T<DIM>>::Rec *crec,
-                                                   StepArgs sa, double *acc, double *acc_next) {
+                                                   R64Sums sums, R64Rec *crec, StepArgs sa,
+                                                   double *acc, double *acc_next) {
     __shared__ double red[8];
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_trigger();
@@ -62,9 +72,14 @@ __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCf
             for (int d = 0; d < DIM; d++) u[d] = p[d] * iM;
         }
         for (int d = 0; d < DIM; d++) av[d] = u[d];
-        double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        if (pop > 1) srd_matrix<DIM, double>(c, Lx, R);
-        SrdCell<F64T<DIM>>::put(crec, cell, u, pop, R);
+        R64Rec rec;
+        for (int d = 0; d < 3; d++) {
+            rec.u[d] = u[d];
+            rec.L[d] = Lx[d];
+        }
+        rec.pop = (double)pop;
+        rec.pad_ = 0.0;
+        crec[cell] = rec;
     }
     for (int d = 0; d < DIM; d++) {
         const double t = block_sum256(av[d], red);
@@ -76,8 +91,7 @@ __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCf
 // RES_SUM:  only add each particle to this step's sums (bootstrap).
 template <int DIM, int MODE>
 __global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCfg c,
-                                                   Fp64State a, int n,
-                                                   const typename SrdCell<F64T<DIM>>::Rec *crec,
+                                                   Fp64State a, int n, const R64Rec *crec,
                                                    R64Sums sums, double *acc,
                                                    unsigned long long *status, StepArgs sa) {
     __shared__ double red[8];
@@ -94,12 +108,14 @@ __global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCf
         double v[3] = {0.0, 0.0, 0.0};
         if (MODE == RES_STEP) {
             const int kc = cur_key<DIM>(c, r, sa);
-            const typename SrdCell<F64T<DIM>>::Rec &cr = crec[kc];
+            const R64Rec cr = crec[kc];
             if (cr.pop > 1.0) {
+                double R[9];
+                srd_matrix<DIM, double>(c, cr.L, R);
                 double w[3] = {0, 0, 0}, tt[3] = {0, 0, 0};
                 for (int d = 0; d < DIM; d++) w[d] = r.v[d] - cr.u[d];
                 for (int x = 0; x < DIM; x++)
-                    for (int y = 0; y < DIM; y++) tt[x] += cr.R[x * 3 + y] * w[y];
+                    for (int y = 0; y < DIM; y++) tt[x] += R[x * 3 + y] * w[y];
                 for (int d = 0; d < DIM; d++) r.v[d] = cr.u[d] + tt[d];
             }
             double t = r.v[0] * r.v[0];
