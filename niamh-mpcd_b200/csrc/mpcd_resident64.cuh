@@ -26,7 +26,7 @@
 namespace mpcd {
 
 // FP64 cell sums: mass, mass-weighted momentum (with the step's gravity
-// kick) and population, one array each, so that the atomics of one cell's
+// kick) and, with several species, population, one array each, so that the atomics of one cell's
 // particles fall on different sectors (the L2 serialises atomics on one
 // sector).  Each array holds nc entries.
 struct R64Sums {
@@ -62,10 +62,13 @@ __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCf
         const double M = sums.M[cell];
         double p[3] = {0.0, 0.0, 0.0};
         for (int d = 0; d < DIM; d++) p[d] = sums.p[d][cell];
-        const int pop = sums.pop[cell];
+        // one species: the population is the mass sum over the mass (exact:
+        // n equal terms, far below 2^52); several: the counted population
+        const bool one = c.n_species == 1;
+        const int pop = one ? (int)llrint(M / c.mass[0]) : sums.pop[cell];
         sums.M[cell] = 0.0;
         for (int d = 0; d < DIM; d++) sums.p[d][cell] = 0.0;
-        sums.pop[cell] = 0;
+        if (!one) sums.pop[cell] = 0;
         double u[3] = {0.0, 0.0, 0.0};
         if (M > 0.0) {
             const double iM = 1.0 / M;
@@ -134,7 +137,7 @@ __global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCf
         const double m = c.mass[sp];
         atomicAdd(sums.M + k, m);
         for (int d = 0; d < DIM; d++) atomicAdd(sums.p[d] + k, v[d] * m);
-        atomicAdd(sums.pop + k, 1);
+        if (c.n_species > 1) atomicAdd(sums.pop + k, 1);
     }
     if (MODE == RES_STEP) {
         const double t = block_sum256(ke, red);
