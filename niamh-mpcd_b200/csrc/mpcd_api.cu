@@ -871,8 +871,8 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     const size_t nc = (size_t)c.ncells;
     double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
     double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
-    ResSum *sum_cur = h->rsum + (step & 1u) * nc;
-    ResSum *sum_nxt = h->rsum + ((step + 1u) & 1u) * nc;
+    const ResPlanes sum_cur{(long long *)(h->rsum + (step & 1u) * nc), (int)nc};
+    const ResPlanes sum_nxt{(long long *)(h->rsum + ((step + 1u) & 1u) * nc), (int)nc};
     unsigned long long *ms_cur = h->rmsum ? h->rmsum + (step & 1u) * nc : nullptr;
     unsigned long long *ms_nxt = h->rmsum ? h->rmsum + ((step + 1u) & 1u) * nc : nullptr;
     int launches = 0;

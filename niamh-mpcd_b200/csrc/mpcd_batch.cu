@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256) k_bat_key(const BatchBox *box, const int 
 // Cell pass of the ensemble: as k_res_cells, one box per block.
 __global__ void __launch_bounds__(256) k_bat_cells(const __grid_constant__ DevCfg c,
                                                    const BatchBox *box, const int *cblk_box,
-                                                   const BatchStep *st, ResSum *sums,
+                                                   const BatchStep *st, ResPlanes sums,
                                                    ResRec *crec, double *acc, double *acc_next,
                                                    int nb) {
     __shared__ float4 srec[2 * kCellsPerBlock];
@@ -135,12 +135,12 @@ __global__ void __launch_bounds__(256) k_bat_cells(const __grid_constant__ DevCf
         for (int j = threadIdx.x; j < nb * ACC_WORDS; j += blockDim.x) acc_next[j] = 0.0;
     ResSum s[kResCellsPer];
 #pragma unroll
-    for (int q = 0; q < kResCellsPer; q++) s[q] = sums[c0 + q * 256 + threadIdx.x];
+    for (int q = 0; q < kResCellsPer; q++) s[q] = sums.load(c0 + q * 256 + threadIdx.x);
 #pragma unroll
     for (int q = 0; q < kResCellsPer; q++) {
         const int cell = c0 + q * 256 + threadIdx.x;
         const int local = cell - bx.cell0;
-        sums[cell] = ResSum{{0, 0, 0}, 0};
+        sums.clear(cell);
         const int pop = local < bx.ncells ? (int)s[q].n : 0;
         // the record of k_res_cells (one species): u in FP32, the FP32 axis
         float u[3] = {0.f, 0.f, 0.f};
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(256) k_bat_cells(const __grid_constant__ DevCf
 template <int MODE>
 __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_bat_parts(
     const __grid_constant__ DevCfg c, const BatchBox *box, const int *chunk_box,
-    const BatchStep *st, MixState a, const ResRec *__restrict__ crec, ResSum *sums,
+    const BatchStep *st, MixState a, const ResRec *__restrict__ crec, ResPlanes sums,
     double *acc, unsigned long long *status) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     __shared__ double red[8];
@@ -510,8 +510,8 @@ extern "C" int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *
 static int record_step(mpcd_batch *b, bool sorted, int parity, int state_cur,
                        cudaGraphExec_t *out) {
     const size_t nc = (size_t)b->ncells;
-    ResSum *sum_cur = b->rsum + (size_t)parity * nc;
-    ResSum *sum_nxt = b->rsum + (size_t)(1 - parity) * nc;
+    const ResPlanes sum_cur{(long long *)(b->rsum + (size_t)parity * nc), (int)nc};
+    const ResPlanes sum_nxt{(long long *)(b->rsum + (size_t)(1 - parity) * nc), (int)nc};
     double *acc_cur = b->acc + (size_t)parity * b->nb * ACC_WORDS;
     double *acc_nxt = b->acc + (size_t)(1 - parity) * b->nb * ACC_WORDS;
     const int pbytes = res_table_bytes(3);
@@ -568,7 +568,8 @@ extern "C" int mpcd_batch_step(mpcd_batch *b, int nsteps) {
             BCK(cudaMemsetAsync(b->acc, 0, sizeof(double) * 2 * b->nb * ACC_WORDS, b->stream));
             k_bat_parts<RES_SUM><<<b->nchunks, kResThreads, pbytes, b->stream>>>(
                 b->dc, b->box, b->chunk_box, b->st, b->mx[b->cur], b->crec,
-                b->rsum + (size_t)parity * b->ncells, b->acc, b->status);
+                ResPlanes{(long long *)(b->rsum + (size_t)parity * b->ncells), b->ncells},
+                b->acc, b->status);
             BCK(cudaGetLastError());
             b->sums_ready = true;
         }

@@ -52,10 +52,30 @@ struct ResRec {
 
 // Fixed-point cell sums: p = sum w v * 2^32 with w = 1 for one species
 // (the cell's momentum is then m p) and w = m for several species; n =
-// population.
+// population.  In memory the sums of nc cells are four planes of nc words,
+// p0, p1, p2 and n (ResPlanes), so that the global additions of one cell
+// fall on four sectors rather than one (the L2 serialises atomics on a
+// sector); ResSum is a cell's sums in registers, and the 32-byte unit of
+// allocation.
 struct __align__(16) ResSum {
     long long p[3];
     long long n;
+};
+struct ResPlanes {
+    long long *w;  // word d of cell k at w[d * nc + k]
+    int nc;
+    __device__ __forceinline__ long long *at(int d, int k) const {
+        return w + (size_t)d * (size_t)nc + (size_t)k;
+    }
+    __device__ __forceinline__ ResSum load(int k) const {
+        ResSum s;
+        for (int d = 0; d < 3; d++) s.p[d] = *at(d, k);
+        s.n = *at(3, k);
+        return s;
+    }
+    __device__ __forceinline__ void clear(int k) const {
+        for (int d = 0; d < 4; d++) *at(d, k) = 0ll;
+    }
 };
 constexpr double kSumFx = 4294967296.0;  // 2^32
 constexpr double kSumFxInv = 2.3283064365386963e-10;
@@ -123,12 +143,11 @@ __device__ __forceinline__ long long res_fix(double x, int &bad) {
     return __double2ll_rn(x);
 }
 
-__device__ __forceinline__ void res_global_add(ResSum *gs, unsigned long long *gm, int k,
+__device__ __forceinline__ void res_global_add(ResPlanes gs, unsigned long long *gm, int k,
                                                const long long x[4], unsigned cnt, bool multi) {
-    unsigned long long *g = (unsigned long long *)&gs[k];
     for (int d = 0; d < 3; d++)
-        if (x[d]) atomicAdd(g + d, (unsigned long long)x[d]);
-    atomicAdd(g + 3, (unsigned long long)cnt);
+        if (x[d]) atomicAdd((unsigned long long *)gs.at(d, k), (unsigned long long)x[d]);
+    atomicAdd((unsigned long long *)gs.at(3, k), (unsigned long long)cnt);
     if (multi) atomicAdd(&gm[k], (unsigned long long)x[3]);
 }
 
@@ -162,7 +181,7 @@ __device__ __forceinline__ int res_slot(ResTable &t, const int *mask, const int 
 // Add one particle (velocity v, weight w = 1 or its mass) to cell k.
 template <int DIM>
 __device__ __forceinline__ void res_add(ResTable &t, const int *mask, const int *shift,
-                                        ResSum *sums, unsigned long long *msum, int k,
+                                        ResPlanes sums, unsigned long long *msum, int k,
                                         const int idx[3], const float v[3], double w, bool multi,
                                         int &bad) {
     const int nc = multi ? DIM + 1 : DIM;
@@ -211,7 +230,7 @@ __device__ __forceinline__ void res_add(ResTable &t, const int *mask, const int 
 // adds them with all its lanes busy; most slots of a table are unused.
 // Requires kResThreads threads.
 template <int DIM>
-__device__ __forceinline__ void res_flush(const ResTable &t, ResSum *sums,
+__device__ __forceinline__ void res_flush(const ResTable &t, ResPlanes sums,
                                           unsigned long long *msum, bool multi) {
     const int nc = multi ? DIM + 1 : DIM;
     constexpr int kPer = kResSlots / (kResThreads / 32);
@@ -307,7 +326,7 @@ __device__ __forceinline__ void res_axis3(uint64_t seed, uint32_t replica, uint3
 constexpr int kResCellsPer = 2;
 template <int DIM>
 __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCfg c,
-                                                   ResSum *sums, unsigned long long *msum,
+                                                   ResPlanes sums, unsigned long long *msum,
                                                    ResRec *crec, StepArgs sa, double *acc,
                                                    double *acc_next) {
     __shared__ float4 srec[2 * 256 * kResCellsPer];
@@ -337,7 +356,7 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
         s[q] = ResSum{{0, 0, 0}, 0};
         ms[q] = 0ull;
         if (cell < c.ncells) {
-            s[q] = sums[cell];
+            s[q] = sums.load(cell);
             if (msum) ms[q] = msum[cell];
         }
     }
@@ -345,7 +364,7 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
     for (int q = 0; q < kResCellsPer; q++) {
         const int cell = c0 + q * 256 + threadIdx.x;
         if (cell >= c.ncells) continue;
-        sums[cell] = ResSum{{0, 0, 0}, 0};
+        sums.clear(cell);
         if (msum) msum[cell] = 0ull;
         const int pop = (int)s[q].n;
         // u = weighted sum / divisor: the population (one species, in FP32:
@@ -450,7 +469,7 @@ enum { RES_STEP = 0, RES_SUM = 1 };
 template <int DIM, int MODE, bool LEAN>
 __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     const __grid_constant__ DevCfg c, MixState a, int n,
-    const ResRec *__restrict__ crec, ResSum *sums, unsigned long long *msum, double *acc,
+    const ResRec *__restrict__ crec, ResPlanes sums, unsigned long long *msum, double *acc,
     unsigned long long *status, StepArgs sa) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     __shared__ double red[8];
