@@ -55,6 +55,9 @@ struct mpcd_handle {
     LcCells lcc;     // per-cell nematic arrays (lc != 0)
     double *lcbuf;
     double *modes;   // transverse momentum modes (mpcd_transverse_modes)
+    bool res_attr;       // the resident kernels' shared-memory attributes are set
+    void *xfer;          // device staging of FP64 uploads and downloads (mixed form)
+    size_t xfer_bytes;
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
     ResSum *rsum;              // resident family: cell sums, two steps by parity
     double *r64sum;            // FP64 resident family: M, p[3] sums (4 x nc), two steps by parity
@@ -265,6 +268,7 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->status);
     cudaFree(h->crec);
     cudaFree(h->modes);
+    cudaFree(h->xfer);
     cudaFree(h->rsum);
     cudaFree(h->rmsum);
     cudaFree(h->r64sum);
@@ -412,15 +416,16 @@ static int ensure_capacity(mpcd_handle *h, int n) {
     return MPCD_OK;
 }
 
+// host_check: validate Q and V on the host (the mixed form's device-side
+// conversion checks them itself).
 static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V,
-                         const int *spid) {
+                         const int *spid, bool host_check = true) {
     int dim = h->dc.dim;
-    for (int i = 0; i < n; i++) {
-        int s = spid ? spid[i] : 0;
-        if (s < 0 || s >= h->dc.n_species) return MPCD_ERR_ARG;
+    for (int i = 0; spid && i < n; i++)
+        if (spid[i] < 0 || spid[i] >= h->dc.n_species) return MPCD_ERR_ARG;
+    for (int i = 0; host_check && i < n; i++)
         for (int d = 0; d < dim; d++)
             if (!std::isfinite(Q[3 * i + d]) || !std::isfinite(V[3 * i + d])) return MPCD_ERR_ARG;
-    }
     int r = ensure_capacity(h, n);
     if (r != MPCD_OK) return r;
     h->n = n;
@@ -428,8 +433,9 @@ static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V
     h->sorted_for = -1;
     h->sums_for = -1;
     h->sort_age = -1;
-    // global number density as globalDensities (init.c:1002-1018) unless given
-    if (!(h->cfg.gndnst > 0.0)) {
+    // global number density as globalDensities (init.c:1002-1018) unless
+    // given; phantom walls and the nematic activity use it
+    if (!(h->cfg.gndnst > 0.0) && (h->dc.any_phantom || h->dc.lc)) {
         std::vector<int> pop((size_t)h->dc.ncells, 0);
         for (int i = 0; i < n; i++) {
             int idx[3] = {0, 0, 0};
@@ -456,10 +462,73 @@ static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V
     return MPCD_OK;
 }
 
+static int grid_for(const mpcd_handle *h, int n) {
+    int g = (n + 255) / 256;
+    int cap = h->sm_count * 8;
+    if (g > cap) g = cap;
+    return g < 1 ? 1 : g;
+}
+
+// Device staging buffer of at least 'bytes' (grown, never shrunk).
+static int xfer_reserve(mpcd_handle *h, size_t bytes) {
+    if (bytes <= h->xfer_bytes) return MPCD_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->xfer);
+    h->xfer = nullptr;
+    h->xfer_bytes = 0;
+    if (cudaMalloc(&h->xfer, bytes) != cudaSuccess) return MPCD_ERR_NOMEM;
+    h->xfer_bytes = bytes;
+    return MPCD_OK;
+}
+
+// The mixed form's positions and velocities are converted on the device
+// when the state has nothing else to carry: no nematic orientations, one
+// species (decided from the configuration: the buffers may not exist yet).
+static bool mix_device_xfer(const mpcd_handle *h) {
+    return h->prec == MPCD_PREC_MIXED && !h->dc.lc && h->dc.n_species == 1;
+}
+
+// Upload of Q and V in the caller's layout to the mixed state: two copies
+// into the staging buffer and a conversion kernel.
+static int mix_upload_device(mpcd_handle *h, int n, const double *Q, const double *V) {
+    const size_t N = (size_t)n;
+    int r = xfer_reserve(h, N * 48 + 16);
+    if (r != MPCD_OK) return r;
+    double *dq = (double *)h->xfer, *dv = dq + 3 * N;
+    int *derr = (int *)(dv + 3 * N);
+    CK(cudaMemcpyAsync(dq, Q, N * 24, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dv, V, N * 24, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(derr, 0, sizeof(int), h->stream));
+    k_mix_from_f64<<<grid_for(h, n), 256, 0, h->stream>>>(h->mx[0], h->dc, n, dq, dv, derr);
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return herr ? MPCD_ERR_ARG : MPCD_OK;
+}
+
+// Download of the mixed state into Q and V in the caller's layout and order.
+static int mix_download_device(mpcd_handle *h, double *Q, double *V) {
+    const size_t N = (size_t)h->n;
+    int r = xfer_reserve(h, N * 48 + 16);
+    if (r != MPCD_OK) return r;
+    double *dq = (double *)h->xfer, *dv = dq + 3 * N;
+    int *derr = (int *)(dv + 3 * N);
+    CK(cudaMemsetAsync(derr, 0, sizeof(int), h->stream));
+    k_mix_to_f64<<<grid_for(h, h->n), 256, 0, h->stream>>>(h->mx[h->cur], h->dc, h->n, dq, dv,
+                                                            derr);
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (Q) CK(cudaMemcpyAsync(Q, dq, N * 24, cudaMemcpyDeviceToHost, h->stream));
+    if (V) CK(cudaMemcpyAsync(V, dv, N * 24, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return herr ? MPCD_ERR_STATE : MPCD_OK;
+}
+
 extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
                                  const double *U, const int *spid) {
     if (!h || n < 0 || (n > 0 && (!Q || !V))) return MPCD_ERR_ARG;
-    int r = upload_common(h, n, Q, V, spid);
+    const bool dev = mix_device_xfer(h);
+    int r = upload_common(h, n, Q, V, spid, !dev);
     if (r != MPCD_OK) return r;
     if (n == 0) return MPCD_OK;
     int dim = h->dc.dim;
@@ -490,6 +559,12 @@ extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const d
                                    h->stream));
                 CK(cudaStreamSynchronize(h->stream));
             }
+    } else if (dev) {
+        r = mix_upload_device(h, n, Q, V);
+        if (r != MPCD_OK) {
+            h->n = 0;  // a rejected upload leaves no state
+            return r;
+        }
     } else {
         r = mix_upload(h->mx[0], h->dc, n, Q, V, U, spid, h->stream);
         if (r != MPCD_OK) return r;
@@ -523,8 +598,8 @@ extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double 
     size_t N = (size_t)n;
     if (n == 0) return MPCD_OK;
     CK(cudaStreamSynchronize(h->stream));
-    std::vector<int> pid(N);
     if (h->prec == MPCD_PREC_FP64) {
+        std::vector<int> pid(N);
         const Fp64State &st = h->f[h->cur];
         CK(cudaMemcpy(pid.data(), st.pid, N * 4, cudaMemcpyDeviceToHost));
         std::vector<double> tmp(N);
@@ -553,6 +628,11 @@ extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double 
                     for (size_t i = 0; i < N; i++) U[3 * (size_t)pid[i] + d] = tmp[i];
                 }
         }
+    } else if (mix_device_xfer(h) && (Q || V)) {
+        int r = mix_download_device(h, Q, V);
+        if (r != MPCD_OK) return r;
+        if (U)
+            for (size_t i = 0; i < 3 * N; i++) U[i] = 0.0;
     } else {
         int r = mix_download(h->mx[h->cur], h->dc, n, Q, V, U);
         if (r != MPCD_OK) return r;
@@ -577,12 +657,6 @@ extern "C" int mpcd_download_particles_strided(mpcd_handle *h, void *base, size_
     return MPCD_OK;
 }
 
-static int grid_for(const mpcd_handle *h, int n) {
-    int g = (n + 255) / 256;
-    int cap = h->sm_count * 8;
-    if (g > cap) g = cap;
-    return g < 1 ? 1 : g;
-}
 
 // Tile geometry: cells per tile so that a tile holds about 'target'
 // particles on average; staging capacity 1.5x that plus a margin.
@@ -894,14 +968,24 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     const int pgrid = (int)((h->n + kResChunk - 1) / kResChunk);
     const int pbytes = res_table_bytes(h->rmsum ? DIM + 1 : DIM);
     typedef ResRec CRec;
+    if (!h->res_attr) {
+        // once per handle (the driver keeps them for the device): the
+        // largest table any handle may use (several species) and the
+        // carve-out, for each variant of the particle pass
+        for (auto k : {k_res_parts<DIM, RES_SUM, false>, k_res_parts<DIM, RES_STEP, true>,
+                       k_res_parts<DIM, RES_STEP, false>}) {
+            CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    res_table_bytes(DIM + 1)));
+            CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        }
+        h->res_attr = true;
+    }
     if (h->sums_for != (int64_t)step) {
         CK(cudaMemsetAsync(h->rsum, 0, sizeof(ResSum) * 2 * nc, h->stream));
         if (h->rmsum)
             CK(cudaMemsetAsync(h->rmsum, 0, sizeof(unsigned long long) * 2 * nc, h->stream));
         CK(cudaMemsetAsync(acc_cur, 0, sizeof(double) * ACC_WORDS, h->stream));
         auto ksum = k_res_parts<DIM, RES_SUM, false>;
-        CK(cudaFuncSetAttribute(ksum, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
-        CK(cudaFuncSetAttribute(ksum, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         ksum<<<pgrid, kResThreads, pbytes, h->stream>>>(c, h->mx[h->cur], h->n,
                                                         (const CRec *)h->crec, sum_cur, ms_cur,
                                                         acc_cur, h->status, sa);
@@ -911,8 +995,6 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
                   256, 0, h->stream, c, sum_cur, ms_cur, (CRec *)h->crec, sa, acc_cur, acc_nxt));
     const bool lean = c.all_periodic && !h->rmsum && !c.grav_flag;
     auto kstep = lean ? k_res_parts<DIM, RES_STEP, true> : k_res_parts<DIM, RES_STEP, false>;
-    CK(cudaFuncSetAttribute(kstep, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
-    CK(cudaFuncSetAttribute(kstep, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     time_begin(h);
     CK(launch_pdl(kstep, pgrid, kResThreads, pbytes, h->stream, c, h->mx[h->cur], h->n,
                   (const CRec *)h->crec, sum_nxt, ms_nxt, acc_cur, h->status, sa));

@@ -290,6 +290,58 @@ static __global__ void __launch_bounds__(256) k_gather_mix(MixState a, MixState 
     }
 }
 
+// Device-side conversion to and from the packed representation, for
+// uploads and downloads of positions and velocities in the caller's FP64
+// layout (3 doubles per particle, original order).  A non-finite value or a
+// position outside the grid (upload), or an original index out of range
+// (download), counts in *err and leaves that particle unwritten.
+static __global__ void __launch_bounds__(256) k_mix_from_f64(MixState s,
+                                                             const __grid_constant__ DevCfg c,
+                                                             int n, const double *Q,
+                                                             const double *V, int *err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int ci[3] = {0, 0, 0};
+        uint32_t f[3] = {0u, 0u, 0u};
+        bool ok = true;
+        for (int d = 0; d < c.dim; d++) {
+            const double q = Q[3 * (size_t)i + d], v = V[3 * (size_t)i + d];
+            if (!isfinite(q) || !isfinite(v)) {
+                ok = false;
+                break;
+            }
+            fx_from_double(q, ci[d], f[d]);
+            if (ci[d] < 0 || ci[d] > c.L[d]) ok = false;
+        }
+        if (!ok) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        s.P[i] = pos_pack(ci, f);
+        s.W[i] = make_float4((float)V[3 * (size_t)i], (float)V[3 * (size_t)i + 1],
+                             c.dim == 3 ? (float)V[3 * (size_t)i + 2] : 0.f, __int_as_float(i));
+    }
+}
+static __global__ void __launch_bounds__(256) k_mix_to_f64(MixState s,
+                                                           const __grid_constant__ DevCfg c,
+                                                           int n, double *Q, double *V, int *err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 w = s.W[i];
+        const int pid = __float_as_int(w.w);
+        if (pid < 0 || pid >= n) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        int ci[3];
+        uint32_t f[3];
+        pos_unpack(s.P[i], ci, f);
+        const float v[3] = {w.x, w.y, w.z};
+        for (int d = 0; d < 3; d++) {
+            Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;
+            V[3 * (size_t)pid + d] = d < c.dim ? (double)v[d] : 0.0;
+        }
+    }
+}
+
 // Host-side conversion to and from the packed representation.
 static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *Q,
                              const double *V, const double *Uo, const int *spid,

@@ -132,7 +132,19 @@ class Solver:
         _check(self.lib.mpcd_globals(self.h, C.byref(kb), _p(av)), "mpcd_globals")
         return kb.value, av
 
-    def download(self):
+    def download(self, out=None):
+        """Positions, velocities and orientations in the original particle
+        order.  out=(Q, V) writes into the caller's (n, 3) float64 arrays
+        (pinned host memory makes the copies direct) and skips the
+        orientations; the third result is then None."""
+        if out is not None:
+            Q, V = out
+            assert Q.shape == (self.n, 3) and V.shape == (self.n, 3)
+            assert Q.dtype == np.float64 and V.dtype == np.float64
+            assert Q.flags.c_contiguous and V.flags.c_contiguous
+            _check(self.lib.mpcd_download_state(self.h, _p(Q), _p(V), None),
+                   "mpcd_download_state")
+            return Q, V, None
         Q = np.zeros((self.n, 3))
         V = np.zeros((self.n, 3))
         U = np.zeros((self.n, 3))
