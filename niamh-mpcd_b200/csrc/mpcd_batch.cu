@@ -55,6 +55,8 @@ struct BatchBox {
     uint64_t seed;
     uint32_t replica;
     int key0;  // first sort key: the box's cells in brick order, then its padding key
+    int g0;    // first of the box's particles in the caller's (box-major) order
+    int pad_;
 };
 
 struct BatchStep {
@@ -91,6 +93,62 @@ __global__ void k_bat_shift(const BatchBox *box, int nb, BatchStep *st, const ui
 
 __global__ void k_bat_advance(uint32_t *counter) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *counter += 1u;
+}
+
+// Conversion of the caller's FP64 positions and velocities (3 doubles per
+// particle, boxes one after another) into the slot layout, on the device:
+// slot s of box b holds the box's particle s - part0 (or is padding: pid
+// -1).  A position outside its box counts in *err.
+__global__ void __launch_bounds__(256) k_bat_from_f64(const BatchBox *box, const int *chunk_box,
+                                                      MixState a, int nslots, const double *Q,
+                                                      const double *V, int *err) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots;
+         s += gridDim.x * blockDim.x) {
+        const BatchBox &bx = box[chunk_box[s / kResChunk]];
+        const int j = s - bx.part0;
+        if (j >= bx.npart) {
+            a.P[s] = make_uint4(0u, 0u, 0u, 0u);
+            a.W[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+            continue;
+        }
+        const size_t gi = (size_t)bx.g0 + (size_t)j;
+        int ci[3];
+        uint32_t f[3];
+        bool ok = true;
+        for (int d = 0; d < 3; d++) {
+            const double q = Q[3 * gi + d];
+            if (!(q >= 0.0 && q < (double)bx.L[d]) || !isfinite(V[3 * gi + d])) ok = false;
+            fx_from_double(ok ? q : 0.0, ci[d], f[d]);
+            if (ci[d] >= bx.L[d]) ci[d] -= bx.L[d];
+        }
+        if (!ok) atomicAdd(err, 1);
+        a.P[s] = pos_pack(ci, f);
+        a.W[s] = make_float4((float)V[3 * gi], (float)V[3 * gi + 1], (float)V[3 * gi + 2],
+                             __int_as_float((int)gi));
+    }
+}
+
+// The inverse: each real slot's particle to its place in the caller's order.
+__global__ void __launch_bounds__(256) k_bat_to_f64(MixState a, int nslots, int n, double *Q,
+                                                    double *V, int *err) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots;
+         s += gridDim.x * blockDim.x) {
+        const float4 w = a.W[s];
+        const int pid = __float_as_int(w.w);
+        if (pid < 0) continue;
+        if (pid >= n) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        int ci[3];
+        uint32_t f[3];
+        pos_unpack(a.P[s], ci, f);
+        const float v[3] = {w.x, w.y, w.z};
+        for (int d = 0; d < 3; d++) {
+            Q[3 * (size_t)pid + d] = (double)ci[d] + (double)f[d] * kFxInv;
+            V[3 * (size_t)pid + d] = (double)v[d];
+        }
+    }
 }
 
 // Sort key of every slot on the current grid and its rank, for the
@@ -289,6 +347,8 @@ struct mpcd_batch {
     uint32_t next_step = 0;  // host mirror of the device step counter
     int sort_interval = 20, sort_age = -1;
     bool sums_ready = false;
+    void *xfer = nullptr;  // device staging of uploads and downloads
+    size_t xfer_bytes = 0;
     int sm_count = 0;
 };
 
@@ -327,6 +387,21 @@ void batch_free(mpcd_batch *b) {
         cudaFree(*p);
         *p = nullptr;
     }
+    cudaFree(b->xfer);
+    b->xfer = nullptr;
+    b->xfer_bytes = 0;
+}
+
+// Staging buffer of at least 'bytes' (grown, never shrunk).
+int batch_xfer_reserve(mpcd_batch *b, size_t bytes) {
+    if (bytes <= b->xfer_bytes) return MPCD_OK;
+    cudaStreamSynchronize(b->stream);
+    cudaFree(b->xfer);
+    b->xfer = nullptr;
+    b->xfer_bytes = 0;
+    if (cudaMalloc(&b->xfer, bytes) != cudaSuccess) return MPCD_ERR_NOMEM;
+    b->xfer_bytes = bytes;
+    return MPCD_OK;
 }
 
 }  // namespace
@@ -435,24 +510,11 @@ extern "C" int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *
     b->n = n;
     b->nchunks = (int)b->hchunk_box.size();
     b->nscan = (b->nkeys + kScanTile - 1) / kScanTile;
-    // host conversion into the slot layout (padding slots: pid -1)
-    std::vector<uint4> P((size_t)slot0, make_uint4(0u, 0u, 0u, 0u));
-    std::vector<float4> W((size_t)slot0, make_float4(0.f, 0.f, 0.f, __int_as_float_host(-1)));
-    size_t gi = 0;
-    for (int k = 0; k < b->nb; k++) {
-        const BatchBox &bx = b->hbox[k];
-        for (int j = 0; j < bx.npart; j++, gi++) {
-            int ci[3];
-            uint32_t f[3];
-            for (int d = 0; d < 3; d++) {
-                const double q = Q[3 * gi + d];
-                if (!(q >= 0.0 && q < (double)bx.L[d])) return MPCD_ERR_ARG;
-                fx_from_double(q, ci[d], f[d]);
-                if (ci[d] >= bx.L[d]) ci[d] -= bx.L[d];
-            }
-            P[bx.part0 + j] = pos_pack(ci, f);
-            W[bx.part0 + j] = make_float4((float)V[3 * gi], (float)V[3 * gi + 1],
-                                          (float)V[3 * gi + 2], __int_as_float_host((int)gi));
+    {
+        int g0 = 0;
+        for (int k = 0; k < b->nb; k++) {
+            b->hbox[k].g0 = g0;
+            g0 += b->hbox[k].npart;
         }
     }
     // (re)allocate
@@ -481,14 +543,33 @@ extern "C" int mpcd_batch_upload(mpcd_batch *b, const int *npart, const double *
     BALLOC(b->acc, sizeof(double) * 2 * b->nb * ACC_WORDS);
     BALLOC(b->status, sizeof(unsigned long long) * ST_WORDS);
 #undef BALLOC
-    BCK(cudaMemcpyAsync(b->mx[0].P, P.data(), sizeof(uint4) * slot0, cudaMemcpyHostToDevice,
-                        b->stream));
-    BCK(cudaMemcpyAsync(b->mx[0].W, W.data(), sizeof(float4) * slot0, cudaMemcpyHostToDevice,
-                        b->stream));
     BCK(cudaMemcpyAsync(b->box, b->hbox.data(), sizeof(BatchBox) * b->nb,
                         cudaMemcpyHostToDevice, b->stream));
     BCK(cudaMemcpyAsync(b->chunk_box, b->hchunk_box.data(), sizeof(int) * b->nchunks,
                         cudaMemcpyHostToDevice, b->stream));
+    {
+        // the caller's arrays through the staging buffer, converted on the
+        // device into the slot layout
+        const int r = batch_xfer_reserve(b, (size_t)n * 48 + 16);
+        if (r != MPCD_OK) return r;
+        double *dq = (double *)b->xfer, *dv = dq + 3 * (size_t)n;
+        int *derr = (int *)(dv + 3 * (size_t)n);
+        if (n > 0) {
+            BCK(cudaMemcpyAsync(dq, Q, (size_t)n * 24, cudaMemcpyHostToDevice, b->stream));
+            BCK(cudaMemcpyAsync(dv, V, (size_t)n * 24, cudaMemcpyHostToDevice, b->stream));
+        }
+        BCK(cudaMemsetAsync(derr, 0, sizeof(int), b->stream));
+        k_bat_from_f64<<<grid_for(b, slot0), 256, 0, b->stream>>>(b->box, b->chunk_box, b->mx[0],
+                                                                  slot0, dq, dv, derr);
+        int herr = 0;
+        BCK(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+        if (herr) {
+            b->nslots = 0;  // a rejected upload leaves nothing to step
+            b->n = 0;
+            return MPCD_ERR_ARG;
+        }
+    }
     BCK(cudaMemcpyAsync(b->cblk_box, b->hcblk_box.data(), sizeof(int) * b->ncblk,
                         cudaMemcpyHostToDevice, b->stream));
     BCK(cudaMemcpyAsync(b->counter, &step0, sizeof(uint32_t), cudaMemcpyHostToDevice,
@@ -599,27 +680,22 @@ extern "C" int mpcd_batch_set_sort_interval(mpcd_batch *b, int steps) {
 // Particles of all boxes back, in the upload's order (concatenated boxes).
 extern "C" int mpcd_batch_download(mpcd_batch *b, double *Q, double *V) {
     if (!b || !Q || !V) return MPCD_ERR_ARG;
-    BCK(cudaStreamSynchronize(b->stream));
-    std::vector<uint4> P((size_t)b->nslots);
-    std::vector<float4> W((size_t)b->nslots);
-    BCK(cudaMemcpy(P.data(), b->mx[b->cur].P, sizeof(uint4) * b->nslots,
-                   cudaMemcpyDeviceToHost));
-    BCK(cudaMemcpy(W.data(), b->mx[b->cur].W, sizeof(float4) * b->nslots,
-                   cudaMemcpyDeviceToHost));
-    for (size_t i = 0; i < (size_t)b->nslots; i++) {
-        const int pid = __float_as_int_host(W[i].w);
-        if (pid < 0) continue;
-        if (pid >= b->n) return MPCD_ERR_STATE;
-        int ci[3];
-        uint32_t f[3];
-        pos_unpack(P[i], ci, f);
-        const float v[3] = {W[i].x, W[i].y, W[i].z};
-        for (int d = 0; d < 3; d++) {
-            Q[3 * (size_t)pid + d] = (double)ci[d] + (double)f[d] * kFxInv;
-            V[3 * (size_t)pid + d] = (double)v[d];
-        }
+    const size_t n = (size_t)b->n;
+    const int r = batch_xfer_reserve(b, n * 48 + 16);
+    if (r != MPCD_OK) return r;
+    double *dq = (double *)b->xfer, *dv = dq + 3 * n;
+    int *derr = (int *)(dv + 3 * n);
+    BCK(cudaMemsetAsync(derr, 0, sizeof(int), b->stream));
+    k_bat_to_f64<<<grid_for(b, b->nslots), 256, 0, b->stream>>>(b->mx[b->cur], b->nslots, b->n,
+                                                                dq, dv, derr);
+    int herr = 0;
+    BCK(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    if (n > 0) {
+        BCK(cudaMemcpyAsync(Q, dq, n * 24, cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaMemcpyAsync(V, dv, n * 24, cudaMemcpyDeviceToHost, b->stream));
     }
-    return MPCD_OK;
+    BCK(cudaStreamSynchronize(b->stream));
+    return herr ? MPCD_ERR_STATE : MPCD_OK;
 }
 
 // Per-box global measures of the last step: kbt[b] = TEMP, avv[3b..3b+2] =

@@ -100,3 +100,26 @@ def test_batch_runs_on_the_legacy_default_stream():
         bat.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_batch_upload_rejects_positions_outside_their_box():
+    """The device-side conversion of an upload checks every position against
+    its own box; a rejected upload leaves nothing to step, and a valid one
+    afterwards works."""
+    base = W.cfg_srd3d((8, 8, 8), precision=abi.PREC_MIXED, seed=3)
+    bat = Batch(base, [(8, 8, 8), (6, 6, 6)])
+    rng = np.random.default_rng(3)
+    q1, q2 = rng.random((500, 3)) * 8, rng.random((300, 3)) * 6
+    q2[7, 2] = 6.5  # inside the first box's size, outside its own
+    v = rng.standard_normal((800, 3))
+    with pytest.raises(Exception):
+        bat.upload([500, 300], np.vstack([q1, q2]), v)
+    with pytest.raises(Exception):
+        bat.step(1)
+    q2[7, 2] = 5.5
+    bat.upload([500, 300], np.vstack([q1, q2]), v)
+    bat.step(2)
+    q, vv = bat.download()
+    assert q.shape == (800, 3) and np.all(np.isfinite(vv))
+    assert np.all(q[:500] < 8) and np.all(q[500:] < 6)
+    bat.close()

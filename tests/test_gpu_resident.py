@@ -223,3 +223,27 @@ def test_transverse_modes_match_host_restatement(prec, tol):
     host = transverse_modes(q, v, L)
     scale = np.abs(v).sum()
     assert np.abs(dev - host).max() / scale < tol
+
+
+def test_mixed_upload_rejects_bad_input_on_the_device():
+    """The mixed form converts uploads on the device: a position outside the
+    grid or a non-finite velocity is an error, and nothing is left to step."""
+    from mpcd_b200.gpu import MPCDError
+    cfg = W.cfg_srd3d((6, 6, 6), precision=abi.PREC_MIXED, seed=5)
+    Q, V, U, sp = W.synthetic_state(cfg, 10, seed=6)
+    g = Solver(cfg)
+    for bad in ("pos", "vel"):
+        Qb, Vb = Q.copy(), V.copy()
+        if bad == "pos":
+            Qb[11, 0] = 6.0 + 1.5
+        else:
+            Vb[13, 2] = np.nan
+        with pytest.raises(MPCDError):
+            g.upload(Qb, Vb, U, sp)
+        with pytest.raises(MPCDError):
+            g.step(1, 1)
+    g.upload(Q, V, U, sp)
+    g.step(2, 1)
+    q, v, _ = g.download()
+    assert np.all(np.isfinite(v)) and np.all((q >= 0) & (q < 6))
+    g.close()
