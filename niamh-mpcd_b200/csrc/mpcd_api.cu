@@ -410,7 +410,7 @@ static int ensure_capacity(mpcd_handle *h, int n) {
     }
     if ((r = dev_alloc((void **)&h->key, N * sizeof(int)))) return r;
     if ((r = dev_alloc((void **)&h->rank, N * sizeof(int)))) return r;
-    if (h->prec == MPCD_PREC_MIXED && (r = dev_alloc((void **)&h->perm, N * sizeof(int))))
+    if ((r = dev_alloc((void **)&h->perm, N * sizeof(int))))
         return r;
     h->cap = want;
     return MPCD_OK;
@@ -825,15 +825,16 @@ static int launch_scatter(mpcd_handle *h, const MixState &a, const MixState &b,
     k_gather_mix<<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->perm);
     return 2;
 }
+// The FP64 state's reorder is a gather too: each 8-byte element scattered
+// to its sorted place would write a part of a 32-byte sector.
 static int launch_scatter(mpcd_handle *h, const Fp64State &a, const Fp64State &b,
                           const int *start) {
+    k_perm<<<grid_for(h, h->n), 256, 0, h->stream>>>(h->n, h->key, h->rank, start, h->perm);
     if (h->dc.dim == 3)
-        k_scatter_f64v<3><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key,
-                                                                    h->rank, start);
+        k_gather_f64<3><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->perm);
     else
-        k_scatter_f64v<2><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->key,
-                                                                    h->rank, start);
-    return 1;
+        k_gather_f64<2><<<grid_for(h, h->n), 256, 0, h->stream>>>(a, b, h->n, h->perm);
+    return 2;
 }
 
 static void host_shift(const mpcd_handle *h, uint32_t step, double s[3]) {

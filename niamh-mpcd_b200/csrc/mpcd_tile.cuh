@@ -631,6 +631,26 @@ __global__ void __launch_bounds__(256) k_key_f64(const __grid_constant__ DevCfg 
     if (esc_local) atomicAdd(&status[ST_ESCAPED], (unsigned long long)esc_local);
 }
 
+// Reorder into the other buffer as a gather: destination j reads the
+// particle perm[j] (k_perm), so the writes are coalesced.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_gather_f64(Fp64State a, Fp64State b, int n,
+                                                    const int *perm) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int i = __ldg(perm + j);
+        for (int d = 0; d < DIM; d++) {
+            b.q[d][j] = a.q[d][i];
+            b.v[d][j] = a.v[d][i];
+        }
+        b.pid[j] = a.pid[i];
+        if (a.sp) b.sp[j] = a.sp[i];
+        if (a.u[0]) {
+            b.u[0][j] = a.u[0][i];
+            b.u[1][j] = a.u[1][i];
+        }
+    }
+}
+
 // Reorder by (key, rank) into the other buffer.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_scatter_f64v(Fp64State a, Fp64State b, int n,
