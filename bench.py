@@ -351,6 +351,7 @@ def run_other(args, rank, world):
         Q, V, U, sp = W.synthetic_state(cfg, ppc, seed=31 + rank)
         g = Solver(cfg)
         g.set_stream(stream.cuda_stream)
+        g.set_strategy(args.strategy, args.tile)
         g.upload(Q, V, U, sp)
         g.step(args.warmup, 1)
         torch.cuda.synchronize()
