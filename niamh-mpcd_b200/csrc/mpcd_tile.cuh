@@ -253,6 +253,16 @@ struct F64T {
     }
 };
 
+// Lanes per cell in the tile kernel's per-cell phase, and the sum over such
+// a group of lanes (a power of two within a warp; every lane of the warp
+// calls it, and each ends with its own group's total).
+constexpr int kCellLanes = 8;
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int o = kCellLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // --------------------------------------------------------- smem layout
 struct TileLayout {
     int ct;   // cells per tile
@@ -400,15 +410,25 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             }
             __syncthreads();
         }
-        // ---- per cell ----
-        for (int cl = cl_a + tid; cl < cl_b; cl += nth) {
+        // ---- per cell: a group of kCellLanes lanes per cell, its lanes
+        // taking the cell's particles in turn; the groups of a warp step
+        // through their cells together, so every shuffle has all 32 lanes
+        // (a group without a cell adds zeros) ----
+        const int sub = tid & (kCellLanes - 1);
+        const int groups = nth / kCellLanes;
+        for (int base = cl_a + (tid >> 5) * (32 / kCellLanes); base < cl_b;
+             base += groups) {
+            const int cl = base + ((tid & 31) / kCellLanes);
+            const bool have = cl < cl_b;
             const int lc = cl - cl_a;
-            const int j0 = s_start[cl] - p0, j1 = s_start[cl + 1] - p0, pop = j1 - j0;
+            const int j0 = have ? s_start[cl] - p0 : 0;
+            const int j1 = have ? s_start[cl + 1] - p0 : 0;
+            const int pop = j1 - j0;
             const int cell = c0 + cl;
             int cc[3] = {0, 0, 0};
-            if (c.any_phantom || rat) cell_coords(c, cell, cc[0], cc[1], cc[2]);
+            if (have && (c.any_phantom || rat)) cell_coords(c, cell, cc[0], cc[1], cc[2]);
             double M = 0.0, pv[3] = {0, 0, 0}, pq[3] = {0, 0, 0};
-            for (int j = j0; j < j1; j++) {
+            for (int j = j0 + sub; j < j1; j += kCellLanes) {
                 double m = c.mass[s_sp ? s_sp[j] : 0];
                 double v[3];
                 T::vel(s_rec[j], v);
@@ -420,13 +440,18 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                     for (int d = 0; d < DIM; d++) pq[d] += q[d] * m;
                 }
             }
+            M = group_sum(M);
+            for (int d = 0; d < DIM; d++) {
+                pv[d] = group_sum(pv[d]);
+                if (rat) pq[d] = group_sum(pq[d]);
+            }
             double u[3] = {0, 0, 0}, cm[3] = {0, 0, 0};
             if (M > 0.0)
                 for (int d = 0; d < DIM; d++) {
                     u[d] = pv[d] / M;
                     if (rat) cm[d] = pq[d] / M;
                 }
-            if (c.any_phantom && pop > 0 && pop < c.gndnst &&
+            if (have && c.any_phantom && pop > 0 && pop < c.gndnst &&
                 cell_cut_by_phantom<DIM>(c, cc[0], cc[1], cc[2], sa.s)) {
                 double invN = 1.0 / (c.gndnst - (double)pop);
                 double sig = sqrt(c.kbt / invN);
@@ -437,58 +462,68 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                     u[d] /= c.gndnst;
                 }
             }
-            for (int d = 0; d < DIM; d++) av[d] += u[d];
-            for (int d = 0; d < 3; d++) s_u[3 * lc + d] = u[d];
-            if (pop > 1) {
-                if (!andersen) {
+            const bool lead = have && sub == 0;
+            if (lead) {
+                for (int d = 0; d < DIM; d++) av[d] += u[d];
+                for (int d = 0; d < 3; d++) s_u[3 * lc + d] = u[d];
+            }
+            if (!andersen) {
+                if (lead && pop > 1) {
                     double Lx[3] = {0, 0, 1};
-                    if (DIM == 3)
-                        mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
+                    if (DIM == 3) mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
                     srd_matrix<DIM, VT>(c, Lx, &s_R[9 * lc]);
+                }
+                continue;
+            }
+            // Andersen: the cell's sum of thermal velocities (every group of
+            // the warp takes part in the shuffles; a group's own cell may
+            // have fewer than two particles and ignore the result)
+            double rs[3] = {0, 0, 0};
+            for (int j = j0 + sub; j < j1; j += kCellLanes) {
+                double m = c.mass[s_sp ? s_sp[j] : 0];
+                for (int d = 0; d < DIM; d++) rs[d] += m * (double)s_rv[3 * j + d];
+            }
+            for (int d = 0; d < DIM; d++) rs[d] = group_sum(rs[d]);
+            if (lead && pop > 1)
+                for (int d = 0; d < 3; d++) s_rs[3 * lc + d] = d < DIM ? rs[d] / M : 0.0;
+            if (!rat) continue;
+            double I6[6] = {0, 0, 0, 0, 0, 0}, Lm[3] = {0, 0, 0};
+            for (int j = j0 + sub; j < j1; j += kCellLanes) {
+                double m = c.mass[s_sp ? s_sp[j] : 0];
+                double q[3], v[3], r[3] = {0, 0, 0}, dv[3] = {0, 0, 0}, am[3];
+                T::rel(c, s_rec[j], sa, cc, q);
+                T::vel(s_rec[j], v);
+                for (int d = 0; d < DIM; d++) {
+                    r[d] = q[d] - cm[d];
+                    dv[d] = m * (v[d] - (double)s_rv[3 * j + d]);
+                }
+                I6[0] += m * (r[1] * r[1] + r[2] * r[2]);
+                I6[1] += m * (r[0] * r[0] + r[2] * r[2]);
+                I6[2] += m * (r[0] * r[0] + r[1] * r[1]);
+                I6[3] += m * r[0] * r[1];
+                I6[4] += m * r[0] * r[2];
+                I6[5] += m * r[1] * r[2];
+                cross3(r, dv, am);
+                for (int d = 0; d < 3; d++) Lm[d] += am[d];
+            }
+            for (int k = 0; k < 6; k++) I6[k] = group_sum(I6[k]);
+            for (int d = 0; d < 3; d++) Lm[d] = group_sum(Lm[d]);
+            if (lead && pop > 1) {
+                double II[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                if (DIM == 3) {
+                    if (pop >= 3) {
+                        double I[9] = {I6[0], -I6[3], -I6[4], -I6[3], I6[1],
+                                       -I6[5], -I6[4], -I6[5], I6[2]};
+                        inv3(I, II);
+                    }
                 } else {
-                    double rs[3] = {0, 0, 0};
-                    for (int j = j0; j < j1; j++) {
-                        double m = c.mass[s_sp ? s_sp[j] : 0];
-                        for (int d = 0; d < DIM; d++) rs[d] += m * (double)s_rv[3 * j + d];
-                    }
-                    for (int d = 0; d < 3; d++) s_rs[3 * lc + d] = d < DIM ? rs[d] / M : 0.0;
-                    if (rat) {
-                        double I6[6] = {0, 0, 0, 0, 0, 0}, Lm[3] = {0, 0, 0};
-                        for (int j = j0; j < j1; j++) {
-                            double m = c.mass[s_sp ? s_sp[j] : 0];
-                            double q[3], v[3], r[3] = {0, 0, 0}, dv[3] = {0, 0, 0}, am[3];
-                            T::rel(c, s_rec[j], sa, cc, q);
-                            T::vel(s_rec[j], v);
-                            for (int d = 0; d < DIM; d++) {
-                                r[d] = q[d] - cm[d];
-                                dv[d] = m * (v[d] - (double)s_rv[3 * j + d]);
-                            }
-                            I6[0] += m * (r[1] * r[1] + r[2] * r[2]);
-                            I6[1] += m * (r[0] * r[0] + r[2] * r[2]);
-                            I6[2] += m * (r[0] * r[0] + r[1] * r[1]);
-                            I6[3] += m * r[0] * r[1];
-                            I6[4] += m * r[0] * r[2];
-                            I6[5] += m * r[1] * r[2];
-                            cross3(r, dv, am);
-                            for (int d = 0; d < 3; d++) Lm[d] += am[d];
-                        }
-                        double II[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-                        if (DIM == 3) {
-                            if (pop >= 3) {
-                                double I[9] = {I6[0], -I6[3], -I6[4], -I6[3], I6[1],
-                                               -I6[5], -I6[4], -I6[5], I6[2]};
-                                inv3(I, II);
-                            }
-                        } else {
-                            II[8] = 1. / I6[2];
-                        }
-                        for (int x = 0; x < 3; x++) {
-                            double w = 0.0;
-                            for (int y = 0; y < 3; y++) w += II[x * 3 + y] * Lm[y];
-                            s_W[3 * lc + x] = w;
-                            s_cm[3 * lc + x] = cm[x];
-                        }
-                    }
+                    II[8] = 1. / I6[2];
+                }
+                for (int x = 0; x < 3; x++) {
+                    double w = 0.0;
+                    for (int y = 0; y < 3; y++) w += II[x * 3 + y] * Lm[y];
+                    s_W[3 * lc + x] = w;
+                    s_cm[3 * lc + x] = cm[x];
                 }
             }
         }
