@@ -112,67 +112,107 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling (every 200 ms) around the timed region: a reader
-    thread stamps each sample with the host clock on arrival, and stop()
-    keeps the samples that arrived inside [t0, t1] (the nearest one if the
-    region was shorter than a sampling period)."""
+    """SM clock and clock-event reasons of this process's GPU, sampled during
+    the timed region: NVML read every 10 ms by a thread (the timed region of
+    the default run is a fraction of a second), or nvidia-smi every 200 ms
+    where NVML cannot be loaded.  The GPU is found by its PCI address, so
+    the samples are this device's whatever CUDA_VISIBLE_DEVICES says.  Each
+    sample carries the host time of its reading, and stop() keeps those that
+    fall inside [t0, t1] (the nearest one if the region was shorter than a
+    sampling period).  Only reads: no clock or setting is changed."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, gpu_index):
-        self.samples = []
+    def __init__(self, dev):
+        import torch
+        pr = torch.cuda.get_device_properties(dev)
+        self.busid = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        self.samples = []  # (host time, sm MHz, max sm MHz, set of reason names)
+        self.p = None
+        self.nv = None
+        self.halt = threading.Event()
         try:
-            self.p = subprocess.Popen(
-                ["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(self.busid.encode())
+            self.nv = pynvml
+            self.bits = [(nm, getattr(pynvml, "nvmlClocksEventReason" + cap))
+                         for nm, cap in zip(self.NAMES, ["HwSlowdown", "HwThermalSlowdown",
+                                                         "SwThermalSlowdown", "SwPowerCap"])]
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.th = threading.Thread(target=self._poll, daemon=True)
         except Exception:
-            self.p = None
-            return
-        self.th = threading.Thread(target=self._read, daemon=True)
+            self.nv = None
+            try:
+                self.p = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.busid}", f"--query-gpu={self.Q}",
+                     "--format=csv,noheader,nounits", "-lms", "200"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            except Exception:
+                self.p = None
+                return
+            self.th = threading.Thread(target=self._read, daemon=True)
         self.th.start()
+
+    def _poll(self):
+        nv = self.nv
+        while not self.halt.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                return
+            self.samples.append((time.time(), sm, self.smax,
+                                 {nm for nm, bit in self.bits if mask & bit}))
+            self.halt.wait(0.01)
 
     def _read(self):
         for line in self.p.stdout:
-            self.samples.append((time.time(), line))
-
-    def wait_ready(self, timeout=15.0):
-        t0 = time.time()
-        while self.p is not None and not self.samples and time.time() - t0 < timeout:
-            time.sleep(0.05)
-
-    def stop(self, t0, t1):
-        if self.p is None:
-            return None
-        time.sleep(0.25)  # let the sample that covers t1 arrive
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        inside = [s for s in self.samples if t0 <= s[0] <= t1 + 0.2]
-        if not inside and self.samples:
-            inside = [min(self.samples, key=lambda s: abs(s[0] - 0.5 * (t0 + t1)))]
-        sm, smax, reasons = [], 0.0, set()
-        for _, line in inside:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = max(smax, float(parts[2]))
+                sm, smax = float(parts[1]), float(parts[2])
             except ValueError:
                 continue
-            for nm, val in zip(self.NAMES, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+            rs = {nm for nm, val in zip(self.NAMES, parts[5:9])
+                  if val.lower().startswith("active")}
+            self.samples.append((time.time(), sm, smax, rs))
+
+    def wait_ready(self, timeout=15.0):
+        t0 = time.time()
+        while (self.p is not None or self.nv is not None) and not self.samples \
+                and time.time() - t0 < timeout:
+            time.sleep(0.01)
+
+    def stop(self, t0, t1):
+        if self.nv is None and self.p is None:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm),
+        if self.nv is not None:
+            self.halt.set()
+            self.th.join(timeout=2)
+            slack = 0.01
+        else:
+            time.sleep(0.25)  # let the sample that covers t1 arrive
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            slack = 0.2
+        inside = [s for s in self.samples if t0 <= s[0] <= t1 + slack]
+        if not inside and self.samples:
+            inside = [min(self.samples, key=lambda s: abs(s[0] - 0.5 * (t0 + t1)))]
+        if not inside:
+            return None
+        reasons = set().union(*(s[3] for s in inside))
+        return {"sm_mhz": statistics.median(s[1] for s in inside),
+                "sm_max_mhz": max(s[2] for s in inside),
+                "reasons": sorted(reasons), "samples": len(inside),
+                "source": "nvml" if self.nv is not None else "nvidia-smi",
                 "timed_region_s": round(t1 - t0, 3)}
 
 

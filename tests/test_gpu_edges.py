@@ -1,0 +1,117 @@
+"""Edge cases of the default SRD path (the resident kernel families of both
+precision forms) through the C ABI, against the CPU oracle:
+
+- one cell holding thousands of particles next to an ordinary fluid: the
+  mixed form's per-block sum table and the FP64 form's atomics take any
+  population, so the dense cell collides like the oracle's (the tile
+  kernels' staging limit does not apply here);
+- particles whose mass-weighted velocity is above the mixed form's limb
+  range (|m v| >= 256), which skip the shared-memory table and add
+  straight to the 64-bit global sums;
+- an empty state: the upload is accepted and a step is refused with an
+  error status, without a launch.
+"""
+import numpy as np
+import pytest
+
+from checkers import Oracle
+from mpcd_b200 import abi
+from mpcd_b200 import workloads as W
+from mpcd_b200.gpu import MPCDError, Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense_cell_state(cfg, ppc, seed, cell, extra):
+    """Uniform fluid of ppc particles per cell, plus `extra` particles
+    inside one cell (away from its faces), velocities Maxwellian kT = 1."""
+    Q, V, U, sp = W.synthetic_state(cfg, ppc, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    q = np.zeros((extra, 3))
+    for d in range(cfg.dim):
+        q[:, d] = cell[d] + 0.05 + 0.9 * rng.random(extra)
+    v = np.zeros((extra, 3))
+    v[:, :cfg.dim] = rng.standard_normal((extra, cfg.dim))
+    Q = np.concatenate([Q, q])
+    V = np.concatenate([V, v])
+    U = np.concatenate([U, np.zeros((extra, 3))])
+    return Q, V, U, np.zeros(len(Q), dtype=np.int32)
+
+
+def _compare(prec, qg, vg, qo, vo, L, vtol_rel):
+    d = qg - qo
+    d -= np.round(d / L) * L
+    dq = np.abs(d).max(axis=1)
+    scale = np.maximum(1.0, np.abs(vo).max(axis=1))
+    dv = np.abs(vg - vo).max(axis=1) / scale
+    if prec == abi.PREC_FP64:
+        assert dv.max() < 1e-11 and dq.max() < 1e-11 * L.max(), (dv.max(), dq.max())
+    else:
+        # FP32 velocities and cell records: a few particles may land a
+        # rounding away from a cell face and take another cell's rotation
+        bad = np.mean((dv > vtol_rel) | (dq > 1e-4))
+        assert bad < 2e-3, (bad, dv.max(), dq.max())
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_FP64])
+def test_dense_cell_collides_like_the_oracle(prec):
+    L = (6, 6, 6)
+    cfg = W.cfg_srd3d(L, seed=61)
+    cfgp = W.cfg_srd3d(L, precision=prec, seed=61)
+    Q, V, U, sp = _dense_cell_state(cfg, 10, 62, (2, 3, 1), 5000)
+    o = Oracle(cfg, Q, V, U, sp)
+    g = Solver(cfgp)
+    g.set_kernel(abi.KERNEL_RESIDENT)
+    g.set_sort_interval(2)  # re-sort with the dense cell too
+    g.upload(Q, V, U, sp)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(L, dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.overflow == 0 and st.nonfinite == 0
+    # momentum is conserved by every collision (exactly in the mixed form's
+    # fixed-point sums, to FP32 rounding in its velocities)
+    p0, p1 = V.sum(axis=0), g.download()[1].sum(axis=0)
+    tol = 1e-9 if prec == abi.PREC_FP64 else 2e-6 * np.abs(V).sum()
+    assert np.abs(p1 - p0).max() < tol
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_FP64])
+def test_fast_particles_in_populated_cells(prec):
+    # |v| of 260-400 at dt = 0.01: up to 4 cells per step in an 8-cell box,
+    # inside cells of 10 ordinary particles, so that they collide
+    L = (8, 8, 8)
+    cfg = W.cfg_srd3d(L, seed=63, dt=0.01)
+    cfgp = W.cfg_srd3d(L, precision=prec, seed=63, dt=0.01)
+    Q, V, U, sp = W.synthetic_state(cfg, 10, seed=64)
+    rng = np.random.default_rng(65)
+    fast = rng.choice(len(Q), 40, replace=False)
+    V[fast] = rng.uniform(260.0, 400.0, (40, 3)) * np.where(rng.random((40, 3)) < 0.5, -1, 1)
+    o = Oracle(cfg, Q, V, U, sp)
+    g = Solver(cfgp)
+    g.set_kernel(abi.KERNEL_RESIDENT)
+    g.upload(Q, V, U, sp)
+    for s in (1, 2):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(L, dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    p0, p1 = V.sum(axis=0), g.download()[1].sum(axis=0)
+    tol = 1e-8 if prec == abi.PREC_FP64 else 2e-6 * np.abs(V).sum()
+    assert np.abs(p1 - p0).max() < tol
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_FP64])
+def test_empty_state_is_refused_not_stepped(prec):
+    cfg = W.cfg_srd3d((4, 4, 4), precision=prec, seed=66)
+    g = Solver(cfg)
+    g.upload(np.zeros((0, 3)), np.zeros((0, 3)))
+    with pytest.raises(MPCDError):
+        g.step(1, 1)
+    assert g.status().steps == 0
