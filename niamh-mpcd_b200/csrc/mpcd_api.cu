@@ -1043,7 +1043,18 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
         h->cur = 1 - h->cur;
         h->sort_age = 0;
     }
-    const int pgrid = (int)((h->n + 255) / 256);
+    // one wave: the blocks of the particle pass that fit on the device at
+    // once (the kernel strides over the particles)
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_r64_parts<DIM, RES_STEP>, 256,
+                                                          0) != cudaSuccess || b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    const long long pwant = ((long long)h->n + 255) / 256, pcap = (long long)h->sm_count * per_sm;
+    const int pgrid = (int)(pwant < pcap ? pwant : pcap);
     if (h->sums_for != (int64_t)step) {
         CK(cudaMemsetAsync(h->r64sum, 0, sizeof(double) * 8 * nc, h->stream));
         CK(cudaMemsetAsync(h->r64pop, 0, sizeof(int) * 2 * nc, h->stream));

@@ -7,7 +7,8 @@
 //                sums of the previous particle pass, the random axis
 //                (stochrotMPC, mpc.c:1275-1333), the avVel term; writes a
 //                64-byte record {u, pop, axis} and clears the sums.
-//   k_r64_parts  one thread per particle: its cell on this step's grid
+//   k_r64_parts  one thread per particle (one wave of blocks, each thread
+//                striding over the particles): its cell on this step's grid
 //                (recomputed from its position exactly as the split family
 //                does), the rotation matrix from the record's axis (rotate,
 //                mpc.c:1181-1257, the split family's srd_matrix), v' = u +
@@ -92,8 +93,12 @@ __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCf
 
 // RES_STEP: collide, stream, write back, add to the next step's sums.
 // RES_SUM:  only add each particle to this step's sums (bootstrap).
+// Four blocks of 256 threads per SM (64 registers, no spills).
+#ifndef R64_MINB
+#define R64_MINB 4
+#endif
 template <int DIM, int MODE>
-__global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCfg c,
+__global__ void __launch_bounds__(256, R64_MINB) k_r64_parts(const __grid_constant__ DevCfg c,
                                                    Fp64State a, int n, const R64Rec *crec,
                                                    R64Sums sums, double *acc,
                                                    unsigned long long *status, StepArgs sa) {
@@ -102,10 +107,21 @@ __global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCf
     pdl_wait();  // records, sums and particles are complete from here on
     double ke = 0.0;
     int bounce = 0, esc = 0;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
+    // one wave of blocks striding over the particles: the block-end
+    // reduction and the block turnover are paid once per resident block
+    // rather than once per 256 particles
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        // the particle stays in place, so its id is neither read nor
+        // written; otherwise as F64T::load: the shifted position and the
+        // velocity with this step's kick
         F64Rec r;
-        F64T<DIM>::load(c, a, i, sa, r);  // shifted position, velocity with this step's kick
+        r.pid = 0;
+        for (int d = 0; d < 3; d++) {
+            r.q[d] = d < DIM ? shift_fwd(a.q[d][i], sa.s[d], c.L[d]) : 0.0;
+            r.v[d] = d < DIM ? a.v[d][i] : 0.0;
+            if (d < DIM && c.grav_flag) r.v[d] = r.v[d] + c.dt * c.grav[d];
+        }
         const int sp = F64T<DIM>::sp(a, i);
         int k;
         double v[3] = {0.0, 0.0, 0.0};
@@ -124,9 +140,12 @@ __global__ void __launch_bounds__(256) k_r64_parts(const __grid_constant__ DevCf
             double t = r.v[0] * r.v[0];
             t += r.v[1] * r.v[1];
             t += r.v[2] * r.v[2];
-            ke = c.mass[sp] * t;
+            ke += c.mass[sp] * t;
             k = F64T<DIM>::finish(c, r, sp, sa, bounce, esc);
-            F64T<DIM>::store(a, i, r);
+            for (int d = 0; d < DIM; d++) {
+                a.q[d][i] = r.q[d];
+                a.v[d][i] = r.v[d];
+            }
             // the next step's cell pass sees the velocity with its kick
             for (int d = 0; d < DIM; d++)
                 v[d] = c.grav_flag ? r.v[d] + c.dt * c.grav[d] : r.v[d];
