@@ -33,6 +33,7 @@ PPC = 10
 # algorithmic bytes per particle-step (state read+written once, cell record
 # written+read once per ppc particles): 3D SRD mixed 62.4 B, FP64 102.4 B
 ALG_BYTES = {"mixed": 62.4, "fp64": 102.4}
+SORT_INTERVAL = 30  # the library's default re-sort interval of the resident families
 WORKLOAD = "3D SRD fluid, periodic 64^3 cells, 10 particles/cell (2,621,440), rot 130 deg"
 L2_NOTE = {
     "none": ("not flushed: steps run back to back; each step reads and writes 2 x 84 MB of "
@@ -250,10 +251,12 @@ def run_gpu(args, rank, world):
         g.set_stream(stream.cuda_stream)
         g.set_strategy(args.strategy, args.tile)
         g.set_kernel(args.kernel)
-        if args.sort_interval > 0:
-            g.set_sort_interval(args.sort_interval)
         g.upload(Q, V, U, sp)
         g.step(args.warmup, 1)
+        # a new re-sort cycle: the first timed step re-sorts, so a window of K
+        # steps carries ceil(K / interval) sorts (at least the steady
+        # state's share, 1 per interval)
+        g.set_sort_interval(args.sort_interval if args.sort_interval > 0 else SORT_INTERVAL)
         torch.cuda.synchronize()
         clk = Clocks(dev) if form == "mixed" else None
         if clk:
@@ -331,8 +334,9 @@ def run_gpu(args, rank, world):
             "kernel_launches": kern_n,
         }
         # e2e through the C ABI with host buffers: upload from pinned host
-        # memory, K drop-in timestep() calls each returning the step's global
-        # measures to the host, download of the final state
+        # memory, K steps with every step's global measures (TEMP, avVel)
+        # returned to the host (mpcd_step_record), download of the final
+        # state into pinned arrays
         if form == "mixed":
             Qh = torch.from_numpy(Q).pin_memory().numpy()
             Vh = torch.from_numpy(V).pin_memory().numpy()
@@ -342,8 +346,7 @@ def run_gpu(args, rank, world):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             g.upload(Qh, Vh, None, sp)
-            for k in range(args.steps):
-                g.timestep(1000 + k)
+            kb_steps, av_steps = g.step_record(args.steps, 1000)
             q2, v2, _ = g.download(out=(Qo, Vo))
             torch.cuda.synchronize()
             e2e_s = max_over_ranks(time.perf_counter() - t0, world)
@@ -351,6 +354,8 @@ def run_gpu(args, rank, world):
                 "value": job_rate(n, world, args.steps, e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": (Q.nbytes + V.nbytes + sp.nbytes) / args.steps,
                 "d2h_bytes_per_step": (q2.nbytes + v2.nbytes) / args.steps + 32,
+                "path": "mpcd_upload_state, mpcd_step_record (every step's TEMP and avVel "
+                        "to the host), mpcd_download_state",
             }
         g.close()
         del Q, V, U
@@ -614,7 +619,9 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "global_batch": n * world, "form": "mixed",
                        "parallelism": f"replicas x{world}",
-                       "l2": L2_NOTE[args.flush]},
+                       "l2": L2_NOTE[args.flush],
+                       "sort_interval": args.sort_interval or SORT_INTERVAL,
+                       "sorts_in_window": -(-args.steps // (args.sort_interval or SORT_INTERVAL))},
             "fp64": {"value": v64, "ms_per_step": f64["ms_total"] / args.steps,
                      "achieved_gbs": ach64, "frac": ach64 / peak},
             "mixed_over_fp64": value / v64,

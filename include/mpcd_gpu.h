@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define MPCD_ABI_VERSION 2
+#define MPCD_ABI_VERSION 3
 
 #define MPCD_MAX_SPECIES 10 /* reference MAXSPECI, definitions.h:66 */
 #define MPCD_MAX_WALLS 16
@@ -163,7 +163,9 @@ int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
 /* Same, reading an array of records with a byte stride, so a caller can pass
  * the reference's particleMPC array (SRDclss.h:34-44) directly:
  * stride = sizeof(particleMPC), offsets = offsetof(particleMPC, Q/V/U/SPID).
- * off_U may be (size_t)-1 to skip orientations. */
+ * off_U may be (size_t)-1 to skip orientations (nematic states then start
+ * every orientation at (1, 0)); off_spid (size_t)-1 gives every particle
+ * species 0. */
 int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *base,
                                   size_t stride, size_t off_Q, size_t off_V,
                                   size_t off_U, size_t off_spid);
@@ -171,7 +173,10 @@ int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *base,
 /* Copy the particle state back in the caller's original particle order. */
 int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double *U);
 
-/* Strided counterpart of mpcd_download_state (writes Q, V, U fields only). */
+/* Strided counterpart of mpcd_download_state: writes the Q and V fields of
+ * each record and, for a nematic state (lc != 0) with off_U != (size_t)-1,
+ * the U field (the orientation, third component 0 in 2D); other bytes of the
+ * records are left as they are. */
 int mpcd_download_particles_strided(mpcd_handle *h, void *base, size_t stride,
                                     size_t off_Q, size_t off_V, size_t off_U);
 
@@ -185,15 +190,37 @@ int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0);
 int mpcd_timestep(mpcd_handle *h, uint32_t runtime, double AVNOW[3],
                   double *KBTNOW);
 
+/* nsteps timesteps numbered step0, step0+1, ... (as mpcd_step) with every
+ * step's global measures returned: kbtnow[k] = TEMP and avnow[3k..3k+2] =
+ * avVel of step step0 + k (therm.c:209-235, 362-367), what nsteps calls of
+ * mpcd_timestep return.  The measures come back in batches, read while the
+ * next batch runs, so the host does not wait for each step as it does with
+ * mpcd_timestep.  Returns when the last step has finished. */
+int mpcd_step_record(mpcd_handle *h, int nsteps, uint32_t step0, double *kbtnow,
+                     double *avnow);
+
 /* Global measures of the last executed step (blocks until it finishes). */
 int mpcd_globals(mpcd_handle *h, double *kbtnow, double avnow[3]);
 
 /* Re-bin on the unshifted grid and compute per-cell properties for output
- * (the re-bin + localPROP at the end of timestep, mpc.c:4936-4942).
- * Arrays hold (L0+1)(L1+1)(L2+1) cells, index (a*(L1+1)+b)*(L2+1)+c; any
- * pointer may be NULL.  vcm/cm hold 3 doubles per cell. */
+ * (the re-bin + localPROP at the end of timestep, mpc.c:4936-4942), on the
+ * device; only the cell arrays are copied back.  Arrays hold
+ * (L0+1)(L1+1)(L2+1) cells, index (a*(L1+1)+b)*(L2+1)+c; any pointer may be
+ * NULL.  vcm/cm hold 3 doubles per cell (CM = sum m Q / M, computed for
+ * every operator; the reference fills it for MPC-AT+a and nematics only,
+ * mpc.c:75).  The FP64 sums are added in arrival order, so they agree with
+ * the reference's list-order sums to rounding. */
 int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
                     double *cm);
+
+/* Parity check (no counterpart in the reference): the population of every
+ * cell of the NEXT step's shifted grid (step last + 1, (L+1)^D cells in the
+ * layout of mpcd_cell_props), exactly as the step's own kernels hold it for
+ * that step's collision (the counting sort's offsets, or the resident
+ * families' population sums).  They are the cell lists the reference's
+ * bin() (mpc.c:948-992) builds at the start of that step.
+ * MPCD_ERR_STATE before the first step after an upload. */
+int mpcd_debug_cell_counts(mpcd_handle *h, int *pop);
 
 /* Transverse momentum modes of the smallest wavevectors (an analysis
  * helper with no counterpart in the reference): for each ordered pair of
@@ -262,8 +289,8 @@ int mpcd_set_kernel(mpcd_handle *h, int kernel);
 
 /* MPCD_KERNEL_RESIDENT re-sorts the state by cell every 'steps' steps
  * (default 30) to keep particles that are close in space close in memory;
- * the sort changes no result, only the speed.  No counterpart in the
- * reference. */
+ * the sort changes no result, only the speed.  The call starts a new cycle:
+ * the next step re-sorts.  No counterpart in the reference. */
 int mpcd_set_sort_interval(mpcd_handle *h, int steps);
 
 /* ---------------------------------------------------------------------
@@ -303,20 +330,27 @@ int mpcd_batch_info(mpcd_batch *b, int *n, int *slots, int *cells);
  * framework's memory manager.  Q and V are the caller's DEVICE arrays of n
  * particles (3 doubles each, AoS), updated in place in the caller's order;
  * globals, if not NULL, is a device array of 4 doubles receiving
- * KBTNOW and AVNOW[3] (TEMP and avVel).  cfg must select the SRD operator
- * (MPCD_COLL_ARBAXIS) in FP64 form without phantom walls or nematic order.
+ * KBTNOW and AVNOW[3] (TEMP and avVel); counters, if not NULL, is a device
+ * array of MPCD_NOALLOC_COUNTERS uint64 to which the step ADDS its error
+ * counts (escaped, bounce_limit, nonfinite, as in mpcd_status), so a caller
+ * that zeroes it once accumulates over calls.  cfg must select the SRD
+ * operator (MPCD_COLL_ARBAXIS) in FP64 form with one species, without
+ * phantom walls or nematic order (MPCD_ERR_UNSUPPORTED otherwise).
  * All scratch is one fixed device array of this library (11.6 MiB, held on
  * every GPU that loads it until exit), so n is limited to
  * MPCD_NOALLOC_MAX_PARTICLES and the (L+1)^D cell grid to
  * MPCD_NOALLOC_MAX_CELLS; larger sizes return MPCD_ERR_SIZE.  The first call
- * on a device looks up the array's device address; make that first call
- * before any stream capture.  Calls share the array: work of two calls that
- * overlaps on the GPU races and must be serialised by the caller.  stream is
- * a cudaStream_t (NULL: the default stream); the call is asynchronous. */
+ * in a CUDA context (on each device, and again after a device reset) looks up
+ * the array's device address; make that first call before any stream
+ * capture.  Calls share the array: work of two calls that overlaps on the GPU
+ * races and must be serialised by the caller.  stream is a cudaStream_t
+ * (NULL: the default stream); the call is asynchronous. */
 #define MPCD_NOALLOC_MAX_PARTICLES 65536
 #define MPCD_NOALLOC_MAX_CELLS 32768
+#define MPCD_NOALLOC_COUNTERS 3
 int mpcd_srd_step_noalloc(const mpcd_config *cfg, int n, double *Q, double *V,
-                          uint32_t step, double *globals, void *stream);
+                          uint32_t step, double *globals, unsigned long long *counters,
+                          void *stream);
 
 #ifdef __cplusplus
 }

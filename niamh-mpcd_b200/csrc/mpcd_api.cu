@@ -23,6 +23,7 @@
 #include "mpcd_resident.cuh"
 #include "mpcd_resident64.cuh"
 #include "mpcd_lc.cuh"
+#include "mpcd_xfer.cuh"
 
 using namespace mpcd;
 
@@ -55,7 +56,11 @@ struct mpcd_handle {
     LcCells lcc;     // per-cell nematic arrays (lc != 0)
     double *lcbuf;
     double *modes;   // transverse momentum modes (mpcd_transverse_modes)
+    bool stepped;        // a step ran since the last upload (mpcd_debug_cell_counts)
+    double *props;       // mpcd_cell_props accumulators: 7 doubles + 1 int per cell
+    double *host_ring;   // pinned: per-step globals of mpcd_step_record
     bool res_attr;       // the resident kernels' shared-memory attributes are set
+    int r64_per_sm;      // resident blocks per SM of the FP64 particle pass (0: not yet known)
     void *xfer;          // device staging of FP64 uploads and downloads (mixed form)
     size_t xfer_bytes;
     int64_t sorted_for;  // step whose shifted grid the current order bins; -1 none
@@ -96,6 +101,17 @@ static void time_clear(mpcd_handle *h) {
         cudaEventDestroy(p.second);
     }
     h->tev.clear();
+}
+
+// Per-step global accumulators (ACC_KE, ACC_VCM) live in a ring of
+// kAccRing slots indexed by the step number: the kernels of step t clear
+// the slot of step t + 1, so the slots of the last kAccRing - 1 steps stay
+// readable (mpcd_step_record reads them in batches).
+constexpr int kAccRing = 128;
+constexpr int kRecordBatch = 32;  // steps per read-back of mpcd_step_record
+static_assert(2 * kRecordBatch < kAccRing, "a batch is read while the next one runs");
+static double *acc_at(const mpcd_handle *h, uint32_t step) {
+    return h->acc + (size_t)(step % (uint32_t)kAccRing) * ACC_WORDS;
 }
 
 #define CK(call)                                                        \
@@ -274,7 +290,9 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->r64sum);
     cudaFree(h->r64pop);
     cudaFree(h->lcbuf);
+    cudaFree(h->props);
     if (h->host_acc) cudaFreeHost(h->host_acc);
+    if (h->host_ring) cudaFreeHost(h->host_ring);
     time_clear(h);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -318,7 +336,7 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     ALLOC(h->start[0], sizeof(int) * (nk + 1));
     ALLOC(h->start[1], sizeof(int) * (nk + 1));
     ALLOC(h->part, sizeof(int) * h->nscan);
-    ALLOC(h->acc, sizeof(double) * 2 * ACC_WORDS);
+    ALLOC(h->acc, sizeof(double) * kAccRing * ACC_WORDS);
     ALLOC(h->status, sizeof(unsigned long long) * ST_WORDS);
     ALLOC(h->crec, (size_t)nc * 128);
     if (cfg->precision == MPCD_PREC_MIXED && !dc.lc) {
@@ -355,7 +373,8 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
         cudaMemsetAsync(h->fill, 0, sizeof(int) * nk, h->stream) != cudaSuccess ||
         cudaMemsetAsync(h->status, 0, sizeof(unsigned long long) * ST_WORDS, h->stream) !=
             cudaSuccess ||
-        cudaMemsetAsync(h->acc, 0, sizeof(double) * 2 * ACC_WORDS, h->stream) != cudaSuccess) {
+        cudaMemsetAsync(h->acc, 0, sizeof(double) * kAccRing * ACC_WORDS, h->stream) !=
+            cudaSuccess) {
         mpcd_destroy(h);
         return MPCD_ERR_CUDA;
     }
@@ -416,16 +435,8 @@ static int ensure_capacity(mpcd_handle *h, int n) {
     return MPCD_OK;
 }
 
-// host_check: validate Q and V on the host (the mixed form's device-side
-// conversion checks them itself).
-static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V,
-                         const int *spid, bool host_check = true) {
-    int dim = h->dc.dim;
-    for (int i = 0; spid && i < n; i++)
-        if (spid[i] < 0 || spid[i] >= h->dc.n_species) return MPCD_ERR_ARG;
-    for (int i = 0; host_check && i < n; i++)
-        for (int d = 0; d < dim; d++)
-            if (!std::isfinite(Q[3 * i + d]) || !std::isfinite(V[3 * i + d])) return MPCD_ERR_ARG;
+// Reset of the per-state bookkeeping for n uploaded particles.
+static int upload_common(mpcd_handle *h, int n) {
     int r = ensure_capacity(h, n);
     if (r != MPCD_OK) return r;
     h->n = n;
@@ -433,32 +444,7 @@ static int upload_common(mpcd_handle *h, int n, const double *Q, const double *V
     h->sorted_for = -1;
     h->sums_for = -1;
     h->sort_age = -1;
-    // global number density as globalDensities (init.c:1002-1018) unless
-    // given; phantom walls and the nematic activity use it
-    if (!(h->cfg.gndnst > 0.0) && (h->dc.any_phantom || h->dc.lc)) {
-        std::vector<int> pop((size_t)h->dc.ncells, 0);
-        for (int i = 0; i < n; i++) {
-            int idx[3] = {0, 0, 0};
-            for (int d = 0; d < dim; d++) {
-                int a = (int)Q[3 * i + d];
-                if (a < 0) a = 0;
-                if (a > h->dc.L[d]) a = h->dc.L[d];
-                idx[d] = a;
-            }
-            pop[((size_t)idx[0] * h->dc.N1[1] + idx[1]) * h->dc.N1[2] + idx[2]]++;
-        }
-        double cnt = 0.0, sumN = 0.0;
-        for (int a = 0; a < h->dc.L[0]; a++)
-            for (int b = 0; b < h->dc.L[1]; b++)
-                for (int z = 0; z < h->dc.L[2]; z++) {
-                    int p = pop[((size_t)a * h->dc.N1[1] + b) * h->dc.N1[2] + z];
-                    if (p > 0) {
-                        cnt += 1.0;
-                        sumN += (double)p;
-                    }
-                }
-        h->dc.gndnst = cnt > 0.0 ? sumN / cnt : 0.0;
-    }
+    h->stepped = false;
     return MPCD_OK;
 }
 
@@ -481,93 +467,85 @@ static int xfer_reserve(mpcd_handle *h, size_t bytes) {
     return MPCD_OK;
 }
 
-// The mixed form's positions and velocities are converted on the device
-// when the state has nothing else to carry: no nematic orientations, one
-// species (decided from the configuration: the buffers may not exist yet).
-static bool mix_device_xfer(const mpcd_handle *h) {
-    return h->prec == MPCD_PREC_MIXED && !h->dc.lc && h->dc.n_species == 1;
-}
-
-// Upload of Q and V in the caller's layout to the mixed state: two copies
-// into the staging buffer and a conversion kernel.
-static int mix_upload_device(mpcd_handle *h, int n, const double *Q, const double *V) {
-    const size_t N = (size_t)n;
-    int r = xfer_reserve(h, N * 48 + 16);
+// Staging layout of an upload or download of N particles: Q, V (and U) as
+// 3 doubles per particle, the species ids, and 32 bytes of flags and sums.
+struct Staging {
+    double *Q, *V, *U;
+    int *sp;
+    int *err;
+    unsigned long long *sums;  // GnDNST: occupied cells, particles
+};
+static int staging(mpcd_handle *h, size_t N, bool withU, bool withSp, Staging *x) {
+    const size_t vec = (N * 24 + 255) / 256 * 256, ids = (N * 4 + 255) / 256 * 256;
+    int r = xfer_reserve(h, 2 * vec + (withU ? vec : 0) + (withSp ? ids : 0) + 256);
     if (r != MPCD_OK) return r;
-    double *dq = (double *)h->xfer, *dv = dq + 3 * N;
-    int *derr = (int *)(dv + 3 * N);
-    CK(cudaMemcpyAsync(dq, Q, N * 24, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(dv, V, N * 24, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(derr, 0, sizeof(int), h->stream));
-    k_mix_from_f64<<<grid_for(h, n), 256, 0, h->stream>>>(h->mx[0], h->dc, n, dq, dv, derr);
-    int herr = 0;
-    CK(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    return herr ? MPCD_ERR_ARG : MPCD_OK;
-}
-
-// Download of the mixed state into Q and V in the caller's layout and order.
-static int mix_download_device(mpcd_handle *h, double *Q, double *V) {
-    const size_t N = (size_t)h->n;
-    int r = xfer_reserve(h, N * 48 + 16);
-    if (r != MPCD_OK) return r;
-    double *dq = (double *)h->xfer, *dv = dq + 3 * N;
-    int *derr = (int *)(dv + 3 * N);
-    CK(cudaMemsetAsync(derr, 0, sizeof(int), h->stream));
-    k_mix_to_f64<<<grid_for(h, h->n), 256, 0, h->stream>>>(h->mx[h->cur], h->dc, h->n, dq, dv,
-                                                            derr);
-    int herr = 0;
-    CK(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    if (Q) CK(cudaMemcpyAsync(Q, dq, N * 24, cudaMemcpyDeviceToHost, h->stream));
-    if (V) CK(cudaMemcpyAsync(V, dv, N * 24, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    return herr ? MPCD_ERR_STATE : MPCD_OK;
+    char *p = (char *)h->xfer;
+    x->Q = (double *)p;
+    x->V = (double *)(p + vec);
+    p += 2 * vec;
+    x->U = withU ? (double *)p : nullptr;
+    if (withU) p += vec;
+    x->sp = withSp ? (int *)p : nullptr;
+    if (withSp) p += ids;
+    x->err = (int *)p;
+    x->sums = (unsigned long long *)(p + 16);
+    return MPCD_OK;
 }
 
 extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
                                  const double *U, const int *spid) {
     if (!h || n < 0 || (n > 0 && (!Q || !V))) return MPCD_ERR_ARG;
-    const bool dev = mix_device_xfer(h);
-    int r = upload_common(h, n, Q, V, spid, !dev);
+    int r = upload_common(h, n);
     if (r != MPCD_OK) return r;
     if (n == 0) return MPCD_OK;
-    int dim = h->dc.dim;
-    size_t N = (size_t)n;
+    const size_t N = (size_t)n;
+    // species ids are checked whenever given (with one species every id
+    // must be 0)
+    const bool withU = U && h->dc.lc, withSp = spid != nullptr;
+    // several species without ids: every particle species 0 (the kernels
+    // read a null id array as species 0 only with one species)
+    const bool zeroSp = !spid && h->dc.n_species > 1;
+    Staging x;
+    r = staging(h, N, withU, withSp || zeroSp, &x);
+    if (r != MPCD_OK) return r;
+    CK(cudaMemcpyAsync(x.Q, Q, N * 24, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(x.V, V, N * 24, cudaMemcpyHostToDevice, h->stream));
+    if (withU) CK(cudaMemcpyAsync(x.U, U, N * 24, cudaMemcpyHostToDevice, h->stream));
+    if (withSp) CK(cudaMemcpyAsync(x.sp, spid, N * 4, cudaMemcpyHostToDevice, h->stream));
+    if (zeroSp) CK(cudaMemsetAsync(x.sp, 0, N * 4, h->stream));
+    CK(cudaMemsetAsync(x.err, 0, 256, h->stream));
+    const int g = grid_for(h, n);
     if (h->prec == MPCD_PREC_FP64) {
-        std::vector<double> tmp(N);
-        std::vector<int> ids(N);
-        for (int d = 0; d < dim; d++) {
-            for (size_t i = 0; i < N; i++) tmp[i] = Q[3 * i + d];
-            CK(cudaMemcpyAsync(h->f[0].q[d], tmp.data(), N * 8, cudaMemcpyHostToDevice, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            for (size_t i = 0; i < N; i++) tmp[i] = V[3 * i + d];
-            CK(cudaMemcpyAsync(h->f[0].v[d], tmp.data(), N * 8, cudaMemcpyHostToDevice, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-        }
-        for (size_t i = 0; i < N; i++) ids[i] = (int)i;
-        CK(cudaMemcpyAsync(h->f[0].pid, ids.data(), N * 4, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        if (h->f[0].sp) {
-            for (size_t i = 0; i < N; i++) ids[i] = spid ? spid[i] : 0;
-            CK(cudaMemcpyAsync(h->f[0].sp, ids.data(), N * 4, cudaMemcpyHostToDevice, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-        }
-        if (h->f[0].u[0])
-            for (int d = 0; d < 2; d++) {
-                for (size_t i = 0; i < N; i++) tmp[i] = U ? U[3 * i + d] : (d == 0 ? 1.0 : 0.0);
-                CK(cudaMemcpyAsync(h->f[0].u[d], tmp.data(), N * 8, cudaMemcpyHostToDevice,
-                                   h->stream));
-                CK(cudaStreamSynchronize(h->stream));
-            }
-    } else if (dev) {
-        r = mix_upload_device(h, n, Q, V);
-        if (r != MPCD_OK) {
-            h->n = 0;  // a rejected upload leaves no state
-            return r;
-        }
+        if (h->dc.dim == 3)
+            k_f64_from_aos<3><<<g, 256, 0, h->stream>>>(h->f[0], h->dc, n, x.Q, x.V, x.U, x.sp,
+                                                        x.err);
+        else
+            k_f64_from_aos<2><<<g, 256, 0, h->stream>>>(h->f[0], h->dc, n, x.Q, x.V, x.U, x.sp,
+                                                        x.err);
     } else {
-        r = mix_upload(h->mx[0], h->dc, n, Q, V, U, spid, h->stream);
-        if (r != MPCD_OK) return r;
+        k_mix_from_f64<<<g, 256, 0, h->stream>>>(h->mx[0], h->dc, n, x.Q, x.V, x.U, x.sp, x.err);
+    }
+    // global number density as globalDensities (init.c:1002-1018) unless
+    // given; phantom walls and the nematic activity use it
+    const bool density = !(h->cfg.gndnst > 0.0) && (h->dc.any_phantom || h->dc.lc);
+    if (density) {
+        k_pop_unshifted<<<g, 256, 0, h->stream>>>(h->dc, n, x.Q, h->count);
+        k_gndnst_reduce<<<grid_for(h, h->dc.ncells), 256, 0, h->stream>>>(h->dc, h->count,
+                                                                         x.sums);
+    }
+    CK(cudaGetLastError());
+    int herr[8];
+    CK(cudaMemcpyAsync(herr, x.err, 32, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (herr[0]) {
+        h->n = 0;  // a rejected upload leaves no state
+        return MPCD_ERR_ARG;
+    }
+    if (density) {
+        unsigned long long occ, sum;
+        memcpy(&occ, &herr[4], 8);
+        memcpy(&sum, &herr[6], 8);
+        h->dc.gndnst = occ > 0 ? (double)sum / (double)occ : 0.0;
     }
     return MPCD_OK;
 }
@@ -576,84 +554,68 @@ extern "C" int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *
                                              size_t stride, size_t off_Q, size_t off_V,
                                              size_t off_U, size_t off_spid) {
     if (!h || n < 0 || (n > 0 && !base) || stride == 0) return MPCD_ERR_ARG;
-    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n);
+    const bool has_U = off_U != (size_t)-1, has_sp = off_spid != (size_t)-1;
+    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n), U(has_U ? (size_t)3 * n : 0);
     std::vector<int> sp((size_t)n);
     const char *b = (const char *)base;
     for (int i = 0; i < n; i++) {
         const char *rec = b + (size_t)i * stride;
         memcpy(&Q[3 * (size_t)i], rec + off_Q, 3 * sizeof(double));
         memcpy(&V[3 * (size_t)i], rec + off_V, 3 * sizeof(double));
-        if (off_spid != (size_t)-1)
+        if (has_U) memcpy(&U[3 * (size_t)i], rec + off_U, 3 * sizeof(double));
+        if (has_sp)
             memcpy(&sp[i], rec + off_spid, sizeof(int));
         else
             sp[i] = 0;
     }
-    (void)off_U;
-    return mpcd_upload_state(h, n, Q.data(), V.data(), nullptr, sp.data());
+    return mpcd_upload_state(h, n, Q.data(), V.data(), has_U ? U.data() : nullptr, sp.data());
 }
 
 extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double *U) {
     if (!h) return MPCD_ERR_ARG;
-    int n = h->n, dim = h->dc.dim;
-    size_t N = (size_t)n;
+    const int n = h->n;
+    const size_t N = (size_t)n;
     if (n == 0) return MPCD_OK;
-    CK(cudaStreamSynchronize(h->stream));
+    Staging x;
+    int r = staging(h, N, U != nullptr, false, &x);
+    if (r != MPCD_OK) return r;
+    CK(cudaMemsetAsync(x.err, 0, sizeof(int), h->stream));
+    const int g = grid_for(h, n);
     if (h->prec == MPCD_PREC_FP64) {
-        std::vector<int> pid(N);
-        const Fp64State &st = h->f[h->cur];
-        CK(cudaMemcpy(pid.data(), st.pid, N * 4, cudaMemcpyDeviceToHost));
-        std::vector<double> tmp(N);
-        for (int d = 0; d < 3; d++) {
-            if (d < dim) {
-                if (Q) {
-                    CK(cudaMemcpy(tmp.data(), st.q[d], N * 8, cudaMemcpyDeviceToHost));
-                    for (size_t i = 0; i < N; i++) Q[3 * (size_t)pid[i] + d] = tmp[i];
-                }
-                if (V) {
-                    CK(cudaMemcpy(tmp.data(), st.v[d], N * 8, cudaMemcpyDeviceToHost));
-                    for (size_t i = 0; i < N; i++) V[3 * (size_t)pid[i] + d] = tmp[i];
-                }
-            } else {
-                for (size_t i = 0; i < N; i++) {
-                    if (Q) Q[3 * i + d] = 0.0;
-                    if (V) V[3 * i + d] = 0.0;
-                }
-            }
-        }
-        if (U) {
-            for (size_t i = 0; i < 3 * N; i++) U[i] = 0.0;
-            if (st.u[0])
-                for (int d = 0; d < 2; d++) {
-                    CK(cudaMemcpy(tmp.data(), st.u[d], N * 8, cudaMemcpyDeviceToHost));
-                    for (size_t i = 0; i < N; i++) U[3 * (size_t)pid[i] + d] = tmp[i];
-                }
-        }
-    } else if (mix_device_xfer(h) && (Q || V)) {
-        int r = mix_download_device(h, Q, V);
-        if (r != MPCD_OK) return r;
-        if (U)
-            for (size_t i = 0; i < 3 * N; i++) U[i] = 0.0;
+        if (h->dc.dim == 3)
+            k_f64_to_aos<3><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, x.Q, x.V, x.U, x.err);
+        else
+            k_f64_to_aos<2><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, x.Q, x.V, x.U, x.err);
     } else {
-        int r = mix_download(h->mx[h->cur], h->dc, n, Q, V, U);
-        if (r != MPCD_OK) return r;
+        k_mix_to_f64<<<g, 256, 0, h->stream>>>(h->mx[h->cur], h->dc, n, x.Q, x.V, x.U, x.err);
     }
-    return MPCD_OK;
+    CK(cudaGetLastError());
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, x.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (Q) CK(cudaMemcpyAsync(Q, x.Q, N * 24, cudaMemcpyDeviceToHost, h->stream));
+    if (V) CK(cudaMemcpyAsync(V, x.V, N * 24, cudaMemcpyDeviceToHost, h->stream));
+    if (U) CK(cudaMemcpyAsync(U, x.U, N * 24, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return herr ? MPCD_ERR_STATE : MPCD_OK;
 }
 
 extern "C" int mpcd_download_particles_strided(mpcd_handle *h, void *base, size_t stride,
                                                size_t off_Q, size_t off_V, size_t off_U) {
     if (!h || (h->n > 0 && !base) || stride == 0) return MPCD_ERR_ARG;
     int n = h->n;
-    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n);
-    int r = mpcd_download_state(h, Q.data(), V.data(), nullptr);
+    // orientations only where the state carries them (nematic order): an
+    // isotropic fluid's records keep whatever U the caller holds
+    const bool has_U = off_U != (size_t)-1 && h->dc.lc;
+    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n), U(has_U ? (size_t)3 * n : 0);
+    int r = mpcd_download_state(h, Q.data(), V.data(), has_U ? U.data() : nullptr);
     if (r != MPCD_OK) return r;
     char *b = (char *)base;
     for (int i = 0; i < n; i++) {
         char *rec = b + (size_t)i * stride;
         memcpy(rec + off_Q, &Q[3 * (size_t)i], 3 * sizeof(double));
         memcpy(rec + off_V, &V[3 * (size_t)i], 3 * sizeof(double));
+        if (has_U) memcpy(rec + off_U, &U[3 * (size_t)i], 3 * sizeof(double));
     }
-    (void)off_U;
     return MPCD_OK;
 }
 
@@ -857,8 +819,8 @@ static int run_step(mpcd_handle *h, typename T::State *st, uint32_t step) {
         sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0) & kShiftMask;
         sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0) & kShiftMask;
     }
-    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
-    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    double *acc_cur = acc_at(h, step);
+    double *acc_nxt = acc_at(h, step + 1u);
     int launches = 0;
     if (h->sorted_for != (int64_t)step) {
         launch_key<DIM, T>(h, st[h->cur], sa);
@@ -944,8 +906,8 @@ static int run_step_res(mpcd_handle *h, uint32_t step) {
     }
     const DevCfg &c = h->dc;
     const size_t nc = (size_t)c.ncells;
-    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
-    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    double *acc_cur = acc_at(h, step);
+    double *acc_nxt = acc_at(h, step + 1u);
     const ResPlanes sum_cur{(long long *)(h->rsum + (step & 1u) * nc), (int)nc};
     const ResPlanes sum_nxt{(long long *)(h->rsum + ((step + 1u) & 1u) * nc), (int)nc};
     unsigned long long *ms_cur = h->rmsum ? h->rmsum + (step & 1u) * nc : nullptr;
@@ -1021,8 +983,8 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
     host_shift(h, step + 1u, sa.sn);
     const DevCfg &c = h->dc;
     const size_t nc = (size_t)c.ncells;
-    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
-    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    double *acc_cur = acc_at(h, step);
+    double *acc_nxt = acc_at(h, step + 1u);
     auto sums_of = [&](uint32_t parity) {
         R64Sums r;
         double *b = h->r64sum + (size_t)(parity & 1u) * 4 * nc;
@@ -1043,17 +1005,18 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
         h->cur = 1 - h->cur;
         h->sort_age = 0;
     }
-    // one wave: the blocks of the particle pass that fit on the device at
-    // once (the kernel strides over the particles)
-    static int per_sm = 0;
-    if (per_sm == 0) {
+    // one wave: the blocks of the particle pass that fit on the handle's
+    // device at once (the kernel strides over the particles); the grid also
+    // fixes the order of the FP64 KE sums, so KE rounding depends on it
+    if (h->r64_per_sm == 0) {
         int b = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_r64_parts<DIM, RES_STEP>, 256,
                                                           0) != cudaSuccess || b < 1)
             b = 1;
-        per_sm = b;
+        h->r64_per_sm = b;
     }
-    const long long pwant = ((long long)h->n + 255) / 256, pcap = (long long)h->sm_count * per_sm;
+    const long long pwant = ((long long)h->n + 255) / 256,
+                    pcap = (long long)h->sm_count * h->r64_per_sm;
     const int pgrid = (int)(pwant < pcap ? pwant : pcap);
     if (h->sums_for != (int64_t)step) {
         CK(cudaMemsetAsync(h->r64sum, 0, sizeof(double) * 8 * nc, h->stream));
@@ -1097,8 +1060,8 @@ static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
         sa.ks[d] = (uint32_t)(sa.s[d] * 4294967296.0) & kShiftMask;
         sa.ksn[d] = (uint32_t)(sa.sn[d] * 4294967296.0) & kShiftMask;
     }
-    double *acc_cur = h->acc + (size_t)(step & 1u) * ACC_WORDS;
-    double *acc_nxt = h->acc + (size_t)((step + 1u) & 1u) * ACC_WORDS;
+    double *acc_cur = acc_at(h, step);
+    double *acc_nxt = acc_at(h, step + 1u);
     int launches = 0;
     if (h->sorted_for != (int64_t)step) {
         launch_key<2, T>(h, st[h->cur], sa);
@@ -1176,6 +1139,7 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
         if (r != MPCD_OK) return r;
         h->last_step = step;
         h->steps++;
+        h->stepped = true;
     }
     return MPCD_OK;
 }
@@ -1189,6 +1153,7 @@ extern "C" int mpcd_set_kernel(mpcd_handle *h, int kernel) {
 extern "C" int mpcd_set_sort_interval(mpcd_handle *h, int steps) {
     if (!h || steps < 1) return MPCD_ERR_ARG;
     h->sort_interval = steps;
+    h->sort_age = -1;  // a new cycle: the next step re-sorts
     return MPCD_OK;
 }
 
@@ -1205,7 +1170,7 @@ extern "C" int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particle
 
 extern "C" int mpcd_globals(mpcd_handle *h, double *kbtnow, double avnow[3]) {
     if (!h) return MPCD_ERR_ARG;
-    CK(cudaMemcpyAsync(h->host_acc, h->acc + (size_t)(h->last_step & 1u) * ACC_WORDS,
+    CK(cudaMemcpyAsync(h->host_acc, acc_at(h, h->last_step),
                        sizeof(double) * ACC_WORDS,
                        cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -1222,6 +1187,64 @@ extern "C" int mpcd_timestep(mpcd_handle *h, uint32_t runtime, double AVNOW[3],
     int r = mpcd_step(h, 1, runtime);
     if (r != MPCD_OK) return r;
     return mpcd_globals(h, KBTNOW, AVNOW);
+}
+
+extern "C" int mpcd_step_record(mpcd_handle *h, int nsteps, uint32_t step0, double *kbtnow,
+                                double *avnow) {
+    if (!h || nsteps < 0 || (nsteps > 0 && (!kbtnow || !avnow))) return MPCD_ERR_ARG;
+    if (h->n <= 0) return MPCD_ERR_STATE;
+    if (!h->host_ring &&
+        cudaMallocHost((void **)&h->host_ring, sizeof(double) * 2 * kRecordBatch * ACC_WORDS) !=
+            cudaSuccess)
+        return MPCD_ERR_NOMEM;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    for (auto &e : ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            for (auto &f : ev)
+                if (f) cudaEventDestroy(f);
+            return MPCD_ERR_CUDA;
+        }
+    const int dim = h->dc.dim;
+    const double inv_nd = 1.0 / (double)((long long)h->n * dim);
+    // the globals of batch b in host half b & 1, converted while batch b + 1
+    // runs on the GPU
+    auto convert = [&](int b, int cnt) {
+        CK(cudaEventSynchronize(ev[b & 1]));
+        const double *src = h->host_ring + (size_t)(b & 1) * kRecordBatch * ACC_WORDS;
+        for (int j = 0; j < cnt; j++) {
+            const size_t k = (size_t)b * kRecordBatch + (size_t)j;
+            kbtnow[k] = src[j * ACC_WORDS + ACC_KE] * inv_nd;
+            for (int d = 0; d < 3; d++)
+                avnow[3 * k + d] = d < dim ? src[j * ACC_WORDS + ACC_VCM + d] / h->dc.vol : 0.0;
+        }
+        return MPCD_OK;
+    };
+    int r = MPCD_OK;
+    const int nb = (nsteps + kRecordBatch - 1) / kRecordBatch;
+    for (int b = 0; b < nb && r == MPCD_OK; b++) {
+        const int cnt = std::min(kRecordBatch, nsteps - b * kRecordBatch);
+        const uint32_t s0 = step0 + (uint32_t)(b * kRecordBatch);
+        r = mpcd_step(h, cnt, s0);
+        if (r != MPCD_OK) break;
+        // the batch's ring slots, in at most two contiguous pieces
+        double *dst = h->host_ring + (size_t)(b & 1) * kRecordBatch * ACC_WORDS;
+        int done = 0;
+        while (done < cnt && r == MPCD_OK) {
+            const uint32_t slot = (s0 + (uint32_t)done) % (uint32_t)kAccRing;
+            const int piece = std::min(cnt - done, kAccRing - (int)slot);
+            if (cudaMemcpyAsync(dst + (size_t)done * ACC_WORDS, h->acc + (size_t)slot * ACC_WORDS,
+                                sizeof(double) * ACC_WORDS * piece, cudaMemcpyDeviceToHost,
+                                h->stream) != cudaSuccess)
+                r = MPCD_ERR_CUDA;
+            done += piece;
+        }
+        if (r == MPCD_OK && cudaEventRecord(ev[b & 1], h->stream) != cudaSuccess)
+            r = MPCD_ERR_CUDA;
+        if (r == MPCD_OK && b > 0) r = convert(b - 1, kRecordBatch);
+    }
+    if (r == MPCD_OK && nb > 0) r = convert(nb - 1, nsteps - (nb - 1) * kRecordBatch);
+    for (auto &e : ev) cudaEventDestroy(e);
+    return r;
 }
 
 extern "C" int mpcd_get_status(mpcd_handle *h, mpcd_status *st) {
@@ -1361,40 +1384,69 @@ extern "C" int mpcd_transverse_modes(mpcd_handle *h, double *out, int *nmodes) {
 extern "C" int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
                                double *cm) {
     if (!h) return MPCD_ERR_ARG;
-    // Re-bin on the unshifted grid on the host from the downloaded state (an
-    // output-step operation, off the timestep's hot path).
-    int n = h->n, dim = h->dc.dim, nc = h->dc.ncells;
-    std::vector<double> Q((size_t)3 * n), V((size_t)3 * n);
-    int r = mpcd_download_state(h, Q.data(), V.data(), nullptr);
+    // the re-bin on the unshifted grid and the per-cell moments, on the
+    // device; only the cell arrays come back
+    const int n = h->n, dim = h->dc.dim;
+    const size_t nc = (size_t)h->dc.ncells;
+    if (!h->props) CK(cudaMalloc((void **)&h->props, nc * (7 * sizeof(double) + sizeof(int))));
+    CellProps p;
+    p.mass = h->props;
+    p.sv = p.mass + nc;
+    p.sq = p.sv + 3 * nc;
+    p.pop = (int *)(p.sq + 3 * nc);
+    CK(cudaMemsetAsync(h->props, 0, nc * (7 * sizeof(double) + sizeof(int)), h->stream));
+    if (n > 0) {
+        const int g = grid_for(h, n);
+        if (h->prec == MPCD_PREC_FP64) {
+            if (dim == 3)
+                k_props_f64<3><<<g, 256, 0, h->stream>>>(h->dc, h->f[h->cur], n, p);
+            else
+                k_props_f64<2><<<g, 256, 0, h->stream>>>(h->dc, h->f[h->cur], n, p);
+        } else {
+            if (dim == 3)
+                k_props_mix<3><<<g, 256, 0, h->stream>>>(h->dc, h->mx[h->cur], n, p);
+            else
+                k_props_mix<2><<<g, 256, 0, h->stream>>>(h->dc, h->mx[h->cur], n, p);
+        }
+        k_props_finish<<<grid_for(h, (int)nc), 256, 0, h->stream>>>(h->dc, p);
+    }
+    CK(cudaGetLastError());
+    if (pop) CK(cudaMemcpyAsync(pop, p.pop, nc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (mass)
+        CK(cudaMemcpyAsync(mass, p.mass, nc * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (vcm)
+        CK(cudaMemcpyAsync(vcm, p.sv, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream));
+    if (cm)
+        CK(cudaMemcpyAsync(cm, p.sq, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_debug_cell_counts(mpcd_handle *h, int *pop) {
+    if (!h || !pop) return MPCD_ERR_ARG;
+    if (!h->stepped || h->n <= 0) return MPCD_ERR_STATE;
+    const int nc = h->dc.ncells;
+    const int64_t next = (int64_t)h->last_step + 1;
+    int r = xfer_reserve(h, (size_t)nc * sizeof(int) + 256);
     if (r != MPCD_OK) return r;
-    std::vector<int> p((size_t)nc, 0);
-    std::vector<double> m((size_t)nc, 0.0), sv((size_t)nc * 3, 0.0), sq((size_t)nc * 3, 0.0);
-    for (int i = 0; i < n; i++) {
-        int idx[3] = {0, 0, 0};
-        for (int d = 0; d < dim; d++) {
-            int a = (int)Q[3 * (size_t)i + d];
-            if (a < 0) a = 0;
-            if (a > h->dc.L[d]) a = h->dc.L[d];
-            idx[d] = a;
-        }
-        size_t k = ((size_t)idx[0] * h->dc.N1[1] + idx[1]) * h->dc.N1[2] + idx[2];
-        double ms = h->dc.mass[0];
-        p[k]++;
-        m[k] += ms;
-        for (int d = 0; d < dim; d++) {
-            sv[3 * k + d] += V[3 * (size_t)i + d] * ms;
-            sq[3 * k + d] += Q[3 * (size_t)i + d] * ms;
-        }
+    int *out = (int *)h->xfer;
+    const int g = grid_for(h, nc);
+    const size_t snc = (size_t)nc;
+    if (h->sums_for == next && h->rsum) {
+        const long long *plane = (const long long *)(h->rsum + (size_t)(next & 1) * snc) + 3 * snc;
+        k_counts_plane<<<g, 256, 0, h->stream>>>(plane, nc, out);
+    } else if (h->sums_for == next && h->r64sum) {
+        const double *M = h->r64sum + (size_t)(next & 1) * 4 * snc;
+        const int *cnt = h->dc.n_species > 1 ? h->r64pop + (size_t)(next & 1) * snc : nullptr;
+        k_counts_r64<<<g, 256, 0, h->stream>>>(M, cnt, h->dc.mass[0], nc, out);
+    } else if (h->sorted_for == next) {
+        k_counts_start<<<g, 256, 0, h->stream>>>(h->start[h->scur], nc, out);
+    } else {
+        return MPCD_ERR_STATE;
     }
-    for (int k = 0; k < nc; k++) {
-        if (pop) pop[k] = p[k];
-        if (mass) mass[k] = m[k];
-        for (int d = 0; d < 3; d++) {
-            double a = (d < dim && m[k] > 0.0) ? sv[3 * (size_t)k + d] / m[k] : 0.0;
-            double b = (d < dim && m[k] > 0.0) ? sq[3 * (size_t)k + d] / m[k] : 0.0;
-            if (vcm) vcm[3 * (size_t)k + d] = a;
-            if (cm) cm[3 * (size_t)k + d] = b;
-        }
-    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(pop, out, snc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return MPCD_OK;
 }

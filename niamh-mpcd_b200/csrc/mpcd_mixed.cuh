@@ -291,14 +291,16 @@ static __global__ void __launch_bounds__(256) k_gather_mix(MixState a, MixState 
 }
 
 // Device-side conversion to and from the packed representation, for
-// uploads and downloads of positions and velocities in the caller's FP64
-// layout (3 doubles per particle, original order).  A non-finite value or a
-// position outside the grid (upload), or an original index out of range
-// (download), counts in *err and leaves that particle unwritten.
+// uploads and downloads in the caller's FP64 layout (3 doubles per vector,
+// original particle order).  A non-finite value, a position outside the grid
+// or a species id out of range (upload), or an original index out of range
+// (download), counts in *err and leaves that particle unwritten.  Without U,
+// a nematic state starts every orientation at (1, 0).
 static __global__ void __launch_bounds__(256) k_mix_from_f64(MixState s,
                                                              const __grid_constant__ DevCfg c,
                                                              int n, const double *Q,
-                                                             const double *V, int *err) {
+                                                             const double *V, const double *U,
+                                                             const int *spid, int *err) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int ci[3] = {0, 0, 0};
         uint32_t f[3] = {0u, 0u, 0u};
@@ -312,6 +314,8 @@ static __global__ void __launch_bounds__(256) k_mix_from_f64(MixState s,
             fx_from_double(q, ci[d], f[d]);
             if (ci[d] < 0 || ci[d] > c.L[d]) ok = false;
         }
+        const int sp = spid ? spid[i] : 0;
+        if (sp < 0 || sp >= c.n_species) ok = false;
         if (!ok) {
             atomicAdd(err, 1);
             continue;
@@ -319,11 +323,16 @@ static __global__ void __launch_bounds__(256) k_mix_from_f64(MixState s,
         s.P[i] = pos_pack(ci, f);
         s.W[i] = make_float4((float)V[3 * (size_t)i], (float)V[3 * (size_t)i + 1],
                              c.dim == 3 ? (float)V[3 * (size_t)i + 2] : 0.f, __int_as_float(i));
+        if (s.sp) s.sp[i] = sp;
+        if (s.U)
+            s.U[i] = U ? make_float2((float)U[3 * (size_t)i], (float)U[3 * (size_t)i + 1])
+                       : make_float2(1.f, 0.f);
     }
 }
 static __global__ void __launch_bounds__(256) k_mix_to_f64(MixState s,
                                                            const __grid_constant__ DevCfg c,
-                                                           int n, double *Q, double *V, int *err) {
+                                                           int n, double *Q, double *V, double *U,
+                                                           int *err) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 w = s.W[i];
         const int pid = __float_as_int(w.w);
@@ -339,91 +348,13 @@ static __global__ void __launch_bounds__(256) k_mix_to_f64(MixState s,
             Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;
             V[3 * (size_t)pid + d] = d < c.dim ? (double)v[d] : 0.0;
         }
-    }
-}
-
-// Host-side conversion to and from the packed representation.
-static inline int mix_upload(MixState &s, const DevCfg &c, int n, const double *Q,
-                             const double *V, const double *Uo, const int *spid,
-                             cudaStream_t stream) {
-    std::vector<uint4> P((size_t)n);
-    std::vector<float4> W((size_t)n);
-    for (int i = 0; i < n; i++) {
-        int ci[3] = {0, 0, 0};
-        uint32_t f[3] = {0u, 0u, 0u};
-        for (int d = 0; d < c.dim; d++) {
-            fx_from_double(Q[3 * (size_t)i + d], ci[d], f[d]);
-            if (ci[d] < 0 || ci[d] > c.L[d]) return MPCD_ERR_ARG;
-        }
-        P[i] = pos_pack(ci, f);
-        W[i] = make_float4((float)V[3 * (size_t)i], (float)V[3 * (size_t)i + 1],
-                           c.dim == 3 ? (float)V[3 * (size_t)i + 2] : 0.f,
-                           __int_as_float_host(i));
-    }
-    if (cudaMemcpyAsync(s.P, P.data(), (size_t)n * sizeof(uint4), cudaMemcpyHostToDevice,
-                        stream) != cudaSuccess)
-        return MPCD_ERR_CUDA;
-    if (cudaMemcpyAsync(s.W, W.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice,
-                        stream) != cudaSuccess)
-        return MPCD_ERR_CUDA;
-    std::vector<float2> Uh;
-    if (s.U) {
-        Uh.resize((size_t)n);
-        for (int i = 0; i < n; i++)
-            Uh[i] = Uo ? make_float2((float)Uo[3 * (size_t)i], (float)Uo[3 * (size_t)i + 1])
-                       : make_float2(1.f, 0.f);
-        if (cudaMemcpyAsync(s.U, Uh.data(), (size_t)n * sizeof(float2), cudaMemcpyHostToDevice,
-                            stream) != cudaSuccess)
-            return MPCD_ERR_CUDA;
-    }
-    std::vector<int> sp;
-    if (s.sp) {
-        sp.resize((size_t)n);
-        for (int i = 0; i < n; i++) sp[i] = spid ? spid[i] : 0;
-        if (cudaMemcpyAsync(s.sp, sp.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice,
-                            stream) != cudaSuccess)
-            return MPCD_ERR_CUDA;
-    }
-    if (cudaStreamSynchronize(stream) != cudaSuccess) return MPCD_ERR_CUDA;
-    return MPCD_OK;
-}
-
-static inline int mix_download(const MixState &s, const DevCfg &c, int n, double *Q,
-                               double *V, double *Uo) {
-    std::vector<uint4> P((size_t)n);
-    std::vector<float4> W((size_t)n);
-    std::vector<float2> Uh;
-    if (s.U && Uo) {
-        Uh.resize((size_t)n);
-        if (cudaMemcpy(Uh.data(), s.U, (size_t)n * sizeof(float2), cudaMemcpyDeviceToHost) !=
-            cudaSuccess)
-            return MPCD_ERR_CUDA;
-    }
-    if (cudaMemcpy(P.data(), s.P, (size_t)n * sizeof(uint4), cudaMemcpyDeviceToHost) !=
-        cudaSuccess)
-        return MPCD_ERR_CUDA;
-    if (cudaMemcpy(W.data(), s.W, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost) !=
-        cudaSuccess)
-        return MPCD_ERR_CUDA;
-    for (int i = 0; i < n; i++) {
-        int pid = __float_as_int_host(W[i].w);
-        if (pid < 0 || pid >= n) return MPCD_ERR_STATE;
-        int ci[3];
-        uint32_t f[3];
-        pos_unpack(P[i], ci, f);
-        float v[3] = {W[i].x, W[i].y, W[i].z};
-        for (int d = 0; d < 3; d++) {
-            if (Q) Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;
-            if (V) V[3 * (size_t)pid + d] = d < c.dim ? (double)v[d] : 0.0;
-        }
-        if (Uo) {
-            bool has = !Uh.empty();
-            Uo[3 * (size_t)pid] = has ? (double)Uh[i].x : 0.0;
-            Uo[3 * (size_t)pid + 1] = has ? (double)Uh[i].y : 0.0;
-            Uo[3 * (size_t)pid + 2] = 0.0;
+        if (U) {
+            const float2 u = s.U ? s.U[i] : make_float2(0.f, 0.f);
+            U[3 * (size_t)pid] = (double)u.x;
+            U[3 * (size_t)pid + 1] = (double)u.y;
+            U[3 * (size_t)pid + 2] = 0.0;
         }
     }
-    return MPCD_OK;
 }
 
 }  // namespace mpcd

@@ -17,10 +17,12 @@
 // clears what must start at zero itself; two calls whose GPU work overlaps
 // (different streams, or host threads) race on the array and corrupt each
 // other's results, so a caller must serialise them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "mpcd_gpu.h"
 #include "mpcd_device.cuh"
@@ -67,21 +69,71 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_dev[kMaxDevices];  // device address of g_scratch per device
+// Device address of g_scratch, looked up once per CUDA context (the
+// host-side symbol is only a stand-in, not a device address).  The cache is
+// keyed by the context's unique id, so a device reset (which destroys the
+// primary context; the module can then load at another address) makes the
+// next call look the address up again.
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    unsigned char *ptr;
+};
+constexpr int kMaxContexts = 64;
+ScratchSlot g_slots[kMaxContexts];
+int g_nslots = 0;
+std::mutex g_slots_mu;
 
-// Device address of g_scratch on the current device, looked up once per
-// device (the host-side symbol is only a stand-in, not a device address).
+// Unique id of the current CUDA context, through the driver's
+// cuCtxGetCurrent and cuCtxGetId, fetched from the runtime so that the
+// library does not link the driver library itself.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+int current_context_id(unsigned long long *id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (CtxGetCurrentFn)p;
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)p;
+    });
+    if (!get_current || !get_id) return MPCD_ERR_CUDA;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS)
+        return MPCD_ERR_CUDA;
+    return MPCD_OK;
+}
+
 int scratch_address(unsigned char **out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MPCD_ERR_CUDA;
-    if (dev < 0 || dev >= kMaxDevices) return MPCD_ERR_UNSUPPORTED;
-    if (!g_scratch_dev[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return MPCD_ERR_CUDA;
-        g_scratch_dev[dev] = (unsigned char *)p;
+    // make the device's primary context current (it allocates nothing)
+    if (cudaSetDevice(dev) != cudaSuccess) return MPCD_ERR_CUDA;
+    unsigned long long id = 0;
+    if (current_context_id(&id) != MPCD_OK) return MPCD_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_slots_mu);
+    for (int i = 0; i < g_nslots; i++)
+        if (g_slots[i].ctx_id == id) {
+            *out = g_slots[i].ptr;
+            return MPCD_OK;
+        }
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return MPCD_ERR_CUDA;
+    // a full table drops its oldest entry (a process that has reset its
+    // devices more than kMaxContexts times)
+    if (g_nslots == kMaxContexts) {
+        for (int i = 1; i < kMaxContexts; i++) g_slots[i - 1] = g_slots[i];
+        g_nslots--;
     }
-    *out = g_scratch_dev[dev];
+    g_slots[g_nslots++] = ScratchSlot{id, (unsigned char *)p};
+    *out = (unsigned char *)p;
     return MPCD_OK;
 }
 
@@ -110,16 +162,27 @@ __global__ void __launch_bounds__(256) k_na_store(Fp64State b, int n, double *Q,
     }
 }
 
-__global__ void k_na_globals(const double *acc, int n, int dim, double vol, double *out) {
+// The step's global measures (KBTNOW, AVNOW) into the caller's globals,
+// and its error counters added to the caller's counters (either may be
+// null).
+__global__ void k_na_finish(const double *acc, const unsigned long long *status, int n,
+                            int dim, double vol, double *out, unsigned long long *counters) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
-        out[0] = n > 0 ? acc[ACC_KE] / (double)(n * dim) : 0.0;
-        for (int d = 0; d < 3; d++) out[1 + d] = d < dim ? acc[ACC_VCM + d] / vol : 0.0;
+        if (out) {
+            out[0] = n > 0 ? acc[ACC_KE] / (double)(n * dim) : 0.0;
+            for (int d = 0; d < 3; d++) out[1 + d] = d < dim ? acc[ACC_VCM + d] / vol : 0.0;
+        }
+        if (counters) {
+            counters[0] += status[ST_ESCAPED];
+            counters[1] += status[ST_BOUNCE];
+            counters[2] += status[ST_NONFINITE];
+        }
     }
 }
 
 template <int DIM>
 int noalloc_step(const DevCfg &c, int n, double *Q, double *V, uint32_t step, double *globals,
-                 cudaStream_t s, unsigned char *base) {
+                 unsigned long long *counters, cudaStream_t s, unsigned char *base) {
     Fp64State A, B;
     memset(&A, 0, sizeof(A));
     memset(&B, 0, sizeof(B));
@@ -183,20 +246,24 @@ int noalloc_step(const DevCfg &c, int n, double *Q, double *V, uint32_t step, do
     k_scan_apply<<<nscan, 256, 0, s>>>(count, nc, part, startB, fill, nullptr);
     k_srd_parts<DIM, F64T<DIM>, MODE_FINAL><<<gp, 256, 0, s>>>(c, B, A, n, crec, tb, sa);
     k_na_store<DIM><<<gp, 256, 0, s>>>(A, n, Q, V);
-    if (globals) k_na_globals<<<1, 32, 0, s>>>(acc, n, DIM, c.vol, globals);
+    if (globals || counters)
+        k_na_finish<<<1, 32, 0, s>>>(acc, status, n, DIM, c.vol, globals, counters);
     return cudaGetLastError() == cudaSuccess ? MPCD_OK : MPCD_ERR_CUDA;
 }
 
 }  // namespace
 
 extern "C" int mpcd_srd_step_noalloc(const mpcd_config *cfg, int n, double *Q, double *V,
-                                     uint32_t step, double *globals, void *stream) {
+                                     uint32_t step, double *globals,
+                                     unsigned long long *counters, void *stream) {
     if (!cfg || n < 0 || (n > 0 && (!Q || !V))) return MPCD_ERR_ARG;
     DevCfg c;
     int r = mpcd_build_devcfg(cfg, &c);
     if (r != MPCD_OK) return r;
-    // the SRD operator, FP64 state, no phantom walls, no nematic order
-    if (c.op != MPCD_COLL_ARBAXIS || c.any_phantom || c.lc || cfg->precision != MPCD_PREC_FP64)
+    // the SRD operator, FP64 state, one species (the caller passes no
+    // species ids), no phantom walls, no nematic order
+    if (c.op != MPCD_COLL_ARBAXIS || c.any_phantom || c.lc || c.n_species != 1 ||
+        cfg->precision != MPCD_PREC_FP64)
         return MPCD_ERR_UNSUPPORTED;
     if (n > kMaxParticles || c.ncells > kMaxCells) return MPCD_ERR_SIZE;
     if (!(cfg->gndnst > 0.0)) c.gndnst = 0.0;  // phantom-free: GnDNST unused
@@ -205,6 +272,6 @@ extern "C" int mpcd_srd_step_noalloc(const mpcd_config *cfg, int n, double *Q, d
     if (r != MPCD_OK) return r;
     if (n == 0) return MPCD_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    return c.dim == 3 ? noalloc_step<3>(c, n, Q, V, step, globals, s, base)
-                      : noalloc_step<2>(c, n, Q, V, step, globals, s, base);
+    return c.dim == 3 ? noalloc_step<3>(c, n, Q, V, step, globals, counters, s, base)
+                      : noalloc_step<2>(c, n, Q, V, step, globals, counters, s, base);
 }

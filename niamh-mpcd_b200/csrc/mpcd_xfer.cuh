@@ -1,0 +1,232 @@
+// mpcd_xfer.cuh -- device-side conversions between the caller's layout and
+// the handle's state, and the per-cell quantities read back for output.
+//
+//   k_f64_from_aos / k_f64_to_aos  the reference's particle arrays (3 doubles
+//        per vector, original particle order, SRDclss.h:34-44) to and from
+//        the FP64 form's structure of arrays, restoring the original order on
+//        the way back; the mixed form's counterparts are k_mix_from_f64 /
+//        k_mix_to_f64 (mpcd_mixed.cuh).
+//   k_pop_unshifted + k_gndnst_reduce  the initial binning on the unshifted
+//        grid and the global number density GnDNST (globalDensities,
+//        init.c:1002-1018): the mean population of the occupied cells of the
+//        L^D box (the extra layer excluded), as integer counts.
+//   k_props_*  the end-of-step re-bin on the unshifted grid and localPROP's
+//        POP, MASS, VCM and CM per cell (mpc.c:4936-4942, 64-216), which the
+//        reference's output writers read (pout.c:640-1757).
+//   k_counts_*  the populations of the cells of the next step's shifted grid
+//        exactly as the step's own kernels hold them (the sort's starts, the
+//        resident families' population sums), for parity checks.
+#pragma once
+
+#include "mpcd_fp64.cuh"
+#include "mpcd_mixed.cuh"
+
+namespace mpcd {
+
+// Caller arrays (AoS) -> FP64 state.  A non-finite position or velocity or
+// a species id out of range counts in *err and leaves that particle
+// unwritten (the upload is then rejected).  Without U, a nematic state
+// starts every orientation at (1, 0).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_f64_from_aos(Fp64State s, const __grid_constant__ DevCfg c,
+                                                      int n, const double *Q, const double *V,
+                                                      const double *U, const int *spid,
+                                                      int *err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        bool ok = true;
+        double q[3], v[3];
+        for (int d = 0; d < DIM; d++) {
+            q[d] = Q[3 * (size_t)i + d];
+            v[d] = V[3 * (size_t)i + d];
+            ok = ok && isfinite(q[d]) && isfinite(v[d]);
+        }
+        const int sp = spid ? spid[i] : 0;
+        if (sp < 0 || sp >= c.n_species) ok = false;
+        if (!ok) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        for (int d = 0; d < DIM; d++) {
+            s.q[d][i] = q[d];
+            s.v[d][i] = v[d];
+        }
+        s.pid[i] = i;
+        if (s.sp) s.sp[i] = sp;
+        if (s.u[0]) {
+            s.u[0][i] = U ? U[3 * (size_t)i] : 1.0;
+            s.u[1][i] = U ? U[3 * (size_t)i + 1] : 0.0;
+        }
+    }
+}
+
+// FP64 state -> caller arrays (AoS) in the original order; the components
+// beyond DIM are 0, and so is the orientation's third.  An original index
+// out of range counts in *err.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_f64_to_aos(Fp64State s, int n, double *Q, double *V,
+                                                    double *U, int *err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int p = s.pid[i];
+        if (p < 0 || p >= n) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        const size_t o = 3 * (size_t)p;
+        for (int d = 0; d < 3; d++) {
+            Q[o + d] = d < DIM ? s.q[d][i] : 0.0;
+            V[o + d] = d < DIM ? s.v[d][i] : 0.0;
+        }
+        if (U) {
+            U[o] = s.u[0] ? s.u[0][i] : 0.0;
+            U[o + 1] = s.u[0] ? s.u[1][i] : 0.0;
+            U[o + 2] = 0.0;
+        }
+    }
+}
+
+// Unshifted cell of a caller position (truncation, clamped to the grid, as
+// the initial binning that globalDensities reads), from the staged FP64
+// positions of an upload, counted into count[] (zero at rest).
+__global__ void __launch_bounds__(256) k_pop_unshifted(const __grid_constant__ DevCfg c, int n,
+                                                       const double *Q, int *count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int idx[3] = {0, 0, 0};
+        for (int d = 0; d < c.dim; d++) {
+            int a = (int)Q[3 * (size_t)i + d];
+            if (a < 0) a = 0;
+            if (a > c.L[d]) a = c.L[d];
+            idx[d] = a;
+        }
+        atomicAdd(&count[cell_lin(c, idx[0], idx[1], idx[2])], 1);
+    }
+}
+
+// Occupied cells of the L^D box and their particles (out[0], out[1]); the
+// counts are cleared again for the sort that shares them.
+__global__ void __launch_bounds__(256) k_gndnst_reduce(const __grid_constant__ DevCfg c,
+                                                       int *count, unsigned long long *out) {
+    __shared__ unsigned long long red[2][8];
+    unsigned long long occ = 0, sum = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.ncells; k += gridDim.x * blockDim.x) {
+        const int p = count[k];
+        count[k] = 0;
+        int a, b, z;
+        cell_coords(c, k, a, b, z);
+        if (a < c.L[0] && b < c.L[1] && z < c.L[2] && p > 0) {
+            occ += 1ull;
+            sum += (unsigned long long)p;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        occ += __shfl_xor_sync(0xffffffffu, occ, o);
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][w] = occ;
+        red[1][w] = sum;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        unsigned long long t = 0;
+        for (int j = 0; j < 8; j++) t += red[threadIdx.x][j];
+        atomicAdd(&out[threadIdx.x], t);
+    }
+}
+
+// Per-cell output properties on the unshifted grid: the accumulators.
+struct CellProps {
+    int *pop;
+    double *mass;  // [nc]
+    double *sv;    // [3 nc]: sum m v, then VCM
+    double *sq;    // [3 nc]: sum m Q, then CM
+};
+
+// One particle's contribution: its cell by truncation (clamped), as bin(...,
+// 0) (mpc.c:958-982, no periodic L -> 0 on the unshifted grid).
+template <int DIM>
+__device__ __forceinline__ void props_add(const DevCfg &c, CellProps p, const double q[3],
+                                          const double v[3], double m) {
+    int idx[3] = {0, 0, 0};
+    for (int d = 0; d < DIM; d++) {
+        int a = (int)q[d];
+        if (a < 0) a = 0;
+        if (a > c.L[d]) a = c.L[d];
+        idx[d] = a;
+    }
+    const int k = cell_lin(c, idx[0], idx[1], idx[2]);
+    atomicAdd(&p.pop[k], 1);
+    atomicAdd(&p.mass[k], m);
+    for (int d = 0; d < DIM; d++) {
+        atomicAdd(&p.sv[3 * (size_t)k + d], v[d] * m);
+        atomicAdd(&p.sq[3 * (size_t)k + d], q[d] * m);
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_props_f64(const __grid_constant__ DevCfg c, Fp64State s,
+                                                   int n, CellProps p) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double q[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+        for (int d = 0; d < DIM; d++) {
+            q[d] = s.q[d][i];
+            v[d] = s.v[d][i];
+        }
+        props_add<DIM>(c, p, q, v, c.mass[s.sp ? s.sp[i] : 0]);
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_props_mix(const __grid_constant__ DevCfg c, MixState s,
+                                                   int n, CellProps p) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int ci[3];
+        uint32_t f[3];
+        pos_unpack(s.P[i], ci, f);
+        const float4 w = s.W[i];
+        const float wv[3] = {w.x, w.y, w.z};
+        double q[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+        for (int d = 0; d < DIM; d++) {
+            // the position the download returns (exact in FP64)
+            q[d] = (double)ci[d] + (double)f[d] * kFxInv;
+            v[d] = (double)wv[d];
+        }
+        props_add<DIM>(c, p, q, v, c.mass[s.sp ? s.sp[i] : 0]);
+    }
+}
+
+// VCM = sum m v / M and CM = sum m Q / M in place (localPROP's divisions);
+// empty cells keep zeros.
+__global__ void __launch_bounds__(256) k_props_finish(const __grid_constant__ DevCfg c,
+                                                      CellProps p) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.ncells; k += gridDim.x * blockDim.x) {
+        const double M = p.mass[k];
+        if (!(M > 0.0)) continue;
+        for (int d = 0; d < c.dim; d++) {
+            p.sv[3 * (size_t)k + d] /= M;
+            p.sq[3 * (size_t)k + d] /= M;
+        }
+    }
+}
+
+// Populations of the cells of a step's shifted grid from the counting
+// sort's starts.
+__global__ void __launch_bounds__(256) k_counts_start(const int *start, int nc, int *out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x)
+        out[k] = start[k + 1] - start[k];
+}
+// ... from the mixed resident family's population plane (64-bit words).
+__global__ void __launch_bounds__(256) k_counts_plane(const long long *n_plane, int nc, int *out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x)
+        out[k] = (int)n_plane[k];
+}
+// ... from the FP64 resident family's sums: the counted populations
+// (several species), or, as its cell pass takes them with one species, the
+// mass sum over the mass.
+__global__ void __launch_bounds__(256) k_counts_r64(const double *M, const int *pop, double mass,
+                                                    int nc, int *out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x)
+        out[k] = pop ? pop[k] : (int)llrint(M[k] / mass);
+}
+
+}  // namespace mpcd

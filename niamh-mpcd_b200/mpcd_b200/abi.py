@@ -5,6 +5,8 @@ checks their sizes against the compiled library's own sizeof().
 """
 import ctypes as C
 
+ABI_VERSION = 3
+
 MAX_SPECIES = 10
 MAX_WALLS = 16
 

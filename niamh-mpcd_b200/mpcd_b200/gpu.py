@@ -21,7 +21,7 @@ EXPORTS = [
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
     "mpcd_set_sort_interval", "mpcd_set_timing", "mpcd_kernel_time",
-    "mpcd_transverse_modes",
+    "mpcd_transverse_modes", "mpcd_step_record", "mpcd_debug_cell_counts",
     "mpcd_srd_step_noalloc", "mpcd_batch_create", "mpcd_batch_destroy", "mpcd_batch_upload",
     "mpcd_batch_step", "mpcd_batch_download", "mpcd_batch_globals",
     "mpcd_batch_set_sort_interval", "mpcd_batch_set_stream", "mpcd_batch_info",
@@ -54,6 +54,8 @@ def load():
         lib.mpcd_timestep.argtypes = [vp, C.c_uint32, vp, vp]
         lib.mpcd_globals.argtypes = [vp, vp, vp]
         lib.mpcd_cell_props.argtypes = [vp, vp, vp, vp, vp]
+        lib.mpcd_step_record.argtypes = [vp, C.c_int, C.c_uint32, vp, vp]
+        lib.mpcd_debug_cell_counts.argtypes = [vp, vp]
         lib.mpcd_get_status.argtypes = [vp, vp]
         lib.mpcd_set_stream.argtypes = [vp, vp]
         lib.mpcd_launches_per_step.argtypes = [vp]
@@ -72,7 +74,7 @@ def load():
         lib.mpcd_batch_set_stream.argtypes = [vp, vp]
         lib.mpcd_batch_info.argtypes = [vp, vp, vp, vp]
         lib.mpcd_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]
-        lib.mpcd_srd_step_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_uint32, vp, vp]
+        lib.mpcd_srd_step_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_uint32, vp, vp, vp]
         _lib = lib
     return _lib
 
@@ -86,14 +88,20 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def srd_step_noalloc(cfg, n, q_dev_ptr, v_dev_ptr, step, globals_dev_ptr=None, stream=None):
+def srd_step_noalloc(cfg, n, q_dev_ptr, v_dev_ptr, step, globals_dev_ptr=None, stream=None,
+                     counters_dev_ptr=None):
     """One SRD timestep on caller-owned device arrays (AoS, 3 doubles per
-    particle) with no allocation (mpcd_srd_step_noalloc)."""
+    particle) with no allocation (mpcd_srd_step_noalloc).  counters_dev_ptr:
+    optional device array of 3 uint64 (escaped, bounce_limit, nonfinite) to
+    which the step adds its counts."""
     lib = load()
+
+    def vp(x):
+        return C.c_void_p(x) if x else None
+
     _check(lib.mpcd_srd_step_noalloc(C.byref(cfg), n, C.c_void_p(q_dev_ptr),
-                                     C.c_void_p(v_dev_ptr), step,
-                                     C.c_void_p(globals_dev_ptr) if globals_dev_ptr else None,
-                                     C.c_void_p(stream) if stream else None),
+                                     C.c_void_p(v_dev_ptr), step, vp(globals_dev_ptr),
+                                     vp(counters_dev_ptr), vp(stream)),
            "mpcd_srd_step_noalloc")
 
 
@@ -125,6 +133,23 @@ class Solver:
         kb = C.c_double()
         _check(self.lib.mpcd_timestep(self.h, runtime, _p(av), C.byref(kb)), "mpcd_timestep")
         return kb.value, av
+
+    def step_record(self, nsteps, step0):
+        """nsteps steps from step0 with every step's (KBTNOW, AVNOW)
+        (mpcd_step_record): arrays of shapes (nsteps,) and (nsteps, 3)."""
+        kb = np.zeros(nsteps)
+        av = np.zeros((nsteps, 3))
+        _check(self.lib.mpcd_step_record(self.h, nsteps, step0, _p(kb), _p(av)),
+               "mpcd_step_record")
+        return kb, av
+
+    def debug_cell_counts(self):
+        """Populations of the cells of the next step's shifted grid as the
+        device holds them (mpcd_debug_cell_counts), flat over (L+1)^D."""
+        nc = int(np.prod([int(self.cfg.L[d]) + 1 for d in range(3)]))
+        pop = np.zeros(nc, dtype=np.int32)
+        _check(self.lib.mpcd_debug_cell_counts(self.h, _p(pop)), "mpcd_debug_cell_counts")
+        return pop
 
     def globals(self):
         av = np.zeros(3)

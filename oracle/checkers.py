@@ -50,6 +50,7 @@ class Oracle:
             lib.oracle_ncells.argtypes = [C.c_void_p]
             lib.oracle_escaped.restype = C.c_long
             lib.oracle_escaped.argtypes = [C.c_void_p]
+            lib.oracle_shifted_counts.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
             cls._lib = lib
         return cls._lib
 
@@ -93,6 +94,14 @@ class Oracle:
 
     def gndnst(self):
         return self.lib().oracle_gndnst(self.h)
+
+    def shifted_counts(self, step):
+        """Populations of the cells of step `step`'s shifted grid from the
+        current positions (the cell lists that step collides)."""
+        nc = self.lib().oracle_ncells(self.h)
+        pop = np.zeros(nc, dtype=np.int32)
+        self.lib().oracle_shifted_counts(self.h, step, _p(pop))
+        return pop
 
     def escaped(self):
         return self.lib().oracle_escaped(self.h)

@@ -1014,3 +1014,28 @@ int oracle_get_cells(const oracle_t *o, int *pop, double *mass, double *vcm,
 }
 
 long oracle_escaped(const oracle_t *o) { return o->escaped; }
+
+/* Populations of the cells of step 'step's shifted grid from the current
+ * positions, without changing the state: the shift (ranshift,
+ * rand.c:678-696), gridShift_all's forward wrap (mpc.c:728-736) and bin's
+ * truncation, periodic L -> 0 and clamping (mpc.c:958-982) -- the cell lists
+ * the next oracle_step(o, step) collides. */
+int oracle_shifted_counts(const oracle_t *o, uint32_t step, int *pop) {
+    double s[3] = {0, 0, 0};
+    if (o->cfg.galinv) mpcd_rng_shift(o->cfg.seed, o->cfg.replica, step, o->dim, s);
+    memset(pop, 0, (size_t)o->ncells * sizeof(int));
+    for (int i = 0; i < o->n; i++) {
+        int idx[3] = {0, 0, 0};
+        for (int d = 0; d < o->dim; d++) {
+            double q = o->Q[3 * i + d] + s[d];
+            if (q > o->L[d] && q <= o->L[d] + s[d]) q -= o->L[d];
+            int a = (int)q;
+            if (o->pbc[d] && a == o->L[d]) a = 0;
+            if (a < 0) a = 0;
+            if (a > o->L[d]) a = o->L[d];
+            idx[d] = a;
+        }
+        pop[cell_index(o, idx[0], idx[1], idx[2])]++;
+    }
+    return 0;
+}

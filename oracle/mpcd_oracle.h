@@ -23,5 +23,6 @@ int oracle_get_cells(const oracle_t *o, int *pop, double *mass, double *vcm,
 double oracle_gndnst(const oracle_t *o);
 int oracle_ncells(const oracle_t *o);
 long oracle_escaped(const oracle_t *o);
+int oracle_shifted_counts(const oracle_t *o, uint32_t step, int *pop);
 
 #endif

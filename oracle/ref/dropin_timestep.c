@@ -23,8 +23,8 @@
  *               (mpc.c:4936-4958).
  *
  * Configurations outside the GPU path (MD coupling, swimmers, moving or
- * non-planar walls, thermostats, other collision operators, nematics) make
- * mpcd_create fail or are refused here, and so does a machine without a
+ * non-planar walls, thermostats, other collision operators, 3D or global
+ * nematic order) make mpcd_create fail or are refused here, and so does a machine without a
  * usable GPU; every call then goes to the reference's own timestep (found
  * with dlsym(RTLD_NEXT)), and the run is the reference's.
  *
@@ -131,13 +131,14 @@ static int fill_config(mpcd_config *c, inputList in, spec SP[], bc WALL[]) {
 
 static int setup(particleMPC *pp, spec SP[], bc WALL[], inputList in) {
     mpcd_config c;
-    /* options the GPU path does not carry: MD, swimmers, nematics, the
-     * thermostats, multiphase and incompressibility collisions, the
-     * no-hydrodynamics scramble, activity layers (mpc.c:4706-4760), and the
-     * periodic return to the rest frame that outputResults applies to the
-     * host particles (pout.c:2557) */
+    /* options the GPU path does not carry: MD, swimmers, the thermostats,
+     * multiphase and incompressibility collisions, the no-hydrodynamics
+     * scramble, activity layers (mpc.c:4706-4760), and the periodic return
+     * to the rest frame that outputResults applies to the host particles
+     * (pout.c:2557); nematic order other than the local 2D form makes
+     * mpcd_create fail */
     if (getenv("MPCD_DROPIN_OFF")) return 0;
-    if (MDmode || NS > 0 || in.LC != 0 || in.TSTECH != 0 || in.MULTIPHASE != MPHOFF ||
+    if (MDmode || NS > 0 || in.TSTECH != 0 || in.MULTIPHASE != MPHOFF ||
         in.inCOMP != INCOMPOFF || in.noHI == HIOFF || in.MFPLAYERH > 0 || in.RFRAME)
         return 0;
     if (!fill_config(&c, in, SP, WALL)) return 0;

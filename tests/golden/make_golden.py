@@ -5,7 +5,7 @@ the draw-injecting harness (oracle/ref/ref_harness.c), fed the seeded state of
 each case in tests/cases.py, and stepped; positions, velocities, the step's
 global measures and the cell populations after every step are stored.
 
-    make -C oracle/ref REF=/root/reference && python tests/golden/make_golden.py
+    make -C oracle/ref REF=$MPCD_REFERENCE_DIR && python tests/golden/make_golden.py
 """
 import os
 import sys

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     for name in declared_functions():
         assert name in exported, name
         assert hasattr(lib, name)
-    assert lib.mpcd_abi_version() == 2
+    assert lib.mpcd_abi_version() == abi.ABI_VERSION
 
 
 def test_struct_layout_matches_header():
