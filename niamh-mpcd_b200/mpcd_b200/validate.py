@@ -46,9 +46,19 @@ def theory_nu_reference(coll_op, dim, n, rot_ang=math.pi / 2, dt=0.1, kbt=1.0, m
     """Kinematic viscosity (kinetic, collisional) of theory_trans
     (init.c:800-942) for one species of mass m at number density n, a = 1:
     the correlation factors A, B of the operator (ARBAXIS, MPC-AT, MPC-AT+a),
-    then the kinetic and collisional dynamic viscosities divided by n m."""
+    then the kinetic and collisional dynamic viscosities divided by n m.
+
+    The factor M = n / (n - 1 + e^-n) of the operators without angular
+    momentum conservation is computed there with smrtPow(e, -n)
+    (mtools.c:38-50), whose integer-exponent branch multiplies x by itself
+    "y times" in a loop that does not run for a negative y, so it returns 1
+    for every integer density: M = 1 whenever n is a whole number.  That is
+    what the reference prints (synopsis.dat) and what this restatement
+    returns; theory_nu_srd3d gives the textbook value."""
     en = math.exp(-n)
-    Mf = n / (n - 1.0 + en)
+    # smrtPow(e, -n): 1 for an integer n (see above), e^-n otherwise
+    en_pow = 1.0 if float(n).is_integer() else en
+    Mf = n / (n - 1.0 + en_pow)
     if coll_op == abi.COLL_ARBAXIS:
         A = 2.0 / dim * (1.0 - math.sin(rot_ang) / rot_ang)
         if dim == 2:

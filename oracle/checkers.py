@@ -141,6 +141,9 @@ class Reference:
             lib.ref_get_cells.argtypes = [C.c_void_p] * 4
             lib.ref_gndnst.restype = C.c_double
             lib.ref_unexpected_draws.restype = C.c_long
+            lib.ref_theory_visc.restype = C.c_double
+            lib.ref_theory_visc.argtypes = [C.c_int, C.c_int] + [C.c_double] * 5 + \
+                [C.c_void_p, C.c_void_p]
             cls._libs[path] = lib
         return cls._libs[path]
 
@@ -154,6 +157,15 @@ class Reference:
         r = self._lib.ref_init(C.byref(cfg), self.n, _p(Q), _p(V), _p(U), _p(spid))
         if r != 0:
             raise RuntimeError("ref_init failed")
+
+    @classmethod
+    def theory_visc(cls, coll_op, dim, n, rot_ang, dt, kbt=1.0, m=1.0):
+        """The reference's own theory_trans (init.c:800-942): kinematic
+        viscosity, self-diffusion coefficient and mean free path."""
+        sd, mfp = C.c_double(), C.c_double()
+        nu = cls.lib().ref_theory_visc(coll_op, dim, n, rot_ang, dt, kbt, m, C.byref(sd),
+                                       C.byref(mfp))
+        return nu, sd.value, mfp.value
 
     def step(self, step):
         self._lib.ref_step(step)

@@ -248,6 +248,27 @@ int ref_init(const mpcd_config *cfg, int n, const double *Q, const double *V,
 }
 
 double ref_gndnst(void) { return GnDNST; }
+
+/* The reference's analytic transport coefficients, theory_trans
+ * (init.c:800-942), for one species of mass m at number density n in DIM
+ * dimensions: returns the kinematic viscosity VISC / (n m) (the value
+ * synopsis.dat prints), *sdiff the self-diffusion coefficient and *mfp the
+ * mean free path.  The globals it reads (DIM, GPOP) are set for the call
+ * and restored. */
+double ref_theory_visc(int rtech, int dim, double n, double ra, double dt, double kbt,
+                       double m, double *sdiff, double *mfp) {
+    double MFP = 0, VISC = 0, THERMD = 0, SDIFF = 0, SOS = 0;
+    const int dim0 = DIM, gpop0 = GPOP;
+    DIM = dim;
+    GPOP = 1000;
+    theory_trans(&MFP, &VISC, &THERMD, &SDIFF, &SOS, ra, 0.0, kbt, dt, m * (double)GPOP, rtech,
+                 n, n * m, 0, NULL);
+    DIM = dim0;
+    GPOP = gpop0;
+    if (sdiff) *sdiff = SDIFF;
+    if (mfp) *mfp = MFP;
+    return VISC / (n * m);
+}
 int ref_ncells(void) { return g_ncells; }
 long ref_unexpected_draws(void) { return g_unexpected; }
 

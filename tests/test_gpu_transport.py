@@ -20,7 +20,11 @@ def test_theory_restatement():
     assert col == pytest.approx((20.0 - 1.4) / 2.4 / 20.0, rel=1e-6)
     kin, col = V.theory_nu_reference(abi.COLL_ARBAXIS, 3, 10.0, math.radians(130.0))
     a = 2.0 / 3.0 * (1.0 - math.sin(math.radians(130.0)) / math.radians(130.0))
-    assert col == pytest.approx(a * (10.0 - 1.0 + math.exp(-10.0)) / 12.0 / 0.1 / 10.0, rel=1e-9)
+    # integer density: the reference's smrtPow(e, -n) is 1, so M = 1
+    assert col == pytest.approx(a / 12.0 / 0.1, rel=1e-9)
+    # a non-integer density takes e^-n
+    _, col = V.theory_nu_reference(abi.COLL_ARBAXIS, 3, 9.5, math.radians(130.0))
+    assert col == pytest.approx(a * (9.5 - 1.0 + math.exp(-9.5)) / 12.0 / 0.1 / 9.5, rel=1e-9)
 
 
 def test_channel_fit_recovers_viscosity():

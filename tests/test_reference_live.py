@@ -34,3 +34,25 @@ def test_oracle_tracks_reference(builder, kw, ppc):
     ko, ao = o.globals()
     kr, ar = r.globals()
     assert ko == pytest.approx(kr, rel=1e-12)
+
+
+@pytest.mark.parametrize("coll_op,dim,n,ra,dt", [
+    (abi.COLL_ARBAXIS, 3, 10.0, 2.2689280275926285, 0.1),
+    (abi.COLL_ARBAXIS, 2, 20.0, 1.5707963267948966, 0.1),
+    (abi.COLL_ARBAXIS, 3, 5.0, 1.0, 0.25),
+    (abi.COLL_ARBAXIS, 3, 9.5, 2.2689280275926285, 0.1),
+    (abi.COLL_MPCAT, 2, 12.25, 1.5707963267948966, 0.1),
+    (abi.COLL_MPCAT, 2, 20.0, 1.5707963267948966, 0.1),
+    (abi.COLL_MPCAT, 3, 10.0, 1.5707963267948966, 0.05),
+    (abi.COLL_RAT, 3, 20.0, 1.5707963267948966, 0.1),
+    (abi.COLL_RAT, 2, 20.0, 1.5707963267948966, 0.1),
+    (abi.COLL_RAT, 3, 7.5, 1.5707963267948966, 0.2),
+])
+def test_theory_restatement_matches_reference(coll_op, dim, n, ra, dt):
+    """The restated analytic viscosity (mpcd_b200.validate.theory_nu_reference)
+    against the compiled reference's own theory_trans."""
+    from mpcd_b200 import validate as V
+    kin, col = V.theory_nu_reference(coll_op, dim, n, ra, dt=dt)
+    nu, _, mfp = Reference.theory_visc(coll_op, dim, n, ra, dt)
+    assert kin + col == pytest.approx(nu, rel=1e-12)
+    assert mfp == pytest.approx(dt, rel=1e-15)
