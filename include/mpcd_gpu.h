@@ -279,12 +279,23 @@ int mpcd_set_strategy(mpcd_handle *h, int strategy, int tile_particles);
  *                      group in shared memory;
  *   MPCD_KERNEL_TILE   one block per tile of cells (the kernel every other
  *                      operator uses).
- * MPCD_KERNEL_AUTO picks RESIDENT where it applies and TILE elsewhere. */
+ * For every operator but the nematic ones, FP64 form:
+ *   MPCD_KERNEL_PERSIST one persistent cooperative launch (a block per SM at
+ *                      most) holds the whole box in its blocks' shared memory
+ *                      and runs all the steps of an mpcd_step call, the
+ *                      blocks meeting at a grid barrier twice per step; for
+ *                      small boxes, whose steps are otherwise bound by
+ *                      launch latency.  mpcd_step returns
+ *                      MPCD_ERR_UNSUPPORTED when the box does not fit.
+ * MPCD_KERNEL_AUTO picks PERSIST for FP64 boxes of at most two particles per
+ * thread of the launch (about 75,000 particles on a B200), RESIDENT for other
+ * SRD boxes without phantom walls, and TILE elsewhere. */
 #define MPCD_KERNEL_AUTO 0
 #define MPCD_KERNEL_TILE 1
 #define MPCD_KERNEL_GROUP 2
 #define MPCD_KERNEL_SPLIT 3
 #define MPCD_KERNEL_RESIDENT 4
+#define MPCD_KERNEL_PERSIST 5
 int mpcd_set_kernel(mpcd_handle *h, int kernel);
 
 /* MPCD_KERNEL_RESIDENT re-sorts the state by cell every 'steps' steps

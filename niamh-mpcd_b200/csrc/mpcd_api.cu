@@ -24,6 +24,7 @@
 #include "mpcd_resident64.cuh"
 #include "mpcd_lc.cuh"
 #include "mpcd_xfer.cuh"
+#include "mpcd_persist.cuh"
 
 using namespace mpcd;
 
@@ -59,6 +60,11 @@ struct mpcd_handle {
     bool stepped;        // a step ran since the last upload (mpcd_debug_cell_counts)
     double *props;       // mpcd_cell_props accumulators: 7 doubles + 1 int per cell
     double *host_ring;   // pinned: per-step globals of mpcd_step_record
+    int per_blocks;      // persistent family: blocks of the launch (0: not planned, -1: unfit)
+    int per_planned_n;   // particle count the plan was made for
+    int *per_pop;        // persistent family: populations of the next step's cells
+    void *per_work;      // persistent family: sums, populations, records, barrier counter
+    int64_t per_pop_for; // step whose cells per_pop counts; -1 none
     bool res_attr;       // the resident kernels' shared-memory attributes are set
     int r64_per_sm;      // resident blocks per SM of the FP64 particle pass (0: not yet known)
     void *xfer;          // device staging of FP64 uploads and downloads (mixed form)
@@ -291,6 +297,8 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->r64pop);
     cudaFree(h->lcbuf);
     cudaFree(h->props);
+    cudaFree(h->per_pop);
+    cudaFree(h->per_work);
     if (h->host_acc) cudaFreeHost(h->host_acc);
     if (h->host_ring) cudaFreeHost(h->host_ring);
     time_clear(h);
@@ -365,6 +373,7 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
     }
     h->sorted_for = -1;
     h->sums_for = -1;
+    h->per_pop_for = -1;
     h->sort_interval = 30;
     h->sort_age = -1;
     h->strategy = -1;
@@ -445,6 +454,7 @@ static int upload_common(mpcd_handle *h, int n) {
     h->sums_for = -1;
     h->sort_age = -1;
     h->stepped = false;
+    h->per_pop_for = -1;
     return MPCD_OK;
 }
 
@@ -678,13 +688,101 @@ static int launch_group(mpcd_handle *h, int mode, const typename T::State &a,
     return MPCD_OK;
 }
 
-static int kernel_family(const mpcd_handle *h) {
-    bool srd_plain = h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom && !h->dc.lc;
+// The persistent family's plan for the current state: blocks of the
+// cooperative launch (one per SM at most), or -1 if the box does not fit in
+// their shared memory (FP64 form, isotropic fluids only).  `wanted` is set
+// when the box is small enough for the family to be the default: at most
+// two particles per thread.
+static int per_plan(mpcd_handle *h, bool *wanted = nullptr) {
+    if (wanted) *wanted = false;
+    if (h->per_planned_n != h->n || h->per_blocks == 0) {
+        h->per_planned_n = h->n;
+        h->per_blocks = -1;
+        int coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device);
+        if (h->prec == MPCD_PREC_FP64 && !h->dc.lc && h->n > 0 && coop) {
+            bool fits = true;
+            for (int d = 0; d < 3; d++) fits = fits && h->dc.N1[d] <= 1024;
+            const int blocks =
+                std::max(1, std::min(h->sm_count, (h->n + kPerThreads - 1) / kPerThreads));
+            const PerLayout l = h->dc.dim == 3
+                                    ? per_layout<3>(h->n, h->dc.op, h->dc.n_species, blocks)
+                                    : per_layout<2>(h->n, h->dc.op, h->dc.n_species, blocks);
+            auto kfn = h->dc.dim == 3 ? k_persist<3> : k_persist<2>;
+            int per_sm = 0;
+            if (fits && l.bytes <= h->smem_optin &&
+                cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, l.bytes) ==
+                    cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kPerThreads,
+                                                              l.bytes) == cudaSuccess &&
+                per_sm >= 1)
+                h->per_blocks = blocks;
+            cudaGetLastError();
+        }
+    }
+    if (wanted && h->per_blocks > 0)
+        *wanted = (h->n + h->per_blocks - 1) / h->per_blocks <= 2 * kPerThreads;
+    return h->per_blocks;
+}
+
+static int kernel_family(mpcd_handle *h) {
+    if (h->dc.lc) return MPCD_KERNEL_TILE;
+    if (h->kernel == MPCD_KERNEL_PERSIST) return MPCD_KERNEL_PERSIST;
+    bool wanted = false;
+    if (h->kernel == MPCD_KERNEL_AUTO && h->prec == MPCD_PREC_FP64 && per_plan(h, &wanted) > 0 &&
+        wanted)
+        return MPCD_KERNEL_PERSIST;
+    bool srd_plain = h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom;
     if (!srd_plain) return MPCD_KERNEL_TILE;
-    const bool mixed = h->prec == MPCD_PREC_MIXED;
-    (void)mixed;
     if (h->kernel == MPCD_KERNEL_AUTO) return MPCD_KERNEL_RESIDENT;
     return h->kernel;
+}
+
+// nsteps steps of the persistent family: one cooperative launch that keeps
+// the whole box in its blocks' shared memory.
+template <int DIM>
+static int run_steps_per(mpcd_handle *h, int nsteps, uint32_t step0) {
+    const int blocks = per_plan(h);
+    if (blocks <= 0) return MPCD_ERR_UNSUPPORTED;
+    const PerLayout l = per_layout<DIM>(h->n, h->dc.op, h->dc.n_species, blocks);
+    const size_t nc = (size_t)h->dc.ncells;
+    // sums (the largest operator's rows), populations, records, record
+    // populations and the barrier counter
+    const size_t bytes = nc * (kPerRowsMax * 8 + 4 + kPerRecMax * 8 + 4) + 64;
+    if (!h->per_work) {
+        CK(cudaMalloc(&h->per_work, bytes));
+        CK(cudaMemsetAsync(h->per_work, 0, bytes, h->stream));
+    }
+    if (!h->per_pop) CK(cudaMalloc((void **)&h->per_pop, sizeof(int) * nc));
+    PerGlobal g;
+    g.sum = (double *)h->per_work;
+    g.rec = g.sum + kPerRowsMax * nc;
+    g.pop = (int *)(g.rec + kPerRecMax * nc);
+    g.rpop = g.pop + nc;
+    g.bar = (unsigned long long *)(((uintptr_t)(g.rpop + nc) + 15) & ~(uintptr_t)15);
+    g.ncells = (int)nc;
+    CK(cudaMemsetAsync(h->per_pop, 0, sizeof(int) * nc, h->stream));
+    CK(cudaMemsetAsync(g.bar, 0, sizeof(unsigned long long), h->stream));
+    // a launch that continues the previous one finds its first binning
+    // counted already
+    const int count_first = h->per_pop_for == (int64_t)step0 ? 0 : 1;
+    Fp64State st = h->f[h->cur];
+    int n = h->n, ring = kAccRing;
+    double *acc = h->acc;
+    int *pop = h->per_pop;
+    unsigned long long *status = h->status;
+    DevCfg dc = h->dc;
+    void *args[] = {&dc, &st, &n, (void *)&l, &g, &step0, &nsteps, &acc, &ring, &pop, &status,
+                    (void *)&count_first};
+    time_begin(h);
+    CK(cudaLaunchCooperativeKernel((void *)k_persist<DIM>, dim3((unsigned)blocks),
+                                   dim3((unsigned)kPerThreads), args, (size_t)l.bytes, h->stream));
+    time_end(h);
+    h->sorted_for = -1;
+    h->sums_for = -1;
+    h->per_pop_for = (int64_t)step0 + nsteps;
+    h->launches = 1;
+    return MPCD_OK;
 }
 
 template <int DIM, class T>
@@ -1120,6 +1218,15 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
     if (h->n <= 0) return MPCD_ERR_STATE;
     if (h->strategy < 0) h->strategy = default_strategy(h);
     if (h->tile_target <= 0) h->tile_target = h->prec == MPCD_PREC_MIXED ? 1024 : 768;
+    if (nsteps > 0 && !h->dc.lc && kernel_family(h) == MPCD_KERNEL_PERSIST) {
+        const int r = h->dc.dim == 3 ? run_steps_per<3>(h, nsteps, step0)
+                                     : run_steps_per<2>(h, nsteps, step0);
+        if (r != MPCD_OK) return r;
+        h->last_step = step0 + (uint32_t)(nsteps - 1);
+        h->steps += (uint64_t)nsteps;
+        h->stepped = true;
+        return MPCD_OK;
+    }
     for (int k = 0; k < nsteps; k++) {
         uint32_t step = step0 + (uint32_t)k;
         int r;
@@ -1145,7 +1252,7 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
 }
 
 extern "C" int mpcd_set_kernel(mpcd_handle *h, int kernel) {
-    if (!h || kernel < MPCD_KERNEL_AUTO || kernel > MPCD_KERNEL_RESIDENT) return MPCD_ERR_ARG;
+    if (!h || kernel < MPCD_KERNEL_AUTO || kernel > MPCD_KERNEL_PERSIST) return MPCD_ERR_ARG;
     h->kernel = kernel;
     return MPCD_OK;
 }
@@ -1440,6 +1547,9 @@ extern "C" int mpcd_debug_cell_counts(mpcd_handle *h, int *pop) {
         const double *M = h->r64sum + (size_t)(next & 1) * 4 * snc;
         const int *cnt = h->dc.n_species > 1 ? h->r64pop + (size_t)(next & 1) * snc : nullptr;
         k_counts_r64<<<g, 256, 0, h->stream>>>(M, cnt, h->dc.mass[0], nc, out);
+    } else if (h->per_pop_for == next && h->per_pop) {
+        CK(cudaMemcpyAsync(out, h->per_pop, snc * sizeof(int), cudaMemcpyDeviceToDevice,
+                           h->stream));
     } else if (h->sorted_for == next) {
         k_counts_start<<<g, 256, 0, h->stream>>>(h->start[h->scur], nc, out);
     } else {

@@ -24,6 +24,14 @@ __device__ __forceinline__ void pdl_trigger() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Prefetch of [p, p + bytes) from this GPU's global memory into L2
+// (cp.async.bulk.prefetch.L2, sm_90 and later): one instruction that takes no
+// registers or shared memory and has no completion to wait for.  p and bytes
+// must be multiples of 16.  A later load of the range finds it in L2.
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 static inline float __int_as_float_host(int i) {
     float f;
     std::memcpy(&f, &i, 4);

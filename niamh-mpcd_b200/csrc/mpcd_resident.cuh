@@ -98,6 +98,10 @@ constexpr int kResThreads = 256;
 constexpr int kResChunk = kResThreads * MPCD_RES_PPT;  // particles per block
 static_assert(kResChunk <= 2048, "limb sums are sized for at most 2048 particles");
 constexpr int kResProbe = 32;
+#ifndef MPCD_RES_BULK_PF
+#define MPCD_RES_BULK_PF 1  // bulk L2 prefetch of each block's particles
+#endif
+static_assert(kResChunk <= 8 * 256, "the prefetch covers eight 256-particle pieces");
 // Inside a block the fixed-point values are summed as two signed 32-bit
 // limbs, x = hi * 2^20 + lo with |lo| <= 2^19 (fx_limbs), so that the
 // shared-memory atomics are native 32-bit integer operations (64-bit and
@@ -479,6 +483,21 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     ResTable t;
     t.bind(res_smem, nc);
     pdl_trigger();
+#if MPCD_RES_BULK_PF
+    // The block's whole chunk of particle records is requested into L2 at
+    // once (16 bulk prefetches of 4 KB by warp 0), so that the loop's loads,
+    // one particle ahead of the arithmetic, wait for L2 rather than for
+    // DRAM.  A prefetch only moves lines into L2, which stays coherent with
+    // the kernel before this one still writing them.
+    if (tid < 16) {
+        const int j0 = blockIdx.x * kResChunk + (tid & 7) * 256;
+        const int cnt = min(256, n - j0);
+        if (cnt > 0) {
+            const void *src = tid < 8 ? (const void *)(a.P + j0) : (const void *)(a.W + j0);
+            prefetch_l2_bulk(src, (uint32_t)cnt * 16u);
+        }
+    }
+#endif
     {
         // keys to -1, everything after them to 0, in 16-byte stores (while
         // the kernel before this one may still be running)

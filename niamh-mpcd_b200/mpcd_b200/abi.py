@@ -35,6 +35,7 @@ KERNEL_TILE = 1
 KERNEL_GROUP = 2
 KERNEL_SPLIT = 3
 KERNEL_RESIDENT = 4
+KERNEL_PERSIST = 5
 
 STRATEGY_SCATTER = 0
 STRATEGY_RECOMPUTE = 1

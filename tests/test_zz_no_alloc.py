@@ -83,6 +83,7 @@ def test_noalloc_reports_escapes_to_the_callers_counters():
     dv = torch.tensor(V, dtype=torch.float64, device="cuda")
     cnt = torch.zeros(3, dtype=torch.int64, device="cuda")
     ref = Solver(cfg)
+    ref.set_kernel(abi.KERNEL_SPLIT)  # the kernels the allocation-free step runs
     ref.upload(Q, V, U, sp)
     ref.timestep(1)
     gpu.srd_step_noalloc(cfg, n, dq.data_ptr(), dv.data_ptr(), 1, None,
