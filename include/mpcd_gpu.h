@@ -305,6 +305,41 @@ int mpcd_set_kernel(mpcd_handle *h, int kernel);
 int mpcd_set_sort_interval(mpcd_handle *h, int steps);
 
 /* ---------------------------------------------------------------------
+ * Autotuner (no counterpart in the reference, which has one serial path).
+ * mpcd_autotune times the execution plans that apply to the handle's
+ * configuration on its current state -- kernel family, write-out strategy,
+ * tile size, re-sort interval -- for trial_steps steps each (0: 60) after 3
+ * warm-up steps, applies the fastest, and restores the state, error counters
+ * and step bookkeeping, so that the trajectory continues as if the call had
+ * not been made (its draws are keyed by the caller's step numbers).  With a
+ * cache_path (may be NULL) the choice is looked up first, by device name and
+ * workload (mpcd_tune_key), and stored after a tuning; a cached choice is
+ * applied without trials.  Every plan gives the same results to the form's
+ * rounding. */
+typedef struct mpcd_tune_choice {
+    int kernel;          /* MPCD_KERNEL_*                                    */
+    int strategy;        /* MPCD_STRATEGY_*, -1 for the default              */
+    int tile_particles;  /* particles per tile, 0 for the default            */
+    int sort_interval;   /* steps between re-sorts (resident families)       */
+    double us_per_step;  /* measured step time of the chosen plan            */
+    int from_cache;      /* 1: taken from the cache file without trials      */
+    int candidates;      /* plans timed (0 when taken from the cache)        */
+} mpcd_tune_choice;
+int mpcd_autotune(mpcd_handle *h, int trial_steps, const char *cache_path,
+                  mpcd_tune_choice *out);
+/* The cache key of a workload on a device (needs no GPU): device name, dim,
+ * box, particle count, operator, nematic switch, precision, walls, species,
+ * gravity.  MPCD_ERR_SIZE if it does not fit in len bytes. */
+int mpcd_tune_key(const mpcd_config *cfg, int n, const char *device, char *key,
+                  size_t len);
+/* Cache file access (needs no GPU): lookup returns 1 and fills *out if the
+ * key has an entry (the last one), 0 if not; store appends an entry. */
+int mpcd_tune_cache_lookup(const char *path, const char *key,
+                           mpcd_tune_choice *out);
+int mpcd_tune_cache_store(const char *path, const char *key,
+                          const mpcd_tune_choice *c);
+
+/* ---------------------------------------------------------------------
  * Ensembles: many independent periodic 3D SRD boxes of different sizes
  * stepped together (mixed precision).  No counterpart in the reference,
  * which runs one box per process.  Every kernel of a step runs once for the

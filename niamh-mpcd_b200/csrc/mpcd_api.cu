@@ -1560,3 +1560,182 @@ extern "C" int mpcd_debug_cell_counts(mpcd_handle *h, int *pop) {
     CK(cudaStreamSynchronize(h->stream));
     return MPCD_OK;
 }
+
+// The device arrays of state buffer b that a step reads and writes, with
+// their sizes for the current particle count.
+static void state_views(const mpcd_handle *h, int b, std::vector<std::pair<void *, size_t>> &v) {
+    const size_t N = (size_t)h->n;
+    v.clear();
+    if (h->prec == MPCD_PREC_FP64) {
+        const Fp64State &f = h->f[b];
+        for (int d = 0; d < h->dc.dim; d++) {
+            v.emplace_back(f.q[d], N * 8);
+            v.emplace_back(f.v[d], N * 8);
+        }
+        v.emplace_back(f.pid, N * 4);
+        if (f.sp) v.emplace_back(f.sp, N * 4);
+        for (int d = 0; d < 2; d++)
+            if (f.u[d]) v.emplace_back(f.u[d], N * 8);
+    } else {
+        const MixState &m = h->mx[b];
+        v.emplace_back(m.P, N * 16);
+        v.emplace_back(m.W, N * 16);
+        if (m.sp) v.emplace_back(m.sp, N * 4);
+        if (m.U) v.emplace_back(m.U, N * 8);
+    }
+}
+
+static void apply_choice(mpcd_handle *h, const mpcd_tune_choice &c) {
+    h->kernel = c.kernel;
+    h->strategy = c.strategy;
+    h->tile_target = c.tile_particles;
+    h->sort_interval = c.sort_interval > 0 ? c.sort_interval : 30;
+    h->sort_age = -1;
+}
+
+extern "C" int mpcd_autotune(mpcd_handle *h, int trial_steps, const char *cache_path,
+                             mpcd_tune_choice *out) {
+    if (!h || !out || trial_steps < 0) return MPCD_ERR_ARG;
+    if (h->n <= 0) return MPCD_ERR_STATE;
+    if (trial_steps == 0) trial_steps = 60;
+    memset(out, 0, sizeof(*out));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, h->device));
+    char key[512];
+    int r = mpcd_tune_key(&h->cfg, h->n, prop.name, key, sizeof(key));
+    if (r != MPCD_OK) return r;
+    if (cache_path && mpcd_tune_cache_lookup(cache_path, key, out) == 1) {
+        apply_choice(h, *out);
+        return MPCD_OK;
+    }
+    // the plans that apply to this configuration
+    std::vector<mpcd_tune_choice> cands;
+    auto add = [&](int kernel, int strategy, int tile, int sort) {
+        mpcd_tune_choice c;
+        memset(&c, 0, sizeof(c));
+        c.kernel = kernel;
+        c.strategy = strategy;
+        c.tile_particles = tile;
+        c.sort_interval = sort;
+        cands.push_back(c);
+    };
+    if (h->dc.lc) {
+        for (int t : {320, 640, 1280}) add(MPCD_KERNEL_TILE, -1, t, 30);
+    } else {
+        if (h->prec == MPCD_PREC_FP64 && per_plan(h) > 0) add(MPCD_KERNEL_PERSIST, -1, 0, 30);
+        if (h->dc.op == MPCD_COLL_ARBAXIS && !h->dc.any_phantom) {
+            for (int si : {10, 20, 30, 60}) add(MPCD_KERNEL_RESIDENT, -1, 0, si);
+            for (int st : {MPCD_STRATEGY_SCATTER, MPCD_STRATEGY_RECOMPUTE})
+                add(MPCD_KERNEL_SPLIT, st, 0, 30);
+        }
+        for (int t : {512, 1024, 2048})
+            for (int st : {MPCD_STRATEGY_SCATTER, MPCD_STRATEGY_RECOMPUTE})
+                add(MPCD_KERNEL_TILE, st, t, 30);
+        for (int st : {MPCD_STRATEGY_SCATTER, MPCD_STRATEGY_RECOMPUTE})
+            add(MPCD_KERNEL_GROUP, st, 0, 30);
+    }
+    // snapshot of the state, the error counters and the bookkeeping
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<std::pair<void *, size_t>> views;
+    state_views(h, h->cur, views);
+    size_t total = sizeof(unsigned long long) * ST_WORDS;
+    for (auto &vw : views) total += (vw.second + 255) / 256 * 256;
+    char *snap = nullptr;
+    if (cudaMalloc((void **)&snap, total) != cudaSuccess) return MPCD_ERR_NOMEM;
+    {
+        size_t o = 0;
+        for (auto &vw : views) {
+            CK(cudaMemcpyAsync(snap + o, vw.first, vw.second, cudaMemcpyDeviceToDevice, h->stream));
+            o += (vw.second + 255) / 256 * 256;
+        }
+        CK(cudaMemcpyAsync(snap + o, h->status, sizeof(unsigned long long) * ST_WORDS,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    }
+    const int kernel0 = h->kernel, strategy0 = h->strategy, tile0 = h->tile_target,
+              sort0 = h->sort_interval;
+    const uint64_t steps0 = h->steps;
+    const uint32_t last0 = h->last_step;
+    const bool stepped0 = h->stepped;
+    auto restore = [&]() -> int {
+        state_views(h, 0, views);
+        size_t o = 0;
+        for (auto &vw : views) {
+            if (cudaMemcpyAsync(vw.first, snap + o, vw.second, cudaMemcpyDeviceToDevice,
+                                h->stream) != cudaSuccess)
+                return MPCD_ERR_CUDA;
+            o += (vw.second + 255) / 256 * 256;
+        }
+        if (cudaMemcpyAsync(h->status, snap + o, sizeof(unsigned long long) * ST_WORDS,
+                            cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
+            return MPCD_ERR_CUDA;
+        h->cur = 0;
+        h->sorted_for = -1;
+        h->sums_for = -1;
+        h->sort_age = -1;
+        h->per_pop_for = -1;
+        h->steps = steps0;
+        h->last_step = last0;
+        h->stepped = stepped0;
+        return MPCD_OK;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const uint32_t base = last0 + 1u;
+    int best = -1, timed = 0;
+    float best_ms = 0.f;
+    for (size_t i = 0; i < cands.size() && r == MPCD_OK; i++) {
+        r = restore();
+        if (r != MPCD_OK) break;
+        apply_choice(h, cands[i]);
+        if (mpcd_step(h, 3, base) != MPCD_OK) {  // this plan does not apply: skip it
+            cudaGetLastError();
+            continue;
+        }
+        // the timed window starts with a re-sort and covers at least one
+        // interval, so each plan pays its re-sorts at (or above) their
+        // steady-state rate
+        const int steps = cands[i].kernel == MPCD_KERNEL_RESIDENT
+                              ? std::max(trial_steps, cands[i].sort_interval)
+                              : trial_steps;
+        h->sort_age = -1;
+        cudaEventRecord(e0, h->stream);
+        if (mpcd_step(h, steps, base + 3u) != MPCD_OK) {
+            cudaGetLastError();
+            cudaStreamSynchronize(h->stream);
+            continue;
+        }
+        cudaEventRecord(e1, h->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            r = MPCD_ERR_CUDA;
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)steps;
+        cands[i].us_per_step = 1e3 * (double)ms;
+        timed++;
+        if (best < 0 || ms < best_ms) {
+            best = (int)i;
+            best_ms = ms;
+        }
+    }
+    const int rr = restore();
+    if (r == MPCD_OK) r = rr;
+    if (r == MPCD_OK && cudaStreamSynchronize(h->stream) != cudaSuccess) r = MPCD_ERR_CUDA;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(snap);
+    if (r != MPCD_OK || best < 0) {
+        h->kernel = kernel0;
+        h->strategy = strategy0;
+        h->tile_target = tile0;
+        h->sort_interval = sort0;
+        return r != MPCD_OK ? r : MPCD_ERR_STATE;
+    }
+    *out = cands[best];
+    out->candidates = timed;
+    apply_choice(h, *out);
+    if (cache_path) mpcd_tune_cache_store(cache_path, key, out);
+    return MPCD_OK;
+}

@@ -112,6 +112,18 @@ class Config(C.Structure):
     ]
 
 
+class TuneChoice(C.Structure):
+    _fields_ = [
+        ("kernel", C.c_int),
+        ("strategy", C.c_int),
+        ("tile_particles", C.c_int),
+        ("sort_interval", C.c_int),
+        ("us_per_step", C.c_double),
+        ("from_cache", C.c_int),
+        ("candidates", C.c_int),
+    ]
+
+
 class Status(C.Structure):
     _fields_ = [
         ("steps", C.c_uint64),

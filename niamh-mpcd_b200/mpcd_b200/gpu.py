@@ -22,6 +22,7 @@ EXPORTS = [
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
     "mpcd_set_sort_interval", "mpcd_set_timing", "mpcd_kernel_time",
     "mpcd_transverse_modes", "mpcd_step_record", "mpcd_debug_cell_counts",
+    "mpcd_autotune", "mpcd_tune_key", "mpcd_tune_cache_lookup", "mpcd_tune_cache_store",
     "mpcd_srd_step_noalloc", "mpcd_batch_create", "mpcd_batch_destroy", "mpcd_batch_upload",
     "mpcd_batch_step", "mpcd_batch_download", "mpcd_batch_globals",
     "mpcd_batch_set_sort_interval", "mpcd_batch_set_stream", "mpcd_batch_info",
@@ -56,6 +57,10 @@ def load():
         lib.mpcd_cell_props.argtypes = [vp, vp, vp, vp, vp]
         lib.mpcd_step_record.argtypes = [vp, C.c_int, C.c_uint32, vp, vp]
         lib.mpcd_debug_cell_counts.argtypes = [vp, vp]
+        lib.mpcd_autotune.argtypes = [vp, C.c_int, C.c_char_p, vp]
+        lib.mpcd_tune_key.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_size_t]
+        lib.mpcd_tune_cache_lookup.argtypes = [C.c_char_p, C.c_char_p, vp]
+        lib.mpcd_tune_cache_store.argtypes = [C.c_char_p, C.c_char_p, vp]
         lib.mpcd_get_status.argtypes = [vp, vp]
         lib.mpcd_set_stream.argtypes = [vp, vp]
         lib.mpcd_launches_per_step.argtypes = [vp]
@@ -86,6 +91,30 @@ def _check(r, what):
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def tune_key(cfg, n, device):
+    """The autotuner's cache key of a workload on a device (no GPU needed)."""
+    lib = load()
+    buf = C.create_string_buffer(512)
+    _check(lib.mpcd_tune_key(C.byref(cfg), n, device.encode(), buf, 512), "mpcd_tune_key")
+    return buf.value.decode()
+
+
+def tune_cache_lookup(path, key):
+    """The cached choice for key (abi.TuneChoice) or None (no GPU needed)."""
+    lib = load()
+    c = abi.TuneChoice()
+    r = lib.mpcd_tune_cache_lookup(str(path).encode(), key.encode(), C.byref(c))
+    if r < 0:
+        _check(r, "mpcd_tune_cache_lookup")
+    return c if r == 1 else None
+
+
+def tune_cache_store(path, key, choice):
+    lib = load()
+    _check(lib.mpcd_tune_cache_store(str(path).encode(), key.encode(), C.byref(choice)),
+           "mpcd_tune_cache_store")
 
 
 def srd_step_noalloc(cfg, n, q_dev_ptr, v_dev_ptr, step, globals_dev_ptr=None, stream=None,
@@ -227,6 +256,15 @@ class Solver:
 
     def set_sort_interval(self, steps):
         _check(self.lib.mpcd_set_sort_interval(self.h, steps), "mpcd_set_sort_interval")
+
+    def autotune(self, trial_steps=0, cache_path=None):
+        """Time the applicable execution plans and apply the fastest
+        (mpcd_autotune); returns the abi.TuneChoice."""
+        c = abi.TuneChoice()
+        _check(self.lib.mpcd_autotune(self.h, trial_steps,
+                                      None if cache_path is None else str(cache_path).encode(),
+                                      C.byref(c)), "mpcd_autotune")
+        return c
 
     def set_stream(self, stream_ptr):
         _check(self.lib.mpcd_set_stream(self.h, C.c_void_p(stream_ptr)), "mpcd_set_stream")
