@@ -188,6 +188,7 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     for (int s = 0; s < cfg->n_species; s++) {
         if (!(cfg->species[s].mass > 0.0)) return MPCD_ERR_ARG;
         dc->mass[s] = cfg->species[s].mass;
+        dc->sig[s] = std::sqrt(cfg->kbt / cfg->species[s].mass);
         dc->damp[s] = cfg->species[s].damp;
         dc->rfc[s] = cfg->species[s].rfc;
         dc->tumble[s] = cfg->species[s].tumble;

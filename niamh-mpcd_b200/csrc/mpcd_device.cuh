@@ -78,6 +78,7 @@ struct DevCfg {
     double cosA, sinA;  // cos(RA) and the sine with the reference's sign (-sin RA)
     double grav[3];
     double mass[MPCD_MAX_SPECIES], damp[MPCD_MAX_SPECIES];
+    double sig[MPCD_MAX_SPECIES];  // sqrt(kbt / mass): the thermal draw's width
     double rfc[MPCD_MAX_SPECIES], tumble[MPCD_MAX_SPECIES], chihi[MPCD_MAX_SPECIES];
     double act[MPCD_MAX_SPECIES], mfpot[MPCD_MAX_SPECIES], sigwidth[MPCD_MAX_SPECIES];
     double sigpos[MPCD_MAX_SPECIES], minactratio[MPCD_MAX_SPECIES];
@@ -285,19 +286,25 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
 
 // Is the (shifted-grid) cell (a,b,z) cut by a phantom wall at its shifted
 // position?  Corner test of ghostPart, mpc.c:380-470.
+// The walls are axis-aligned planes (one non-zero component of A), so the
+// other axes' terms of W are 0 * (q - Q) = 0 for every corner: the corner
+// test reduces to the two corner coordinates along the wall's axis, with the
+// same arithmetic for the remaining term.
 template <int DIM>
 __device__ bool cell_cut_by_phantom(const DevCfg &c, int a, int b, int z,
                                     const double *s) {
-    const int nc = 1 << DIM;
+    const int cc[3] = {a, b, z};
     for (int w = 0; w < c.n_walls; w++) {
         const DevWall &wl = c.walls[w];
         if (!wl.phantom) continue;
-        double wq[3];
-        for (int d = 0; d < 3; d++) wq[d] = wl.Q[d] + (d < DIM ? s[d] : 0.0);
-        for (int j = 0; j < nc; j++) {
-            double q[3] = {(double)a + (double)(j & 1), (double)b + (double)((j >> 1) & 1),
-                           (double)z + (double)((j >> 2) & 1)};
-            if (wall_W(wl, q, wq, DIM) < 0.0) return true;
+        const int ax = wl.axis;
+        const double wq = wl.Q[ax] + (ax < DIM ? s[ax] : 0.0);
+        for (int j = 0; j < 2; j++) {
+            double W = 0.0;
+            W += wl.A[ax] * (((double)cc[ax] + (double)j) - wq);
+            W -= wl.R;
+            if (wl.inv) W *= -1.0;
+            if (W < 0.0) return true;
         }
     }
     return false;
@@ -362,7 +369,7 @@ __device__ __forceinline__ void cross3(const double *x, const double *y,
 template <int DIM>
 __device__ __forceinline__ void thermal(const DevCfg &c, uint32_t step,
                                         uint32_t pid, int sp, double *rv) {
-    double sig = sqrt(c.kbt / c.mass[sp]);
+    const double sig = c.sig[sp];  // sqrt(kbt / mass), correctly rounded on the host
     float g[2];
     mpcd_rng_normal2(c.seed, c.replica, step, MPCD_STREAM_THERMAL, pid, 0u, g);
     rv[0] = sig * (double)g[0];

@@ -596,7 +596,13 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             }
             int k = T::finish(c, r, sp, sa, bounce, esc);
             const int gi = p0 + j;
-            if (MODE == MODE_INPLACE) {
+            if (MODE == MODE_INPLACE && andersen) {
+                // the rank is fetched after the loop, several at once (the
+                // particle's thermal-velocity slots are free by now)
+                T::store(a, gi, r);
+                tb.key[gi] = k;
+                *(int *)(s_rv + 3 * j) = k;
+            } else if (MODE == MODE_INPLACE) {
                 T::store(a, gi, r);
                 tb.key[gi] = k;
                 tb.rank[gi] = atomicAdd(&tb.count_next[k], 1);
@@ -606,6 +612,24 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                 int dst = tb.start_next[k] + atomicAdd(&tb.fill[k], 1);
                 T::store(b, dst, r);
                 T::store_sp(b, dst, sp);
+            }
+        }
+        if (MODE == MODE_INPLACE && andersen) {
+            // the ranks in the next step's cells, four atomics in flight at
+            // a time (each thread fetches those of its own particles)
+            for (int j0 = tid; j0 < np; j0 += 4 * nth) {
+                int kk[4], rk[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int j = j0 + u * nth;
+                    kk[u] = j < np ? *(const int *)(s_rv + 3 * j) : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    rk[u] = j0 + u * nth < np ? atomicAdd(&tb.count_next[kk[u]], 1) : 0;
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (j0 + u * nth < np) tb.rank[p0 + j0 + u * nth] = rk[u];
             }
         }
         __syncthreads();
