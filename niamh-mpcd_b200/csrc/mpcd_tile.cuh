@@ -17,8 +17,10 @@
 //   COUNT    write nothing, only count the next keys;
 //   FINAL    recompute and write each particle straight to its slot of the
 //            next step's order (needs the scan of COUNT's histogram).
-// INPLACE+scatter moves 144 B/particle (mixed), COUNT+FINAL 96 B; the
-// autotuner picks per configuration.
+// INPLACE+scatter moves 144 B/particle (mixed), COUNT+FINAL 96 B, at twice
+// the arithmetic.  The default is COUNT+FINAL for SRD and INPLACE+scatter for
+// the Andersen operators; mpcd_autotune times both (and the tile sizes) on the
+// live state and applies the faster.
 #pragma once
 
 #include "mpcd_device.cuh"

@@ -82,13 +82,22 @@ def theory_nu_reference(coll_op, dim, n, rot_ang=math.pi / 2, dt=0.1, kbt=1.0, m
 
 
 def channel_viscosity(L=(32, 32, 16), ppc=20, g=5e-4, warm=12000, steps=24000, every=10,
-                      precision=abi.PREC_MIXED, seed=21, edge=2, nblk=8):
+                      precision=abi.PREC_MIXED, seed=21, edge=2, nblk=8, start="rest"):
     """Kinematic viscosity from the steady profile of the MPC-AT+a channel
     (phantom no-slip walls at y = 0 and y = L1, periodic x and z, body force
     g along x): mass-weighted x velocity per y layer, averaged over time,
-    fitted by a parabola over the layers at least `edge` cells from a wall."""
+    fitted by a parabola over the layers at least `edge` cells from a wall.
+    start="parabola" starts the flow from the steady profile of the analytic
+    viscosity (theory_trans) instead of rest, so that a run much shorter than
+    the channel's momentum diffusion time H^2 / (pi^2 nu) samples the steady
+    state."""
     cfg = W.cfg_channel3d(tuple(L), g=g, precision=precision, seed=seed)
     Q, V, U, sp = W.synthetic_state(cfg, ppc, seed=seed + 1)
+    Q[:, 1] = 0.02 + Q[:, 1] * (L[1] - 0.04) / L[1]  # off the walls' planes
+    if start == "parabola":
+        kin, col = theory_nu_reference(abi.COLL_RAT, 3, float(ppc))
+        H = float(L[1])
+        V[:, 0] += g * Q[:, 1] * (H - Q[:, 1]) / (2.0 * (kin + col))
     s = Solver(cfg)
     s.upload(Q, V, U, sp)
     s.step(warm, 1)
@@ -188,7 +197,76 @@ def measure_viscosity(L=32, ppc=10, steps=40000, every=10, precision=abi.PREC_MI
             "precision": "fp64" if precision == abi.PREC_FP64 else "mixed"}
 
 
+def fit_decay(t, s, noise, snr_min=10.0):
+    """Decay rate of a signal s(t) = s0 exp(-rate t) + noise: a straight line
+    through ln s over the samples (from the first) where s is still above
+    snr_min times the noise; returns the rate and the number of samples
+    used."""
+    ok = s > snr_min * noise
+    last = int(np.argmin(ok)) if not ok.all() else len(s)
+    use = np.arange(max(last, 3))
+    slope, _ = np.polyfit(t[use], np.log(np.abs(s[use])), 1)
+    return -slope, len(use)
+
+
+def shear_wave_viscosity(L=64, ppc=10, amp=0.1, nrep=16, steps=2400, every=20,
+                         precisions=(abi.PREC_FP64, abi.PREC_MIXED), seed=100):
+    """Kinematic viscosity of the 3D SRD fluid (130 degrees, dt 0.1) from the
+    decay of an imposed transverse shear wave: v_x += amp sin(k y), k =
+    2 pi / L, on the thermal state, whose mode j = sum v_x exp(-i k y)
+    (mpcd_transverse_modes, pair a = x, b = y) relaxes as exp(-nu k^2 t) --
+    the decay of a transverse momentum fluctuation that the autocorrelation
+    C(k, t) measures, driven far above the thermal noise.  nrep replicas
+    (independent states and draws), each stepped in every given form from the
+    same state with the same draws, so that the forms' difference is paired.
+    Returns per form the mean nu and its standard error, and the paired
+    differences to the first form."""
+    k = 2.0 * math.pi / L
+    nus = {p: [] for p in precisions}
+    for r in range(nrep):
+        for p in precisions:
+            cfg = W.cfg_srd3d((L, L, L), precision=p, seed=seed + 7 * r)
+            Q, V, U, sp = W.synthetic_state(cfg, ppc, seed=seed + 7 * r + 1)
+            V[:, 0] += amp * np.sin(k * Q[:, 1])
+            V[:, 0] -= V[:, 0].mean()
+            n = len(Q)
+            noise = math.sqrt(n * cfg.kbt / 2.0)
+            g = Solver(cfg)
+            g.upload(Q, V, U, sp)
+            sig = [-g.transverse_modes()[2].imag]
+            for s in range(0, steps, every):
+                g.step(every, 1 + s)
+                sig.append(-g.transverse_modes()[2].imag)
+            g.close()
+            t = np.arange(len(sig)) * every * cfg.dt
+            rate, _ = fit_decay(t, np.array(sig), noise)
+            nus[p].append(rate / (k * k))
+    out = {"L": L, "ppc": ppc, "amp": amp, "replicas": nrep, "steps": steps, "every": every}
+    base = np.array(nus[precisions[0]])
+    for p in precisions:
+        a = np.array(nus[p])
+        name = "fp64" if p == abi.PREC_FP64 else "mixed"
+        out[name] = {"nu": float(a.mean()), "nu_err": float(a.std(ddof=1) / math.sqrt(len(a)))}
+        if p != precisions[0]:
+            d = a / base - 1.0
+            out[name]["rel_diff_to_" + ("fp64" if precisions[0] == abi.PREC_FP64 else "mixed")] = \
+                {"mean": float(d.mean()), "err": float(d.std(ddof=1) / math.sqrt(len(d)))}
+    kin, col = theory_nu_srd3d(ppc, math.radians(130.0), 0.1)
+    out["theory_textbook"] = kin + col
+    rk, rc = theory_nu_reference(abi.COLL_ARBAXIS, 3, float(ppc), math.radians(130.0), 0.1)
+    out["theory_reference_synopsis"] = rk + rc
+    return out
+
+
 def main():
+    """Command line of the transport checks:
+      --shear                 64^3 SRD viscosity from the shear-wave decay,
+                              FP64 and mixed paired (--reps, --amp)
+      --channel [--full]      MPC-AT+a channel viscosity from the steady
+                              profile (--full: configuration 3, 128x64x64,
+                              g = 1e-4, started from the parabola)
+      (neither)               SRD viscosity from the transverse-momentum
+                              autocorrelation of an equilibrium run."""
     ap = argparse.ArgumentParser()
     ap.add_argument("--L", type=int, default=32)
     ap.add_argument("--steps", type=int, default=40000)
@@ -196,12 +274,26 @@ def main():
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--channel", action="store_true",
                     help="Poiseuille channel (MPC-AT+a, phantom walls) instead of SRD modes")
+    ap.add_argument("--full", action="store_true",
+                    help="channel of configuration 3: 128x64x64, g = 1e-4, parabola start")
+    ap.add_argument("--shear", action="store_true",
+                    help="64^3 SRD viscosity from the decay of an imposed shear wave")
+    ap.add_argument("--reps", type=int, default=32)
+    ap.add_argument("--amp", type=float, default=0.25)
     ap.add_argument("--warm", type=int, default=12000)
     args = ap.parse_args()
     prec = abi.PREC_MIXED if args.form == "mixed" else abi.PREC_FP64
+    if args.shear:
+        print(json.dumps(shear_wave_viscosity(L=64, nrep=args.reps, amp=args.amp)))
+        return
     if args.channel:
-        res = channel_viscosity(warm=args.warm, steps=args.steps if args.steps != 40000 else 24000,
-                                every=args.every, precision=prec)
+        if args.full:
+            res = channel_viscosity(L=(128, 64, 64), ppc=20, g=1e-4, warm=20000, steps=40000,
+                                    every=200, precision=prec, edge=3, start="parabola")
+        else:
+            res = channel_viscosity(warm=args.warm,
+                                    steps=args.steps if args.steps != 40000 else 24000,
+                                    every=args.every, precision=prec)
         kin, col = theory_nu_reference(abi.COLL_RAT, 3, 20.0)
         res.update(theory_kinetic=kin, theory_collisional=col, theory_total=kin + col)
         res.pop("profile")

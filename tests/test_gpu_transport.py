@@ -84,3 +84,13 @@ def test_channel_profile_viscosity(prec):
     kin, col = V.theory_nu_reference(abi.COLL_RAT, 3, 20.0)
     assert r["fit_rms"] < 0.03 * r["v_max"], r
     assert r["nu"] == pytest.approx(kin + col, rel=0.15), r
+
+
+def test_decay_fit_recovers_rate():
+    """fit_decay on a noisy synthetic exponential: the rate to 1%."""
+    rng = np.random.default_rng(9)
+    t = np.arange(120) * 2.0
+    s = 5e4 * np.exp(-0.004 * t) + rng.normal(0.0, 300.0, t.size)
+    rate, used = V.fit_decay(t, s, 300.0)
+    assert rate == pytest.approx(0.004, rel=0.01)
+    assert 10 < used <= t.size
