@@ -592,16 +592,31 @@ extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double 
     if (r != MPCD_OK) return r;
     CK(cudaMemsetAsync(x.err, 0, sizeof(int), h->stream));
     const int g = grid_for(h, n);
-    if (h->prec == MPCD_PREC_FP64) {
-        if (h->dc.dim == 3)
-            k_f64_to_aos<3><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, x.Q, x.V, x.U, x.err);
-        else
-            k_f64_to_aos<2><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, x.Q, x.V, x.U, x.err);
-    } else {
-        k_mix_to_f64<<<g, 256, 0, h->stream>>>(h->mx[h->cur], h->dc, n, x.Q, x.V, x.U, x.err);
-    }
+    // the inverse of the state's order (into the sort's scratch), then a
+    // gather in the caller's order: coalesced stores to the caller's arrays
+    int *inv = h->perm;
+    CK(cudaMemsetAsync(inv, 0xFF, N * sizeof(int), h->stream));  // -1: no slot yet
+    if (h->prec == MPCD_PREC_FP64)
+        k_inv_pid_f64<<<g, 256, 0, h->stream>>>(h->f[h->cur].pid, n, inv, x.err);
+    else
+        k_inv_pid_mix<<<g, 256, 0, h->stream>>>(h->mx[h->cur].W, n, inv, x.err);
     CK(cudaGetLastError());
     int herr = 0;
+    CK(cudaMemcpyAsync(&herr, x.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (herr) return MPCD_ERR_STATE;  // not a permutation: nothing to gather
+    if (h->prec == MPCD_PREC_FP64) {
+        if (h->dc.dim == 3)
+            k_f64_gather_aos<3><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, inv, x.Q, x.V, x.U,
+                                                          x.err);
+        else
+            k_f64_gather_aos<2><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, inv, x.Q, x.V, x.U,
+                                                          x.err);
+    } else {
+        k_mix_gather_aos<<<g, 256, 0, h->stream>>>(h->mx[h->cur], h->dc, n, inv, x.Q, x.V, x.U,
+                                                   x.err);
+    }
+    CK(cudaGetLastError());
     CK(cudaMemcpyAsync(&herr, x.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     if (Q) CK(cudaMemcpyAsync(Q, x.Q, N * 24, cudaMemcpyDeviceToHost, h->stream));
     if (V) CK(cudaMemcpyAsync(V, x.V, N * 24, cudaMemcpyDeviceToHost, h->stream));

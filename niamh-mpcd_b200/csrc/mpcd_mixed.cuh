@@ -290,12 +290,12 @@ static __global__ void __launch_bounds__(256) k_gather_mix(MixState a, MixState 
     }
 }
 
-// Device-side conversion to and from the packed representation, for
-// uploads and downloads in the caller's FP64 layout (3 doubles per vector,
-// original particle order).  A non-finite value, a position outside the grid
-// or a species id out of range (upload), or an original index out of range
-// (download), counts in *err and leaves that particle unwritten.  Without U,
-// a nematic state starts every orientation at (1, 0).
+// Device-side conversion of an upload in the caller's FP64 layout (3 doubles
+// per vector, original particle order) to the packed representation (the
+// download's gather is k_mix_gather_aos in mpcd_xfer.cuh).  A non-finite
+// value, a position outside the grid or a species id out of range counts in
+// *err and leaves that particle unwritten.  Without U, a nematic state starts
+// every orientation at (1, 0).
 static __global__ void __launch_bounds__(256) k_mix_from_f64(MixState s,
                                                              const __grid_constant__ DevCfg c,
                                                              int n, const double *Q,
@@ -329,32 +329,4 @@ static __global__ void __launch_bounds__(256) k_mix_from_f64(MixState s,
                        : make_float2(1.f, 0.f);
     }
 }
-static __global__ void __launch_bounds__(256) k_mix_to_f64(MixState s,
-                                                           const __grid_constant__ DevCfg c,
-                                                           int n, double *Q, double *V, double *U,
-                                                           int *err) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 w = s.W[i];
-        const int pid = __float_as_int(w.w);
-        if (pid < 0 || pid >= n) {
-            atomicAdd(err, 1);
-            continue;
-        }
-        int ci[3];
-        uint32_t f[3];
-        pos_unpack(s.P[i], ci, f);
-        const float v[3] = {w.x, w.y, w.z};
-        for (int d = 0; d < 3; d++) {
-            Q[3 * (size_t)pid + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;
-            V[3 * (size_t)pid + d] = d < c.dim ? (double)v[d] : 0.0;
-        }
-        if (U) {
-            const float2 u = s.U ? s.U[i] : make_float2(0.f, 0.f);
-            U[3 * (size_t)pid] = (double)u.x;
-            U[3 * (size_t)pid + 1] = (double)u.y;
-            U[3 * (size_t)pid + 2] = 0.0;
-        }
-    }
-}
-
 }  // namespace mpcd

@@ -1,11 +1,12 @@
 // mpcd_xfer.cuh -- device-side conversions between the caller's layout and
 // the handle's state, and the per-cell quantities read back for output.
 //
-//   k_f64_from_aos / k_f64_to_aos  the reference's particle arrays (3 doubles
-//        per vector, original particle order, SRDclss.h:34-44) to and from
-//        the FP64 form's structure of arrays, restoring the original order on
-//        the way back; the mixed form's counterparts are k_mix_from_f64 /
-//        k_mix_to_f64 (mpcd_mixed.cuh).
+//   k_f64_from_aos (k_mix_from_f64 in mpcd_mixed.cuh for the mixed form)
+//        the reference's particle arrays (3 doubles per vector, original
+//        particle order, SRDclss.h:34-44) to the state;
+//   k_inv_pid_* + k_*_gather_aos  back: the inverse of the state's order,
+//        then a gather in the original order (coalesced writes; components
+//        beyond DIM and the orientation's third are 0);
 //   k_pop_unshifted + k_gndnst_reduce  the initial binning on the unshifted
 //        grid and the global number density GnDNST (globalDensities,
 //        init.c:1002-1018): the mean population of the occupied cells of the
@@ -59,15 +60,41 @@ __global__ void __launch_bounds__(256) k_f64_from_aos(Fp64State s, const __grid_
     }
 }
 
-// FP64 state -> caller arrays (AoS) in the original order; the components
-// beyond DIM are 0, and so is the orientation's third.  An original index
-// out of range counts in *err.
-template <int DIM>
-__global__ void __launch_bounds__(256) k_f64_to_aos(Fp64State s, int n, double *Q, double *V,
-                                                    double *U, int *err) {
+// The inverse of the state's order: inv[pid] = slot for every slot (a
+// scatter of 4-byte indices), so that a download can gather each caller-order
+// record and write the caller's arrays with coalesced stores.  An original
+// index out of range counts in *err.
+__global__ void __launch_bounds__(256) k_inv_pid_f64(const int *pid, int n, int *inv, int *err) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int p = s.pid[i];
+        const int p = pid[i];
         if (p < 0 || p >= n) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        inv[p] = i;
+    }
+}
+__global__ void __launch_bounds__(256) k_inv_pid_mix(const float4 *W, int n, int *inv, int *err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int p = __float_as_int(W[i].w);
+        if (p < 0 || p >= n) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        inv[p] = i;
+    }
+}
+
+// FP64 state -> caller arrays (AoS), gathered through inv (caller index ->
+// slot; a slot outside [0, n), which only a corrupted state leaves, counts
+// in *err).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_f64_gather_aos(Fp64State s, int n, const int *inv,
+                                                        double *Q, double *V, double *U,
+                                                        int *err) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int i = inv[p];
+        if (i < 0 || i >= n) {
             atomicAdd(err, 1);
             continue;
         }
@@ -79,6 +106,35 @@ __global__ void __launch_bounds__(256) k_f64_to_aos(Fp64State s, int n, double *
         if (U) {
             U[o] = s.u[0] ? s.u[0][i] : 0.0;
             U[o + 1] = s.u[0] ? s.u[1][i] : 0.0;
+            U[o + 2] = 0.0;
+        }
+    }
+}
+
+// Mixed state -> caller arrays (AoS, FP64), gathered through inv.
+__global__ void __launch_bounds__(256) k_mix_gather_aos(MixState s, const __grid_constant__ DevCfg c,
+                                                        int n, const int *inv, double *Q,
+                                                        double *V, double *U, int *err) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int i = inv[p];
+        if (i < 0 || i >= n) {
+            atomicAdd(err, 1);
+            continue;
+        }
+        int ci[3];
+        uint32_t f[3];
+        pos_unpack(s.P[i], ci, f);
+        const float4 w = s.W[i];
+        const float v[3] = {w.x, w.y, w.z};
+        const size_t o = 3 * (size_t)p;
+        for (int d = 0; d < 3; d++) {
+            Q[o + d] = d < c.dim ? (double)ci[d] + (double)f[d] * kFxInv : 0.0;
+            V[o + d] = d < c.dim ? (double)v[d] : 0.0;
+        }
+        if (U) {
+            const float2 u = s.U ? s.U[i] : make_float2(0.f, 0.f);
+            U[o] = (double)u.x;
+            U[o + 1] = (double)u.y;
             U[o + 2] = 0.0;
         }
     }
