@@ -181,10 +181,21 @@ def _cell_momenta(Q, V, L):
     return p
 
 
+# Per-cell momentum bound of the collision.  FP64: round-off of FP64 sums,
+# below 1e-10 of the cell's momentum scale.  Mixed: v' = u + R (v - u) is
+# formed and stored in FP32; each component of v' carries about ten
+# roundings (2^-24 relative each) of terms no larger than |v - u|, so a
+# cell's momentum changes by at most ~6e-7 sum_i |v_i - u| per component --
+# below 5e-7 of the test's scale (the mean per-cell sum of |v| over the three
+# components, about 24 at 10 particles per cell, kT = 1) for cells of up to
+# about 25 particles.  No 32-bit velocity store can meet 1e-10: its
+# rounding alone is 2^-24 of |v| per particle.
 @pytest.mark.parametrize("prec,kernel,tol", [
     (abi.PREC_FP64, abi.KERNEL_SPLIT, 1e-10),
-    (abi.PREC_MIXED, abi.KERNEL_SPLIT, 2e-6),
-    (abi.PREC_MIXED, abi.KERNEL_RESIDENT, 2e-6),
+    (abi.PREC_FP64, abi.KERNEL_RESIDENT, 1e-10),
+    (abi.PREC_FP64, abi.KERNEL_PERSIST, 1e-10),
+    (abi.PREC_MIXED, abi.KERNEL_SPLIT, 5e-7),
+    (abi.PREC_MIXED, abi.KERNEL_RESIDENT, 5e-7),
 ])
 def test_collision_conserves_each_cells_momentum(prec, kernel, tol):
     # no grid shift and no streaming to speak of (dt = 1e-30): the collision
@@ -246,4 +257,25 @@ def test_mixed_upload_rejects_bad_input_on_the_device():
     g.step(2, 1)
     q, v, _ = g.download()
     assert np.all(np.isfinite(v)) and np.all((q >= 0) & (q < 6))
+    g.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(abi.PREC_FP64, 1e-10), (abi.PREC_MIXED, 5e-7)])
+def test_collision_conserves_each_cells_momentum_64cubed(prec, tol):
+    """The per-cell bound above on the 64^3 workload (2,621,440 particles,
+    262,144 cells), default kernel family of each form."""
+    L = (64, 64, 64)
+    cfg = W.cfg_srd3d(L, precision=prec, seed=23, galinv=0, dt=1e-30)
+    Q, V, U, sp = W.synthetic_state(cfg, 10, seed=24)
+    g = Solver(cfg)
+    g.upload(Q, V, U, sp)
+    q0, v0, _ = g.download()
+    g.step(1, 1)
+    q1, v1, _ = g.download()
+    np.testing.assert_allclose(q1, q0, rtol=0, atol=1e-12)
+    p0 = _cell_momenta(q0, v0, L)
+    p1 = _cell_momenta(q1, v1, L)
+    scale = np.abs(v0).sum() / len(p0)
+    assert np.abs(p1 - p0).max() / scale < tol
+    assert np.abs(v1 - v0).max() > 0.1
     g.close()
