@@ -170,8 +170,72 @@ int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *base,
                                   size_t stride, size_t off_Q, size_t off_V,
                                   size_t off_U, size_t off_spid);
 
+/* Initial velocity distributions: the reference's vDist codes
+ * (definitions.h:149-157, push init.c:1261-1291).  READ (1) is an upload. */
+#define MPCD_VDIST_RANDVEL 0  /* uniform, each component in +-sqrt(kT/m)  */
+#define MPCD_VDIST_HOMO 2     /* speed sqrt(DIM kT/m), random direction     */
+#define MPCD_VDIST_HOMOAXIS 3 /* each component +-sqrt(DIM kT/m)           */
+#define MPCD_VDIST_GAUSS 4    /* Maxwell-Boltzmann                          */
+
+/* Initial orientation distributions: the reference's oDist codes
+ * (definitions.h:165-183, orient init.c:1307-1405). */
+#define MPCD_ODIST_RANDORIENT 0
+#define MPCD_ODIST_ALIGNX 1
+#define MPCD_ODIST_ALIGNY 2
+#define MPCD_ODIST_ALIGNZ 3
+#define MPCD_ODIST_ALIGN45 4
+#define MPCD_ODIST_PLANEZ 5
+#define MPCD_ODIST_PLANEY 6
+#define MPCD_ODIST_PLANEX 7
+#define MPCD_ODIST_ALIGNTR 8
+#define MPCD_ODIST_ALIGNDEFECTPAIR 9
+
+/* The initial state the reference builds from its JSON species entries. */
+typedef struct mpcd_init_params {
+    int population[MPCD_MAX_SPECIES]; /* POP (json 'pop', or 'dens' times
+                                         the accessible volume)           */
+    int vdist[MPCD_MAX_SPECIES];      /* VDIST (json 'vDist')             */
+    int odist[MPCD_MAX_SPECIES];      /* ODIST (json 'oDist'), nematic    */
+    int rframe;                       /* in.RFRAME (json 'rFrame')        */
+    int pad_;
+} mpcd_init_params;
+
+/* Build the initial particle state on the device, as setcoord
+ * (init.c:1565-1600), galileantrans (mtools.c:673-711, when rframe and more
+ * than 2 particles) and the VSC temperature scaling (scaleT, therm.c:106-143)
+ * of initializeSIM (init.c:2092-2170) do: the first population[0] particles
+ * are species 0, and so on; positions uniform in the box, placed anew while
+ * any interacting wall has W <= TOL; velocities from vdist; orientations
+ * (nematic configs) from odist at the first position; then V scaled so that
+ * TEMP about the initial mean velocity is kbt.  Random draws are keyed by
+ * (seed, replica) at step 0.  *kbtnow (may be NULL) receives TEMP after the
+ * scaling, what the reference computes at init.c:2170.  The state replaces
+ * any uploaded one and downloads like an upload.  MPCD_ERR_ARG if a species
+ * with particles has no accessible volume (the reference loops for ever
+ * there) or a particle is still inside a wall after the attempts its
+ * species' accessible fraction allows (64 / fraction, at least 256). */
+int mpcd_init_state(mpcd_handle *h, const mpcd_init_params *p, double *kbtnow);
+
+/* Volume accessible to species 'species': the box volume (XYZ[2] = 1 in 2D)
+ * less the parts where some wall the species interacts with has W < 0.
+ * The reference estimates it by Monte Carlo with 1000 points per unit volume
+ * (accessibleVolume, init.c:954-989); with axis-aligned planar walls it is a
+ * product of per-axis intervals, computed here exactly.  Host only: no
+ * device work. */
+int mpcd_accessible_volume(const mpcd_config *cfg, int species, double *vol);
+
 /* Copy the particle state back in the caller's original particle order. */
 int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double *U);
+
+/* The species id of every particle, in the caller's original order. */
+int mpcd_download_species(mpcd_handle *h, int *spid);
+
+/* The handle's configuration, with gndnst the global number density in use
+ * (given, or computed at the last upload). */
+int mpcd_get_config(const mpcd_handle *h, mpcd_config *cfg);
+
+/* Number of particles in the handle's state. */
+int mpcd_particle_count(const mpcd_handle *h, int *n);
 
 /* Strided counterpart of mpcd_download_state: writes the Q and V fields of
  * each record and, for a nematic state (lc != 0) with off_U != (size_t)-1,
@@ -397,6 +461,78 @@ int mpcd_batch_info(mpcd_batch *b, int *n, int *slots, int *cells);
 int mpcd_srd_step_noalloc(const mpcd_config *cfg, int n, double *Q, double *V,
                           uint32_t step, double *globals, unsigned long long *counters,
                           void *stream);
+
+/* ---- checkpoints in the reference's format ----------------------------
+ * The reference checkpoints a run as text: checkpoint (pout.c:2325-2396)
+ * writes, and readchckpnt (read.c:669-834) reads, the run's counters, input
+ * parameters, output flags, species, walls, every particle (S_flag, SPID, q,
+ * Q, V, U, T) and the swimmers.  An mpcd_ckpt holds every field of such a
+ * file.  The library reads the fields it uses (configuration, counters,
+ * particles), replaces them from a handle, and carries all others through
+ * unchanged, so a run can move between the reference program and this
+ * library in either direction.  Host only, except the two calls that take a
+ * handle. */
+typedef struct mpcd_ckpt mpcd_ckpt;
+
+/* Counters and global measures of a checkpoint (the first lines of the
+ * file): in.simSteps, in.warmupSteps, runtime, warmtime, KBTNOW, AVV,
+ * AVNOW. */
+typedef struct mpcd_ckpt_run {
+    int sim_steps, warmup_steps;
+    int runtime, warmtime;
+    double kbtnow;
+    double avv[3], avnow[3];
+} mpcd_ckpt_run;
+
+/* Parse a checkpoint file; *out is freed with mpcd_ckpt_free.  MPCD_ERR_ARG
+ * for a file that ends early or holds a field that is not a number. */
+int mpcd_ckpt_read(const char *path, mpcd_ckpt **out);
+
+/* A checkpoint of cfg with no particles: the fields the library does not
+ * own take the values a JSON run with the defaults of readJson would hold
+ * (no thermostat, no outputs, static walls, no swimmers). */
+int mpcd_ckpt_create(const mpcd_config *cfg, mpcd_ckpt **out);
+
+int mpcd_ckpt_free(mpcd_ckpt *ck);
+
+/* Write the checkpoint.  precise = 0 prints every field as checkpoint does
+ * (doubles with "%lf", six decimals): a file read and written again is
+ * identical byte for byte.  precise = 1 prints doubles with 17 significant
+ * digits, which readchckpnt reads back exactly (a lossless checkpoint in the
+ * same layout). */
+int mpcd_ckpt_write(const mpcd_ckpt *ck, const char *path, int precise);
+
+/* The configuration the checkpoint describes (seed = in.seed, gndnst =
+ * GnDNST, capacity 0).  MPCD_ERR_UNSUPPORTED when the run uses something
+ * outside this library: MD coupling, swimmers, a thermostat, moving,
+ * rotating or non-planar walls, an external magnetic field, or another
+ * collision operator. */
+int mpcd_ckpt_config(const mpcd_ckpt *ck, mpcd_config *cfg);
+
+int mpcd_ckpt_get_run(const mpcd_ckpt *ck, mpcd_ckpt_run *run);
+int mpcd_ckpt_set_run(mpcd_ckpt *ck, const mpcd_ckpt_run *run);
+
+/* Particle count, and the particles (any output may be NULL; 3 doubles per
+ * vector). */
+int mpcd_ckpt_count(const mpcd_ckpt *ck, int *n);
+int mpcd_ckpt_particles(const mpcd_ckpt *ck, double *Q, double *V, double *U, int *spid);
+
+/* Replace the checkpoint's particles (n of them; U and spid may be NULL for
+ * zero orientations and species 0); the species populations follow.
+ * Particles keep their S_flag, q and T where the count is unchanged; new
+ * ones get S_flag 1 (STREAM) and zero q and T. */
+int mpcd_ckpt_set_particles(mpcd_ckpt *ck, int n, const double *Q, const double *V,
+                            const double *U, const int *spid);
+
+/* The checkpoint's particles into the handle (mpcd_upload_state), as
+ * initializeRecovery (init.c:2193-2215) bins them after readchckpnt. */
+int mpcd_ckpt_upload(const mpcd_ckpt *ck, mpcd_handle *h);
+
+/* The handle's particles into the checkpoint (mpcd_ckpt_set_particles with
+ * the handle's positions, velocities, species and, for a nematic state,
+ * orientations; an isotropic state leaves the file's orientations), and the
+ * handle's GnDNST. */
+int mpcd_ckpt_capture(mpcd_ckpt *ck, mpcd_handle *h);
 
 #ifdef __cplusplus
 }

@@ -25,6 +25,7 @@
 #include "mpcd_lc.cuh"
 #include "mpcd_xfer.cuh"
 #include "mpcd_persist.cuh"
+#include "mpcd_init.cuh"
 
 using namespace mpcd;
 
@@ -388,7 +389,11 @@ extern "C" int mpcd_create(const mpcd_config *cfg, mpcd_handle **out) {
         mpcd_destroy(h);
         return MPCD_ERR_CUDA;
     }
-    if (cudaMallocHost((void **)&h->host_acc, sizeof(double) * ACC_WORDS) != cudaSuccess) {
+    // pinned host buffers of the globals read-back (allocated here: a
+    // pinned allocation costs milliseconds, too much inside a caller's loop)
+    if (cudaMallocHost((void **)&h->host_acc, sizeof(double) * ACC_WORDS) != cudaSuccess ||
+        cudaMallocHost((void **)&h->host_ring, sizeof(double) * 2 * kRecordBatch * ACC_WORDS) !=
+            cudaSuccess) {
         mpcd_destroy(h);
         return MPCD_ERR_NOMEM;
     }
@@ -503,28 +508,11 @@ static int staging(mpcd_handle *h, size_t N, bool withU, bool withSp, Staging *x
     return MPCD_OK;
 }
 
-extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
-                                 const double *U, const int *spid) {
-    if (!h || n < 0 || (n > 0 && (!Q || !V))) return MPCD_ERR_ARG;
-    int r = upload_common(h, n);
-    if (r != MPCD_OK) return r;
-    if (n == 0) return MPCD_OK;
-    const size_t N = (size_t)n;
-    // species ids are checked whenever given (with one species every id
-    // must be 0)
-    const bool withU = U && h->dc.lc, withSp = spid != nullptr;
-    // several species without ids: every particle species 0 (the kernels
-    // read a null id array as species 0 only with one species)
-    const bool zeroSp = !spid && h->dc.n_species > 1;
-    Staging x;
-    r = staging(h, N, withU, withSp || zeroSp, &x);
-    if (r != MPCD_OK) return r;
-    CK(cudaMemcpyAsync(x.Q, Q, N * 24, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(x.V, V, N * 24, cudaMemcpyHostToDevice, h->stream));
-    if (withU) CK(cudaMemcpyAsync(x.U, U, N * 24, cudaMemcpyHostToDevice, h->stream));
-    if (withSp) CK(cudaMemcpyAsync(x.sp, spid, N * 4, cudaMemcpyHostToDevice, h->stream));
-    if (zeroSp) CK(cudaMemsetAsync(x.sp, 0, N * 4, h->stream));
-    CK(cudaMemsetAsync(x.err, 0, 256, h->stream));
+// Staged particles (caller order, 3 doubles per vector) -> the handle's
+// state, and the global number density.  Waits for the stream; a rejected
+// state (non-finite values, species out of range, a particle the
+// initialisation could not place) leaves no state.
+static int upload_from_staging(mpcd_handle *h, int n, const Staging &x) {
     const int g = grid_for(h, n);
     if (h->prec == MPCD_PREC_FP64) {
         if (h->dc.dim == 3)
@@ -561,6 +549,143 @@ extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const d
     return MPCD_OK;
 }
 
+extern "C" int mpcd_upload_state(mpcd_handle *h, int n, const double *Q, const double *V,
+                                 const double *U, const int *spid) {
+    if (!h || n < 0 || (n > 0 && (!Q || !V))) return MPCD_ERR_ARG;
+    int r = upload_common(h, n);
+    if (r != MPCD_OK) return r;
+    if (n == 0) return MPCD_OK;
+    const size_t N = (size_t)n;
+    // species ids are checked whenever given (with one species every id
+    // must be 0)
+    const bool withU = U && h->dc.lc, withSp = spid != nullptr;
+    // several species without ids: every particle species 0 (the kernels
+    // read a null id array as species 0 only with one species)
+    const bool zeroSp = !spid && h->dc.n_species > 1;
+    Staging x;
+    r = staging(h, N, withU, withSp || zeroSp, &x);
+    if (r != MPCD_OK) return r;
+    CK(cudaMemcpyAsync(x.Q, Q, N * 24, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(x.V, V, N * 24, cudaMemcpyHostToDevice, h->stream));
+    if (withU) CK(cudaMemcpyAsync(x.U, U, N * 24, cudaMemcpyHostToDevice, h->stream));
+    if (withSp) CK(cudaMemcpyAsync(x.sp, spid, N * 4, cudaMemcpyHostToDevice, h->stream));
+    if (zeroSp) CK(cudaMemsetAsync(x.sp, 0, N * 4, h->stream));
+    CK(cudaMemsetAsync(x.err, 0, 256, h->stream));
+    return upload_from_staging(h, n, x);
+}
+
+// Exact accessible volume for axis-aligned planar walls: each wall the
+// species interacts with bounds one axis (W = A (x - Q) - R, negated when
+// inverted, is >= 0 on one side of x0 = Q + R/A); the volume is the product
+// of the remaining intervals.  A wall whose normal lies outside the first
+// DIM axes has the constant W = -R (R when inverted) there.
+static double accessible_volume(const DevCfg &dc, const mpcd_config *cfg, int species) {
+    double lo[3] = {0.0, 0.0, 0.0}, hi[3];
+    for (int d = 0; d < 3; d++) hi[d] = (double)dc.L[d];
+    for (int j = 0; j < dc.n_walls; j++) {
+        if (!cfg->walls[j].inter[species]) continue;
+        const DevWall &w = dc.walls[j];
+        const int ax = w.axis;
+        if (ax >= dc.dim) {
+            const double W = w.inv ? w.R : -w.R;
+            if (W < 0.0) return 0.0;
+            continue;
+        }
+        const double A = w.A[ax], x0 = w.Q[ax] + w.R / A;
+        const bool above = (A > 0.0) != (w.inv != 0);
+        if (above)
+            lo[ax] = std::max(lo[ax], x0);
+        else
+            hi[ax] = std::min(hi[ax], x0);
+    }
+    double v = 1.0;
+    for (int d = 0; d < 3; d++) v *= std::max(0.0, hi[d] - lo[d]);
+    return v;
+}
+
+extern "C" int mpcd_accessible_volume(const mpcd_config *cfg, int species, double *vol) {
+    if (!cfg || !vol) return MPCD_ERR_ARG;
+    DevCfg dc;
+    int r = build_devcfg(cfg, &dc);
+    if (r != MPCD_OK) return r;
+    if (species < 0 || species >= cfg->n_species) return MPCD_ERR_ARG;
+    *vol = accessible_volume(dc, cfg, species);
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_init_state(mpcd_handle *h, const mpcd_init_params *p, double *kbtnow) {
+    if (!h || !p) return MPCD_ERR_ARG;
+    const DevCfg &dc = h->dc;
+    InitPlan plan;
+    memset(&plan, 0, sizeof(plan));
+    long long total = 0;
+    const double box = (double)dc.L[0] * dc.L[1] * dc.L[2];
+    for (int s = 0; s < MPCD_MAX_SPECIES; s++) {
+        const int pop = p->population[s];
+        if (pop < 0 || (s >= dc.n_species && pop != 0)) return MPCD_ERR_ARG;
+        plan.off[s] = (int)std::min<long long>(total, INT32_MAX);
+        total += pop;
+        if (s >= dc.n_species) continue;
+        const int vd = p->vdist[s], od = p->odist[s];
+        if (vd != MPCD_VDIST_RANDVEL && vd != MPCD_VDIST_HOMO && vd != MPCD_VDIST_HOMOAXIS &&
+            vd != MPCD_VDIST_GAUSS)
+            return MPCD_ERR_UNSUPPORTED;
+        if (dc.lc && (od < MPCD_ODIST_RANDORIENT || od > MPCD_ODIST_ALIGNDEFECTPAIR))
+            return MPCD_ERR_UNSUPPORTED;
+        plan.vdist[s] = vd;
+        plan.odist[s] = od;
+        if (pop > 0) {
+            const double frac = accessible_volume(dc, &h->cfg, s) / box;
+            if (!(frac > 0.0)) return MPCD_ERR_ARG;
+            plan.max_attempts[s] = (int)std::min(std::max(64.0 / frac, 256.0), 4194304.0);
+        }
+    }
+    plan.off[MPCD_MAX_SPECIES] = (int)std::min<long long>(total, INT32_MAX);
+    if (total > INT32_MAX) return MPCD_ERR_SIZE;
+    const int n = (int)total;
+    plan.rframe = p->rframe && n > 2;  // init.c:2140-2143
+    int r = upload_common(h, n);
+    if (r != MPCD_OK) return r;
+    if (n == 0) {
+        if (kbtnow) *kbtnow = 0.0;
+        return MPCD_OK;
+    }
+    Staging x;
+    r = staging(h, (size_t)n, dc.lc != 0, dc.n_species > 1, &x);
+    if (r != MPCD_OK) {
+        h->n = 0;
+        return r;
+    }
+    const int g = grid_for(h, n);
+    double *work = nullptr;  // block partials (8 per block), then 3 x 8 sums
+    if (cudaMalloc((void **)&work, sizeof(double) * (8 * (size_t)g + 24)) != cudaSuccess) {
+        h->n = 0;
+        return MPCD_ERR_NOMEM;
+    }
+    double *part = work, *sums = work + 8 * (size_t)g;
+    cudaError_t e = cudaMemsetAsync(x.err, 0, 256, h->stream);
+    k_init_gen<<<g, 256, 0, h->stream>>>(dc, plan, n, x.Q, x.V, x.U, x.sp, x.err, part);
+    k_init_reduce<<<1, 256, 0, h->stream>>>(part, g, 7, sums);
+    k_init_adjust<<<g, 256, 0, h->stream>>>(dc, plan, n, x.V, sums, nullptr, part);
+    k_init_reduce<<<1, 256, 0, h->stream>>>(part, g, 1, sums + 8);
+    k_init_adjust<<<g, 256, 0, h->stream>>>(dc, plan, n, x.V, sums, sums + 8, part);
+    k_init_reduce<<<1, 256, 0, h->stream>>>(part, g, 1, sums + 16);
+    double t_after = 0.0;
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&t_after, sums + 16, sizeof(double), cudaMemcpyDeviceToHost,
+                            h->stream);
+    if (e == cudaSuccess) r = upload_from_staging(h, n, x);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(work);
+    if (e != cudaSuccess || r != MPCD_OK) {
+        h->n = 0;
+        return e != cudaSuccess ? MPCD_ERR_CUDA : r;
+    }
+    if (kbtnow) *kbtnow = t_after / ((double)n * dc.dim);
+    return MPCD_OK;
+}
+
 extern "C" int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *base,
                                              size_t stride, size_t off_Q, size_t off_V,
                                              size_t off_U, size_t off_spid) {
@@ -582,13 +707,15 @@ extern "C" int mpcd_upload_particles_strided(mpcd_handle *h, int n, const void *
     return mpcd_upload_state(h, n, Q.data(), V.data(), has_U ? U.data() : nullptr, sp.data());
 }
 
-extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double *U) {
+// The state in the caller's original particle order; any output may be
+// null (then not gathered).
+static int download_impl(mpcd_handle *h, double *Q, double *V, double *U, int *spid) {
     if (!h) return MPCD_ERR_ARG;
     const int n = h->n;
     const size_t N = (size_t)n;
     if (n == 0) return MPCD_OK;
     Staging x;
-    int r = staging(h, N, U != nullptr, false, &x);
+    int r = staging(h, N, U != nullptr, spid != nullptr, &x);
     if (r != MPCD_OK) return r;
     CK(cudaMemsetAsync(x.err, 0, sizeof(int), h->stream));
     const int g = grid_for(h, n);
@@ -608,21 +735,44 @@ extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double 
     if (h->prec == MPCD_PREC_FP64) {
         if (h->dc.dim == 3)
             k_f64_gather_aos<3><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, inv, x.Q, x.V, x.U,
-                                                          x.err);
+                                                          x.sp, x.err);
         else
             k_f64_gather_aos<2><<<g, 256, 0, h->stream>>>(h->f[h->cur], n, inv, x.Q, x.V, x.U,
-                                                          x.err);
+                                                          x.sp, x.err);
     } else {
         k_mix_gather_aos<<<g, 256, 0, h->stream>>>(h->mx[h->cur], h->dc, n, inv, x.Q, x.V, x.U,
-                                                   x.err);
+                                                   x.sp, x.err);
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(&herr, x.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     if (Q) CK(cudaMemcpyAsync(Q, x.Q, N * 24, cudaMemcpyDeviceToHost, h->stream));
     if (V) CK(cudaMemcpyAsync(V, x.V, N * 24, cudaMemcpyDeviceToHost, h->stream));
     if (U) CK(cudaMemcpyAsync(U, x.U, N * 24, cudaMemcpyDeviceToHost, h->stream));
+    if (spid) CK(cudaMemcpyAsync(spid, x.sp, N * 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return herr ? MPCD_ERR_STATE : MPCD_OK;
+}
+
+extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double *U) {
+    return download_impl(h, Q, V, U, nullptr);
+}
+
+extern "C" int mpcd_download_species(mpcd_handle *h, int *spid) {
+    if (!h || (h->n > 0 && !spid)) return MPCD_ERR_ARG;
+    return download_impl(h, nullptr, nullptr, nullptr, spid);
+}
+
+extern "C" int mpcd_get_config(const mpcd_handle *h, mpcd_config *cfg) {
+    if (!h || !cfg) return MPCD_ERR_ARG;
+    *cfg = h->cfg;
+    cfg->gndnst = h->dc.gndnst;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_particle_count(const mpcd_handle *h, int *n) {
+    if (!h || !n) return MPCD_ERR_ARG;
+    *n = h->n;
+    return MPCD_OK;
 }
 
 extern "C" int mpcd_download_particles_strided(mpcd_handle *h, void *base, size_t stride,

@@ -46,7 +46,11 @@ enum {
     MPCD_STREAM_THERMAL = 3, /* Andersen thermal velocities, per particle  */
     MPCD_STREAM_GHOST = 4,   /* phantom-particle momentum, per cell        */
     MPCD_STREAM_LC = 5,      /* Maier-Saupe Metropolis uniforms, per particle */
-    MPCD_STREAM_ORTH = 6     /* orthogonal-axis choice, per cell           */
+    MPCD_STREAM_ORTH = 6,    /* orthogonal-axis choice, per cell           */
+    /* initial state (step 0), per particle: */
+    MPCD_STREAM_INIT_POS = 7, /* positions, 4 uniforms per placement attempt */
+    MPCD_STREAM_INIT_VEL = 8, /* velocities                                  */
+    MPCD_STREAM_INIT_ORI = 9  /* orientations                                */
 };
 
 /* Maximum Philox blocks a rejection loop may consume (2 attempts per block).

@@ -6,7 +6,8 @@
 //        particle order, SRDclss.h:34-44) to the state;
 //   k_inv_pid_* + k_*_gather_aos  back: the inverse of the state's order,
 //        then a gather in the original order (coalesced writes; components
-//        beyond DIM and the orientation's third are 0);
+//        beyond DIM and the orientation's third are 0; species ids on
+//        request);
 //   k_pop_unshifted + k_gndnst_reduce  the initial binning on the unshifted
 //        grid and the global number density GnDNST (globalDensities,
 //        init.c:1002-1018): the mean population of the occupied cells of the
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(256) k_inv_pid_mix(const float4 *W, int n, int
 template <int DIM>
 __global__ void __launch_bounds__(256) k_f64_gather_aos(Fp64State s, int n, const int *inv,
                                                         double *Q, double *V, double *U,
-                                                        int *err) {
+                                                        int *spo, int *err) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         const int i = inv[p];
         if (i < 0 || i >= n) {
@@ -108,13 +109,15 @@ __global__ void __launch_bounds__(256) k_f64_gather_aos(Fp64State s, int n, cons
             U[o + 1] = s.u[0] ? s.u[1][i] : 0.0;
             U[o + 2] = 0.0;
         }
+        if (spo) spo[p] = s.sp ? s.sp[i] : 0;
     }
 }
 
 // Mixed state -> caller arrays (AoS, FP64), gathered through inv.
 __global__ void __launch_bounds__(256) k_mix_gather_aos(MixState s, const __grid_constant__ DevCfg c,
                                                         int n, const int *inv, double *Q,
-                                                        double *V, double *U, int *err) {
+                                                        double *V, double *U, int *spo,
+                                                        int *err) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         const int i = inv[p];
         if (i < 0 || i >= n) {
@@ -137,6 +140,7 @@ __global__ void __launch_bounds__(256) k_mix_gather_aos(MixState s, const __grid
             U[o + 1] = (double)u.y;
             U[o + 2] = 0.0;
         }
+        if (spo) spo[p] = s.sp ? s.sp[i] : 0;
     }
 }
 

@@ -124,6 +124,59 @@ class TuneChoice(C.Structure):
     ]
 
 
+# initial distributions: the reference's vDist / oDist codes
+VDIST_RANDVEL = 0
+VDIST_HOMO = 2
+VDIST_HOMOAXIS = 3
+VDIST_GAUSS = 4
+ODIST_RANDORIENT = 0
+ODIST_ALIGNX = 1
+ODIST_ALIGNY = 2
+ODIST_ALIGNZ = 3
+ODIST_ALIGN45 = 4
+ODIST_PLANEZ = 5
+ODIST_PLANEY = 6
+ODIST_PLANEX = 7
+ODIST_ALIGNTR = 8
+ODIST_ALIGNDEFECTPAIR = 9
+
+
+class InitParams(C.Structure):
+    _fields_ = [
+        ("population", C.c_int * MAX_SPECIES),
+        ("vdist", C.c_int * MAX_SPECIES),
+        ("odist", C.c_int * MAX_SPECIES),
+        ("rframe", C.c_int),
+        ("pad_", C.c_int),
+    ]
+
+
+def init_params(population, vdist=VDIST_RANDVEL, odist=ODIST_ALIGNY, rframe=1):
+    """InitParams for per-species populations; vdist/odist a code or a
+    per-species list (defaults: the reference's JSON defaults vDist 0,
+    oDist 2, rFrame 1)."""
+    p = InitParams()
+    pops = list(population)
+    for s, n in enumerate(pops):
+        p.population[s] = int(n)
+        p.vdist[s] = int(vdist[s] if hasattr(vdist, "__len__") else vdist)
+        p.odist[s] = int(odist[s] if hasattr(odist, "__len__") else odist)
+    p.rframe = int(rframe)
+    return p
+
+
+class CkptRun(C.Structure):
+    _fields_ = [
+        ("sim_steps", C.c_int),
+        ("warmup_steps", C.c_int),
+        ("runtime", C.c_int),
+        ("warmtime", C.c_int),
+        ("kbtnow", C.c_double),
+        ("avv", C.c_double * 3),
+        ("avnow", C.c_double * 3),
+    ]
+
+
 class Status(C.Structure):
     _fields_ = [
         ("steps", C.c_uint64),

@@ -16,7 +16,8 @@ LIB_PATH = os.environ.get(
 
 EXPORTS = [
     "mpcd_abi_version", "mpcd_create", "mpcd_destroy", "mpcd_upload_state",
-    "mpcd_upload_particles_strided", "mpcd_download_state",
+    "mpcd_upload_particles_strided", "mpcd_init_state", "mpcd_accessible_volume",
+    "mpcd_download_state",
     "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
     "mpcd_launches_per_step", "mpcd_set_strategy", "mpcd_set_kernel",
@@ -26,6 +27,10 @@ EXPORTS = [
     "mpcd_srd_step_noalloc", "mpcd_batch_create", "mpcd_batch_destroy", "mpcd_batch_upload",
     "mpcd_batch_step", "mpcd_batch_download", "mpcd_batch_globals",
     "mpcd_batch_set_sort_interval", "mpcd_batch_set_stream", "mpcd_batch_info",
+    "mpcd_download_species", "mpcd_get_config", "mpcd_particle_count", "mpcd_ckpt_read", "mpcd_ckpt_create",
+    "mpcd_ckpt_free", "mpcd_ckpt_write", "mpcd_ckpt_config", "mpcd_ckpt_get_run",
+    "mpcd_ckpt_set_run", "mpcd_ckpt_count", "mpcd_ckpt_particles", "mpcd_ckpt_set_particles",
+    "mpcd_ckpt_upload", "mpcd_ckpt_capture",
 ]
 
 _lib = None
@@ -48,7 +53,24 @@ def load():
         lib.mpcd_upload_particles_strided.argtypes = [vp, C.c_int, vp, C.c_size_t,
                                                       C.c_size_t, C.c_size_t, C.c_size_t,
                                                       C.c_size_t]
+        lib.mpcd_init_state.argtypes = [vp, vp, vp]
+        lib.mpcd_accessible_volume.argtypes = [vp, C.c_int, vp]
         lib.mpcd_download_state.argtypes = [vp, vp, vp, vp]
+        lib.mpcd_download_species.argtypes = [vp, vp]
+        lib.mpcd_particle_count.argtypes = [vp, vp]
+        lib.mpcd_get_config.argtypes = [vp, vp]
+        lib.mpcd_ckpt_read.argtypes = [C.c_char_p, C.POINTER(vp)]
+        lib.mpcd_ckpt_create.argtypes = [vp, C.POINTER(vp)]
+        lib.mpcd_ckpt_free.argtypes = [vp]
+        lib.mpcd_ckpt_write.argtypes = [vp, C.c_char_p, C.c_int]
+        lib.mpcd_ckpt_config.argtypes = [vp, vp]
+        lib.mpcd_ckpt_get_run.argtypes = [vp, vp]
+        lib.mpcd_ckpt_set_run.argtypes = [vp, vp]
+        lib.mpcd_ckpt_count.argtypes = [vp, vp]
+        lib.mpcd_ckpt_particles.argtypes = [vp, vp, vp, vp, vp]
+        lib.mpcd_ckpt_set_particles.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+        lib.mpcd_ckpt_upload.argtypes = [vp, vp]
+        lib.mpcd_ckpt_capture.argtypes = [vp, vp]
         lib.mpcd_download_particles_strided.argtypes = [vp, vp, C.c_size_t, C.c_size_t,
                                                         C.c_size_t, C.c_size_t]
         lib.mpcd_step.argtypes = [vp, C.c_int, C.c_uint32]
@@ -117,6 +139,85 @@ def tune_cache_store(path, key, choice):
            "mpcd_tune_cache_store")
 
 
+def accessible_volume(cfg, species=0):
+    """Volume accessible to a species (mpcd_accessible_volume; host only)."""
+    lib = load()
+    v = C.c_double()
+    _check(lib.mpcd_accessible_volume(C.byref(cfg), species, C.byref(v)),
+           "mpcd_accessible_volume")
+    return v.value
+
+
+class Checkpoint:
+    """A checkpoint in the reference's text format (mpcd_ckpt_*): read from
+    a file or made from a config; host-side except upload/capture."""
+
+    def __init__(self, path=None, cfg=None):
+        self.lib = load()
+        h = C.c_void_p()
+        if path is not None:
+            _check(self.lib.mpcd_ckpt_read(str(path).encode(), C.byref(h)), "mpcd_ckpt_read")
+        else:
+            _check(self.lib.mpcd_ckpt_create(C.byref(cfg), C.byref(h)), "mpcd_ckpt_create")
+        self.h = h
+
+    def write(self, path, precise=False):
+        _check(self.lib.mpcd_ckpt_write(self.h, str(path).encode(), int(bool(precise))),
+               "mpcd_ckpt_write")
+
+    def config(self):
+        cfg = abi.Config()
+        _check(self.lib.mpcd_ckpt_config(self.h, C.byref(cfg)), "mpcd_ckpt_config")
+        return cfg
+
+    def run(self):
+        r = abi.CkptRun()
+        _check(self.lib.mpcd_ckpt_get_run(self.h, C.byref(r)), "mpcd_ckpt_get_run")
+        return r
+
+    def set_run(self, run):
+        _check(self.lib.mpcd_ckpt_set_run(self.h, C.byref(run)), "mpcd_ckpt_set_run")
+
+    def count(self):
+        n = C.c_int()
+        _check(self.lib.mpcd_ckpt_count(self.h, C.byref(n)), "mpcd_ckpt_count")
+        return n.value
+
+    def particles(self):
+        n = self.count()
+        Q, V, U = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        sp = np.zeros(n, dtype=np.int32)
+        _check(self.lib.mpcd_ckpt_particles(self.h, _p(Q), _p(V), _p(U), _p(sp)),
+               "mpcd_ckpt_particles")
+        return Q, V, U, sp
+
+    def set_particles(self, Q, V, U=None, spid=None):
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        spid = None if spid is None else np.ascontiguousarray(spid, dtype=np.int32)
+        _check(self.lib.mpcd_ckpt_set_particles(self.h, len(Q), _p(Q), _p(V), _p(U), _p(spid)),
+               "mpcd_ckpt_set_particles")
+
+    def upload(self, solver):
+        _check(self.lib.mpcd_ckpt_upload(self.h, solver.h), "mpcd_ckpt_upload")
+        solver.n = self.count()
+
+    def capture(self, solver):
+        _check(self.lib.mpcd_ckpt_capture(self.h, solver.h), "mpcd_ckpt_capture")
+
+    def close(self):
+        if self.h:
+            self.lib.mpcd_ckpt_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def srd_step_noalloc(cfg, n, q_dev_ptr, v_dev_ptr, step, globals_dev_ptr=None, stream=None,
                      counters_dev_ptr=None):
     """One SRD timestep on caller-owned device arrays (AoS, 3 doubles per
@@ -153,6 +254,27 @@ class Solver:
         _check(self.lib.mpcd_upload_state(self.h, len(Q), _p(Q), _p(V), _p(U), _p(spid)),
                "mpcd_upload_state")
         self.n = len(Q)
+
+    def init_state(self, params):
+        """Build the initial state on the device (mpcd_init_state) from an
+        abi.InitParams; returns TEMP after the temperature scaling."""
+        k = C.c_double()
+        self.n = 0  # a failed initialisation leaves no state
+        _check(self.lib.mpcd_init_state(self.h, C.byref(params), C.byref(k)), "mpcd_init_state")
+        self.n = sum(params.population)
+        return k.value
+
+    def config(self):
+        """The handle's configuration, gndnst the value in use."""
+        cfg = abi.Config()
+        _check(self.lib.mpcd_get_config(self.h, C.byref(cfg)), "mpcd_get_config")
+        return cfg
+
+    def species(self):
+        """Species id of every particle, in the original order."""
+        sp = np.zeros(self.n, dtype=np.int32)
+        _check(self.lib.mpcd_download_species(self.h, _p(sp)), "mpcd_download_species")
+        return sp
 
     def step(self, nsteps, step0):
         _check(self.lib.mpcd_step(self.h, nsteps, step0), "mpcd_step")

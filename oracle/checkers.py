@@ -51,6 +51,8 @@ class Oracle:
             lib.oracle_escaped.restype = C.c_long
             lib.oracle_escaped.argtypes = [C.c_void_p]
             lib.oracle_shifted_counts.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+            lib.oracle_init_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int] + \
+                [C.c_void_p] * 5
             cls._lib = lib
         return cls._lib
 
@@ -118,6 +120,20 @@ class Oracle:
             pass
 
 
+def oracle_init_state(cfg, params, max_attempts=1 << 22):
+    """The oracle's initial state (oracle_init_state): Q, V, U (n x 3), spid
+    and TEMP after the scaling."""
+    n = sum(params.population)
+    Q, V, U = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+    sp = np.zeros(n, dtype=np.int32)
+    kb = C.c_double()
+    r = Oracle.lib().oracle_init_state(C.byref(cfg), C.byref(params), max_attempts, _p(Q),
+                                       _p(V), _p(U), _p(sp), C.byref(kb))
+    if r != 0:
+        raise RuntimeError("oracle_init_state failed")
+    return Q, V, U, sp, kb.value
+
+
 class Reference:
     """The reference's own timestep (process-global state: one at a time)."""
 
@@ -142,6 +158,12 @@ class Reference:
             lib.ref_gndnst.restype = C.c_double
             lib.ref_unexpected_draws.restype = C.c_long
             lib.ref_theory_visc.restype = C.c_double
+            lib.ref_init_state.argtypes = [C.c_void_p] * 7
+            lib.ref_accessible_volume.restype = C.c_double
+            lib.ref_accessible_volume.argtypes = [C.c_int]
+            lib.ref_checkpoint_write.argtypes = [C.c_char_p, C.c_int, C.c_int]
+            lib.ref_checkpoint_read.argtypes = [C.c_char_p] + [C.c_void_p] * 6
+            lib.ref_checkpoint_particles.argtypes = [C.c_void_p] * 4
             lib.ref_theory_visc.argtypes = [C.c_int, C.c_int] + [C.c_double] * 5 + \
                 [C.c_void_p, C.c_void_p]
             cls._libs[path] = lib
@@ -157,6 +179,56 @@ class Reference:
         r = self._lib.ref_init(C.byref(cfg), self.n, _p(Q), _p(V), _p(U), _p(spid))
         if r != 0:
             raise RuntimeError("ref_init failed")
+
+    @classmethod
+    def from_init(cls, cfg, params, timing=False):
+        """The reference's own initialisation (setcoord, galileantrans, the
+        VSC scaling) through ref_init_state; returns the Reference, which can
+        step on from there, and the arrays Q, V, U, spid and TEMP after the
+        scaling."""
+        self = cls.__new__(cls)
+        self.cfg = cfg
+        self.n = n = sum(params.population)
+        self._lib = cls.lib(timing)
+        Q, V, U = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        sp = np.zeros(n, dtype=np.int32)
+        kb = C.c_double()
+        r = self._lib.ref_init_state(C.byref(cfg), C.byref(params), _p(Q), _p(V), _p(U),
+                                     _p(sp), C.byref(kb))
+        if r != 0:
+            raise RuntimeError("ref_init_state failed")
+        return self, Q, V, U, sp, kb.value
+
+    @classmethod
+    def accessible_volume(cls, cfg, species=0):
+        """The reference's Monte Carlo accessibleVolume (init.c:954-989) with
+        its own generator (the timing build), for cfg's walls."""
+        lib = cls.lib(timing=True)
+        z = np.zeros(3)
+        if lib.ref_init(C.byref(cfg), 0, _p(z), _p(z), None, None) != 0:
+            raise RuntimeError("ref_init failed")
+        return lib.ref_accessible_volume(species)
+
+    def checkpoint_write(self, path, runtime, warmtime=0):
+        """The reference's checkpoint() of the current state to path."""
+        if self._lib.ref_checkpoint_write(str(path).encode(), runtime, warmtime) != 0:
+            raise RuntimeError("ref_checkpoint_write failed")
+
+    @classmethod
+    def checkpoint_read(cls, path, abi_config):
+        """The reference's readchckpnt() of path: (config as the reference
+        holds it, Q, V, U, spid, runtime, warmtime, KBTNOW, AVNOW)."""
+        lib = cls.lib()
+        cfg = abi_config()
+        n, rt, wt, kb = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        av = np.zeros(3)
+        lib.ref_checkpoint_read(str(path).encode(), C.byref(cfg), C.byref(n), C.byref(rt),
+                                C.byref(wt), C.byref(kb), _p(av))
+        m = n.value
+        Q, V, U = np.zeros((m, 3)), np.zeros((m, 3)), np.zeros((m, 3))
+        sp = np.zeros(m, dtype=np.int32)
+        lib.ref_checkpoint_particles(_p(Q), _p(V), _p(U), _p(sp))
+        return cfg, Q, V, U, sp, rt.value, wt.value, kb.value, av
 
     @classmethod
     def theory_visc(cls, coll_op, dim, n, rot_ang, dt, kbt=1.0, m=1.0):

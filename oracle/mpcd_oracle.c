@@ -1039,3 +1039,226 @@ int oracle_shifted_counts(const oracle_t *o, uint32_t step, int *pop) {
     }
     return 0;
 }
+
+/* ============================================================ initial state
+ * initializeSIM's particle set-up (init.c:2092-2170) for QDIST = PRF:
+ * setcoord (init.c:1565-1600) with place, push and orient per particle and
+ * the mean velocity AVV; checkplaceMPC/replace (init.c:1240-1246, 1428-1449)
+ * per particle; galileantrans (mtools.c:673-711) when RFRAME and GPOP > 2;
+ * TEMP about AVV and the VSC scaling (scaleT, therm.c:106-143).  Draws: the
+ * counter-based generator at step 0, per particle, in the streams
+ * MPCD_STREAM_INIT_POS (attempt a: uniforms 4a + d), MPCD_STREAM_INIT_VEL and
+ * MPCD_STREAM_INIT_ORI.  Sums run serially in particle order, as the
+ * reference's loops do. */
+static double init_u(const mpcd_config *c, uint32_t stream, int i, uint32_t k) {
+    return mpcd_rng_uniform(c->seed, c->replica, 0u, stream, (uint32_t)i, k);
+}
+
+/* norm (mtools.c:246-251) with fneq (mtools.c:74-76) */
+static void init_norm(double *x, int dim) {
+    double l = 0.0;
+    for (int i = 0; i < dim; i++) l += x[i] * x[i];
+    l = sqrt(l);
+    if (fabs(l - 0.0) >= TOL)
+        for (int i = 0; i < dim; i++) x[i] = x[i] / l;
+}
+
+/* genrand_coneNP(vec, pi, dim), rand.c:397-425 */
+static void init_cone(const mpcd_config *c, int i, uint32_t *k, double *vec, int dim) {
+    const double theta = MPCD_PI;
+    double ct = cos(theta);
+    if (dim == 3) {
+        double z = init_u(c, MPCD_STREAM_INIT_ORI, i, (*k)++) * (1.0 - ct) + ct;
+        double phi = init_u(c, MPCD_STREAM_INIT_ORI, i, (*k)++) * 2.0 * MPCD_PI;
+        vec[0] = z;
+        vec[1] = sqrt(1.0 - z * z) * cos(phi);
+        vec[2] = sqrt(1.0 - z * z) * sin(phi);
+    } else {
+        double phi = theta * (1. - 2. * init_u(c, MPCD_STREAM_INIT_ORI, i, (*k)++));
+        vec[0] = cos(phi);
+        vec[1] = sin(phi);
+    }
+}
+
+/* orient, init.c:1307-1405 */
+static void init_orient(const mpcd_config *c, int dim, const int *XYZ, int i, int PL,
+                        const double *Q, double *U) {
+    uint32_t k = 0;
+    double noise;
+    int d;
+    if (PL == MPCD_ODIST_RANDORIENT) {
+        init_cone(c, i, &k, U, dim);
+    } else if (PL == MPCD_ODIST_ALIGNX) {
+        noise = 1.0 + 0.02 * (init_u(c, MPCD_STREAM_INIT_ORI, i, k++) - 0.5);
+        U[0] = 0.9999 * noise;
+        U[1] = 0.01414178 * noise;
+        if (dim >= 3) U[2] = 0.000008 * noise;
+    } else if (PL == MPCD_ODIST_ALIGNY) {
+        noise = 1.0 + 0.02 * (init_u(c, MPCD_STREAM_INIT_ORI, i, k++) - 0.5);
+        U[1] = 0.9999 * noise;
+        U[0] = 0.01414178 * noise;
+        if (dim >= 3) U[2] = 0.000008 * noise;
+    } else if (PL == MPCD_ODIST_ALIGNZ) {
+        noise = 1.0 + 0.02 * (init_u(c, MPCD_STREAM_INIT_ORI, i, k++) - 0.5);
+        U[2] = 0.9999 * noise;
+        U[0] = 0.007071 * noise;
+        U[1] = 0.007071 * noise;
+    } else if (PL == MPCD_ODIST_ALIGN45) {
+        if (dim == 2)
+            for (d = 0; d < dim; d++) U[d] = 1. / sqrt(2.);
+        else
+            for (d = 0; d < dim; d++) U[d] = 1. / sqrt(3.);
+    } else if (PL == MPCD_ODIST_PLANEZ) {
+        init_cone(c, i, &k, U, 2);
+    } else if (PL == MPCD_ODIST_PLANEY) {
+        init_cone(c, i, &k, U, 2);
+        U[2] = U[1];
+        U[1] = 0.0;
+    } else if (PL == MPCD_ODIST_PLANEX) {
+        init_cone(c, i, &k, U, 2);
+        U[2] = U[0];
+        U[0] = 0.0;
+    } else if (PL == MPCD_ODIST_ALIGNTR) {
+        double L2 = 0.0;
+        for (d = 0; d < dim; d++) L2 += XYZ[d] * XYZ[d];
+        L2 = sqrt(L2);
+        for (d = 0; d < dim; d++) U[d] = XYZ[d] / L2;
+    } else if (PL == MPCD_ODIST_ALIGNDEFECTPAIR) {
+        double QP[2], QM[2], UP[2], UM[2], kP = 0.5, kM = -0.5, phiP, phiM, wP, wM, wY, r, R;
+        R = 0.5 * sqrt(2.25 * ((double)XYZ[0]) * ((double)XYZ[0]) +
+                       ((double)XYZ[1]) * ((double)XYZ[1]));
+        QP[0] = ((double)XYZ[0]) * 0.25;
+        QP[1] = ((double)XYZ[1]) * 0.5;
+        phiP = atan2(QP[1] - Q[1], QP[0] - Q[0]);
+        UP[0] = cos(kP * phiP);
+        UP[1] = sin(kP * phiP);
+        r = sqrt(pow(QP[0] - Q[0], 2.0) + pow(QP[1] - Q[1], 2.0));
+        wP = 1.0 - r / R;
+        QM[0] = ((double)XYZ[0]) * 0.75;
+        QM[1] = ((double)XYZ[1]) * 0.5;
+        phiM = atan2(-QM[1] + Q[1], -QM[0] + Q[0]);
+        UM[0] = cos(kM * phiM);
+        UM[1] = sin(kM * phiM);
+        r = sqrt(pow(QM[0] - Q[0], 2.0) + pow(QM[1] - Q[1], 2.0));
+        wM = 1.0 - r / R;
+        if (Q[1] <= 0.5 * ((double)XYZ[1]))
+            wY = 1.0 - 2.0 * Q[1] / (double)XYZ[1];
+        else
+            wY = 1.0 - 2.0 * ((double)XYZ[1] - Q[1]) / (double)XYZ[1];
+        U[0] = wP * UP[0] + wM * UM[0] + wY;
+        U[1] = wP * UP[1] + wM * UM[1];
+        if (dim > 2) U[2] = 0.0;
+        init_norm(U, dim);
+    }
+}
+
+/* push, init.c:1261-1291 */
+static void init_push(const mpcd_config *c, int dim, int i, int PL, double MASS, double *V) {
+    const double KBT = c->kbt;
+    int d;
+    if (PL == MPCD_VDIST_RANDVEL) {
+        for (d = 0; d < dim; d++)
+            V[d] = sqrt(KBT / MASS) * (2. * init_u(c, MPCD_STREAM_INIT_VEL, i, d) - 1.);
+    } else if (PL == MPCD_VDIST_HOMOAXIS) {
+        for (d = 0; d < dim; d++) {
+            V[d] = sqrt(dim * KBT / MASS);
+            V[d] *= init_u(c, MPCD_STREAM_INIT_VEL, i, d) <= 0.5 ? -1.0 : 1.0;
+        }
+    } else {
+        /* genrand_gaussMB (rand.c:510-513): sqrt(KBT/M) times a float normal */
+        for (d = 0; d < dim; d++)
+            V[d] = sqrt(KBT / MASS) *
+                   mpcd_rng_normal(c->seed, c->replica, 0u, MPCD_STREAM_INIT_VEL, (uint32_t)i,
+                                   (uint32_t)d);
+        if (PL == MPCD_VDIST_HOMO) {
+            init_norm(V, dim);
+            double normalize = sqrt((double)dim * KBT / MASS);
+            for (d = 0; d < dim; d++) V[d] *= normalize;
+        }
+    }
+}
+
+/* Q, V, U (3 doubles per particle) and spid of the initial state; returns
+ * 0, or -1 for bad arguments or a particle not placed within max_attempts. */
+int oracle_init_state(const mpcd_config *cfg, const mpcd_init_params *p, int max_attempts,
+                      double *Q, double *V, double *U, int *spid, double *kbtnow) {
+    const int dim = cfg->dim;
+    int XYZ[3], i, j, d, s, n = 0;
+    for (d = 0; d < 3; d++) XYZ[d] = d < dim ? cfg->L[d] : 1;
+    for (s = 0; s < cfg->n_species; s++) n += p->population[s];
+    /* setcoord: species in order, then place/push/orient */
+    double AVV[3] = {0.0, 0.0, 0.0};
+    int k = 0;
+    for (s = 0; s < cfg->n_species; s++)
+        for (j = 0; j < p->population[s]; j++) spid[k++] = s;
+    for (i = 0; i < n; i++) {
+        double *q = Q + 3 * i, *v = V + 3 * i, *u = U ? U + 3 * i : NULL;
+        for (d = 0; d < 3; d++) {
+            q[d] = 0.0;
+            v[d] = 0.0;
+            if (u) u[d] = 0.0;
+        }
+        for (d = 0; d < dim; d++) q[d] = init_u(cfg, MPCD_STREAM_INIT_POS, i, d) * XYZ[d];
+        init_push(cfg, dim, i, p->vdist[spid[i]], cfg->species[spid[i]].mass, v);
+        for (d = 0; d < dim; d++) AVV[d] += v[d];
+        if (u && cfg->lc) init_orient(cfg, dim, XYZ, i, p->odist[spid[i]], q, u);
+    }
+    for (d = 0; d < dim; d++) AVV[d] /= (double)n;
+    /* checkplace for every particle: re-place while an interacting wall has
+     * W <= TOL */
+    for (i = 0; i < n; i++) {
+        double *q = Q + 3 * i;
+        int a, inside = 1;
+        for (a = 0; a < max_attempts && inside; a++) {
+            if (a > 0)
+                for (d = 0; d < dim; d++)
+                    q[d] = (double)XYZ[d] * init_u(cfg, MPCD_STREAM_INIT_POS, i, 4u * a + d);
+            inside = 0;
+            for (j = 0; j < cfg->n_walls && !inside; j++) {
+                const mpcd_wall *wl = &cfg->walls[j];
+                if (!wl->inter[spid[i]]) continue;
+                double W = 0.0;
+                for (d = 0; d < dim; d++) W += wl->A[d] * (q[d] - wl->Q[d]);
+                W -= wl->R;
+                if (wl->inv) W *= -1.0;
+                if (W <= TOL) inside = 1;
+            }
+        }
+        if (inside) return -1;
+    }
+    /* galileantrans with VEL = AVV */
+    if (p->rframe && n > 2) {
+        double NET[3] = {0.0, 0.0, 0.0}, totM = 0.0;
+        for (i = 0; i < n; i++) {
+            double M = cfg->species[spid[i]].mass;
+            totM += M;
+            for (d = 0; d < dim; d++) NET[d] += M * V[3 * i + d];
+        }
+        for (d = 0; d < dim; d++) NET[d] /= totM;
+        for (d = 0; d < dim; d++) NET[d] -= AVV[d];
+        for (i = 0; i < n; i++)
+            for (d = 0; d < dim; d++) V[3 * i + d] -= NET[d];
+    }
+    /* TEMP about AVV (therm.c:209-235), then VSC: V *= sqrt(KBT/KBTNOW) */
+    for (int pass = 0; pass < 2; pass++) {
+        double KBT = 0.0;
+        for (i = 0; i < n; i++) {
+            const double *v = V + 3 * i;
+            double t = (v[0] - AVV[0]) * (v[0] - AVV[0]);
+            t += (v[1] - AVV[1]) * (v[1] - AVV[1]);
+            t += (v[2] - AVV[2]) * (v[2] - AVV[2]);
+            KBT += cfg->species[spid[i]].mass * t;
+        }
+        KBT /= (double)(n * dim);
+        if (pass == 1) {
+            if (kbtnow) *kbtnow = KBT;
+            break;
+        }
+        if (KBT > 0.0) {
+            double TSC = sqrt(cfg->kbt / KBT);
+            for (i = 0; i < n; i++)
+                for (d = 0; d < dim; d++) V[3 * i + d] *= TSC;
+        }
+    }
+    return 0;
+}

@@ -24,5 +24,7 @@ double oracle_gndnst(const oracle_t *o);
 int oracle_ncells(const oracle_t *o);
 long oracle_escaped(const oracle_t *o);
 int oracle_shifted_counts(const oracle_t *o, uint32_t step, int *pop);
+int oracle_init_state(const mpcd_config *cfg, const mpcd_init_params *p, int max_attempts,
+                      double *Q, double *V, double *U, int *spid, double *kbtnow);
 
 #endif

@@ -43,6 +43,8 @@
 #include "mpc.h"
 #include "init.h"
 #include "therm.h"
+#include "pout.h"
+#include "read.h"
 
 /* reference globals (globals.h:24-65, common symbols of the core library) */
 extern int DBUG, DIM, MDmode, GPOP, NSPECI, NBC, NS;
@@ -52,6 +54,8 @@ extern int BMHASSPARE;
 extern double BMSPARE;
 
 void setPBC(bc *WALL);                         /* read.c:584 */
+void galileantrans(particleMPC *pp, bc WALL[], simptr simMD, spec SP[], double KBT,
+                   double VEL[], int POP, int NBC, int MDmode, int dimension); /* mtools.c:673 */
 double calcW(bc WALL, particleMPC P);          /* bc.c:55    */
 unsigned long RandomSeedSRD(unsigned long s);  /* rand.c:293 */
 
@@ -71,11 +75,13 @@ static int g_ncells = 0;
 /* draw bookkeeping */
 static uint64_t g_seed = 0;
 static uint32_t g_replica = 0, g_step = 0;
-enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC };
+enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT };
 static int g_phase = PH_NONE;
 static int g_cell = 0;
 static particleMPC *g_cursor = NULL;
 static int g_comp = 0;
+static uint32_t g_stream = 0; /* PH_INIT: the stream of the current draws */
+static int *g_attempt = NULL; /* PH_INIT: placement attempts per particle */
 static int g_pid = 0;
 static uint32_t g_k = 0;
 static int *g_ghost = NULL;
@@ -85,9 +91,10 @@ static long g_unexpected = 0;
 static int cell_id(const cell *c) { return (int)(c - g_cells); }
 
 /* ------------------------------------------------------------ set-up/API */
+static int g_clx = 0; /* rows of g_CL as allocated (readchckpnt rewrites XYZ_P1) */
 int ref_free(void) {
     if (g_CL) {
-        for (int i = 0; i < XYZ_P1[0]; i++) free(g_CL[i]);
+        for (int i = 0; i < g_clx; i++) free(g_CL[i]);
         free(g_CL);
     }
     free(g_cells);
@@ -203,6 +210,7 @@ int ref_init(const mpcd_config *cfg, int n, const double *Q, const double *V,
     g_ncells = XYZ_P1[0] * XYZ_P1[1] * XYZ_P1[2];
     g_cells = (cell *)calloc((size_t)g_ncells, sizeof(cell));
     g_CL = (cell ***)malloc((size_t)XYZ_P1[0] * sizeof(cell **));
+    g_clx = XYZ_P1[0];
     for (i = 0; i < XYZ_P1[0]; i++) {
         g_CL[i] = (cell **)malloc((size_t)XYZ_P1[1] * sizeof(cell *));
         for (j = 0; j < XYZ_P1[1]; j++)
@@ -270,6 +278,192 @@ double ref_theory_visc(int rtech, int dim, double n, double ra, double dt, doubl
     return VISC / (n * m);
 }
 int ref_ncells(void) { return g_ncells; }
+
+/* The reference's initial particle state: setcoord (init.c:1565-1600),
+ * galileantrans when rframe and GPOP > 2, TEMP and the VSC scaling, in the
+ * order of initializeSIM (init.c:2092-2170), then the first binning so that
+ * ref_step can continue from it.  With the injected draws the positions,
+ * velocities and orientations use the counter-based streams at step 0.
+ * Writes Q, V, U (3 doubles per particle), spid and TEMP after scaling. */
+int ref_init_state(const mpcd_config *cfg, const mpcd_init_params *p, double *Q, double *V,
+                   double *U, int *spid, double *kbt_after) {
+    int n = 0, i, s, d, k = 0;
+    for (s = 0; s < cfg->n_species; s++) n += p->population[s];
+    int *sp = (int *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int));
+    double *z = (double *)calloc((size_t)(n > 0 ? n : 1) * 3, sizeof(double));
+    for (s = 0; s < cfg->n_species; s++)
+        for (i = 0; i < p->population[s]; i++) sp[k++] = s;
+    ref_init(cfg, n, z, z, NULL, sp);
+    free(z);
+    free(sp);
+    for (s = 0; s < NSPECI; s++) {
+        g_SP[s].QDIST = PRF;
+        g_SP[s].VDIST = p->vdist[s];
+        g_SP[s].ODIST = p->odist[s];
+    }
+    free(g_attempt);
+    g_attempt = (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int));
+    char dir[4] = "";
+    g_step = 0;
+    g_phase = PH_INIT;
+    setcoord(dir, g_SP, g_pp, g_in.KBT, g_AVV, g_WALL, NULL, 0, g_in.LC);
+    g_phase = PH_NONE;
+    free(g_attempt);
+    g_attempt = NULL;
+    if (p->rframe && GPOP > 2)
+        galileantrans(g_pp, g_WALL, NULL, g_SP, g_in.KBT, g_AVV, GPOP, NBC, 0, DIM);
+    g_KBTNOW = TEMP(g_pp, g_SP, g_WALL, g_AVV);
+    scaleT(g_in.KBT, g_KBTNOW, g_in.dt, g_in.TAU, g_AVV, g_AVNOW, VSC, g_SP, g_in.LC, g_WALL,
+           g_pp, g_CL);
+    g_KBTNOW = TEMP(g_pp, g_SP, g_WALL, g_AVV);
+    if (kbt_after) *kbt_after = g_KBTNOW;
+    for (i = 0; i < n; i++) {
+        for (d = 0; d < 3; d++) {
+            Q[3 * i + d] = g_pp[i].Q[d];
+            V[3 * i + d] = g_pp[i].V[d];
+            if (U) U[3 * i + d] = g_pp[i].U[d];
+        }
+        spid[i] = g_pp[i].SPID;
+    }
+    /* the state's first binning, as ref_init does for uploaded particles */
+    for (i = 0; i < g_ncells; i++) g_cells[i].pp = NULL;
+    binin(g_pp, g_CL);
+    localPROP(g_CL, g_SP, *g_SS, g_in.RTECH, g_in.LC);
+    globalDensities(g_CL, g_SP);
+    if (cfg->gndnst > 0.0) GnDNST = cfg->gndnst;
+    for (d = 0; d < 3; d++) g_AVV[d] = 0.0;
+    return 0;
+}
+
+/* The reference's own checkpoint writer (checkpoint, pout.c:2325-2396) on
+ * the current state, with run counters runtime and warmtime. */
+int ref_checkpoint_write(const char *path, int runtime, int warmtime) {
+    if (!g_pp) return -1;
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    kinTheory *th = (kinTheory *)calloc((size_t)(NSPECI > 0 ? NSPECI : 1), sizeof(kinTheory));
+    kinTheory thg;
+    memset(&thg, 0, sizeof(thg));
+    g_in.simSteps = 1000;
+    g_in.stepsMD = 20;
+    checkpoint(f, g_in, g_SP, g_pp, 0, g_WALL, g_oflags, runtime, warmtime, 0.0, g_AVS, g_avDIR,
+               0.0, 0.0, g_KBTNOW, g_AVV, g_AVNOW, th, thg, *g_SS, NULL);
+    fclose(f);
+    free(th);
+    return 0;
+}
+
+/* The reference's own checkpoint reader (readchckpnt, read.c:669-834) on a
+ * file: the configuration as the reference holds it after reading (into
+ * cfg), the particle count, run counters, KBTNOW and AVNOW; the particles
+ * stay for ref_checkpoint_particles.  Overwrites the reference's globals. */
+static particleMPC *g_rd = NULL;
+static int g_rd_n = 0;
+int ref_checkpoint_read(const char *path, mpcd_config *cfg, int *n, int *runtime, int *warmtime,
+                        double *kbtnow, double *avnow) {
+    inputList in;
+    memset(&in, 0, sizeof(in));
+    in.chckpntInputFile = (char *)path;
+    spec *SP = NULL;
+    particleMPC *pp = NULL;
+    cell ***CL = NULL;
+    int md = 0, i, j, d;
+    bc *WALL = (bc *)calloc(MAXBC, sizeof(bc));
+    outputFlagsList out;
+    memset(&out, 0, sizeof(out));
+    kinTheory *th = (kinTheory *)calloc(MAXSPECI, sizeof(kinTheory));
+    kinTheory thg;
+    double AVVEL, AVS, avDIR[3], S4, stdN, AVV[3];
+    specSwimmer ss;
+    memset(&ss, 0, sizeof(ss));
+    swimmer *sw = NULL;
+    readchckpnt(&in, &SP, &pp, &CL, &md, &WALL, &out, runtime, warmtime, &th, &thg, &AVVEL, &AVS,
+                avDIR, &S4, &stdN, kbtnow, AVV, avnow, &ss, &sw);
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->dim = DIM;
+    for (d = 0; d < 3; d++) {
+        cfg->L[d] = XYZ[d];
+        cfg->grav[d] = in.GRAV[d];
+    }
+    cfg->dt = in.dt;
+    cfg->kbt = in.KBT;
+    cfg->coll_op = in.RTECH;
+    cfg->lc = in.LC;
+    cfg->rot_ang = in.RA;
+    cfg->galinv = in.GALINV;
+    cfg->gndnst = GnDNST;
+    cfg->seed = (uint64_t)in.seed;
+    cfg->n_species = NSPECI;
+    for (i = 0; i < NSPECI && i < MPCD_MAX_SPECIES; i++) {
+        mpcd_species *s = &cfg->species[i];
+        s->mass = SP[i].MASS;
+        s->damp = SP[i].DAMP;
+        s->rfc = SP[i].RFC;
+        s->tumble = SP[i].TUMBLE;
+        s->chihi = SP[i].CHIHI;
+        s->act = SP[i].ACT;
+        s->mfpot = SP[i].MFPOT;
+        s->sigwidth = SP[i].SIGWIDTH;
+        s->sigpos = SP[i].SIGPOS;
+        s->minactratio = SP[i].MINACTRATIO;
+    }
+    cfg->n_walls = NBC;
+    for (i = 0; i < NBC && i < MPCD_MAX_WALLS; i++) {
+        mpcd_wall *w = &cfg->walls[i];
+        const bc *b = &WALL[i];
+        for (d = 0; d < 3; d++) {
+            w->A[d] = b->A[d];
+            w->Q[d] = b->Q[d];
+            w->DVxyz[d] = b->DVxyz[d];
+            w->MUxyz[d] = b->MUxyz[d];
+            w->DUxyz[d] = b->DUxyz[d];
+        }
+        w->R = b->R;
+        w->inv = b->INV;
+        w->phantom = b->PHANTOM;
+        w->coll_type = b->COLL_TYPE;
+        w->DN = b->DN;
+        w->DT = b->DT;
+        w->DVN = b->DVN;
+        w->DVT = b->DVT;
+        w->MVN = b->MVN;
+        w->MVT = b->MVT;
+        w->MUN = b->MUN;
+        w->MUT = b->MUT;
+        for (j = 0; j < MPCD_MAX_SPECIES; j++) w->inter[j] = b->INTER[j];
+    }
+    free(g_rd);
+    g_rd = pp;
+    g_rd_n = GPOP;
+    *n = GPOP;
+    for (i = 0; i < XYZ_P1[0]; i++) {
+        for (j = 0; j < XYZ_P1[1]; j++) free(CL[i][j]);
+        free(CL[i]);
+    }
+    free(CL);
+    free(SP);
+    free(WALL);
+    free(th);
+    free(sw);
+    return 0;
+}
+
+int ref_checkpoint_particles(double *Q, double *V, double *U, int *spid) {
+    for (int i = 0; i < g_rd_n; i++) {
+        for (int d = 0; d < 3; d++) {
+            if (Q) Q[3 * i + d] = g_rd[i].Q[d];
+            if (V) V[3 * i + d] = g_rd[i].V[d];
+            if (U) U[3 * i + d] = g_rd[i].U[d];
+        }
+        if (spid) spid[i] = g_rd[i].SPID;
+    }
+    return 0;
+}
+
+/* The reference's Monte Carlo accessible volume (init.c:954-989) of species
+ * 'spid' for the walls of the last ref_init; with the reference's own
+ * generator (libmpcdref_time.so) it is the value readJson computes. */
+double ref_accessible_volume(int spid) { return accessibleVolume(g_WALL, spid); }
 long ref_unexpected_draws(void) { return g_unexpected; }
 
 /* One call of the reference timestep() (mpc.c:4496) numbered 'step'. */
@@ -327,7 +521,10 @@ int ref_get_cells(int *pop, double *mass, double *vcm, double *cm) {
  * ====================================================================== */
 static float next_normal(void) {
     float g = 0.0f;
-    if (g_phase == PH_COLLIDE && g_cursor) {
+    if (g_phase == PH_INIT) {
+        g = mpcd_rng_normal(g_seed, g_replica, 0u, MPCD_STREAM_INIT_VEL, (uint32_t)g_pid,
+                            (uint32_t)g_comp++);
+    } else if (g_phase == PH_COLLIDE && g_cursor) {
         int pid = (int)(g_cursor - g_pp);
         g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_THERMAL,
                             (uint32_t)pid, (uint32_t)g_comp);
@@ -357,6 +554,8 @@ unsigned long genrand_int32(void) {
 long genrand_int31(void) { return (long)(genrand_int32() >> 1); }
 
 double genrand_real(void) {
+    if (g_phase == PH_INIT)
+        return mpcd_rng_uniform(g_seed, g_replica, 0u, g_stream, (uint32_t)g_pid, g_k++);
     if (g_phase == PH_LC)
         return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_LC,
                                 (uint32_t)g_pid, g_k++);
@@ -390,8 +589,25 @@ void genrand_sphere(double vec[], int dimension) {
     for (int i = 0; i < dimension; i++) vec[i] = (i == 0);
 }
 void genrand_coneNP(double vec[], double theta, int dimension) {
-    (void)theta;
-    genrand_sphere(vec, dimension);
+    if (g_phase != PH_INIT) {
+        genrand_sphere(vec, dimension);
+        return;
+    }
+    /* rand.c:397-425, restated: it lives in the replaced rand.c */
+    double z, phi, ct = cos(theta);
+    if (dimension == _3D) {
+        z = genrand_real() * (1.0 - ct) + ct;
+        phi = genrand_real() * 2.0 * pi;
+        vec[0] = z;
+        vec[1] = sqrt(1.0 - z * z) * cos(phi);
+        vec[2] = sqrt(1.0 - z * z) * sin(phi);
+    } else if (dimension == _2D) {
+        phi = theta * (1. - 2. * genrand_real());
+        vec[0] = cos(phi);
+        vec[1] = sin(phi);
+    } else {
+        g_unexpected++;
+    }
 }
 void genrand_cone(double axis[], double vecOut[], double theta, int dimension) {
     (void)axis;
@@ -503,5 +719,48 @@ void genrand_maierSaupe(double DIR[], double rotAx[], double rotAngle,
     g_pid = (int)(p - g_pp);
     g_k = 0;
     orig(DIR, rotAx, rotAngle, U, KBT, S, effM);
+}
+/* Initialisation: place, push, orient and replace (init.c:1219-1405) learn
+ * their particle from the address they are given. */
+static int pid_of(const void *field, size_t off) {
+    return (int)(((const char *)field - off - (const char *)g_pp) / sizeof(particleMPC));
+}
+typedef void (*place_fn)(double *, int, FILE *);
+void place(double Q[], int PL, FILE *fin) {
+    static place_fn orig = NULL;
+    if (!orig) orig = (place_fn)dlsym(RTLD_NEXT, "place");
+    g_pid = pid_of(Q, offsetof(particleMPC, Q));
+    g_stream = MPCD_STREAM_INIT_POS;
+    g_k = 0;
+    if (g_attempt) g_attempt[g_pid] = 0;
+    orig(Q, PL, fin);
+}
+typedef void (*replace_fn)(particleMPC *);
+void replace(particleMPC *p) {
+    static replace_fn orig = NULL;
+    if (!orig) orig = (replace_fn)dlsym(RTLD_NEXT, "replace");
+    g_pid = (int)(p - g_pp);
+    g_stream = MPCD_STREAM_INIT_POS;
+    g_k = 4u * (uint32_t)(g_attempt ? ++g_attempt[g_pid] : 1);
+    orig(p);
+}
+typedef void (*push_fn)(double *, double, int, double, FILE *);
+void push(double V[], double KBT, int PL, double MASS, FILE *fin) {
+    static push_fn orig = NULL;
+    if (!orig) orig = (push_fn)dlsym(RTLD_NEXT, "push");
+    g_pid = pid_of(V, offsetof(particleMPC, V));
+    g_stream = MPCD_STREAM_INIT_VEL;
+    g_k = 0;
+    g_comp = 0;
+    orig(V, KBT, PL, MASS, fin);
+}
+typedef void (*orient_fn)(double *, double *, int);
+void orient(double U[], double Q[], int PL) {
+    static orient_fn orig = NULL;
+    if (!orig) orig = (orient_fn)dlsym(RTLD_NEXT, "orient");
+    g_pid = pid_of(U, offsetof(particleMPC, U));
+    g_stream = MPCD_STREAM_INIT_ORI;
+    g_k = 0;
+    orig(U, Q, PL);
 }
 #endif /* REF_INJECT */

@@ -33,3 +33,70 @@ def build(name, precision=abi.PREC_FP64, seed=777):
 
 def state(cfg, ppc, sseed):
     return W.synthetic_state(cfg, ppc, seed=sseed)
+
+
+def slab_walls(L, ylo, yhi, inverted=False):
+    """Periodic box with two solid walls inside it across y, at ylo (normal
+    +y) and yhi (normal -y, or +y inverted): the fluid fills ylo < y < yhi,
+    so a uniform placement in the box is often rejected."""
+    w = list(abi.periodic_walls(3, L))
+    w.append(abi.make_wall((0, 1, 0), (0, ylo, 0), 0.0, MVN=-1.0, MVT=-1.0))
+    if inverted:
+        w.append(abi.make_wall((0, 1, 0), (0, yhi, 0), 0.0, MVN=-1.0, MVT=-1.0, inv=1))
+    else:
+        w.append(abi.make_wall((0, -1, 0), (0, yhi, 0), 0.0, MVN=-1.0, MVT=-1.0))
+    return w
+
+
+def _two_species_channel(L):
+    """Channel of two species (masses 1 and 2.5); species 1 ignores the
+    y walls, so the two see different accessible volumes."""
+    cfg = W.base_config(3, L, coll_op=abi.COLL_MPCAT,
+                        species=[W._species(1.0), W._species(2.5)],
+                        walls=slab_walls(L, 1.25, L[1] - 0.5))
+    for w in range(cfg.n_walls):
+        cfg.walls[w].inter[0] = 1
+        cfg.walls[w].inter[1] = 1 if w < cfg.n_walls - 2 else 0
+    return cfg
+
+
+def _nematic_all_odist(L):
+    """2D nematic with ten species, species s initialised with oDist s."""
+    sp = [W._species(mass=1.0 + 0.25 * s, rfc=0.01, tumble=0.5, chihi=0.5, act=0.05,
+                     mfpot=10.0) for s in range(abi.MAX_SPECIES)]
+    cfg = W.base_config(2, L, coll_op=abi.COLL_DIPOLE_DIR_SUM, lc=abi.LC_LOCAL, species=sp)
+    for w in range(cfg.n_walls):
+        for s in range(abi.MAX_SPECIES):
+            cfg.walls[w].inter[s] = 1
+    return cfg
+
+
+_VD = (abi.VDIST_RANDVEL, abi.VDIST_HOMO, abi.VDIST_HOMOAXIS, abi.VDIST_GAUSS)
+
+# initial-state cases: name -> (config builder, populations, vdist, odist,
+# rframe); every config uses generator key 777
+INIT_CASES = {
+    "init_srd3d_gauss": (lambda: W.cfg_srd3d((8, 8, 8)), [2560], abi.VDIST_GAUSS, 0, 1),
+    "init_srd3d_randvel": (lambda: W.cfg_srd3d((8, 8, 8)), [2560], abi.VDIST_RANDVEL, 0, 0),
+    "init_slab_homo": (lambda: W.base_config(3, (10, 12, 8), coll_op=abi.COLL_MPCAT,
+                                             walls=slab_walls((10, 12, 8), 1.5, 9.75)),
+                       [6000], abi.VDIST_HOMO, 0, 1),
+    "init_slab_inv_homoaxis": (lambda: W.base_config(3, (10, 12, 8), coll_op=abi.COLL_RAT,
+                                                     walls=slab_walls((10, 12, 8), 2.25, 7.5,
+                                                                      True)),
+                               [4000], abi.VDIST_HOMOAXIS, 0, 1),
+    "init_two_species": (lambda: _two_species_channel((6, 8, 5)), [1500, 900],
+                         [abi.VDIST_GAUSS, abi.VDIST_RANDVEL], 0, 1),
+    "init_nematic_odist": (lambda: _nematic_all_odist((12, 10)), [60] * abi.MAX_SPECIES,
+                           [_VD[s % 4] for s in range(abi.MAX_SPECIES)],
+                           list(range(abi.MAX_SPECIES)), 1),
+}
+
+
+def init_case(name, precision=abi.PREC_FP64):
+    """(config, InitParams) of an initial-state case."""
+    builder, pops, vd, od, rframe = INIT_CASES[name]
+    cfg = builder()
+    cfg.precision = precision
+    cfg.seed = 777
+    return cfg, abi.init_params(pops, vdist=vd, odist=od, rframe=rframe)

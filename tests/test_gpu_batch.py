@@ -123,3 +123,40 @@ def test_batch_upload_rejects_positions_outside_their_box():
     assert q.shape == (800, 3) and np.all(np.isfinite(vv))
     assert np.all(q[:500] < 8) and np.all(q[500:] < 6)
     bat.close()
+
+
+def test_batch_per_box_momentum_and_temperature_against_fp64():
+    """Each box of the mixed ensemble against the FP64 form of the same box
+    (a single-box FP64 handle with the same generator key, so the same grid
+    shifts, axes and initial state): after 40 steps (a re-sort included) the
+    box's temperature (TEMP, therm.c:209-235) agrees to 1e-5 relative and its
+    momentum to 1e-6 of the box's momentum scale, the FP32 rounding of the
+    mixed form; the FP64 boxes conserve momentum to 1e-12 of that scale."""
+    states = _states()
+    base = W.cfg_srd3d(SIZES[0], precision=abi.PREC_MIXED, seed=SEEDS[0])
+    bat = Batch(base, SIZES, SEEDS)
+    npart = [len(Q) for _, Q, _ in states]
+    bat.upload(npart, np.concatenate([Q for _, Q, _ in states]),
+               np.concatenate([V for _, _, V in states]), step0=1)
+    nsteps = 40
+    bat.step(nsteps)
+    Qb, Vb = bat.download()
+    kb, _ = bat.globals()
+    off = 0
+    for b, (cfg, Q, V) in enumerate(states):
+        c64 = W.cfg_srd3d(SIZES[b], precision=abi.PREC_FP64, seed=SEEDS[b])
+        c64.replica = b
+        g = Solver(c64)
+        g.upload(Q, V, None, np.zeros(len(Q), dtype=np.int32))
+        g.step(nsteps, 1)
+        _, v64, _ = g.download()
+        k64, _ = g.globals()
+        n = len(Q)
+        scale = np.abs(V).sum()
+        p0 = V.sum(axis=0)
+        assert np.abs(v64.sum(axis=0) - p0).max() / scale < 1e-12, b
+        assert np.abs(Vb[off:off + n].sum(axis=0) - v64.sum(axis=0)).max() / scale < 1e-6, b
+        assert kb[b] == pytest.approx(k64, rel=1e-5), b
+        off += n
+        g.close()
+    bat.close()
