@@ -213,7 +213,11 @@ typedef struct mpcd_init_params {
  * any uploaded one and downloads like an upload.  MPCD_ERR_ARG if a species
  * with particles has no accessible volume (the reference loops for ever
  * there) or a particle is still inside a wall after the attempts its
- * species' accessible fraction allows (64 / fraction, at least 256). */
+ * species' accessible fraction allows (64 / fraction, at least 256).
+ * MPCD_ERR_UNSUPPORTED for vdist READ, and for a 2D nematic, the odist
+ * codes ALIGNZ, PLANEY and PLANEX: they give the orientation a z component,
+ * which the reference keeps and rotates back into the plane, but a 2D state
+ * here does not hold. */
 int mpcd_init_state(mpcd_handle *h, const mpcd_init_params *p, double *kbtnow);
 
 /* Volume accessible to species 'species': the box volume (XYZ[2] = 1 in 2D)
@@ -461,6 +465,58 @@ int mpcd_batch_info(mpcd_batch *b, int *n, int *slots, int *cells);
 int mpcd_srd_step_noalloc(const mpcd_config *cfg, int n, double *Q, double *V,
                           uint32_t step, double *globals, unsigned long long *counters,
                           void *stream);
+
+/* ---- output fields ----------------------------------------------------
+ * Per-species populations of the end-of-step cells (as mpcd_cell_props
+ * re-bins them): counts[s * ncells + c], cells of the (L+1)^D grid in
+ * row-major order; with one species, the cell populations. */
+int mpcd_cell_species(mpcd_handle *h, int *counts);
+
+/* The flow field's running sum (localFLOW + sumFLOW, mpc.c:226-246, which
+ * the reference runs after every step while flow output is on): enable = 1
+ * starts an empty sum (and every following step adds the end-of-step cell
+ * velocities to it), 0 stops and frees it. */
+int mpcd_flow_enable(mpcd_handle *h, int enable);
+
+/* Copy the flow sum (3 doubles per cell of the (L+1)^D grid) and the number
+ * of steps in it; reset = 1 empties it, as flowout does after writing
+ * (pout.c:1695).  MPCD_ERR_STATE when the flow sum is off. */
+int mpcd_flow_read(mpcd_handle *h, double *flow, long long *nsteps, int reset);
+
+/* Sum over the particles of m v^2 / 2 (enout's MPCD_kin, pout.c:1393-1399). */
+int mpcd_kinetic_energy(mpcd_handle *h, double *ke);
+
+/* The reference's output files, printed from host arrays as its writers
+ * print them (cells of the L^D box in x -> y -> z order; arrays over the
+ * (L+1)^D grid as the calls above return them).  header = 1 creates the
+ * file with the reference's banner and column header (openBasic,
+ * init.c:51-63); header = 0 appends one block.  t is the time printed
+ * (runtime * dt, as outputResults passes it). */
+int mpcd_write_coarse(const char *path, const mpcd_config *cfg, double t, const int *pop,
+                      const double *vcm, const int *spc, int header);      /* coarseout */
+int mpcd_write_velfield(const char *path, const mpcd_config *cfg, double t, const double *vcm,
+                        int header);                                       /* velout */
+int mpcd_write_densityfield(const char *path, const mpcd_config *cfg, double t, const int *pop,
+                            const double *mass, const int *spc, int header); /* densityout */
+int mpcd_write_flowfield(const char *path, const mpcd_config *cfg, double t, const double *flow,
+                         int interval, int header);                        /* flowout */
+int mpcd_write_avvel(const char *path, double t, const double avnow[3], double kbtnow,
+                     const double grad[9], int header);          /* avveloutWithGradVel */
+int mpcd_write_energy(const char *path, double t, double kinetic, double kbtnow,
+                      int header);                                         /* enout */
+
+/* The velocity gradient of localVelGrad (lc.c:2054-2162: D3Q15 or D2Q9
+ * weights over the bulk, edges copied from their inner neighbour) from the
+ * cell velocities, into E (9 doubles per cell of the (L+1)^D grid, zero at
+ * first; entries outside the bulk and the copies, corners of the extra
+ * layer, keep what they held, as the reference's cells do), and its mean
+ * over the L^D box (grad, row-major; may be NULL), what avVel.dat prints. */
+int mpcd_vel_grad(const mpcd_config *cfg, const double *vcm, double *E, double grad[9]);
+
+/* avVel (therm.c:362-367) of cell velocities: their sum over the (L+1)^D
+ * grid / VOL, the AVNOW that outputResults recomputes after its re-bin and
+ * prints in avVel.dat. */
+int mpcd_av_vel(const mpcd_config *cfg, const double *vcm, double avnow[3]);
 
 /* ---- checkpoints in the reference's format ----------------------------
  * The reference checkpoints a run as text: checkpoint (pout.c:2325-2396)

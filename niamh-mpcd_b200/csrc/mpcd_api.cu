@@ -59,7 +59,9 @@ struct mpcd_handle {
     double *lcbuf;
     double *modes;   // transverse momentum modes (mpcd_transverse_modes)
     bool stepped;        // a step ran since the last upload (mpcd_debug_cell_counts)
-    double *props;       // mpcd_cell_props accumulators: 7 doubles + 1 int per cell
+    double *props;       // mpcd_cell_props accumulators: 7 doubles + (1 + species) ints per cell
+    double *flow;        // flow field running sum, 3 doubles per cell (null: off)
+    long long flow_steps;  // steps summed into flow
     double *host_ring;   // pinned: per-step globals of mpcd_step_record
     int per_blocks;      // persistent family: blocks of the launch (0: not planned, -1: unfit)
     int per_planned_n;   // particle count the plan was made for
@@ -299,6 +301,7 @@ extern "C" int mpcd_destroy(mpcd_handle *h) {
     cudaFree(h->r64pop);
     cudaFree(h->lcbuf);
     cudaFree(h->props);
+    cudaFree(h->flow);
     cudaFree(h->per_pop);
     cudaFree(h->per_work);
     if (h->host_acc) cudaFreeHost(h->host_acc);
@@ -631,6 +634,11 @@ extern "C" int mpcd_init_state(mpcd_handle *h, const mpcd_init_params *p, double
             vd != MPCD_VDIST_GAUSS)
             return MPCD_ERR_UNSUPPORTED;
         if (dc.lc && (od < MPCD_ODIST_RANDORIENT || od > MPCD_ODIST_ALIGNDEFECTPAIR))
+            return MPCD_ERR_UNSUPPORTED;
+        // the 2D nematic state holds the orientation's x and y only: the
+        // codes that give a 2D orientation a z component are refused
+        if (dc.lc && dc.dim == 2 &&
+            (od == MPCD_ODIST_ALIGNZ || od == MPCD_ODIST_PLANEY || od == MPCD_ODIST_PLANEX))
             return MPCD_ERR_UNSUPPORTED;
         plan.vdist[s] = vd;
         plan.odist[s] = od;
@@ -1379,18 +1387,27 @@ static int run_step_lc(mpcd_handle *h, typename T::State *st, uint32_t step) {
     return MPCD_OK;
 }
 
+static int flow_accumulate(mpcd_handle *h);
+
 extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
     if (!h || nsteps < 0) return MPCD_ERR_ARG;
     if (h->n <= 0) return MPCD_ERR_STATE;
     if (h->strategy < 0) h->strategy = default_strategy(h);
     if (h->tile_target <= 0) h->tile_target = h->prec == MPCD_PREC_MIXED ? 1024 : 768;
     if (nsteps > 0 && !h->dc.lc && kernel_family(h) == MPCD_KERNEL_PERSIST) {
-        const int r = h->dc.dim == 3 ? run_steps_per<3>(h, nsteps, step0)
-                                     : run_steps_per<2>(h, nsteps, step0);
-        if (r != MPCD_OK) return r;
-        h->last_step = step0 + (uint32_t)(nsteps - 1);
-        h->steps += (uint64_t)nsteps;
-        h->stepped = true;
+        // all steps in one launch, or one launch per step while the flow
+        // field is summed
+        const int chunk = h->flow ? 1 : nsteps;
+        for (int k = 0; k < nsteps; k += chunk) {
+            const uint32_t s0 = step0 + (uint32_t)k;
+            int r = h->dc.dim == 3 ? run_steps_per<3>(h, chunk, s0)
+                                         : run_steps_per<2>(h, chunk, s0);
+            if (r != MPCD_OK) return r;
+            h->last_step = s0 + (uint32_t)(chunk - 1);
+            h->steps += (uint64_t)chunk;
+            h->stepped = true;
+            if (h->flow && (r = flow_accumulate(h)) != MPCD_OK) return r;
+        }
         return MPCD_OK;
     }
     for (int k = 0; k < nsteps; k++) {
@@ -1413,6 +1430,7 @@ extern "C" int mpcd_step(mpcd_handle *h, int nsteps, uint32_t step0) {
         h->last_step = step;
         h->steps++;
         h->stepped = true;
+        if (h->flow && (r = flow_accumulate(h)) != MPCD_OK) return r;
     }
     return MPCD_OK;
 }
@@ -1654,20 +1672,21 @@ extern "C" int mpcd_transverse_modes(mpcd_handle *h, double *out, int *nmodes) {
     return MPCD_OK;
 }
 
-extern "C" int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
-                               double *cm) {
-    if (!h) return MPCD_ERR_ARG;
-    // the re-bin on the unshifted grid and the per-cell moments, on the
-    // device; only the cell arrays come back
-    const int n = h->n, dim = h->dc.dim;
+// The end-of-step cell properties on the unshifted grid (re-bin + the
+// per-cell moments) into h->props, on the handle's stream; returns the
+// views into it.
+static int props_compute(mpcd_handle *h, CellProps *out) {
+    const int n = h->n, dim = h->dc.dim, ns = h->dc.n_species;
     const size_t nc = (size_t)h->dc.ncells;
-    if (!h->props) CK(cudaMalloc((void **)&h->props, nc * (7 * sizeof(double) + sizeof(int))));
+    const size_t bytes = nc * (7 * sizeof(double) + (size_t)(1 + (ns > 1 ? ns : 0)) * sizeof(int));
+    if (!h->props && cudaMalloc((void **)&h->props, bytes) != cudaSuccess) return MPCD_ERR_NOMEM;
     CellProps p;
     p.mass = h->props;
     p.sv = p.mass + nc;
     p.sq = p.sv + 3 * nc;
     p.pop = (int *)(p.sq + 3 * nc);
-    CK(cudaMemsetAsync(h->props, 0, nc * (7 * sizeof(double) + sizeof(int)), h->stream));
+    p.spc = ns > 1 ? p.pop + nc : nullptr;
+    CK(cudaMemsetAsync(h->props, 0, bytes, h->stream));
     if (n > 0) {
         const int g = grid_for(h, n);
         if (h->prec == MPCD_PREC_FP64) {
@@ -1684,6 +1703,19 @@ extern "C" int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *v
         k_props_finish<<<grid_for(h, (int)nc), 256, 0, h->stream>>>(h->dc, p);
     }
     CK(cudaGetLastError());
+    *out = p;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *vcm,
+                               double *cm) {
+    if (!h) return MPCD_ERR_ARG;
+    // the re-bin on the unshifted grid and the per-cell moments, on the
+    // device; only the cell arrays come back
+    const size_t nc = (size_t)h->dc.ncells;
+    CellProps p;
+    int r = props_compute(h, &p);
+    if (r != MPCD_OK) return r;
     if (pop) CK(cudaMemcpyAsync(pop, p.pop, nc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     if (mass)
         CK(cudaMemcpyAsync(mass, p.mass, nc * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -1692,6 +1724,81 @@ extern "C" int mpcd_cell_props(mpcd_handle *h, int *pop, double *mass, double *v
                            h->stream));
     if (cm)
         CK(cudaMemcpyAsync(cm, p.sq, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_cell_species(mpcd_handle *h, int *counts) {
+    if (!h || !counts) return MPCD_ERR_ARG;
+    const size_t nc = (size_t)h->dc.ncells;
+    CellProps p;
+    int r = props_compute(h, &p);
+    if (r != MPCD_OK) return r;
+    if (p.spc)
+        CK(cudaMemcpyAsync(counts, p.spc, (size_t)h->dc.n_species * nc * sizeof(int),
+                           cudaMemcpyDeviceToHost, h->stream));
+    else  // one species: its populations are the cells'
+        CK(cudaMemcpyAsync(counts, p.pop, nc * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_kinetic_energy(mpcd_handle *h, double *ke) {
+    if (!h || !ke) return MPCD_ERR_ARG;
+    *ke = 0.0;
+    if (h->n <= 0) return MPCD_OK;
+    int r = xfer_reserve(h, 256);
+    if (r != MPCD_OK) return r;
+    double *out = (double *)h->xfer;
+    CK(cudaMemsetAsync(out, 0, sizeof(double), h->stream));
+    const int g = grid_for(h, h->n);
+    if (h->prec == MPCD_PREC_FP64)
+        k_kinetic<<<g, 256, 0, h->stream>>>(h->dc, h->f[h->cur], h->n, out);
+    else
+        k_kinetic<<<g, 256, 0, h->stream>>>(h->dc, h->mx[h->cur], h->n, out);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ke, out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_flow_enable(mpcd_handle *h, int enable) {
+    if (!h) return MPCD_ERR_ARG;
+    if (!enable) {
+        cudaFree(h->flow);
+        h->flow = nullptr;
+        h->flow_steps = 0;
+        return MPCD_OK;
+    }
+    const size_t bytes = 3 * (size_t)h->dc.ncells * sizeof(double);
+    if (!h->flow && cudaMalloc((void **)&h->flow, bytes) != cudaSuccess) return MPCD_ERR_NOMEM;
+    CK(cudaMemsetAsync(h->flow, 0, bytes, h->stream));
+    h->flow_steps = 0;
+    return MPCD_OK;
+}
+
+// One step's contribution to the flow field: the end-of-step cell
+// velocities (the re-bin and localPROP of mpc.c:4936-4942) added to the sum.
+static int flow_accumulate(mpcd_handle *h) {
+    CellProps p;
+    int r = props_compute(h, &p);
+    if (r != MPCD_OK) return r;
+    k_flow_add<<<grid_for(h, h->dc.ncells), 256, 0, h->stream>>>(h->dc, p.sv, h->flow);
+    CK(cudaGetLastError());
+    h->flow_steps++;
+    return MPCD_OK;
+}
+
+extern "C" int mpcd_flow_read(mpcd_handle *h, double *flow, long long *nsteps, int reset) {
+    if (!h) return MPCD_ERR_ARG;
+    if (!h->flow) return MPCD_ERR_STATE;
+    const size_t bytes = 3 * (size_t)h->dc.ncells * sizeof(double);
+    if (flow) CK(cudaMemcpyAsync(flow, h->flow, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (nsteps) *nsteps = h->flow_steps;
+    if (reset) {
+        CK(cudaMemsetAsync(h->flow, 0, bytes, h->stream));
+        h->flow_steps = 0;
+    }
     CK(cudaStreamSynchronize(h->stream));
     return MPCD_OK;
 }

@@ -13,8 +13,9 @@
 //        init.c:1002-1018): the mean population of the occupied cells of the
 //        L^D box (the extra layer excluded), as integer counts.
 //   k_props_*  the end-of-step re-bin on the unshifted grid and localPROP's
-//        POP, MASS, VCM and CM per cell (mpc.c:4936-4942, 64-216), which the
-//        reference's output writers read (pout.c:640-1757).
+//        POP, MASS, VCM, CM and per-species populations per cell
+//        (mpc.c:4936-4942, 64-216), which the reference's output writers
+//        read (pout.c:640-1757); k_flow_add the flow field's running sum.
 //   k_counts_*  the populations of the cells of the next step's shifted grid
 //        exactly as the step's own kernels hold them (the sort's starts, the
 //        resident families' population sums), for parity checks.
@@ -194,19 +195,35 @@ __global__ void __launch_bounds__(256) k_gndnst_reduce(const __grid_constant__ D
     }
 }
 
+// One particle's m v^2 / 2 (E = sum v_d^2, then times m/2, as enout).
+__device__ __forceinline__ double kinetic_of(const DevCfg &c, const Fp64State &s, int i) {
+    double e = 0.0;
+    for (int d = 0; d < c.dim; d++) e += s.v[d][i] * s.v[d][i];
+    return e * 0.5 * c.mass[s.sp ? s.sp[i] : 0];
+}
+__device__ __forceinline__ double kinetic_of(const DevCfg &c, const MixState &s, int i) {
+    const float4 w = s.W[i];
+    const double v[3] = {(double)w.x, (double)w.y, (double)w.z};
+    double e = 0.0;
+    for (int d = 0; d < c.dim; d++) e += v[d] * v[d];
+    return e * 0.5 * c.mass[s.sp ? s.sp[i] : 0];
+}
+
 // Per-cell output properties on the unshifted grid: the accumulators.
 struct CellProps {
     int *pop;
     double *mass;  // [nc]
     double *sv;    // [3 nc]: sum m v, then VCM
     double *sq;    // [3 nc]: sum m Q, then CM
+    int *spc;      // [n_species nc]: populations per species (null: one species)
 };
 
 // One particle's contribution: its cell by truncation (clamped), as bin(...,
 // 0) (mpc.c:958-982, no periodic L -> 0 on the unshifted grid).
 template <int DIM>
 __device__ __forceinline__ void props_add(const DevCfg &c, CellProps p, const double q[3],
-                                          const double v[3], double m) {
+                                          const double v[3], int sp) {
+    const double m = c.mass[sp];
     int idx[3] = {0, 0, 0};
     for (int d = 0; d < DIM; d++) {
         int a = (int)q[d];
@@ -216,6 +233,7 @@ __device__ __forceinline__ void props_add(const DevCfg &c, CellProps p, const do
     }
     const int k = cell_lin(c, idx[0], idx[1], idx[2]);
     atomicAdd(&p.pop[k], 1);
+    if (p.spc) atomicAdd(&p.spc[(size_t)sp * c.ncells + k], 1);
     atomicAdd(&p.mass[k], m);
     for (int d = 0; d < DIM; d++) {
         atomicAdd(&p.sv[3 * (size_t)k + d], v[d] * m);
@@ -232,7 +250,7 @@ __global__ void __launch_bounds__(256) k_props_f64(const __grid_constant__ DevCf
             q[d] = s.q[d][i];
             v[d] = s.v[d][i];
         }
-        props_add<DIM>(c, p, q, v, c.mass[s.sp ? s.sp[i] : 0]);
+        props_add<DIM>(c, p, q, v, s.sp ? s.sp[i] : 0);
     }
 }
 
@@ -251,7 +269,7 @@ __global__ void __launch_bounds__(256) k_props_mix(const __grid_constant__ DevCf
             q[d] = (double)ci[d] + (double)f[d] * kFxInv;
             v[d] = (double)wv[d];
         }
-        props_add<DIM>(c, p, q, v, c.mass[s.sp ? s.sp[i] : 0]);
+        props_add<DIM>(c, p, q, v, s.sp ? s.sp[i] : 0);
     }
 }
 
@@ -266,6 +284,34 @@ __global__ void __launch_bounds__(256) k_props_finish(const __grid_constant__ De
             p.sv[3 * (size_t)k + d] /= M;
             p.sq[3 * (size_t)k + d] /= M;
         }
+    }
+}
+
+// FLOW += VCM over every cell of the (L+1)^D grid (sumFLOW, mpc.c:241-246,
+// after localFLOW's per-cell centre-of-mass velocity, mpc.c:226-231 and
+// 3889-3910, which equals localPROP's VCM for MPCD particles alone).
+__global__ void __launch_bounds__(256) k_flow_add(const __grid_constant__ DevCfg c,
+                                                  const double *vcm, double *flow) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < c.ncells; k += gridDim.x * blockDim.x)
+        for (int d = 0; d < c.dim; d++) flow[3 * (size_t)k + d] += vcm[3 * (size_t)k + d];
+}
+
+// Sum of m v^2 / 2 over the particles (per-block sums, one FP64 atomic per
+// block).
+template <class S>
+__global__ void __launch_bounds__(256) k_kinetic(const __grid_constant__ DevCfg c, S s, int n,
+                                                 double *out) {
+    __shared__ double red[8];
+    double e = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        e += kinetic_of(c, s, i);
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        atomicAdd(out, t);
     }
 }
 

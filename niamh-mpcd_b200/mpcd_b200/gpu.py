@@ -30,7 +30,10 @@ EXPORTS = [
     "mpcd_download_species", "mpcd_get_config", "mpcd_particle_count", "mpcd_ckpt_read", "mpcd_ckpt_create",
     "mpcd_ckpt_free", "mpcd_ckpt_write", "mpcd_ckpt_config", "mpcd_ckpt_get_run",
     "mpcd_ckpt_set_run", "mpcd_ckpt_count", "mpcd_ckpt_particles", "mpcd_ckpt_set_particles",
-    "mpcd_ckpt_upload", "mpcd_ckpt_capture",
+    "mpcd_ckpt_upload", "mpcd_ckpt_capture", "mpcd_cell_species", "mpcd_flow_enable",
+    "mpcd_flow_read", "mpcd_kinetic_energy", "mpcd_write_coarse", "mpcd_write_velfield",
+    "mpcd_write_densityfield", "mpcd_write_flowfield", "mpcd_write_avvel", "mpcd_write_energy",
+    "mpcd_vel_grad", "mpcd_av_vel",
 ]
 
 _lib = None
@@ -71,6 +74,19 @@ def load():
         lib.mpcd_ckpt_set_particles.argtypes = [vp, C.c_int, vp, vp, vp, vp]
         lib.mpcd_ckpt_upload.argtypes = [vp, vp]
         lib.mpcd_ckpt_capture.argtypes = [vp, vp]
+        lib.mpcd_cell_species.argtypes = [vp, vp]
+        lib.mpcd_flow_enable.argtypes = [vp, C.c_int]
+        lib.mpcd_flow_read.argtypes = [vp, vp, vp, C.c_int]
+        lib.mpcd_kinetic_energy.argtypes = [vp, vp]
+        lib.mpcd_write_coarse.argtypes = [C.c_char_p, vp, C.c_double, vp, vp, vp, C.c_int]
+        lib.mpcd_write_velfield.argtypes = [C.c_char_p, vp, C.c_double, vp, C.c_int]
+        lib.mpcd_write_densityfield.argtypes = [C.c_char_p, vp, C.c_double, vp, vp, vp, C.c_int]
+        lib.mpcd_write_flowfield.argtypes = [C.c_char_p, vp, C.c_double, vp, C.c_int, C.c_int]
+        lib.mpcd_write_avvel.argtypes = [C.c_char_p, C.c_double, vp, C.c_double, vp, C.c_int]
+        lib.mpcd_write_energy.argtypes = [C.c_char_p, C.c_double, C.c_double, C.c_double,
+                                          C.c_int]
+        lib.mpcd_vel_grad.argtypes = [vp, vp, vp, vp]
+        lib.mpcd_av_vel.argtypes = [vp, vp, vp]
         lib.mpcd_download_particles_strided.argtypes = [vp, vp, C.c_size_t, C.c_size_t,
                                                         C.c_size_t, C.c_size_t]
         lib.mpcd_step.argtypes = [vp, C.c_int, C.c_uint32]
@@ -146,6 +162,68 @@ def accessible_volume(cfg, species=0):
     _check(lib.mpcd_accessible_volume(C.byref(cfg), species, C.byref(v)),
            "mpcd_accessible_volume")
     return v.value
+
+
+class FieldWriter:
+    """The reference's output files (coarsegrain, velfield, densityfield,
+    flowfield, avVel, energy .dat) from cell arrays, through the library's
+    host writers.  Keeps the velocity-gradient array between calls, as the
+    reference's cells keep theirs."""
+
+    def __init__(self, cfg, outdir):
+        self.lib = load()
+        self.cfg = cfg
+        self.dir = str(outdir)
+        L = [cfg.L[d] if d < cfg.dim else 1 for d in range(3)]
+        self.nc = (L[0] + 1) * (L[1] + 1) * (L[2] + 1)
+        self.E = np.zeros(9 * self.nc)
+        self.started = set()
+
+    def _path(self, name):
+        return os.path.join(self.dir, name + ".dat").encode()
+
+    def _hdr(self, name):
+        first = name not in self.started
+        self.started.add(name)
+        return int(first)
+
+    def write(self, t, pop, mass, vcm, spc, kbtnow, kinetic, flow=None, interval=0):
+        """One output step: arrays over the (L+1)^D grid (vcm and flow as
+        (nc, 3)); spc per species (ns, nc) or None for one species."""
+        cfg = C.byref(self.cfg)
+        pop = np.ascontiguousarray(pop, dtype=np.int32)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        vcm = np.ascontiguousarray(vcm, dtype=np.float64)
+        sp = None if spc is None else np.ascontiguousarray(spc, dtype=np.int32)
+        lib = self.lib
+        _check(lib.mpcd_write_coarse(self._path("coarsegrain"), cfg, t, _p(pop), _p(vcm), _p(sp),
+                                     self._hdr("coarsegrain")), "mpcd_write_coarse")
+        _check(lib.mpcd_write_velfield(self._path("velfield"), cfg, t, _p(vcm),
+                                       self._hdr("velfield")), "mpcd_write_velfield")
+        _check(lib.mpcd_write_densityfield(self._path("densityfield"), cfg, t, _p(pop), _p(mass),
+                                           _p(sp), self._hdr("densityfield")),
+               "mpcd_write_densityfield")
+        if flow is not None:
+            fl = np.ascontiguousarray(flow, dtype=np.float64)
+            _check(lib.mpcd_write_flowfield(self._path("flowfield"), cfg, t, _p(fl), interval,
+                                            self._hdr("flowfield")), "mpcd_write_flowfield")
+        grad = np.zeros(9)
+        av = np.zeros(3)
+        _check(lib.mpcd_vel_grad(cfg, _p(vcm), _p(self.E), _p(grad)), "mpcd_vel_grad")
+        _check(lib.mpcd_av_vel(cfg, _p(vcm), _p(av)), "mpcd_av_vel")
+        _check(lib.mpcd_write_avvel(self._path("avVel"), t, _p(av), kbtnow, _p(grad),
+                                    self._hdr("avVel")), "mpcd_write_avvel")
+        _check(lib.mpcd_write_energy(self._path("energy"), t, kinetic, kbtnow,
+                                     self._hdr("energy")), "mpcd_write_energy")
+
+    def write_from(self, solver, t, kbtnow, flow_interval=0):
+        """One output step from a Solver's state (cell fields on the device;
+        the flow sum read and emptied when flow_interval > 0)."""
+        pop, mass, vcm, _ = solver.cell_props()
+        pop, mass, vcm = pop.reshape(-1), mass.reshape(-1), vcm.reshape(-1, 3)
+        spc = solver.cell_species() if self.cfg.n_species > 1 else None
+        flow = solver.flow_read(reset=True)[0] if flow_interval > 0 else None
+        self.write(t, pop, mass, vcm, spc, kbtnow, solver.kinetic_energy(), flow, flow_interval)
 
 
 class Checkpoint:
@@ -269,6 +347,33 @@ class Solver:
         cfg = abi.Config()
         _check(self.lib.mpcd_get_config(self.h, C.byref(cfg)), "mpcd_get_config")
         return cfg
+
+    def cell_species(self):
+        """Per-species populations of the end-of-step cells, (ns, nc)."""
+        ns = self.cfg.n_species
+        L = [self.cfg.L[d] if d < self.cfg.dim else 1 for d in range(3)]
+        nc = (L[0] + 1) * (L[1] + 1) * (L[2] + 1)
+        out = np.zeros(ns * nc, dtype=np.int32)
+        _check(self.lib.mpcd_cell_species(self.h, _p(out)), "mpcd_cell_species")
+        return out.reshape(ns, nc)
+
+    def flow_enable(self, on=True):
+        _check(self.lib.mpcd_flow_enable(self.h, int(bool(on))), "mpcd_flow_enable")
+
+    def flow_read(self, reset=False):
+        """(flow sum (nc, 3), steps summed)."""
+        L = [self.cfg.L[d] if d < self.cfg.dim else 1 for d in range(3)]
+        nc = (L[0] + 1) * (L[1] + 1) * (L[2] + 1)
+        f = np.zeros((nc, 3))
+        k = C.c_longlong()
+        _check(self.lib.mpcd_flow_read(self.h, _p(f), C.byref(k), int(bool(reset))),
+               "mpcd_flow_read")
+        return f, k.value
+
+    def kinetic_energy(self):
+        e = C.c_double()
+        _check(self.lib.mpcd_kinetic_energy(self.h, C.byref(e)), "mpcd_kinetic_energy")
+        return e.value
 
     def species(self):
         """Species id of every particle, in the original order."""

@@ -164,6 +164,10 @@ class Reference:
             lib.ref_checkpoint_write.argtypes = [C.c_char_p, C.c_int, C.c_int]
             lib.ref_checkpoint_read.argtypes = [C.c_char_p] + [C.c_void_p] * 6
             lib.ref_checkpoint_particles.argtypes = [C.c_void_p] * 4
+            lib.ref_set_flow.argtypes = [C.c_int]
+            lib.ref_get_flow.argtypes = [C.c_void_p]
+            lib.ref_get_cell_species.argtypes = [C.c_void_p]
+            lib.ref_write_outputs.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int]
             lib.ref_theory_visc.argtypes = [C.c_int, C.c_int] + [C.c_double] * 5 + \
                 [C.c_void_p, C.c_void_p]
             cls._libs[path] = lib
@@ -208,6 +212,28 @@ class Reference:
         if lib.ref_init(C.byref(cfg), 0, _p(z), _p(z), None, None) != 0:
             raise RuntimeError("ref_init failed")
         return lib.ref_accessible_volume(species)
+
+    def set_flow(self, on=True):
+        """Sum the cell velocities into FLOW after every step (flow output)."""
+        self._lib.ref_set_flow(int(bool(on)))
+
+    def flow(self):
+        nc = self._lib.ref_ncells()
+        f = np.zeros((nc, 3))
+        self._lib.ref_get_flow(_p(f))
+        return f
+
+    def cell_species(self):
+        nc = self._lib.ref_ncells()
+        out = np.zeros(self.cfg.n_species * nc, dtype=np.int32)
+        self._lib.ref_get_cell_species(_p(out))
+        return out.reshape(self.cfg.n_species, nc)
+
+    def write_outputs(self, outdir, runtime, flow_interval=0, header=False):
+        """The reference's own writers of the current state into outdir."""
+        d = str(outdir).rstrip("/") + "/"
+        if self._lib.ref_write_outputs(d.encode(), runtime, flow_interval, int(header)) != 0:
+            raise RuntimeError("ref_write_outputs failed")
 
     def checkpoint_write(self, path, runtime, warmtime=0):
         """The reference's checkpoint() of the current state to path."""

@@ -45,6 +45,7 @@
 #include "therm.h"
 #include "pout.h"
 #include "read.h"
+#include "lc.h"
 
 /* reference globals (globals.h:24-65, common symbols of the core library) */
 extern int DBUG, DIM, MDmode, GPOP, NSPECI, NBC, NS;
@@ -457,6 +458,85 @@ int ref_checkpoint_particles(double *Q, double *V, double *U, int *spid) {
         }
         if (spid) spid[i] = g_rd[i].SPID;
     }
+    return 0;
+}
+
+/* Flow output on: timestep() then sums every step's cell velocities into
+ * FLOW (localFLOW + sumFLOW, mpc.c:4946-4951). */
+int ref_set_flow(int on) {
+    g_oflags.FLOWOUT = on ? OUT : 0;
+    return 0;
+}
+int ref_get_flow(double *flow) {
+    for (int c = 0; c < g_ncells; c++)
+        for (int d = 0; d < 3; d++) flow[3 * c + d] = g_cells[c].FLOW[d];
+    return 0;
+}
+int ref_get_cell_species(int *spc) {
+    for (int s = 0; s < NSPECI; s++)
+        for (int c = 0; c < g_ncells; c++) spc[(size_t)s * g_ncells + c] = g_cells[c].SP[s];
+    return 0;
+}
+
+/* The reference's own writers of the cell fields and global measures, as
+ * outputResults (pout.c:2518-2600) calls them after a step: re-bin,
+ * localPROP, avVel, then coarseout, velout, densityout, flowout (which
+ * empties FLOW), localVelGrad + avveloutWithGradVel, enout.  Files in dir
+ * (ending in '/'), created with their headers when header is set. */
+static FILE *ref_open(void (*opener)(FILE **, char *, char *, char *), const char *dir,
+                      const char *name, int header) {
+    FILE *f = NULL;
+    char d[4096], nm[256], ext[8] = ".dat";
+    snprintf(d, sizeof d, "%s", dir);
+    snprintf(nm, sizeof nm, "%s", name);
+    if (header) {
+        opener(&f, d, nm, ext);
+    } else {
+        char path[4400];
+        snprintf(path, sizeof path, "%s%s.dat", dir, name);
+        f = fopen(path, "a");
+    }
+    return f;
+}
+int ref_write_outputs(const char *dir, int runtime, int flow_interval, int header) {
+    if (!g_pp) return -1;
+    const double t = runtime * g_in.dt;
+    FILE *f;
+    int a, b, c, i, j;
+    bin(g_CL, g_SP, g_WALL, g_in.KBT, g_in.LC, 0);
+    localPROP(g_CL, g_SP, *g_SS, g_in.RTECH, g_in.LC);
+    avVel(g_CL, g_AVNOW);
+    if (!(f = ref_open(opencoarse, dir, "coarsegrain", header))) return -1;
+    coarseout(f, t, g_CL);
+    fclose(f);
+    if (!(f = ref_open(openvel, dir, "velfield", header))) return -1;
+    velout(f, g_CL, t);
+    fclose(f);
+    if (!(f = ref_open(opendensity, dir, "densityfield", header))) return -1;
+    densityout(f, g_CL, t);
+    fclose(f);
+    if (flow_interval > 0) {
+        if (!(f = ref_open(openflow, dir, "flowfield", header))) return -1;
+        flowout(f, g_CL, flow_interval, t);
+        fclose(f);
+    }
+    double grad[3][3];
+    localVelGrad(g_CL);
+    for (i = 0; i < 3; i++)
+        for (j = 0; j < 3; j++) grad[i][j] = 0.;
+    for (a = 0; a < XYZ[0]; a++)
+        for (b = 0; b < XYZ[1]; b++)
+            for (c = 0; c < XYZ[2]; c++)
+                for (i = 0; i < 3; i++)
+                    for (j = 0; j < 3; j++) grad[i][j] += g_CL[a][b][c].E[i][j];
+    for (i = 0; i < 3; i++)
+        for (j = 0; j < 3; j++) grad[i][j] /= VOL;
+    if (!(f = ref_open(openavvel, dir, "avVel", header))) return -1;
+    avveloutWithGradVel(f, t, g_AVNOW, g_KBTNOW, grad);
+    fclose(f);
+    if (!(f = ref_open(openenergy, dir, "energy", header))) return -1;
+    enout(f, g_pp, g_SP, g_WALL, t, g_KBTNOW, 0.0);
+    fclose(f);
     return 0;
 }
 

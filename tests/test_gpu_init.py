@@ -21,10 +21,24 @@ from mpcd_b200.gpu import MPCDError, Solver
 
 pytestmark = pytest.mark.gpu
 
+# orientation codes a 2D nematic state cannot hold (a z component)
+_Z_ODIST = (abi.ODIST_ALIGNZ, abi.ODIST_PLANEY, abi.ODIST_PLANEX)
+
+
+def _gpu_case(name, precision=abi.PREC_FP64):
+    """init_case with the 2D nematic's z-component codes replaced by
+    RANDORIENT (the oracle takes the same parameters)."""
+    cfg, params = init_case(name, precision)
+    if cfg.lc and cfg.dim == 2:
+        for s in range(cfg.n_species):
+            if params.odist[s] in _Z_ODIST:
+                params.odist[s] = abi.ODIST_RANDORIENT
+    return cfg, params
+
 
 @pytest.mark.parametrize("name", sorted(INIT_CASES))
 def test_fp64_init_matches_oracle(name):
-    cfg, params = init_case(name)
+    cfg, params = _gpu_case(name)
     Qo, Vo, Uo, _, ko = oracle_init_state(cfg, params)
     g = Solver(cfg)
     kg = g.init_state(params)
@@ -39,8 +53,8 @@ def test_fp64_init_matches_oracle(name):
 
 @pytest.mark.parametrize("name", sorted(INIT_CASES))
 def test_mixed_init_matches_oracle(name):
-    cfg, params = init_case(name)
-    cfgm, _ = init_case(name, precision=abi.PREC_MIXED)
+    cfg, params = _gpu_case(name)
+    cfgm, _ = _gpu_case(name, precision=abi.PREC_MIXED)
     Qo, Vo, Uo, _, ko = oracle_init_state(cfg, params)
     g = Solver(cfgm)
     kg = g.init_state(params)
@@ -72,7 +86,7 @@ def test_init_is_reproducible_and_keyed_by_seed_and_replica():
 def test_init_then_steps_match_oracle(name):
     """The device-built state steps as the oracle does from its own
     initial state (the FP64 parity bound of the timestep)."""
-    cfg, params = init_case(name)
+    cfg, params = _gpu_case(name)
     Qo, Vo, Uo, sp, _ = oracle_init_state(cfg, params)
     o = Oracle(cfg, Qo, Vo, Uo if cfg.lc else None, sp)
     g = Solver(cfg)
@@ -124,4 +138,9 @@ def test_init_rejects_bad_requests():
     with pytest.raises(MPCDError, match=r"-1 "):
         g.init_state(p)
     assert g.init_state(abi.init_params([0])) == 0.0
+    g.close()
+    cfg, params = init_case("init_nematic_odist")
+    g = Solver(cfg)
+    with pytest.raises(MPCDError, match=r"-2 "):  # z components in 2D
+        g.init_state(params)
     g.close()
