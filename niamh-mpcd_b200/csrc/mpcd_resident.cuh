@@ -101,10 +101,6 @@ constexpr int kResProbe = 32;
 #ifndef MPCD_RES_BULK_PF
 #define MPCD_RES_BULK_PF 1  // bulk L2 prefetch of each block's particles
 #endif
-#ifndef MPCD_RES_PIPE
-#define MPCD_RES_PIPE 2  // particles loaded ahead of the one being processed
-#endif
-static_assert(MPCD_RES_PIPE == 1 || MPCD_RES_PIPE == 2, "pipeline depth 1 or 2");
 static_assert(kResChunk <= 8 * 256, "the prefetch covers eight 256-particle pieces");
 // Inside a block the fixed-point values are summed as two signed 32-bit
 // limbs, x = hi * 2^20 + lo with |lo| <= 2^19 (fx_limbs), so that the
@@ -519,25 +515,18 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
                          (float)(c.dt * c.grav[2])};
     const float cosf_a = (float)c.cosA, sinf_a = (float)c.sinA;
     const int base = blockIdx.x * kResChunk;
-    // Software pipeline.  Depth 1: the next particle is loaded at the top
-    // of an iteration and its cell's record is requested halfway through it
-    // (before the accumulation).  Depth 2: particles are loaded two
-    // iterations ahead, so the next particle is already in registers at the
-    // top of an iteration and its record is requested there, a whole
-    // iteration before it is used.  The cell is the one the particle was
-    // added to at the end of the previous step, which that step left in P.w
-    // (clamped only as a guard).
+    // Software pipeline: the next particle is loaded at the top of an
+    // iteration, and its cell's record is requested halfway through it
+    // (before the accumulation), so neither load is waited for.  The cell
+    // is the one the particle was added to at the end of the previous step,
+    // which that step left in P.w (clamped only as a guard).
     auto cur_cell = [&](const MixRec &q) { return (int)min(q.P.w, (unsigned)(c.ncells - 1)); };
-    MixRec nx, nx2;
+    MixRec nx;
     float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
     if (base + tid < n) {
         nx.P = a.P[base + tid];
         nx.W = a.W[base + tid];
         if (MODE == RES_STEP) res_load(crec + cur_cell(nx), na, nb);
-    }
-    if (MPCD_RES_PIPE == 2 && MPCD_RES_PPT > 1 && base + kResThreads + tid < n) {
-        nx2.P = a.P[base + kResThreads + tid];
-        nx2.W = a.W[base + kResThreads + tid];
     }
 #pragma unroll 1
     for (int it = 0; it < MPCD_RES_PPT; it++) {
@@ -546,16 +535,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
         MixRec r = nx;
         const float4 ca = na, cb = nb;
         const bool more = it + 1 < MPCD_RES_PPT && i + kResThreads < n;
-        if (MPCD_RES_PIPE == 2) {
-            if (more) {
-                nx = nx2;
-                if (MODE == RES_STEP) res_load(crec + cur_cell(nx), na, nb);
-            }
-            if (it + 2 < MPCD_RES_PPT && i + 2 * kResThreads < n) {
-                nx2.P = a.P[i + 2 * kResThreads];
-                nx2.W = a.W[i + 2 * kResThreads];
-            }
-        } else if (more) {
+        if (more) {
             nx.P = a.P[i + kResThreads];
             nx.W = a.W[i + kResThreads];
         }
@@ -582,7 +562,7 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
             }
             r.P.w = (unsigned)k;  // next step's cell, read back by cur_cell
             MixT<DIM>::store(a, i, r);
-            if (MPCD_RES_PIPE == 1 && more) res_load(crec + cur_cell(nx), na, nb);
+            if (more) res_load(crec + cur_cell(nx), na, nb);
             // the next step's load adds the same FP32 gravity kick
             if (!LEAN && c.grav_flag) {
                 r.W.x += gk[0];

@@ -117,7 +117,8 @@ def test_init_full_size_matches_oracle():
     kg = g.init_state(params)
     Qg, Vg, _ = g.download()
     np.testing.assert_array_equal(Qg, Qo)
-    np.testing.assert_allclose(Vg, Vo, rtol=0, atol=1e-13)
+    # the scaling factor comes from 2.6 M-term sums taken in another order
+    np.testing.assert_allclose(Vg, Vo, rtol=2e-13, atol=1e-15)
     assert kg == pytest.approx(ko, rel=1e-12)
     assert kg == pytest.approx(1.0, abs=1e-5)
     g.close()
