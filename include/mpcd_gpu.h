@@ -133,8 +133,10 @@ typedef struct mpcd_status {
     uint64_t steps;         /* steps executed                               */
     uint64_t escaped;       /* particles binned outside the grid (bin(),
                                mpc.c:970-982)                               */
-    uint64_t bounce_limit;  /* particles that hit the NBOUNCE limit
-                               (bc.c:1461-1488)                             */
+    uint64_t bounce_limit;  /* particles that exceeded NBOUNCE wall
+                               collisions in a step (bcCNT, bc.c:1461-1492);
+                               the reference's remedies are applied: longer
+                               rewinds, then re-thermalisation            */
     uint64_t nonfinite;     /* non-finite velocities seen by the step       */
     uint64_t overflow;      /* particles of cells too populous for one tile
                                (streamed without collision)                 */
@@ -219,6 +221,13 @@ typedef struct mpcd_init_params {
  * which the reference keeps and rotates back into the plane, but a 2D state
  * here does not hold. */
 int mpcd_init_state(mpcd_handle *h, const mpcd_init_params *p, double *kbtnow);
+
+/* The species' velocity distributions (VDIST codes, one per species; all
+ * RANDVEL, the reference's JSON default, until set).  A particle that
+ * exceeds the bounce limit at the walls is given a fresh velocity of its
+ * species' distribution (bc.c:1477-1488).  mpcd_init_state sets them from
+ * its parameters. */
+int mpcd_set_species_vdist(mpcd_handle *h, const int *vdist);
 
 /* Volume accessible to species 'species': the box volume (XYZ[2] = 1 in 2D)
  * less the parts where some wall the species interacts with has W < 0.

@@ -649,6 +649,9 @@ extern "C" int mpcd_init_state(mpcd_handle *h, const mpcd_init_params *p, double
         }
     }
     plan.off[MPCD_MAX_SPECIES] = (int)std::min<long long>(total, INT32_MAX);
+    // the species' velocity distributions also serve the bounce-limit
+    // re-thermalisation from now on (VDIST, bc.c:1482)
+    for (int s = 0; s < dc.n_species; s++) h->dc.vdist[s] = p->vdist[s];
     if (total > INT32_MAX) return MPCD_ERR_SIZE;
     const int n = (int)total;
     plan.rframe = p->rframe && n > 2;  // init.c:2140-2143
@@ -768,6 +771,16 @@ extern "C" int mpcd_download_state(mpcd_handle *h, double *Q, double *V, double 
 extern "C" int mpcd_download_species(mpcd_handle *h, int *spid) {
     if (!h || (h->n > 0 && !spid)) return MPCD_ERR_ARG;
     return download_impl(h, nullptr, nullptr, nullptr, spid);
+}
+
+extern "C" int mpcd_set_species_vdist(mpcd_handle *h, const int *vdist) {
+    if (!h || !vdist) return MPCD_ERR_ARG;
+    for (int s = 0; s < h->dc.n_species; s++)
+        if (vdist[s] != MPCD_VDIST_RANDVEL && vdist[s] != MPCD_VDIST_HOMO &&
+            vdist[s] != MPCD_VDIST_HOMOAXIS && vdist[s] != MPCD_VDIST_GAUSS)
+            return MPCD_ERR_UNSUPPORTED;
+    for (int s = 0; s < h->dc.n_species; s++) h->dc.vdist[s] = vdist[s];
+    return MPCD_OK;
 }
 
 extern "C" int mpcd_get_config(const mpcd_handle *h, mpcd_config *cfg) {

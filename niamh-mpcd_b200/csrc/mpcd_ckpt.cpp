@@ -540,6 +540,16 @@ extern "C" int mpcd_ckpt_upload(const mpcd_ckpt *ck, mpcd_handle *h) {
     std::vector<double> Q(3 * n), V(3 * n), U(3 * n);
     std::vector<int> sp(n);
     mpcd_ckpt_particles(ck, Q.data(), V.data(), U.data(), sp.data());
+    // the species' VDIST for the bounce-limit re-thermalisation
+    int vdist[MPCD_MAX_SPECIES] = {0};
+    for (int s = 0; s < ck->nspec && s < MPCD_MAX_SPECIES; s++) {
+        vdist[s] = (int)ck->i(ck->spec_line(s), 3);
+        // READ (1) has no file to read from at a re-thermalisation (the
+        // reference would read from a null file there): uniform instead
+        if (vdist[s] == 1) vdist[s] = MPCD_VDIST_RANDVEL;
+    }
+    int r = mpcd_set_species_vdist(h, vdist);
+    if (r != MPCD_OK) return r;
     return mpcd_upload_state(h, ck->gpop, Q.data(), V.data(), U.data(), sp.data());
 }
 

@@ -45,6 +45,7 @@ static inline int __float_as_int_host(float f) {
 
 constexpr double kTol = 1e-8;  // reference TOL, definitions.h:56
 constexpr int kNBounce = 50;   // reference NBOUNCE, definitions.h:62
+constexpr int kMaxRetherm = 16;  // re-thermalisations of one particle in one step
 
 // Status counters (device, uint64): index into DevStatus words.
 // status words (ST_OVERFLOW = 3 is defined with the tile kernels); ST_SYNC
@@ -79,6 +80,7 @@ struct DevCfg {
     double grav[3];
     double mass[MPCD_MAX_SPECIES], damp[MPCD_MAX_SPECIES];
     double sig[MPCD_MAX_SPECIES];  // sqrt(kbt / mass): the thermal draw's width
+    int vdist[MPCD_MAX_SPECIES];   // VDIST: re-thermalisation velocities (push)
     double rfc[MPCD_MAX_SPECIES], tumble[MPCD_MAX_SPECIES], chihi[MPCD_MAX_SPECIES];
     double act[MPCD_MAX_SPECIES], mfpot[MPCD_MAX_SPECIES], sigwidth[MPCD_MAX_SPECIES];
     double sigpos[MPCD_MAX_SPECIES], minactratio[MPCD_MAX_SPECIES];
@@ -132,6 +134,42 @@ __device__ __forceinline__ int bin_axis(double q, int L, int pbc, int shifted,
         a = a < 0 ? 0 : L;
     }
     return a;
+}
+
+// push (init.c:1261-1291): a velocity of distribution vdist for a particle
+// of mass m, from the counter-based stream (step, stream, id): uniforms
+// k0 + d (RANDVEL, HOMOAXIS) or normals k0 + d (GAUSS, HOMO).  Every step
+// is rounded as the reference's x86-64 build rounds it (no contraction).
+__device__ __forceinline__ void push_velocity(const DevCfg &c, int vdist, double m,
+                                              uint32_t step, uint32_t stream, uint32_t id,
+                                              uint32_t k0, double *v) {
+    const int dim = c.dim;
+    v[0] = v[1] = v[2] = 0.0;
+    if (vdist == MPCD_VDIST_RANDVEL) {
+        const double s = sqrt(c.kbt / m);
+        for (int d = 0; d < dim; d++) {
+            const double u = mpcd_rng_uniform(c.seed, c.replica, step, stream, id, k0 + d);
+            v[d] = __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, u), 1.0));
+        }
+    } else if (vdist == MPCD_VDIST_HOMOAXIS) {
+        const double s = sqrt((double)dim * c.kbt / m);
+        for (int d = 0; d < dim; d++)
+            v[d] = mpcd_rng_uniform(c.seed, c.replica, step, stream, id, k0 + d) <= 0.5 ? -s : s;
+    } else {  // GAUSS and HOMO: genrand_gaussMB per component
+        const double s = sqrt(c.kbt / m);
+        for (int d = 0; d < dim; d++)
+            v[d] = __dmul_rn(s, (double)mpcd_rng_normal(c.seed, c.replica, step, stream, id,
+                                                         k0 + (uint32_t)d));
+        if (vdist == MPCD_VDIST_HOMO) {
+            double l = 0.0;
+            for (int d = 0; d < dim; d++) l = __dadd_rn(l, __dmul_rn(v[d], v[d]));
+            l = sqrt(l);
+            if (fabs(l - 0.0) >= kTol)
+                for (int d = 0; d < dim; d++) v[d] = v[d] / l;
+            const double sc = sqrt((double)dim * c.kbt / m);
+            for (int d = 0; d < dim; d++) v[d] = __dmul_rn(v[d], sc);
+        }
+    }
 }
 
 // --------------------------------------------------------------- walls
@@ -194,9 +232,10 @@ __device__ void ori_bc(const DevWall &wl, const double *n, double *U) {
 // collision.  Returns 1 if the particle hit the bounce limit.
 template <int DIM>
 __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
-                               bool only_solid, double *U = nullptr) {
+                               bool only_solid, uint32_t step, uint32_t pid,
+                               double *U = nullptr) {
     double t_left = c.dt, t_coll = 0.0;
-    int chosen = 0, cnt = 0;
+    int chosen = 0, cnt = 0, cnt2 = 0, flagged = 0;
     const double m = c.mass[sp];
     for (;;) {
         double t_min = t_left, W = 1.0;
@@ -220,7 +259,7 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
             }
         }
         t_coll = t_min;
-        if (W > -kTol) return 0;
+        if (W > -kTol) return flagged;
         cnt++;
         const DevWall &wl = c.walls[chosen];
         if (t_coll > -kTol) {
@@ -270,7 +309,8 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
             for (int d = 0; d < DIM; d++) q[d] = q[d] - (t_left - t_coll) * v[d];
         }
         if (cnt > kNBounce) {
-            if (cnt < 2 * kNBounce) {
+            flagged = 1;
+            if (cnt < 2 * kNBounce && cnt2 == 0) {
                 if (t_left > kTol) {
                     t_left *= 1.1;
                 } else {
@@ -278,7 +318,16 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
                     t_coll = 0.1 * c.dt;
                 }
             } else {
-                return 1;
+                // a fresh velocity of the species' distribution and a whole
+                // step to stream again (bc.c:1477-1488); the reference tries
+                // for ever, here at most kMaxRetherm times
+                if (cnt2 >= kMaxRetherm) return flagged;
+                push_velocity(c, c.vdist[sp], m, step, MPCD_STREAM_RETHERM, pid,
+                              4u * (uint32_t)cnt2, v);
+                t_left = c.dt;
+                t_coll = 0.0;
+                cnt2++;
+                cnt = 0;
             }
         }
     }

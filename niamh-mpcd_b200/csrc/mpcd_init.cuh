@@ -158,29 +158,10 @@ __device__ void init_orient(const DevCfg &c, int i, int odist, const double *q, 
     }
 }
 
-// push (init.c:1261-1291) for particle i of mass m
-__device__ void init_push(const DevCfg &c, int i, int vdist, double m, double *v) {
-    const int dim = c.dim;
-    v[0] = v[1] = v[2] = 0.0;
-    if (vdist == MPCD_VDIST_RANDVEL) {
-        const double s = sqrt(c.kbt / m);
-        for (int d = 0; d < dim; d++)
-            v[d] = __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, init_u(c, MPCD_STREAM_INIT_VEL, i, d)), 1.0));
-    } else if (vdist == MPCD_VDIST_HOMOAXIS) {
-        const double s = sqrt((double)dim * c.kbt / m);
-        for (int d = 0; d < dim; d++)
-            v[d] = init_u(c, MPCD_STREAM_INIT_VEL, i, d) <= 0.5 ? -s : s;
-    } else {  // GAUSS and HOMO: genrand_gaussMB per component
-        const double s = sqrt(c.kbt / m);
-        for (int d = 0; d < dim; d++)
-            v[d] = __dmul_rn(s, (double)mpcd_rng_normal(c.seed, c.replica, 0u, MPCD_STREAM_INIT_VEL,
-                                                         (uint32_t)i, (uint32_t)d));
-        if (vdist == MPCD_VDIST_HOMO) {
-            init_norm(v, dim);
-            const double sc = sqrt((double)dim * c.kbt / m);
-            for (int d = 0; d < dim; d++) v[d] = __dmul_rn(v[d], sc);
-        }
-    }
+// push (init.c:1261-1291) for particle i of mass m: the velocity stream at
+// step 0, uniforms or normals 0..DIM-1
+__device__ __forceinline__ void init_push(const DevCfg &c, int i, int vdist, double m, double *v) {
+    push_velocity(c, vdist, m, 0u, MPCD_STREAM_INIT_VEL, (uint32_t)i, 0u, v);
 }
 
 // Block sums of 'nv' values into part[blockIdx.x * 8 + j], in a fixed order

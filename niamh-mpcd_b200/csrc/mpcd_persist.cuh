@@ -341,7 +341,7 @@ template <int DIM>
 __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &l,
                                               const PerGlobal &g, unsigned char *sm, int j,
                                               const double s[3], const double *rvv,
-                                              int &bounce) {
+                                              uint32_t step, int &bounce) {
     using Q = PerQ<DIM>;
     double *q = (double *)(sm + l.off_q), *v = (double *)(sm + l.off_v);
     const int k = ((const int *)(sm + l.off_k))[j];
@@ -407,7 +407,8 @@ __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &
         qq[d] = shift_back(qs[d], s[d], c.L[d]);
         qq[d] = qq[d] + c.dt * vv[d];
     }
-    bounce += wall_collisions<DIM>(c, qq, vv, sp, false);
+    const uint32_t pid = (uint32_t)((const int *)(sm + l.off_pid))[j];
+    bounce += wall_collisions<DIM>(c, qq, vv, sp, false, step, pid);
     for (int d = 0; d < DIM; d++) {
         q[d * l.chunk + j] = qq[d];
         v[d * l.chunk + j] = vv[d];
@@ -492,7 +493,7 @@ __global__ void __launch_bounds__(kPerThreads)
         if (c.galinv) mpcd_rng_shift(c.seed, c.replica, step + 1u, DIM, sn);
         double ke = 0.0;
         for (int j = tid; j < np; j += nt) {
-            ke += per_collide<DIM>(c, l, g, sm, j, s, rv, bounce);
+            ke += per_collide<DIM>(c, l, g, sm, j, s, rv, step, bounce);
             if (!last) per_enter<DIM>(c, l, g, sm, j, sn, rvn, esc);
         }
         const double t = per_block_sum(ke, red);

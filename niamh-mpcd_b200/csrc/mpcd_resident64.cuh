@@ -112,11 +112,12 @@ __global__ void __launch_bounds__(256, R64_MINB) k_r64_parts(const __grid_consta
     // rather than once per 256 particles
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        // the particle stays in place, so its id is neither read nor
-        // written; otherwise as F64T::load: the shifted position and the
+        // the particle stays in place, so its id is not written, and read
+        // only where walls may re-thermalise it (the draws are keyed by the
+        // id); otherwise as F64T::load: the shifted position and the
         // velocity with this step's kick
         F64Rec r;
-        r.pid = 0;
+        r.pid = (MODE == RES_STEP && c.n_walls > 0) ? a.pid[i] : 0;
         for (int d = 0; d < 3; d++) {
             r.q[d] = d < DIM ? shift_fwd(a.q[d][i], sa.s[d], c.L[d]) : 0.0;
             r.v[d] = d < DIM ? a.v[d][i] : 0.0;

@@ -50,7 +50,9 @@ enum {
     /* initial state (step 0), per particle: */
     MPCD_STREAM_INIT_POS = 7, /* positions, 4 uniforms per placement attempt */
     MPCD_STREAM_INIT_VEL = 8, /* velocities                                  */
-    MPCD_STREAM_INIT_ORI = 9  /* orientations                                */
+    MPCD_STREAM_INIT_ORI = 9, /* orientations                                */
+    MPCD_STREAM_RETHERM = 10  /* bounce-limit re-thermalisation, per particle,
+                                 4 draws per re-thermalisation of a step    */
 };
 
 /* Maximum Philox blocks a rejection loop may consume (2 attempts per block).

@@ -146,7 +146,7 @@ struct MixT {
                 if (!wl.periodic && wall_W(wl, q, wl.Q, DIM) < 0.0) inside = true;
             }
             if (inside) {
-                bounce += wall_collisions<DIM>(c, q, v, sp, true);
+                bounce += wall_collisions<DIM>(c, q, v, sp, true, sa.step, pid(r));
                 for (int d = 0; d < DIM; d++) {
                     fx_from_double(q[d], ci[d], f[d]);
                     vv[d] = (float)v[d];
@@ -233,7 +233,7 @@ struct F64T {
             q[d] = shift_back(r.q[d], sa.s[d], c.L[d]);
             q[d] = q[d] + c.dt * v[d];
         }
-        bounce += wall_collisions<DIM>(c, q, v, sp, false);
+        bounce += wall_collisions<DIM>(c, q, v, sp, false, sa.step, (uint32_t)r.pid);
         int idx[3] = {0, 0, 0};
         for (int d = 0; d < DIM; d++) {
             r.q[d] = q[d];

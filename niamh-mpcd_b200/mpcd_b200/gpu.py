@@ -16,7 +16,8 @@ LIB_PATH = os.environ.get(
 
 EXPORTS = [
     "mpcd_abi_version", "mpcd_create", "mpcd_destroy", "mpcd_upload_state",
-    "mpcd_upload_particles_strided", "mpcd_init_state", "mpcd_accessible_volume",
+    "mpcd_upload_particles_strided", "mpcd_init_state", "mpcd_set_species_vdist",
+    "mpcd_accessible_volume",
     "mpcd_download_state",
     "mpcd_download_particles_strided", "mpcd_step", "mpcd_timestep",
     "mpcd_globals", "mpcd_cell_props", "mpcd_get_status", "mpcd_set_stream",
@@ -57,6 +58,7 @@ def load():
                                                       C.c_size_t, C.c_size_t, C.c_size_t,
                                                       C.c_size_t]
         lib.mpcd_init_state.argtypes = [vp, vp, vp]
+        lib.mpcd_set_species_vdist.argtypes = [vp, vp]
         lib.mpcd_accessible_volume.argtypes = [vp, C.c_int, vp]
         lib.mpcd_download_state.argtypes = [vp, vp, vp, vp]
         lib.mpcd_download_species.argtypes = [vp, vp]
@@ -341,6 +343,13 @@ class Solver:
         _check(self.lib.mpcd_init_state(self.h, C.byref(params), C.byref(k)), "mpcd_init_state")
         self.n = sum(params.population)
         return k.value
+
+    def set_vdist(self, vdist):
+        """The species' velocity distributions (VDIST codes), which a
+        particle past the wall bounce limit is re-thermalised from."""
+        v = np.zeros(abi.MAX_SPECIES, dtype=np.int32)
+        v[:len(vdist)] = vdist
+        _check(self.lib.mpcd_set_species_vdist(self.h, _p(v)), "mpcd_set_species_vdist")
 
     def config(self):
         """The handle's configuration, gndnst the value in use."""

@@ -53,6 +53,9 @@ class Oracle:
             lib.oracle_shifted_counts.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
             lib.oracle_init_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int] + \
                 [C.c_void_p] * 5
+            lib.oracle_bounce_limit.restype = C.c_long
+            lib.oracle_bounce_limit.argtypes = [C.c_void_p]
+            lib.oracle_set_vdist.argtypes = [C.c_void_p, C.c_void_p]
             cls._lib = lib
         return cls._lib
 
@@ -107,6 +110,15 @@ class Oracle:
 
     def escaped(self):
         return self.lib().oracle_escaped(self.h)
+
+    def bounce_limit(self):
+        """Particles that exceeded the bounce limit (summed over steps)."""
+        return self.lib().oracle_bounce_limit(self.h)
+
+    def set_vdist(self, vdist):
+        v = np.zeros(10, dtype=np.int32)
+        v[:len(vdist)] = vdist
+        self.lib().oracle_set_vdist(self.h, _p(v))
 
     def close(self):
         if self.h:
@@ -165,6 +177,7 @@ class Reference:
             lib.ref_checkpoint_read.argtypes = [C.c_char_p] + [C.c_void_p] * 6
             lib.ref_checkpoint_particles.argtypes = [C.c_void_p] * 4
             lib.ref_set_flow.argtypes = [C.c_int]
+            lib.ref_set_vdist.argtypes = [C.c_void_p]
             lib.ref_get_flow.argtypes = [C.c_void_p]
             lib.ref_get_cell_species.argtypes = [C.c_void_p]
             lib.ref_write_outputs.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int]
@@ -212,6 +225,12 @@ class Reference:
         if lib.ref_init(C.byref(cfg), 0, _p(z), _p(z), None, None) != 0:
             raise RuntimeError("ref_init failed")
         return lib.ref_accessible_volume(species)
+
+    def set_vdist(self, vdist):
+        """The species' VDIST (re-thermalised velocities)."""
+        v = np.zeros(10, dtype=np.int32)
+        v[:len(vdist)] = vdist
+        self._lib.ref_set_vdist(_p(v))
 
     def set_flow(self, on=True):
         """Sum the cell velocities into FLOW after every step (flow output)."""

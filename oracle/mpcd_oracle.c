@@ -56,6 +56,8 @@ struct oracle {
     double wallQ[MPCD_MAX_WALLS][3];
     double avnow[3], kbtnow;
     long escaped, bounce_limit;
+    int vdist[MPCD_MAX_SPECIES];  /* VDIST per species, for re-thermalisation */
+    uint32_t step;                /* the step being taken                     */
 };
 
 /* ------------------------------------------------------------ small math */
@@ -819,11 +821,14 @@ static void ori_bc(oracle_t *o, int i, const mpcd_wall *wl, const double *n) {
  * collisions (COLL_TYPE 1): repeatedly find the wall crossed earliest
  * (chooseBC, bc.c:1252-1334), rewind to it, transform velocity (velBC,
  * bc.c:598-746) and position (posBC, bc.c:760-774), stream the rest. */
+static void push_velocity(const mpcd_config *c, int dim, uint32_t step, uint32_t stream,
+                          uint32_t id, uint32_t k0, int PL, double MASS, double *V);
+
 static void wall_collisions(oracle_t *o, int i) {
     int dim = o->dim, nw = o->cfg.n_walls;
     double *q = &o->Q[3 * i], *v = &o->V[3 * i];
     double dt = o->cfg.dt, t_left = dt, t_coll = 0.0;
-    int chosen = 0, cnt = 0, cnt2 = 0;
+    int chosen = 0, cnt = 0, cnt2 = 0, flagged = 0;
     double m = o->cfg.species[o->spid[i]].mass;
     for (;;) {
         double t_min = t_left, W = 1.0;
@@ -895,6 +900,7 @@ static void wall_collisions(oracle_t *o, int i) {
             for (int d = 0; d < dim; d++) q[d] = q[d] - (t_left - t_coll) * v[d];
         }
         if (cnt > NBOUNCE) {
+            flagged = 1; /* bcCNT, bc.c:1462 */
             if (cnt < 2 * NBOUNCE && cnt2 == 0) {
                 if (t_left > TOL) {
                     t_left *= 1.1;
@@ -903,16 +909,30 @@ static void wall_collisions(oracle_t *o, int i) {
                     t_coll = 0.1 * dt;
                 }
             } else {
-                /* the reference re-thermalises here (bc.c:1478-1488) */
-                o->bounce_limit++;
-                break;
+                /* re-thermalise: a fresh velocity of the species'
+                 * distribution and a whole step to stream (bc.c:1477-1488);
+                 * at most 16 times (the reference tries for ever) */
+                if (cnt2 >= 16) break;
+                push_velocity(&o->cfg, dim, o->step, MPCD_STREAM_RETHERM, (uint32_t)i,
+                              4u * (uint32_t)cnt2, o->vdist[o->spid[i]], m, v);
+                t_left = dt;
+                t_coll = 0.0;
+                cnt2++;
+                cnt = 0;
             }
         }
     }
+    if (flagged) o->bounce_limit++;
 }
 
 /* ------------------------------------------------------------------ step */
+int oracle_set_vdist(oracle_t *o, const int *vdist) {
+    for (int s = 0; s < o->cfg.n_species; s++) o->vdist[s] = vdist[s];
+    return 0;
+}
+
 int oracle_step(oracle_t *o, uint32_t step) {
+    o->step = step;
     int dim = o->dim, n = o->n, op = o->cfg.coll_op;
     double s[3] = {0, 0, 0};
     if (o->cfg.lc != 0 && dim != 2) return MPCD_ERR_UNSUPPORTED;
@@ -1152,24 +1172,29 @@ static void init_orient(const mpcd_config *c, int dim, const int *XYZ, int i, in
     }
 }
 
-/* push, init.c:1261-1291 */
-static void init_push(const mpcd_config *c, int dim, int i, int PL, double MASS, double *V) {
+/* push, init.c:1261-1291, drawing from (step, stream, id): uniforms or
+ * normals k0 + d */
+static void push_velocity(const mpcd_config *c, int dim, uint32_t step, uint32_t stream,
+                          uint32_t id, uint32_t k0, int PL, double MASS, double *V) {
     const double KBT = c->kbt;
     int d;
+    for (d = 0; d < 3; d++) V[d] = 0.0;
     if (PL == MPCD_VDIST_RANDVEL) {
         for (d = 0; d < dim; d++)
-            V[d] = sqrt(KBT / MASS) * (2. * init_u(c, MPCD_STREAM_INIT_VEL, i, d) - 1.);
+            V[d] = sqrt(KBT / MASS) *
+                   (2. * mpcd_rng_uniform(c->seed, c->replica, step, stream, id, k0 + d) - 1.);
     } else if (PL == MPCD_VDIST_HOMOAXIS) {
         for (d = 0; d < dim; d++) {
             V[d] = sqrt(dim * KBT / MASS);
-            V[d] *= init_u(c, MPCD_STREAM_INIT_VEL, i, d) <= 0.5 ? -1.0 : 1.0;
+            V[d] *= mpcd_rng_uniform(c->seed, c->replica, step, stream, id, k0 + d) <= 0.5
+                        ? -1.0
+                        : 1.0;
         }
     } else {
         /* genrand_gaussMB (rand.c:510-513): sqrt(KBT/M) times a float normal */
         for (d = 0; d < dim; d++)
             V[d] = sqrt(KBT / MASS) *
-                   mpcd_rng_normal(c->seed, c->replica, 0u, MPCD_STREAM_INIT_VEL, (uint32_t)i,
-                                   (uint32_t)d);
+                   mpcd_rng_normal(c->seed, c->replica, step, stream, id, k0 + (uint32_t)d);
         if (PL == MPCD_VDIST_HOMO) {
             init_norm(V, dim);
             double normalize = sqrt((double)dim * KBT / MASS);
@@ -1199,7 +1224,8 @@ int oracle_init_state(const mpcd_config *cfg, const mpcd_init_params *p, int max
             if (u) u[d] = 0.0;
         }
         for (d = 0; d < dim; d++) q[d] = init_u(cfg, MPCD_STREAM_INIT_POS, i, d) * XYZ[d];
-        init_push(cfg, dim, i, p->vdist[spid[i]], cfg->species[spid[i]].mass, v);
+        push_velocity(cfg, dim, 0u, MPCD_STREAM_INIT_VEL, (uint32_t)i, 0u, p->vdist[spid[i]],
+                      cfg->species[spid[i]].mass, v);
         for (d = 0; d < dim; d++) AVV[d] += v[d];
         if (u && cfg->lc) init_orient(cfg, dim, XYZ, i, p->odist[spid[i]], q, u);
     }
@@ -1262,3 +1288,5 @@ int oracle_init_state(const mpcd_config *cfg, const mpcd_init_params *p, int max
     }
     return 0;
 }
+
+long oracle_bounce_limit(const oracle_t *o) { return o->bounce_limit; }

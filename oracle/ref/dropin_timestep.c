@@ -143,6 +143,19 @@ static int setup(particleMPC *pp, spec SP[], bc WALL[], inputList in) {
         return 0;
     if (!fill_config(&c, in, SP, WALL)) return 0;
     if (mpcd_create(&c, &g_h) != MPCD_OK) return 0;
+    {
+        /* the species' VDIST re-thermalises particles past the bounce
+         * limit (bc.c:1482); READ (1) has no file at that point */
+        int vd[MPCD_MAX_SPECIES] = {0};
+        int s;
+        for (s = 0; s < NSPECI && s < MPCD_MAX_SPECIES; s++)
+            vd[s] = SP[s].VDIST == 1 ? MPCD_VDIST_RANDVEL : SP[s].VDIST;
+        if (mpcd_set_species_vdist(g_h, vd) != MPCD_OK) {
+            mpcd_destroy(g_h);
+            g_h = NULL;
+            return 0;
+        }
+    }
     if (mpcd_upload_particles_strided(g_h, GPOP, pp, sizeof(particleMPC),
                                       offsetof(particleMPC, Q), offsetof(particleMPC, V),
                                       offsetof(particleMPC, U),

@@ -76,13 +76,15 @@ static int g_ncells = 0;
 /* draw bookkeeping */
 static uint64_t g_seed = 0;
 static uint32_t g_replica = 0, g_step = 0;
-enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT };
+enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT, PH_RETHERM };
 static int g_phase = PH_NONE;
 static int g_cell = 0;
 static particleMPC *g_cursor = NULL;
 static int g_comp = 0;
 static uint32_t g_stream = 0; /* PH_INIT: the stream of the current draws */
 static int *g_attempt = NULL; /* PH_INIT: placement attempts per particle */
+static int *g_retherm = NULL; /* re-thermalisations per particle this step */
+static int g_retherm_n = 0;
 static int g_pid = 0;
 static uint32_t g_k = 0;
 static int *g_ghost = NULL;
@@ -461,6 +463,12 @@ int ref_checkpoint_particles(double *Q, double *V, double *U, int *spid) {
     return 0;
 }
 
+/* The species' VDIST (the distribution of a re-thermalised velocity). */
+int ref_set_vdist(const int *vdist) {
+    for (int s = 0; s < NSPECI; s++) g_SP[s].VDIST = vdist[s];
+    return 0;
+}
+
 /* Flow output on: timestep() then sums every step's cell velocities into
  * FLOW (localFLOW + sumFLOW, mpc.c:4946-4951). */
 int ref_set_flow(int on) {
@@ -550,6 +558,13 @@ long ref_unexpected_draws(void) { return g_unexpected; }
 int ref_step(uint32_t step) {
     if (!g_pp) return -1;
     g_step = step;
+    if (g_retherm_n != GPOP) {
+        free(g_retherm);
+        g_retherm = (int *)calloc((size_t)(GPOP > 0 ? GPOP : 1), sizeof(int));
+        g_retherm_n = GPOP;
+    } else if (g_retherm) {
+        memset(g_retherm, 0, (size_t)GPOP * sizeof(int));
+    }
     timestep(g_CL, g_pp, g_SP, g_WALL, NULL, g_SS, NULL, g_AVNOW, g_AVV, g_avDIR,
              g_in, &g_KBTNOW, &g_AVS, (int)step, 0, g_oflags, g_ofiles);
     return 0;
@@ -604,6 +619,9 @@ static float next_normal(void) {
     if (g_phase == PH_INIT) {
         g = mpcd_rng_normal(g_seed, g_replica, 0u, MPCD_STREAM_INIT_VEL, (uint32_t)g_pid,
                             (uint32_t)g_comp++);
+    } else if (g_phase == PH_RETHERM) {
+        g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_RETHERM, (uint32_t)g_pid,
+                            (uint32_t)g_comp++);
     } else if (g_phase == PH_COLLIDE && g_cursor) {
         int pid = (int)(g_cursor - g_pp);
         g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_THERMAL,
@@ -636,6 +654,9 @@ long genrand_int31(void) { return (long)(genrand_int32() >> 1); }
 double genrand_real(void) {
     if (g_phase == PH_INIT)
         return mpcd_rng_uniform(g_seed, g_replica, 0u, g_stream, (uint32_t)g_pid, g_k++);
+    if (g_phase == PH_RETHERM)
+        return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_RETHERM, (uint32_t)g_pid,
+                                g_k++);
     if (g_phase == PH_LC)
         return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_LC,
                                 (uint32_t)g_pid, g_k++);
@@ -829,10 +850,22 @@ void push(double V[], double KBT, int PL, double MASS, FILE *fin) {
     static push_fn orig = NULL;
     if (!orig) orig = (push_fn)dlsym(RTLD_NEXT, "push");
     g_pid = pid_of(V, offsetof(particleMPC, V));
-    g_stream = MPCD_STREAM_INIT_VEL;
-    g_k = 0;
-    g_comp = 0;
+    if (g_phase == PH_INIT) {
+        g_stream = MPCD_STREAM_INIT_VEL;
+        g_k = 0;
+        g_comp = 0;
+        orig(V, KBT, PL, MASS, fin);
+        return;
+    }
+    /* a bounce-limit re-thermalisation inside MPC_BCcollision
+     * (bc.c:1482): draws 4c.. of the particle's stream this step */
+    const int prev = g_phase;
+    const int c = (g_retherm && g_pid >= 0 && g_pid < g_retherm_n) ? g_retherm[g_pid]++ : 0;
+    g_phase = PH_RETHERM;
+    g_k = 4u * (uint32_t)c;
+    g_comp = 4 * c;
     orig(V, KBT, PL, MASS, fin);
+    g_phase = prev;
 }
 typedef void (*orient_fn)(double *, double *, int);
 void orient(double U[], double Q[], int PL) {

@@ -100,3 +100,30 @@ def init_case(name, precision=abi.PREC_FP64):
     cfg.precision = precision
     cfg.seed = 777
     return cfg, abi.init_params(pops, vdist=vd, odist=od, rframe=rframe)
+
+
+def thin_gap(op=abi.COLL_ARBAXIS, precision=abi.PREC_FP64, n=400, vy=10.0, seed=99):
+    """A 4^3 box, periodic in x and z, whose fluid fills a gap 0.01 wide
+    between two no-slip walls across y: particles of |v_y| ~ vy cross it
+    about a hundred times in one step, past the reference's bounce limit
+    (NBOUNCE, bc.c:1461-1488), so the longer rewinds and then the
+    re-thermalisation run.  (Much faster particles rewind out of the box
+    and escape, and the reference's escape re-placement then draws from
+    its own generator.)  Returns (config, Q, V, species)."""
+    import numpy as np
+    L = (4, 4, 4)
+    w = [abi.make_wall((1, 0, 0), (0, 0, 0), 0.0, DN=4.0),
+         abi.make_wall((-1, 0, 0), (4, 0, 0), 0.0, DN=4.0),
+         abi.make_wall((0, 0, 1), (0, 0, 0), 0.0, DN=4.0),
+         abi.make_wall((0, 0, -1), (0, 0, 4), 0.0, DN=4.0),
+         abi.make_wall((0, 1, 0), (0, 1.0, 0), 0.0, MVN=-1.0, MVT=-1.0),
+         abi.make_wall((0, -1, 0), (0, 1.01, 0), 0.0, MVN=-1.0, MVT=-1.0)]
+    cfg = W.base_config(3, L, coll_op=op, walls=w, seed=seed, precision=precision)
+    rng = np.random.default_rng(seed)
+    Q = np.zeros((n, 3))
+    Q[:, 0] = rng.random(n) * 4
+    Q[:, 2] = rng.random(n) * 4
+    Q[:, 1] = 1.0005 + rng.random(n) * 0.009
+    V = rng.standard_normal((n, 3))
+    V[: n // 4, 1] = vy * np.sign(V[: n // 4, 1])
+    return cfg, Q, V, np.zeros(n, dtype=np.int32)

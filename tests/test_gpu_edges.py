@@ -115,3 +115,47 @@ def test_empty_state_is_refused_not_stepped(prec):
     with pytest.raises(MPCDError):
         g.step(1, 1)
     assert g.status().steps == 0
+
+
+@pytest.mark.parametrize("prec,kernel", [
+    (abi.PREC_FP64, abi.KERNEL_AUTO), (abi.PREC_FP64, abi.KERNEL_RESIDENT),
+    (abi.PREC_FP64, abi.KERNEL_TILE), (abi.PREC_FP64, abi.KERNEL_SPLIT),
+    (abi.PREC_FP64, abi.KERNEL_GROUP), (abi.PREC_MIXED, abi.KERNEL_RESIDENT),
+    (abi.PREC_MIXED, abi.KERNEL_TILE)])
+@pytest.mark.parametrize("vdist", [abi.VDIST_RANDVEL, abi.VDIST_GAUSS, abi.VDIST_HOMO])
+def test_bounce_limit_rethermalises_like_the_oracle(prec, kernel, vdist):
+    """Particles that cross a 0.01-wide gap between two walls about a
+    hundred times in a step pass the bounce limit (bc.c:1461-1488): the
+    device lengthens the rewinds, then gives them a fresh velocity of the
+    species' distribution, as the oracle (pinned to the reference) does."""
+    from cases import thin_gap
+    cfg, Q, V, sp = thin_gap(precision=abi.PREC_FP64)
+    cfgp, _, _, _ = thin_gap(precision=prec)
+    o = Oracle(cfg, Q, V, None, sp)
+    o.set_vdist([vdist])
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.set_vdist([vdist])
+    g.upload(Q, V, None, sp)
+    L = np.array(cfg.L[:3], dtype=float)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+    qo, vo, _ = o.particles()
+    qg, vg, _ = g.download()
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    assert o.bounce_limit() > 50
+    if prec == abi.PREC_FP64:
+        assert st.bounce_limit == o.bounce_limit()
+        _compare(prec, qg, vg, qo, vo, L, 0)
+    else:
+        # FP32 velocities: a particle near the limit may take one bounce
+        # more or less than the oracle's and draw differently
+        assert abs(st.bounce_limit - o.bounce_limit()) <= 0.1 * o.bounce_limit()
+        dv = np.abs(vg - vo).max(axis=1) / np.maximum(1.0, np.abs(vo).max(axis=1))
+        assert np.mean(dv > 1e-4) < 0.1, np.mean(dv > 1e-4)
+        d = qg - qo
+        d -= np.round(d / L) * L
+        same = dv <= 1e-4
+        assert np.all(np.isfinite(vg)) and np.abs(d[same]).max() < 1e-4

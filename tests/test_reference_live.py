@@ -56,3 +56,43 @@ def test_theory_restatement_matches_reference(coll_op, dim, n, ra, dt):
     nu, _, mfp = Reference.theory_visc(coll_op, dim, n, ra, dt)
     assert kin + col == pytest.approx(nu, rel=1e-12)
     assert mfp == pytest.approx(dt, rel=1e-15)
+
+
+@pytest.mark.parametrize("vdist", [abi.VDIST_RANDVEL, abi.VDIST_HOMO, abi.VDIST_HOMOAXIS,
+                                   abi.VDIST_GAUSS])
+def test_bounce_limit_rethermalisation_tracks_reference(vdist):
+    """Particles past the bounce limit: the oracle's longer rewinds and
+    re-thermalisations (bc.c:1461-1488, velocities of the species' VDIST
+    from the re-thermalisation stream) follow the reference's.  SRD keeps
+    the fast particles fast through the collision (an Andersen collision
+    would redraw them thermal first)."""
+    from cases import thin_gap
+    cfg, Q, V, sp = thin_gap()
+    o = Oracle(cfg, Q, V, None, sp)
+    o.set_vdist([vdist])
+    r = Reference(cfg, Q, V, None, sp)
+    r.set_vdist([vdist])
+    for s in range(1, 4):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    assert o.bounce_limit() > 50 and o.escaped() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11)
+
+
+def test_bounce_limit_rethermalisation_draws_the_species_distribution():
+    """The re-thermalised velocities follow VDIST: the same run with
+    uniform and with Maxwell-Boltzmann re-thermalisation differs."""
+    from cases import thin_gap
+    out = []
+    for vdist in (abi.VDIST_RANDVEL, abi.VDIST_GAUSS):
+        cfg, Q, V, sp = thin_gap()
+        o = Oracle(cfg, Q, V, None, sp)
+        o.set_vdist([vdist])
+        for s in range(1, 4):
+            o.step(s)
+        out.append(o.particles()[1])
+    assert not np.array_equal(out[0], out[1])
