@@ -76,6 +76,10 @@ struct ResPlanes {
     __device__ __forceinline__ void clear(int k) const {
         for (int d = 0; d < 4; d++) *at(d, k) = 0ll;
     }
+    // clear with an L2 eviction priority (the next particle pass adds to it)
+    __device__ __forceinline__ void clear(int k, uint64_t pol) const {
+        for (int d = 0; d < 4; d++) st_hint(at(d, k), 0ll, pol);
+    }
 };
 constexpr double kSumFx = 4294967296.0;  // 2^32
 constexpr double kSumFxInv = 2.3283064365386963e-10;
@@ -271,6 +275,12 @@ __device__ __forceinline__ void res_load(const ResRec *rec, float4 &ca, float4 &
     ca = __ldg(q);
     cb = __ldg(q + 1);
 }
+__device__ __forceinline__ void res_load(const ResRec *rec, float4 &ca, float4 &cb,
+                                         uint64_t pol) {
+    const float4 *q = (const float4 *)rec;
+    ca = ldg_hint(q, pol);
+    cb = ldg_hint(q + 1, pol);
+}
 
 // v' = u + R (v - u) from a cell's record (Rodrigues form, see ResRec);
 // cells of fewer than two particles leave v unchanged.
@@ -350,6 +360,7 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
         if (DIM == 3 && cell < c.ncells) res_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx[q]);
     }
     pdl_wait();  // the sums are complete from here on
+    const uint64_t keep = l2_evict_last();
     double av[3] = {0, 0, 0};
     if (blockIdx.x == 0 && threadIdx.x < ACC_WORDS) acc_next[threadIdx.x] = 0.0;
     ResSum s[kResCellsPer];
@@ -368,7 +379,7 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
     for (int q = 0; q < kResCellsPer; q++) {
         const int cell = c0 + q * 256 + threadIdx.x;
         if (cell >= c.ncells) continue;
-        sums.clear(cell);
+        sums.clear(cell, keep);
         if (msum) msum[cell] = 0ull;
         const int pop = (int)s[q].n;
         // u = weighted sum / divisor: the population (one species, in FP32:
@@ -394,7 +405,7 @@ __global__ void __launch_bounds__(256) k_res_cells(const __grid_constant__ DevCf
     {
         const int nrec = min(256 * kResCellsPer, c.ncells - c0);
         float4 *dst = (float4 *)(crec + c0);
-        for (int j = threadIdx.x; j < 2 * nrec; j += 256) dst[j] = srec[j];
+        for (int j = threadIdx.x; j < 2 * nrec; j += 256) st_hint(dst + j, srec[j], keep);
     }
     // block sum of the avVel terms: warp shuffles, then one thread per block
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -488,13 +499,16 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     // once (16 bulk prefetches of 4 KB by warp 0), so that the loop's loads,
     // one particle ahead of the arithmetic, wait for L2 rather than for
     // DRAM.  A prefetch only moves lines into L2, which stays coherent with
-    // the kernel before this one still writing them.
+    // the kernel before this one still writing them.  The particle stream
+    // (prefetches, loads, stores) is marked evict_first and the cell records
+    // evict_last, so that the records, written by the cell pass, are still
+    // in L2 when the blocks of the last waves gather them.
     if (tid < 16) {
         const int j0 = blockIdx.x * kResChunk + (tid & 7) * 256;
         const int cnt = min(256, n - j0);
         if (cnt > 0) {
             const void *src = tid < 8 ? (const void *)(a.P + j0) : (const void *)(a.W + j0);
-            prefetch_l2_bulk(src, (uint32_t)cnt * 16u);
+            prefetch_l2_bulk_hint(src, (uint32_t)cnt * 16u, l2_evict_first());
         }
     }
 #endif
@@ -521,12 +535,14 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     // is the one the particle was added to at the end of the previous step,
     // which that step left in P.w (clamped only as a guard).
     auto cur_cell = [&](const MixRec &q) { return (int)min(q.P.w, (unsigned)(c.ncells - 1)); };
+    // the particle stream leaves L2 first; the records stay
+    const uint64_t stream = l2_evict_first(), keep = l2_evict_last();
     MixRec nx;
     float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
     if (base + tid < n) {
-        nx.P = a.P[base + tid];
-        nx.W = a.W[base + tid];
-        if (MODE == RES_STEP) res_load(crec + cur_cell(nx), na, nb);
+        nx.P = ld_hint(a.P + base + tid, stream);
+        nx.W = ld_hint(a.W + base + tid, stream);
+        if (MODE == RES_STEP) res_load(crec + cur_cell(nx), na, nb, keep);
     }
 #pragma unroll 1
     for (int it = 0; it < MPCD_RES_PPT; it++) {
@@ -536,8 +552,8 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
         const float4 ca = na, cb = nb;
         const bool more = it + 1 < MPCD_RES_PPT && i + kResThreads < n;
         if (more) {
-            nx.P = a.P[i + kResThreads];
-            nx.W = a.W[i + kResThreads];
+            nx.P = ld_hint(a.P + i + kResThreads, stream);
+            nx.W = ld_hint(a.W + i + kResThreads, stream);
         }
         if (!LEAN && c.grav_flag) {
             r.W.x += gk[0];
@@ -561,8 +577,9 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
                 k = MixT<DIM>::finish_idx(c, r, sp, sa, bounce, esc, kidx);
             }
             r.P.w = (unsigned)k;  // next step's cell, read back by cur_cell
-            MixT<DIM>::store(a, i, r);
-            if (more) res_load(crec + cur_cell(nx), na, nb);
+            st_hint(a.P + i, r.P, stream);
+            st_hint(a.W + i, r.W, stream);
+            if (more) res_load(crec + cur_cell(nx), na, nb, keep);
             // the next step's load adds the same FP32 gravity kick
             if (!LEAN && c.grav_flag) {
                 r.W.x += gk[0];
