@@ -537,6 +537,13 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
     auto cur_cell = [&](const MixRec &q) { return (int)min(q.P.w, (unsigned)(c.ncells - 1)); };
     // the particle stream leaves L2 first; the records stay
     const uint64_t stream = l2_evict_first(), keep = l2_evict_last();
+    // One species (LEAN): odd lanes add each particle to the table one
+    // iteration late, so that an atomic instruction carries particles of two
+    // different runs of 32 consecutive particles and fewer of its lanes add
+    // to the same cell (same-address lanes serialise).
+    const bool late = LEAN && (tid & 1);
+    int pk = -1, pidx[3] = {0, 0, 0};
+    float pv[3] = {0.f, 0.f, 0.f};
     MixRec nx;
     float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
     if (base + tid < n) {
@@ -590,10 +597,29 @@ __global__ void __launch_bounds__(kResThreads, MPCD_RES_MINB) k_res_parts(
             k = cur_key_idx<DIM>(c, r, sa, kidx);
             a.P[i] = make_uint4(r.P.x, r.P.y, r.P.z, (unsigned)k);
         }
-        const float vs[3] = {r.W.x, r.W.y, DIM == 3 ? r.W.z : 0.f};
-        res_add<DIM>(t, c.res_mask, c.res_shift, sums, msum, k, kidx, vs,
-                     multi ? c.mass[sp] : 1.0, multi, bad);
+        float vs[3] = {r.W.x, r.W.y, DIM == 3 ? r.W.z : 0.f};
+        bool go = true;
+        if (late) {
+            // add the previous iteration's particle, keep this one
+            const int tk = k;
+            k = pk;
+            pk = tk;
+            for (int d = 0; d < 3; d++) {
+                const int ti = kidx[d];
+                kidx[d] = pidx[d];
+                pidx[d] = ti;
+                const float tv = vs[d];
+                vs[d] = pv[d];
+                pv[d] = tv;
+            }
+            go = k >= 0;
+        }
+        if (go)
+            res_add<DIM>(t, c.res_mask, c.res_shift, sums, msum, k, kidx, vs,
+                         multi ? c.mass[sp] : 1.0, multi, bad);
     }
+    if (late && pk >= 0) res_add<DIM>(t, c.res_mask, c.res_shift, sums, msum, pk, pidx, pv, 1.0,
+                                      false, bad);
     __syncthreads();
     res_flush<DIM>(t, sums, msum, multi);
     if (MODE == RES_STEP) {
