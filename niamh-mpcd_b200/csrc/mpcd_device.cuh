@@ -230,6 +230,18 @@ __device__ __forceinline__ void push_velocity(const DevCfg &c, int vdist, double
     }
 }
 
+// push_velocity out of line.  It runs only when a particle passes the wall
+// bounce limit; inlined, its normals and square roots raised the register
+// count of the sorted kernels that stream through walls (the channel's tile
+// kernel from 80 to 120 registers, two blocks per SM instead of three).  The
+// persistent and nematic kernels keep it inline (out of line they measured
+// 19% and 1% slower).
+static __device__ __noinline__ void push_velocity_outline(const DevCfg &c, int vdist, double m,
+                                                          uint32_t step, uint32_t stream,
+                                                          uint32_t id, uint32_t k0, double *v) {
+    push_velocity(c, vdist, m, step, stream, id, k0, v);
+}
+
 // --------------------------------------------------------------- walls
 // Surface function of a planar wall (calcW_PLANE, bc.c:306-316) with the
 // wall displaced by 'off' (the grid shift during the collision stage).
@@ -288,7 +300,7 @@ __device__ void ori_bc(const DevWall &wl, const double *n, double *U) {
 // (the mixed-precision state wraps periodic axes exactly instead).  U, if
 // given, is the nematic orientation, transformed by oriBC at each
 // collision.  Returns 1 if the particle hit the bounce limit.
-template <int DIM>
+template <int DIM, bool OUTLINE = true>
 __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
                                bool only_solid, uint32_t step, uint32_t pid,
                                double *U = nullptr) {
@@ -380,8 +392,12 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
                 // step to stream again (bc.c:1477-1488); the reference tries
                 // for ever, here at most kMaxRetherm times
                 if (cnt2 >= kMaxRetherm) return flagged;
-                push_velocity(c, c.vdist[sp], m, step, MPCD_STREAM_RETHERM, pid,
-                              4u * (uint32_t)cnt2, v);
+                if (OUTLINE)
+                    push_velocity_outline(c, c.vdist[sp], m, step, MPCD_STREAM_RETHERM, pid,
+                                          4u * (uint32_t)cnt2, v);
+                else
+                    push_velocity(c, c.vdist[sp], m, step, MPCD_STREAM_RETHERM, pid,
+                                  4u * (uint32_t)cnt2, v);
                 t_left = c.dt;
                 t_coll = 0.0;
                 cnt2++;
@@ -389,6 +405,15 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
             }
         }
     }
+}
+
+// wall_collisions (solid walls only) out of line, for the mixed form, which
+// calls it only for the few particles that ended a step inside a wall: the
+// hot path of its kernels then carries none of the wall loop's registers.
+template <int DIM>
+__device__ __noinline__ int wall_collisions_rare(const DevCfg &c, double *q, double *v, int sp,
+                                                 uint32_t step, uint32_t pid) {
+    return wall_collisions<DIM>(c, q, v, sp, true, step, pid);
 }
 
 // Is the (shifted-grid) cell (a,b,z) cut by a phantom wall at its shifted

@@ -274,7 +274,7 @@ __device__ int lc_finish<F64T<2>>(const DevCfg &c, F64Rec &r, int sp, const Step
         q[d] = shift_back(r.q[d], sa.s[d], c.L[d]);
         q[d] = q[d] + c.dt * v[d];
     }
-    bounce += wall_collisions<2>(c, q, v, sp, false, sa.step, (uint32_t)r.pid, U);
+    bounce += wall_collisions<2, false>(c, q, v, sp, false, sa.step, (uint32_t)r.pid, U);
     int idx[3] = {0, 0, 0};
     for (int d = 0; d < 2; d++) {
         r.q[d] = q[d];
@@ -302,7 +302,7 @@ __device__ int lc_finish<MixT<2>>(const DevCfg &c, MixRec &r, int sp, const Step
     for (int wi = 0; wi < c.n_walls; wi++)
         if (wall_W(c.walls[wi], q, c.walls[wi].Q, 2) < 0.0) inside = true;
     if (inside) {
-        bounce += wall_collisions<2>(c, q, v, sp, false, sa.step, MixT<2>::pid(r), U);
+        bounce += wall_collisions<2, false>(c, q, v, sp, false, sa.step, MixT<2>::pid(r), U);
         for (int d = 0; d < 2; d++) {
             fx_from_double(q[d], ci[d], f[d]);
             vv[d] = (float)v[d];

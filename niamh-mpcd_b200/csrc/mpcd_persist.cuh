@@ -408,7 +408,7 @@ __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &
         qq[d] = qq[d] + c.dt * vv[d];
     }
     const uint32_t pid = (uint32_t)((const int *)(sm + l.off_pid))[j];
-    bounce += wall_collisions<DIM>(c, qq, vv, sp, false, step, pid);
+    bounce += wall_collisions<DIM, false>(c, qq, vv, sp, false, step, pid);
     for (int d = 0; d < DIM; d++) {
         q[d * l.chunk + j] = qq[d];
         v[d * l.chunk + j] = vv[d];

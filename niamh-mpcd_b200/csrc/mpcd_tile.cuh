@@ -146,7 +146,7 @@ struct MixT {
                 if (!wl.periodic && wall_W(wl, q, wl.Q, DIM) < 0.0) inside = true;
             }
             if (inside) {
-                bounce += wall_collisions<DIM>(c, q, v, sp, true, sa.step, pid(r));
+                bounce += wall_collisions_rare<DIM>(c, q, v, sp, sa.step, pid(r));
                 for (int d = 0; d < DIM; d++) {
                     fx_from_double(q[d], ci[d], f[d]);
                     vv[d] = (float)v[d];
