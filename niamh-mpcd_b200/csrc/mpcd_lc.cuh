@@ -353,7 +353,7 @@ struct LcTileLayout {
 };
 
 template <class T>
-__global__ void __launch_bounds__(256) k_lc_tile(const __grid_constant__ DevCfg c,
+__global__ void __launch_bounds__(256, 3) k_lc_tile(const __grid_constant__ DevCfg c,
                                                  typename T::State a, LcCells lc, TileBufs tb,
                                                  StepArgs sa, LcTileLayout lay) {
     extern __shared__ __align__(16) unsigned char smem[];
