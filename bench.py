@@ -527,6 +527,8 @@ def run_ensemble(args, rank, world):
     # pass first
     Qh = torch.from_numpy(Q).pin_memory().numpy()
     Vh = torch.from_numpy(V).pin_memory().numpy()
+    Qo = torch.empty(Q.shape, dtype=torch.float64).pin_memory().numpy()
+    Vo = torch.empty(V.shape, dtype=torch.float64).pin_memory().numpy()
     for timed in (False, True):
         torch.cuda.synchronize()
         if world > 1:
@@ -534,7 +536,7 @@ def run_ensemble(args, rank, world):
         t0 = time.perf_counter()
         bat.upload(nparts, Qh, Vh, step0=10 ** 6)
         bat.step(args.steps)
-        Qo, Vo = bat.download()
+        bat.download(out=(Qo, Vo))
         torch.cuda.synchronize()
         if timed:
             e2e_s = max_over_ranks(time.perf_counter() - t0, world)

@@ -542,10 +542,19 @@ class Batch:
     def step(self, nsteps=1):
         _check(self.lib.mpcd_batch_step(self.h, nsteps), "mpcd_batch_step")
 
-    def download(self):
+    def download(self, out=None):
+        """Positions and velocities of all boxes in the upload's order;
+        out=(Q, V) writes into the caller's (n, 3) float64 arrays (pinned
+        host memory makes the copies direct)."""
         n = int(self.npart.sum())
-        Q = np.zeros((n, 3))
-        V = np.zeros((n, 3))
+        if out is not None:
+            Q, V = out
+            assert Q.shape == (n, 3) and V.shape == (n, 3)
+            assert Q.dtype == np.float64 and V.dtype == np.float64
+            assert Q.flags.c_contiguous and V.flags.c_contiguous
+        else:
+            Q = np.zeros((n, 3))
+            V = np.zeros((n, 3))
         _check(self.lib.mpcd_batch_download(self.h, _p(Q), _p(V)), "mpcd_batch_download")
         return Q, V
 
