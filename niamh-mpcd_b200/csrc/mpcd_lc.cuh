@@ -352,6 +352,22 @@ struct LcTileLayout {
     int ct, cap, bytes;
 };
 
+// The tile kernel's per-cell sums use a group of 8 lanes per cell, 32 cells
+// at a time (256 threads): the sum over the group, in every lane.
+constexpr int kLcGroups = 32;
+__device__ __forceinline__ double lc_group8_sum(double v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v;
+}
+__device__ __forceinline__ int lc_group8_sum(int v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256, 3) k_lc_tile(const __grid_constant__ DevCfg c,
                                                  typename T::State a, LcCells lc, TileBufs tb,
@@ -431,9 +447,42 @@ __global__ void __launch_bounds__(256, 3) k_lc_tile(const __grid_constant__ DevC
                 s_cell[j] = (unsigned char)(cl - cl_a);
         __syncthreads();
         // ---- per cell: orientation-collision parameters and activity ----
-        for (int cl = cl_a + tid; cl < cl_b; cl += nth) {
+        // A group of 8 lanes per cell (32 cells at a time): each lane sums
+        // every eighth particle of the cell, the group adds its lanes.
+        for (int cb = cl_a; cb < cl_b; cb += kLcGroups) {
+            const int cl = cb + (tid >> 3), gl = tid & 7;
+            const bool has = cl < cl_b;
+            const int j0 = has ? s_start[cl] - p0 : 0, j1 = has ? s_start[cl + 1] - p0 : 0;
+            const int pop = j1 - j0;
+            double avm = 0.0;
+            for (int j = j0 + gl; j < j1; j += 8) avm += c.mfpot[sp_[j].sp];
+            avm = lc_group8_sum(avm);
+            double ACT = 0.0, sw = 0.0, spos = 0.0;
+            if (dipole) {
+                // species populations of the cell, then the activity of the
+                // species that pass the minimum-ratio test
+                unsigned elig = 0u;
+                for (int sx = 0; sx < c.n_species; sx++) {
+                    int n = 0;
+                    for (int j = j0 + gl; j < j1; j += 8) n += sp_[j].sp == sx;
+                    n = lc_group8_sum(n);
+                    if (c.minactratio[sx] == 0.0 || c.minactratio[sx] * c.gndnst < (double)n)
+                        elig |= 1u << sx;
+                }
+                for (int j = j0 + gl; j < j1; j += 8) {
+                    const int sx = sp_[j].sp;
+                    if ((elig >> sx) & 1u) {
+                        ACT += c.act[sx] / c.mass[sx];
+                        sw += c.sigwidth[sx];
+                        spos += c.sigpos[sx];
+                    }
+                }
+                ACT = lc_group8_sum(ACT);
+                sw = lc_group8_sum(sw);
+                spos = lc_group8_sum(spos);
+            }
+            if (!has || gl != 0) continue;
             const int lcx = cl - cl_a, cell = c0 + cl;
-            const int j0 = s_start[cl] - p0, j1 = s_start[cl + 1] - p0, pop = j1 - j0;
             double *C = &s_c[9 * lcx];
             const double d0 = lc.dir[2 * cell], d1 = lc.dir[2 * cell + 1];
             // rotAx = DIR x xhat = (0, 0, -d1), normalised; rotAngle =
@@ -444,23 +493,9 @@ __global__ void __launch_bounds__(256, 3) k_lc_tile(const __grid_constant__ DevC
             double ca = d0 / sqrt(d0 * d0 + d1 * d1) / 1.0;
             C[0] = rz;
             C[1] = -1. * acos(ca);
-            double avm = 0.0;
-            for (int j = j0; j < j1; j++) avm += c.mfpot[sp_[j].sp];
             if (pop > 1) avm /= (float)pop;
             C[2] = avm * 0.5 * 2.0;
-            double ACT = 0.0, sw = 0.0, spos = 0.0;
             if (dipole) {
-                int cnt[MPCD_MAX_SPECIES];
-                for (int s = 0; s < MPCD_MAX_SPECIES; s++) cnt[s] = 0;
-                for (int j = j0; j < j1; j++) cnt[sp_[j].sp]++;
-                for (int j = j0; j < j1; j++) {
-                    int s = sp_[j].sp;
-                    if (c.minactratio[s] == 0.0 || c.minactratio[s] * c.gndnst < (double)cnt[s]) {
-                        ACT += c.act[s] / c.mass[s];
-                        sw += c.sigwidth[s];
-                        spos += c.sigpos[s];
-                    }
-                }
                 if (op == 17 || op == 20) ACT *= c.gndnst / ((double)pop);
                 if (op == 20 || op == 21) {
                     sw /= (double)pop;
@@ -572,15 +607,18 @@ __global__ void __launch_bounds__(256, 3) k_lc_tile(const __grid_constant__ DevC
         }
         __syncthreads();
         // ---- per cell: Andersen sums, angular momentum ----
-        for (int cl = cl_a + tid; cl < cl_b; cl += nth) {
-            const int lcx = cl - cl_a, cell = c0 + cl;
-            const int j0 = s_start[cl] - p0, j1 = s_start[cl + 1] - p0;
-            double *C = &s_c[9 * lcx];
-            const double M = lc.mass[cell], ACT = C[3];
+        // (a group of 8 lanes per cell, as above)
+        for (int cb = cl_a; cb < cl_b; cb += kLcGroups) {
+            const int cl = cb + (tid >> 3), gl = tid & 7;
+            const bool has = cl < cl_b;
+            const int lcx = cl - cl_a, cell = c0 + (has ? cl : cl_a);
+            const int j0 = has ? s_start[cl] - p0 : 0, j1 = has ? s_start[cl + 1] - p0 : 0;
+            const double *C = &s_c[9 * (has ? lcx : 0)];
+            const double ACT = C[3];
             const double D0 = lc.dir[2 * cell], D1 = lc.dir[2 * cell + 1];
             const double cm0 = lc.cm[2 * cell], cm1 = lc.cm[2 * cell + 1];
             double RS0 = 0, RS1 = 0, AS0 = 0, AS1 = 0, Llm = 0, Lnm = 0;
-            for (int j = j0; j < j1; j++) {
+            for (int j = j0 + gl; j < j1; j += 8) {
                 const LcPart &P = sp_[j];
                 double m = c.mass[P.sp];
                 RS0 += m * P.rv[0];
@@ -596,11 +634,20 @@ __global__ void __launch_bounds__(256, 3) k_lc_tile(const __grid_constant__ DevC
                 Llm += r0 * dv1 - r1 * dv0;
                 Lnm += P.tz * dt;
             }
-            C[4] = RS0 / M;
-            C[5] = RS1 / M;
-            C[6] = AS0 / M;
-            C[7] = AS1 / M;
-            C[8] = (1. / lc.izz[cell]) * (Llm + Lnm);
+            RS0 = lc_group8_sum(RS0);
+            RS1 = lc_group8_sum(RS1);
+            AS0 = lc_group8_sum(AS0);
+            AS1 = lc_group8_sum(AS1);
+            Llm = lc_group8_sum(Llm);
+            Lnm = lc_group8_sum(Lnm);
+            if (!has || gl != 0) continue;
+            double *Cw = &s_c[9 * lcx];
+            const double M = lc.mass[cell];
+            Cw[4] = RS0 / M;
+            Cw[5] = RS1 / M;
+            Cw[6] = AS0 / M;
+            Cw[7] = AS1 / M;
+            Cw[8] = (1. / lc.izz[cell]) * (Llm + Lnm);
         }
         __syncthreads();
         // ---- per particle: collision, TEMP, stream, walls, next key ----
