@@ -119,3 +119,29 @@ def synthetic_state(cfg, ppc, seed=2024, dtype=np.float64):
         U[:] = u / np.linalg.norm(u, axis=1, keepdims=True)
     spid = np.zeros(n, dtype=np.int32)
     return Q, V, U, spid
+
+
+def ensemble_sides(nboxes, seed=5000):
+    """Side lengths of configuration 5's ensemble: nboxes cubic boxes with
+    sides drawn uniformly from {8, 12, 16, 24, 32}, the same on every rank."""
+    rng = np.random.default_rng(seed)
+    return rng.choice([8, 12, 16, 24, 32], size=nboxes)
+
+
+def shard_boxes(work, world, rank):
+    """The boxes rank `rank` of `world` steps when an ensemble is split
+    across GPUs: boxes are independent (no data crosses between them), so
+    each goes whole to one rank, the largest first to the least-loaded rank
+    (ties to the lower rank), which keeps the ranks' particle counts within
+    one box of each other.  Every rank computes the same split from the same
+    per-box work (particle counts); returns the rank's box indices in
+    ascending order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    load = [0] * world
+    owner = [0] * len(work)
+    for b in sorted(range(len(work)), key=lambda j: (-int(work[j]), j)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[b] = r
+        load[r] += int(work[b])
+    return [b for b in range(len(work)) if owner[b] == rank]
