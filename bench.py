@@ -11,9 +11,10 @@ the plain FP64 form is measured in the same run ("fp64" key).
 N > 1 runs independent replica boxes, one per rank (the path has no data
 exchange between replicas): weak scaling, value summed over ranks, time the
 max over ranks.  --workload ensemble with N > 1 splits one ensemble of boxes
-across the ranks, balanced by particle count: strong scaling.  --impl reference times the reference's own serial C timestep
-(built from its sources into oracle/_ref/) on a bounded sample of the same
-workload on this host's cores.
+across the ranks, balanced by particle count: strong scaling.  --impl
+reference times the reference's own serial C timestep (built from its
+sources into oracle/_ref/) on a bounded sample of the same workload on this
+host's cores.
 """
 import argparse
 import json
