@@ -131,8 +131,10 @@ typedef struct mpcd_config {
 /* Per-handle error counters (the reference prints warnings instead). */
 typedef struct mpcd_status {
     uint64_t steps;         /* steps executed                               */
-    uint64_t escaped;       /* particles binned outside the grid (bin(),
-                               mpc.c:970-982)                               */
+    uint64_t escaped;       /* particles that left the grid: re-placed at
+                               the end of their step as the reference's
+                               re-bin does (bin(), mpc.c:969-982), or, at
+                               a shifted binning, clamped to the grid      */
     uint64_t bounce_limit;  /* particles that exceeded NBOUNCE wall
                                collisions in a step (bcCNT, bc.c:1461-1492);
                                the reference's remedies are applied: longer

@@ -1293,10 +1293,14 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
     // one wave: the blocks of the particle pass that fit on the handle's
     // device at once (the kernel strides over the particles); the grid also
     // fixes the order of the FP64 KE sums, so KE rounding depends on it
+    // a box periodic on every axis runs the particle pass without the
+    // re-placement of particles that leave the grid (they cannot)
+    const bool open = !c.all_periodic;
+    auto kstep = open ? k_r64_parts<DIM, RES_STEP, true> : k_r64_parts<DIM, RES_STEP, false>;
     if (h->r64_per_sm == 0) {
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_r64_parts<DIM, RES_STEP>, 256,
-                                                          0) != cudaSuccess || b < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kstep, 256, 0) != cudaSuccess ||
+            b < 1)
             b = 1;
         h->r64_per_sm = b;
     }
@@ -1307,14 +1311,14 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
         CK(cudaMemsetAsync(h->r64sum, 0, sizeof(double) * 8 * nc, h->stream));
         CK(cudaMemsetAsync(h->r64pop, 0, sizeof(int) * 2 * nc, h->stream));
         CK(cudaMemsetAsync(acc_cur, 0, sizeof(double) * ACC_WORDS, h->stream));
-        k_r64_parts<DIM, RES_SUM><<<pgrid, 256, 0, h->stream>>>(
+        k_r64_parts<DIM, RES_SUM, false><<<pgrid, 256, 0, h->stream>>>(
             c, h->f[h->cur], h->n, (const Rec *)h->crec, sum_cur, acc_cur, h->status, sa);
         launches += 1;
     }
     CK(launch_pdl(k_r64_cells<DIM>, (int)((nc + 255) / 256), 256, 0, h->stream, c, sum_cur,
                   (Rec *)h->crec, sa, acc_cur, acc_nxt));
     time_begin(h);
-    CK(launch_pdl(k_r64_parts<DIM, RES_STEP>, pgrid, 256, 0, h->stream, c, h->f[h->cur], h->n,
+    CK(launch_pdl(kstep, pgrid, 256, 0, h->stream, c, h->f[h->cur], h->n,
                   (const Rec *)h->crec, sum_nxt, acc_cur, h->status, sa));
     time_end(h);
     launches += 2;

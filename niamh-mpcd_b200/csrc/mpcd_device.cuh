@@ -407,6 +407,59 @@ __device__ int wall_collisions(const DevCfg &c, double *q, double *v, int sp,
     }
 }
 
+// The end-of-step re-bin of the reference (bin(), mpc.c:969-982, on the
+// unshifted grid after streaming and the wall collisions): a particle whose
+// truncated cell index on some axis lies outside [0, L] has left the grid.
+// replacePos_WithCheck (init.c:1462-1483) puts it at the uniform position
+// L u (replace, init.c:1240-1243), again while some wall has W <= TOL there,
+// and bin() gives it a Maxwell-Boltzmann velocity (genrand_gaussMB per
+// component) and, for a nematic, a uniform orientation (genrand_coneNP with
+// theta = pi).  The draws come from the particle's counter-based streams of
+// the step: placement attempt a takes the uniforms DIM a .. DIM a + DIM - 1.
+// The reference tries for ever; here at most kMaxReplace attempts (the
+// last position is kept).  Out of line: it runs only for such particles.
+__device__ __forceinline__ bool left_grid(const DevCfg &c, const double *q, int dim) {
+    for (int d = 0; d < dim; d++) {
+        const int a = (int)q[d];
+        if (a < 0 || a > c.L[d]) return true;
+    }
+    return false;
+}
+constexpr uint32_t kMaxReplace = 64;
+// left_grid for a position word pair (cell index, 32-bit offset) per axis:
+// (int) Q < 0 when Q <= -1, (int) Q > L when Q >= L + 1
+__device__ __forceinline__ bool left_grid_fx(const DevCfg &c, const int *ci, const uint32_t *f,
+                                             int dim) {
+    for (int d = 0; d < dim; d++)
+        if (ci[d] < -1 || (ci[d] == -1 && f[d] == 0u) || ci[d] > c.L[d]) return true;
+    return false;
+}
+template <int DIM>
+__device__ __noinline__ void replace_escaped(const DevCfg &c, double *q, double *v, double *U,
+                                             int sp, uint32_t step, uint32_t pid) {
+    for (uint32_t a = 0; a < kMaxReplace; a++) {
+        for (int d = 0; d < DIM; d++)
+            q[d] = __dmul_rn((double)c.L[d],
+                             mpcd_rng_uniform(c.seed, c.replica, step, MPCD_STREAM_ESCAPE_POS, pid,
+                                              a * (uint32_t)DIM + (uint32_t)d));
+        bool in_wall = false;
+        for (int w = 0; w < c.n_walls; w++)
+            if (wall_W(c.walls[w], q, c.walls[w].Q, DIM) <= kTol) in_wall = true;
+        if (!in_wall) break;
+    }
+    for (int d = 0; d < DIM; d++)
+        v[d] = __dmul_rn(c.sig[sp], (double)mpcd_rng_normal(c.seed, c.replica, step,
+                                                            MPCD_STREAM_ESCAPE_VEL, pid,
+                                                            (uint32_t)d));
+    if (U && DIM == 2) {
+        const double u =
+            mpcd_rng_uniform(c.seed, c.replica, step, MPCD_STREAM_ESCAPE_ORI, pid, 0u);
+        const double phi = __dmul_rn(M_PI, __dsub_rn(1.0, __dmul_rn(2.0, u)));
+        U[0] = cos(phi);
+        U[1] = sin(phi);
+    }
+}
+
 // wall_collisions (solid walls only) out of line, for the mixed form, which
 // calls it only for the few particles that ended a step inside a wall: the
 // hot path of its kernels then carries none of the wall loop's registers.

@@ -275,6 +275,11 @@ __device__ int lc_finish<F64T<2>>(const DevCfg &c, F64Rec &r, int sp, const Step
         q[d] = q[d] + c.dt * v[d];
     }
     bounce += wall_collisions<2, false>(c, q, v, sp, false, sa.step, (uint32_t)r.pid, U);
+    if (left_grid(c, q, 2)) {
+        // the reference's end-of-step re-bin re-places it (mpc.c:969-982)
+        replace_escaped<2>(c, q, v, U, sp, sa.step, (uint32_t)r.pid);
+        esc++;
+    }
     int idx[3] = {0, 0, 0};
     for (int d = 0; d < 2; d++) {
         r.q[d] = q[d];
@@ -307,6 +312,16 @@ __device__ int lc_finish<MixT<2>>(const DevCfg &c, MixRec &r, int sp, const Step
             fx_from_double(q[d], ci[d], f[d]);
             vv[d] = (float)v[d];
         }
+    }
+    if (left_grid_fx(c, ci, f, 2)) {
+        // the reference's end-of-step re-bin re-places it (mpc.c:969-982)
+        double qr[3] = {0, 0, 0}, vr[3] = {vv[0], vv[1], 0.0};
+        replace_escaped<2>(c, qr, vr, U, sp, sa.step, MixT<2>::pid(r));
+        for (int d = 0; d < 2; d++) {
+            fx_from_double(qr[d], ci[d], f[d]);
+            vv[d] = (float)vr[d];
+        }
+        esc++;
     }
     for (int d = 0; d < 2; d++) {
         if (c.pbc[d]) {

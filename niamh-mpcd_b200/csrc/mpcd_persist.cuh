@@ -341,7 +341,7 @@ template <int DIM>
 __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &l,
                                               const PerGlobal &g, unsigned char *sm, int j,
                                               const double s[3], const double *rvv,
-                                              uint32_t step, int &bounce) {
+                                              uint32_t step, int &bounce, int &esc) {
     using Q = PerQ<DIM>;
     double *q = (double *)(sm + l.off_q), *v = (double *)(sm + l.off_v);
     const int k = ((const int *)(sm + l.off_k))[j];
@@ -409,6 +409,11 @@ __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &
     }
     const uint32_t pid = (uint32_t)((const int *)(sm + l.off_pid))[j];
     bounce += wall_collisions<DIM, false>(c, qq, vv, sp, false, step, pid);
+    if (left_grid(c, qq, DIM)) {
+        // the reference's end-of-step re-bin re-places it (mpc.c:969-982)
+        replace_escaped<DIM>(c, qq, vv, nullptr, sp, step, pid);
+        esc++;
+    }
     for (int d = 0; d < DIM; d++) {
         q[d * l.chunk + j] = qq[d];
         v[d * l.chunk + j] = vv[d];
@@ -493,7 +498,7 @@ __global__ void __launch_bounds__(kPerThreads)
         if (c.galinv) mpcd_rng_shift(c.seed, c.replica, step + 1u, DIM, sn);
         double ke = 0.0;
         for (int j = tid; j < np; j += nt) {
-            ke += per_collide<DIM>(c, l, g, sm, j, s, rv, step, bounce);
+            ke += per_collide<DIM>(c, l, g, sm, j, s, rv, step, bounce, esc);
             if (!last) per_enter<DIM>(c, l, g, sm, j, sn, rvn, esc);
         }
         const double t = per_block_sum(ke, red);

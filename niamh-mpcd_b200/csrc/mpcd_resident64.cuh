@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(256) k_r64_cells(const __grid_constant__ DevCf
 #ifndef R64_MINB
 #define R64_MINB 4
 #endif
-template <int DIM, int MODE>
+// OPEN: the box has a side without a periodic wall (see F64T::finish).
+template <int DIM, int MODE, bool OPEN>
 __global__ void __launch_bounds__(256, R64_MINB) k_r64_parts(const __grid_constant__ DevCfg c,
                                                    Fp64State a, int n, const R64Rec *crec,
                                                    R64Sums sums, double *acc,
@@ -113,11 +114,12 @@ __global__ void __launch_bounds__(256, R64_MINB) k_r64_parts(const __grid_consta
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         // the particle stays in place, so its id is not written, and read
-        // only where walls may re-thermalise it (the draws are keyed by the
+        // where walls may re-thermalise it or it may leave the grid (the
+        // draws are keyed by the
         // id); otherwise as F64T::load: the shifted position and the
         // velocity with this step's kick
         F64Rec r;
-        r.pid = (MODE == RES_STEP && c.n_walls > 0) ? a.pid[i] : 0;
+        r.pid = (MODE == RES_STEP && !c.all_periodic) ? a.pid[i] : 0;
         for (int d = 0; d < 3; d++) {
             r.q[d] = d < DIM ? shift_fwd(a.q[d][i], sa.s[d], c.L[d]) : 0.0;
             r.v[d] = d < DIM ? a.v[d][i] : 0.0;
@@ -142,7 +144,7 @@ __global__ void __launch_bounds__(256, R64_MINB) k_r64_parts(const __grid_consta
             t += r.v[1] * r.v[1];
             t += r.v[2] * r.v[2];
             ke += c.mass[sp] * t;
-            k = F64T<DIM>::finish(c, r, sp, sa, bounce, esc);
+            k = F64T<DIM>::template finish<OPEN>(c, r, sp, sa, bounce, esc);
             for (int d = 0; d < DIM; d++) {
                 a.q[d][i] = r.q[d];
                 a.v[d][i] = r.v[d];

@@ -51,8 +51,12 @@ enum {
     MPCD_STREAM_INIT_POS = 7, /* positions, 4 uniforms per placement attempt */
     MPCD_STREAM_INIT_VEL = 8, /* velocities                                  */
     MPCD_STREAM_INIT_ORI = 9, /* orientations                                */
-    MPCD_STREAM_RETHERM = 10  /* bounce-limit re-thermalisation, per particle,
+    MPCD_STREAM_RETHERM = 10, /* bounce-limit re-thermalisation, per particle,
                                  4 draws per re-thermalisation of a step    */
+    /* re-placement of a particle that left the grid, per particle and step: */
+    MPCD_STREAM_ESCAPE_POS = 11, /* position, DIM uniforms per attempt       */
+    MPCD_STREAM_ESCAPE_VEL = 12, /* velocity, DIM normals                    */
+    MPCD_STREAM_ESCAPE_ORI = 13  /* nematic orientation, one uniform         */
 };
 
 /* Maximum Philox blocks a rejection loop may consume (2 attempts per block).

@@ -153,6 +153,16 @@ struct MixT {
                 }
             }
         }
+        if (left_grid_fx(c, ci, f, DIM)) {
+            // the reference's end-of-step re-bin re-places it (mpc.c:969-982)
+            double q[3] = {0, 0, 0}, v[3] = {vv[0], vv[1], vv[2]};
+            replace_escaped<DIM>(c, q, v, nullptr, sp, sa.step, pid(r));
+            for (int d = 0; d < DIM; d++) {
+                fx_from_double(q[d], ci[d], f[d]);
+                vv[d] = (float)v[d];
+            }
+            esc++;
+        }
         for (int d = 0; d < DIM; d++) {
             if (c.pbc[d]) {
                 if (ci[d] < 0 || ci[d] >= c.L[d])
@@ -225,6 +235,10 @@ struct F64T {
     static __device__ __forceinline__ void set_vel(Rec &r, const double v[3]) {
         for (int d = 0; d < DIM; d++) r.v[d] = v[d];
     }
+    // OPEN: the box may have an open side, so that particles can leave the
+    // grid (a box periodic on every axis cannot: its kernels compile the
+    // re-placement out)
+    template <bool OPEN = true>
     static __device__ __forceinline__ int finish(const DevCfg &c, Rec &r, int sp,
                                                  const StepArgs &sa, int &bounce, int &esc) {
         double q[3] = {0, 0, 0}, v[3] = {0, 0, 0};
@@ -234,6 +248,11 @@ struct F64T {
             q[d] = q[d] + c.dt * v[d];
         }
         bounce += wall_collisions<DIM>(c, q, v, sp, false, sa.step, (uint32_t)r.pid);
+        if (OPEN && left_grid(c, q, DIM)) {
+            // the reference's end-of-step re-bin re-places it (mpc.c:969-982)
+            replace_escaped<DIM>(c, q, v, nullptr, sp, sa.step, (uint32_t)r.pid);
+            esc++;
+        }
         int idx[3] = {0, 0, 0};
         for (int d = 0; d < DIM; d++) {
             r.q[d] = q[d];

@@ -212,8 +212,9 @@ int oracle_ncells(const oracle_t *o) { return o->ncells; }
 
 /* -------------------------------------------------------------- binning */
 /* Cell key by truncation; on shifted grids periodic axes map index L to 0
- * (bin, mpc.c:958-968).  Particles outside the grid are counted as escaped
- * and clamped (the reference re-places them at random, mpc.c:970-982). */
+ * (bin, mpc.c:958-968).  A particle outside the grid here is counted as
+ * escaped and clamped; the end-of-step re-bin's re-placement
+ * (mpc.c:969-982) is replace_escaped's, before the unshifted binning. */
 static void bin_cells(oracle_t *o, int shifted) {
     int n = o->n;
     memset(o->cnt, 0, (size_t)o->ncells * sizeof(int));
@@ -931,6 +932,53 @@ int oracle_set_vdist(oracle_t *o, const int *vdist) {
     return 0;
 }
 
+/* The end-of-step re-bin (bin, mpc.c:969-982, unshifted): a particle whose
+ * truncated index on some axis lies outside [0, L] left the grid and is
+ * re-placed: replacePos_WithCheck (init.c:1462-1483) draws the uniform
+ * position L u (replace, init.c:1240-1243) until no wall has W <= TOL there
+ * (every wall, as the reference loops over all of them), then bin() gives it
+ * a Maxwell-Boltzmann velocity (genrand_gaussMB per component) and, for a
+ * nematic, the orientation genrand_coneNP(U, pi, DIM) (rand.c:397-425, 2D
+ * branch).  The reference keeps the particle in its old cell list until the
+ * next bin(); here it is binned at its new position.  Draws: the particle's
+ * counter-based streams of the step; placement attempt a takes uniforms
+ * DIM a .. DIM a + DIM - 1, at most 64 attempts (the reference tries for
+ * ever). */
+static void replace_escaped(oracle_t *o, int i, uint32_t step) {
+    const int dim = o->dim;
+    double *q = &o->Q[3 * i];
+    int out = 0;
+    for (int d = 0; d < dim; d++) {
+        const int a = (int)q[d];
+        if (a < 0 || a > o->L[d]) out = 1;
+    }
+    if (!out) return;
+    o->escaped++;
+    const mpcd_config *c = &o->cfg;
+    for (uint32_t a = 0; a < 64u; a++) {
+        for (int d = 0; d < dim; d++)
+            q[d] = (double)o->L[d] * mpcd_rng_uniform(c->seed, c->replica, step,
+                                                      MPCD_STREAM_ESCAPE_POS, (uint32_t)i,
+                                                      a * (uint32_t)dim + (uint32_t)d);
+        int in_wall = 0;
+        for (int w = 0; w < c->n_walls; w++)
+            if (wall_W(o, w, q) <= TOL) in_wall = 1;
+        if (!in_wall) break;
+    }
+    const double sig = sqrt(c->kbt / c->species[o->spid[i]].mass);
+    for (int d = 0; d < dim; d++)
+        o->V[3 * i + d] = sig * (double)mpcd_rng_normal(c->seed, c->replica, step,
+                                                        MPCD_STREAM_ESCAPE_VEL, (uint32_t)i,
+                                                        (uint32_t)d);
+    if (c->lc != 0 && dim == 2) {
+        const double u = mpcd_rng_uniform(c->seed, c->replica, step, MPCD_STREAM_ESCAPE_ORI,
+                                          (uint32_t)i, 0u);
+        const double phi = MPCD_PI * (1. - 2. * u);
+        o->U[3 * i] = cos(phi);
+        o->U[3 * i + 1] = sin(phi);
+    }
+}
+
 int oracle_step(oracle_t *o, uint32_t step) {
     o->step = step;
     int dim = o->dim, n = o->n, op = o->cfg.coll_op;
@@ -1001,6 +1049,8 @@ int oracle_step(oracle_t *o, uint32_t step) {
     for (int i = 0; i < n; i++)
         for (int d = 0; d < dim; d++) o->Q[3 * i + d] = o->Q[3 * i + d] + o->cfg.dt * o->V[3 * i + d];
     for (int i = 0; i < n; i++) wall_collisions(o, i);
+    /* the re-bin's escape rule (bin, mpc.c:969-982) */
+    for (int i = 0; i < n; i++) replace_escaped(o, i, step);
     /* re-bin on the unshifted grid + localPROP, mpc.c:4936-4942 */
     bin_cells(o, 0);
     local_prop(o);

@@ -76,7 +76,7 @@ static int g_ncells = 0;
 /* draw bookkeeping */
 static uint64_t g_seed = 0;
 static uint32_t g_replica = 0, g_step = 0;
-enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT, PH_RETHERM };
+enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT, PH_RETHERM, PH_ESCAPE };
 static int g_phase = PH_NONE;
 static int g_cell = 0;
 static particleMPC *g_cursor = NULL;
@@ -622,6 +622,9 @@ static float next_normal(void) {
     } else if (g_phase == PH_RETHERM) {
         g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_RETHERM, (uint32_t)g_pid,
                             (uint32_t)g_comp++);
+    } else if (g_phase == PH_ESCAPE) {
+        g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_ESCAPE_VEL, (uint32_t)g_pid,
+                            (uint32_t)g_comp++);
     } else if (g_phase == PH_COLLIDE && g_cursor) {
         int pid = (int)(g_cursor - g_pp);
         g = mpcd_rng_normal(g_seed, g_replica, g_step, MPCD_STREAM_THERMAL,
@@ -660,6 +663,8 @@ double genrand_real(void) {
     if (g_phase == PH_LC)
         return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_LC,
                                 (uint32_t)g_pid, g_k++);
+    if (g_phase == PH_ESCAPE)
+        return mpcd_rng_uniform(g_seed, g_replica, g_step, g_stream, (uint32_t)g_pid, g_k++);
     /* stochrotMPC draws a uniform only for the rotation sign, which
      * (long)genrand_real() truncates to 0 (mpc.c:1291) */
     if (g_phase == PH_COLLIDE) return 0.0;
@@ -690,7 +695,11 @@ void genrand_sphere(double vec[], int dimension) {
     for (int i = 0; i < dimension; i++) vec[i] = (i == 0);
 }
 void genrand_coneNP(double vec[], double theta, int dimension) {
-    if (g_phase != PH_INIT) {
+    if (g_phase == PH_ESCAPE) {
+        /* the orientation of an escaped nematic: the particle's own stream */
+        g_stream = MPCD_STREAM_ESCAPE_ORI;
+        g_k = 0;
+    } else if (g_phase != PH_INIT) {
         genrand_sphere(vec, dimension);
         return;
     }
@@ -821,6 +830,30 @@ void genrand_maierSaupe(double DIR[], double rotAx[], double rotAngle,
     g_k = 0;
     orig(DIR, rotAx, rotAngle, U, KBT, S, effM);
 }
+/* The escape rule of bin() (mpc.c:969-982): replacePos_WithCheck re-places a
+ * particle that left the grid from the particle's position stream of the
+ * step; the velocity (genrand_gaussMB) and orientation (genrand_coneNP)
+ * draws that bin() makes next come from its velocity and orientation
+ * streams.  bin() ends the phase. */
+typedef void (*rpwc_fn)(particleMPC *, bc *);
+void replacePos_WithCheck(particleMPC *pp, bc WALL[]) {
+    static rpwc_fn orig = NULL;
+    if (!orig) orig = (rpwc_fn)dlsym(RTLD_NEXT, "replacePos_WithCheck");
+    g_phase = PH_ESCAPE;
+    g_pid = (int)(pp - g_pp);
+    g_stream = MPCD_STREAM_ESCAPE_POS;
+    g_k = 0;
+    g_comp = 0;
+    orig(pp, WALL);
+}
+typedef void (*bin_fn)(cell ***, spec *, bc *, double, int, int);
+void bin(cell ***CL, spec *SP, bc WALL[], double KBT, int LC, int shifted) {
+    static bin_fn orig = NULL;
+    if (!orig) orig = (bin_fn)dlsym(RTLD_NEXT, "bin");
+    orig(CL, SP, WALL, KBT, LC, shifted);
+    if (g_phase == PH_ESCAPE) g_phase = PH_NONE;
+}
+
 /* Initialisation: place, push, orient and replace (init.c:1219-1405) learn
  * their particle from the address they are given. */
 static int pid_of(const void *field, size_t off) {
@@ -840,6 +873,11 @@ typedef void (*replace_fn)(particleMPC *);
 void replace(particleMPC *p) {
     static replace_fn orig = NULL;
     if (!orig) orig = (replace_fn)dlsym(RTLD_NEXT, "replace");
+    if (g_phase == PH_ESCAPE) {
+        /* attempt a of replacePos_WithCheck: uniforms DIM a .. (g_k runs on) */
+        orig(p);
+        return;
+    }
     g_pid = (int)(p - g_pp);
     g_stream = MPCD_STREAM_INIT_POS;
     g_k = 4u * (uint32_t)(g_attempt ? ++g_attempt[g_pid] : 1);

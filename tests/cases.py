@@ -127,3 +127,43 @@ def thin_gap(op=abi.COLL_ARBAXIS, precision=abi.PREC_FP64, n=400, vy=10.0, seed=
     V = rng.standard_normal((n, 3))
     V[: n // 4, 1] = vy * np.sign(V[: n // 4, 1])
     return cfg, Q, V, np.zeros(n, dtype=np.int32)
+
+
+def open_bottom(op=abi.COLL_ARBAXIS, precision=abi.PREC_FP64, dim=3, n=600, vy=15.0, seed=7):
+    """A box of 6 cells per side, periodic across x (and z in 3D), with a
+    no-slip ceiling at y = 4 and no wall below: the fastest particles leave
+    through the bottom within a step or two, and the reference's end-of-step
+    re-bin re-places them (bin, mpc.c:969-982) at a uniform position that
+    no wall excludes (the ceiling rejects y >= 4) with a fresh thermal
+    velocity and, for the nematic (2D), orientation.  (A particle that ends
+    a step in [-1, 0) is binned to cell 0 by truncation and leaves at a
+    later step; none can end one in [L, L + 1), below the ceiling, where the
+    reference's shifted bin would re-place it instead.)  Returns (config, Q,
+    V, U, species)."""
+    import numpy as np
+    L = (6, 6, 6)[:dim] + (1,) * (3 - dim)
+    w = [abi.make_wall((1, 0, 0), (0, 0, 0), 0.0, DN=6.0),
+         abi.make_wall((-1, 0, 0), (6, 0, 0), 0.0, DN=6.0),
+         abi.make_wall((0, -1, 0), (0, 4.0, 0), 0.0, MVN=-1.0, MVT=-1.0)]
+    if dim == 3:
+        w += [abi.make_wall((0, 0, 1), (0, 0, 0), 0.0, DN=6.0),
+              abi.make_wall((0, 0, -1), (0, 0, 6), 0.0, DN=6.0)]
+    if op == "lc":
+        cfg = W.cfg_nematic2d(L=L[:2], walls=w, seed=seed, precision=precision, gndnst=10.0)
+    else:
+        cfg = W.base_config(dim, L, coll_op=op, walls=w, seed=seed, precision=precision)
+    rng = np.random.default_rng(seed)
+    Q = np.zeros((n, 3))
+    Q[:, 0] = rng.random(n) * 6
+    Q[:, 1] = 0.1 + rng.random(n) * 3.8
+    if dim == 3:
+        Q[:, 2] = rng.random(n) * 6
+    V = rng.standard_normal((n, 3))
+    V[: n // 4, 1] = -vy
+    if dim == 2:
+        V[:, 2] = 0.0
+    U = None
+    if op == "lc":
+        a = rng.random(n) * 2 * np.pi
+        U = np.stack([np.cos(a), np.sin(a), np.zeros(n)], axis=1)
+    return cfg, Q, V, U, np.zeros(n, dtype=np.int32)

@@ -159,3 +159,56 @@ def test_bounce_limit_rethermalises_like_the_oracle(prec, kernel, vdist):
         d -= np.round(d / L) * L
         same = dv <= 1e-4
         assert np.all(np.isfinite(vg)) and np.abs(d[same]).max() < 1e-4
+
+
+@pytest.mark.parametrize("op,dim,kernel", [
+    (abi.COLL_ARBAXIS, 3, abi.KERNEL_AUTO), (abi.COLL_ARBAXIS, 3, abi.KERNEL_RESIDENT),
+    (abi.COLL_ARBAXIS, 3, abi.KERNEL_TILE), (abi.COLL_ARBAXIS, 3, abi.KERNEL_SPLIT),
+    (abi.COLL_ARBAXIS, 3, abi.KERNEL_GROUP), (abi.COLL_RAT, 3, abi.KERNEL_PERSIST),
+    (abi.COLL_RAT, 3, abi.KERNEL_TILE), (abi.COLL_MPCAT, 2, abi.KERNEL_TILE),
+    ("lc", 2, abi.KERNEL_AUTO)])
+def test_escaped_particles_are_replaced_like_the_oracle(op, dim, kernel):
+    """Particles that leave the grid through an open side are re-placed at
+    the end of the step as the reference's re-bin does (bin, mpc.c:969-982,
+    the oracle pinned to the reference): the same positions, velocities,
+    orientations and escape count, FP64, every kernel family."""
+    from cases import open_bottom
+    cfg, Q, V, U, sp = open_bottom(op, dim=dim)
+    o = Oracle(cfg, Q, V, U, sp)
+    g = Solver(cfg)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, sp)
+    L = np.array(cfg.L[:3], dtype=float)
+    for s in (1, 2, 3, 4):
+        o.step(s)
+        g.step(1, s)
+    qo, vo, uo = o.particles()
+    qg, vg, ug = g.download()
+    st = g.status()
+    assert o.escaped() > 20 and st.escaped == o.escaped(), (st.escaped, o.escaped())
+    _compare(abi.PREC_FP64, qg, vg, qo, vo, L, 0)
+    if U is not None:
+        assert np.abs(ug - uo).max() < 1e-11
+    g.close()
+    o.close()
+
+
+@pytest.mark.parametrize("kernel", [abi.KERNEL_RESIDENT, abi.KERNEL_TILE, abi.KERNEL_SPLIT])
+def test_mixed_form_replaces_escaped_particles(kernel):
+    """The mixed form re-places particles that leave the grid too (its
+    fixed-point positions stop at the grid's lower face, so a particle in
+    [-1, 0) is held at 0 and leaves one step later than in the FP64 form):
+    every particle ends inside the grid with a finite velocity, and the
+    escapes are counted."""
+    from cases import open_bottom
+    cfg, Q, V, U, sp = open_bottom(abi.COLL_ARBAXIS, precision=abi.PREC_MIXED)
+    g = Solver(cfg)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, sp)
+    for s in range(1, 6):
+        g.step(1, s)
+    q, v, _ = g.download()
+    st = g.status()
+    assert st.escaped > 20 and st.nonfinite == 0
+    assert np.all(np.isfinite(v)) and np.all(q >= 0.0) and np.all(q <= 6.0)
+    g.close()

@@ -96,3 +96,28 @@ def test_bounce_limit_rethermalisation_draws_the_species_distribution():
             o.step(s)
         out.append(o.particles()[1])
     assert not np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("op,dim", [(abi.COLL_ARBAXIS, 3), (abi.COLL_RAT, 3),
+                                    (abi.COLL_MPCAT, 2), ("lc", 2)])
+def test_escape_replacement_tracks_reference(op, dim):
+    """Particles that leave the grid through an open side: the oracle's
+    re-placement (bin, mpc.c:969-982; replacePos_WithCheck, init.c:1462-1483,
+    with the ceiling rejecting positions above it) and fresh velocities and
+    orientations follow the reference's, draw for draw."""
+    from cases import open_bottom
+    cfg, Q, V, U, sp = open_bottom(op, dim=dim)
+    o = Oracle(cfg, Q, V, U, sp)
+    r = Reference(cfg, Q, V, U, sp)
+    for s in range(1, 5):
+        o.step(s)
+        r.step(s)
+    qo, vo, uo = o.particles()
+    qr, vr, ur = r.particles()
+    assert r.unexpected_draws() == 0
+    assert o.escaped() > 20
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11)
+    if U is not None:
+        np.testing.assert_allclose(uo, ur, rtol=0, atol=1e-11)
+    assert np.all(qo[:, 1] > -1.0)  # nothing left outside the grid
