@@ -53,6 +53,7 @@ extern "C" {
  * that this library implements */
 #define MPCD_COLL_ARBAXIS 0        /* SRD, random axis                     */
 #define MPCD_COLL_MPCAT 2          /* Andersen MPC-AT                      */
+#define MPCD_COLL_LANG 4           /* Langevin MPC (langevinMPC)           */
 #define MPCD_COLL_RAT 3            /* Andersen MPC-AT+a                    */
 #define MPCD_COLL_DIPOLE_DIR_SUM 16 /* nematic, dipole activity summed    */
 #define MPCD_COLL_DIPOLE_DIR_AV 17  /* nematic, dipole activity averaged  */
@@ -126,6 +127,7 @@ typedef struct mpcd_config {
     int n_walls;
     mpcd_wall walls[MPCD_MAX_WALLS];
     int capacity;     /* maximum number of particles                       */
+    double fricco;    /* in.FRICCO: friction of the Langevin operator      */
 } mpcd_config;
 
 /* Per-handle error counters (the reference prints warnings instead). */

@@ -170,8 +170,10 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     if (cfg->lc != MPCD_LC_ISOTROPIC && !(cfg->lc == MPCD_LC_LOCAL && cfg->dim == 2))
         return MPCD_ERR_UNSUPPORTED;
     if (cfg->lc == MPCD_LC_ISOTROPIC && cfg->coll_op != MPCD_COLL_ARBAXIS &&
-        cfg->coll_op != MPCD_COLL_MPCAT && cfg->coll_op != MPCD_COLL_RAT)
+        cfg->coll_op != MPCD_COLL_MPCAT && cfg->coll_op != MPCD_COLL_RAT &&
+        cfg->coll_op != MPCD_COLL_LANG)
         return MPCD_ERR_UNSUPPORTED;
+    if (cfg->coll_op == MPCD_COLL_LANG && !(cfg->fricco >= 0.0)) return MPCD_ERR_ARG;
     dc->dim = cfg->dim;
     dc->op = cfg->coll_op;
     dc->lc = cfg->lc;
@@ -192,6 +194,12 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         if (!(cfg->species[s].mass > 0.0)) return MPCD_ERR_ARG;
         dc->mass[s] = cfg->species[s].mass;
         dc->sig[s] = std::sqrt(cfg->kbt / cfg->species[s].mass);
+        {
+            // as langevinMPC evaluates them (mpc.c:1744-1745)
+            const double M = cfg->species[s].mass, F = cfg->fricco, step = cfg->dt;
+            dc->lang_a[s] = (M - F * step * 0.5) / (M + 0.5 * F * step);
+            dc->lang_b[s] = std::sqrt(F * step) / (M + 0.5 * F * step);
+        }
         dc->damp[s] = cfg->species[s].damp;
         dc->rfc[s] = cfg->species[s].rfc;
         dc->tumble[s] = cfg->species[s].tumble;

@@ -138,6 +138,9 @@ struct DevCfg {
     double grav[3];
     double mass[MPCD_MAX_SPECIES], damp[MPCD_MAX_SPECIES];
     double sig[MPCD_MAX_SPECIES];  // sqrt(kbt / mass): the thermal draw's width
+    // Langevin MPC (langevinMPC, mpc.c:1674-1780): per species
+    // a = (m - F dt / 2) / (m + F dt / 2), b = sqrt(F dt) / (m + F dt / 2)
+    double lang_a[MPCD_MAX_SPECIES], lang_b[MPCD_MAX_SPECIES];
     int vdist[MPCD_MAX_SPECIES];   // VDIST: re-thermalisation velocities (push)
     double rfc[MPCD_MAX_SPECIES], tumble[MPCD_MAX_SPECIES], chihi[MPCD_MAX_SPECIES];
     double act[MPCD_MAX_SPECIES], mfpot[MPCD_MAX_SPECIES], sigwidth[MPCD_MAX_SPECIES];

@@ -62,13 +62,17 @@ struct PerQ {
     static constexpr int Lr = Q2 + NQ2;
     static constexpr int NL = DIM == 3 ? 3 : 1;
     static __host__ __device__ constexpr int nq(int op) {
-        return op == MPCD_COLL_ARBAXIS ? 1 + DIM : (op == MPCD_COLL_MPCAT ? 1 + 2 * DIM : Lr + NL);
+        return op == MPCD_COLL_ARBAXIS
+                   ? 1 + DIM
+                   : (op == MPCD_COLL_MPCAT || op == MPCD_COLL_LANG ? 1 + 2 * DIM : Lr + NL);
     }
     // record: u[D], then SRD 3D: R[9]; Andersen: RS[D]; MPC-AT+a: CM[D], W[NL]
     static constexpr int U = 0, ROT = DIM, RS = DIM, CM = 2 * DIM, W = 3 * DIM;
     static __host__ __device__ constexpr int nr(int op) {
         return op == MPCD_COLL_ARBAXIS ? (DIM == 3 ? DIM + 9 : DIM)
-                                       : (op == MPCD_COLL_MPCAT ? 2 * DIM : 3 * DIM + NL);
+                                       : (op == MPCD_COLL_MPCAT || op == MPCD_COLL_LANG
+                                              ? 2 * DIM
+                                              : 3 * DIM + NL);
     }
     // the most rows any operator uses (compile-time bounds of the unrolled
     // loads, so that the rows stay in registers and load together)
@@ -217,7 +221,8 @@ __device__ __forceinline__ void per_enter(const DevCfg &c, const PerLayout &l, c
     add(Q::M, m);
     for (int d = 0; d < DIM; d++) add(Q::P + d, vv[d] * m);
     if (c.op == MPCD_COLL_ARBAXIS) return;
-    for (int d = 0; d < DIM; d++) add(Q::R + d, rv[d] * m);
+    // Langevin: the plain sum of the noise (langevinMPC, mpc.c:1707-1710)
+    for (int d = 0; d < DIM; d++) add(Q::R + d, c.op == MPCD_COLL_LANG ? rv[d] : rv[d] * m);
     if (c.op != MPCD_COLL_RAT) return;
     for (int d = 0; d < DIM; d++) add(Q::Q1 + d, rel[d] * m);
     double dv[3] = {0, 0, 0};
@@ -289,7 +294,8 @@ __device__ __forceinline__ void per_cell(const DevCfg &c, const PerLayout &l, co
     }
     double rs[3] = {0, 0, 0};
     if (n > 1)
-        for (int d = 0; d < DIM; d++) rs[d] = x[Q::R + d] / M;
+        for (int d = 0; d < DIM; d++)
+            rs[d] = x[Q::R + d] / (c.op == MPCD_COLL_LANG ? (double)n : M);
     for (int d = 0; d < DIM; d++) put(Q::RS + d, rs[d]);
     if (c.op != MPCD_COLL_RAT) return;
     double cm[3] = {0, 0, 0}, W[3] = {0, 0, 0};
@@ -377,7 +383,13 @@ __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &
             const double damp = c.damp[sp];
             double rv[3] = {0, 0, 0};
             for (int d = 0; d < DIM; d++) rv[d] = rvv[d * l.chunk + j];
-            if (c.op == MPCD_COLL_MPCAT) {
+            if (c.op == MPCD_COLL_LANG) {
+                // langevinMPC, mpc.c:1739-1750
+                const double a = c.lang_a[sp], b = c.lang_b[sp];
+                for (int d = 0; d < DIM; d++)
+                    vv[d] = u[d] + a * (vv[d] - u[d]) + b * (rv[d] - rc[Q::RS + d]) -
+                            damp * u[d] / (double)n;
+            } else if (c.op == MPCD_COLL_MPCAT) {
                 // andersenMPC, mpc.c:1353-1444 (damping over POP)
                 for (int d = 0; d < DIM; d++)
                     vv[d] = u[d] + rv[d] - rc[Q::RS + d] - damp * u[d] / (double)n;

@@ -363,6 +363,9 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
 
     const bool andersen = c.op != MPCD_COLL_ARBAXIS;
     const bool rat = c.op == MPCD_COLL_RAT;
+    // Langevin: the cell's plain mean of the noise instead of the
+    // mass-weighted one (langevinMPC, mpc.c:1689-1736)
+    const bool lang = c.op == MPCD_COLL_LANG;
     double ke = 0.0, av[3] = {0, 0, 0};
     int bounce = 0, esc = 0, overflow = 0;
 
@@ -501,12 +504,13 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             // have fewer than two particles and ignore the result)
             double rs[3] = {0, 0, 0};
             for (int j = j0 + sub; j < j1; j += kCellLanes) {
-                double m = c.mass[s_sp ? s_sp[j] : 0];
+                double m = lang ? 1.0 : c.mass[s_sp ? s_sp[j] : 0];
                 for (int d = 0; d < DIM; d++) rs[d] += m * (double)s_rv[3 * j + d];
             }
             for (int d = 0; d < DIM; d++) rs[d] = group_sum(rs[d]);
             if (lead && pop > 1)
-                for (int d = 0; d < 3; d++) s_rs[3 * lc + d] = d < DIM ? rs[d] / M : 0.0;
+                for (int d = 0; d < 3; d++)
+                    s_rs[3 * lc + d] = d < DIM ? rs[d] / (lang ? (double)pop : M) : 0.0;
             if (!rat) continue;
             double I6[6] = {0, 0, 0, 0, 0, 0}, Lm[3] = {0, 0, 0};
             for (int j = j0 + sub; j < j1; j += kCellLanes) {
@@ -590,7 +594,16 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                     const double *u = &s_u[3 * lc], *rs = &s_rs[3 * lc];
                     double damp = c.damp[sp];
                     double nv[3];
-                    if (!rat) {
+                    if (lang) {
+                        // V' = VCM + a (V - VCM) + b (WN - WNS) - DAMP VCM / POP
+                        double v[3];
+                        T::vel(r, v);
+                        const double a = c.lang_a[sp], b = c.lang_b[sp];
+                        for (int d = 0; d < DIM; d++)
+                            nv[d] = u[d] + a * (v[d] - u[d]) +
+                                    b * ((double)s_rv[3 * j + d] - rs[d]) -
+                                    damp * u[d] / (double)pop;
+                    } else if (!rat) {
                         for (int d = 0; d < DIM; d++)
                             nv[d] = u[d] + (double)s_rv[3 * j + d] - rs[d] -
                                     damp * u[d] / (double)pop;

@@ -20,6 +20,7 @@ ERR_SIZE = -6
 
 COLL_ARBAXIS = 0
 COLL_MPCAT = 2
+COLL_LANG = 4
 COLL_RAT = 3
 COLL_DIPOLE_DIR_SUM = 16
 COLL_DIPOLE_DIR_AV = 17
@@ -109,6 +110,7 @@ class Config(C.Structure):
         ("n_walls", C.c_int),
         ("walls", Wall * MAX_WALLS),
         ("capacity", C.c_int),
+        ("fricco", C.c_double),
     ]
 
 

@@ -529,6 +529,35 @@ static void collide_mpcat(oracle_t *o, int c, uint32_t step) {
     }
 }
 
+/* Langevin MPC (langevinMPC, mpc.c:1674-1780): the noise WN of every
+ * particle (its thermal draw), its plain mean WNS over the cell, and
+ * V' = VCM + a (V - VCM) + b (WN - WNS) - DAMP VCM / POP with
+ * a = (m - F dt / 2) / (m + F dt / 2), b = sqrt(F dt) / (m + F dt / 2). */
+static void collide_lang(oracle_t *o, int c, uint32_t step) {
+    int dim = o->dim, s = o->start[c], e = o->start[c + 1];
+    double WNS[3] = {0, 0, 0};
+    const double *u = &o->vcm[3 * c];
+    const double F = o->cfg.fricco, dt = o->cfg.dt;
+    for (int j = s; j < e; j++) {
+        double rv[3];
+        thermal_draw(o, o->list[j], step, rv);
+        for (int d = 0; d < dim; d++) WNS[d] += rv[d];
+    }
+    for (int d = 0; d < dim; d++) WNS[d] /= (double)(e - s);
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double rv[3];
+        thermal_draw(o, i, step, rv);
+        const mpcd_species *sp = &o->cfg.species[o->spid[i]];
+        const double M = sp->mass;
+        const double a = (M - F * dt * 0.5) / (M + 0.5 * F * dt);
+        const double b = sqrt(F * dt) / (M + 0.5 * F * dt);
+        for (int d = 0; d < dim; d++)
+            o->V[3 * i + d] = u[d] + a * (o->V[3 * i + d] - u[d]) + b * (rv[d] - WNS[d]) -
+                              sp->damp * u[d] / (double)(e - s);
+    }
+}
+
 /* Andersen MPC-AT+a (andersenROT, mpc.c:1461-1657): as MPC-AT with the
  * damping not divided by POP, plus the angular-momentum restoring term
  * W x (r - CM), W = I^-1 sum (r-CM) x m(v - RV).  3D: I inverted by
@@ -1017,6 +1046,8 @@ int oracle_step(oracle_t *o, uint32_t step) {
             collide_srd(o, c, step);
         else if (op == MPCD_COLL_MPCAT)
             collide_mpcat(o, c, step);
+        else if (op == MPCD_COLL_LANG)
+            collide_lang(o, c, step);
         else if (op == MPCD_COLL_RAT)
             collide_rat(o, c, step);
         else

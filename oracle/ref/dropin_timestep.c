@@ -71,6 +71,7 @@ static int fill_config(mpcd_config *c, inputList in, spec SP[], bc WALL[]) {
     c->dt = in.dt;
     c->kbt = in.KBT;
     c->coll_op = in.RTECH;
+    c->fricco = in.FRICCO;
     c->lc = in.LC;
     c->rot_ang = in.RA;
     c->galinv = in.GALINV;

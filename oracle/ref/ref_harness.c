@@ -229,6 +229,7 @@ int ref_init(const mpcd_config *cfg, int n, const double *Q, const double *V,
     g_in.C = cos(cfg->rot_ang); /* initvar, init.c:1194-1195 */
     g_in.S = sin(cfg->rot_ang);
     g_in.RTECH = cfg->coll_op;
+    g_in.FRICCO = cfg->fricco;
     g_in.LC = cfg->lc;
     g_in.GALINV = cfg->galinv;
     g_in.TSTECH = NOTHERM;
@@ -391,6 +392,7 @@ int ref_checkpoint_read(const char *path, mpcd_config *cfg, int *n, int *runtime
     cfg->dt = in.dt;
     cfg->kbt = in.KBT;
     cfg->coll_op = in.RTECH;
+    cfg->fricco = in.FRICCO;
     cfg->lc = in.LC;
     cfg->rot_ang = in.RA;
     cfg->galinv = in.GALINV;

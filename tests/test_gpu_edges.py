@@ -212,3 +212,45 @@ def test_mixed_form_replaces_escaped_particles(kernel):
     assert st.escaped > 20 and st.nonfinite == 0
     assert np.all(np.isfinite(v)) and np.all(q >= 0.0) and np.all(q <= 6.0)
     g.close()
+
+
+@pytest.mark.parametrize("prec,kernel,dim", [
+    (abi.PREC_FP64, abi.KERNEL_TILE, 3), (abi.PREC_FP64, abi.KERNEL_PERSIST, 3),
+    (abi.PREC_FP64, abi.KERNEL_AUTO, 2), (abi.PREC_FP64, abi.KERNEL_TILE, 2),
+    (abi.PREC_MIXED, abi.KERNEL_TILE, 3), (abi.PREC_MIXED, abi.KERNEL_TILE, 2)])
+def test_langevin_operator_matches_the_oracle(prec, kernel, dim):
+    """The Langevin MPC operator (langevinMPC, mpc.c:1674-1780) on the tile
+    and persistent kernel families against the oracle (pinned to the
+    reference): two species, damping, a no-slip wall pair."""
+    L = (6, 5, 7) if dim == 3 else (12, 10)
+    sp = [W._species(mass=1.0, damp=0.1), W._species(mass=2.5, damp=0.1)]
+    w = None
+    if dim == 3:
+        w = [abi.make_wall((1, 0, 0), (0, 0, 0), 0.0, DN=6.0),
+             abi.make_wall((-1, 0, 0), (6, 0, 0), 0.0, DN=6.0),
+             abi.make_wall((0, 1, 0), (0, 0, 0), 0.0, MVN=-1.0, MVT=-1.0),
+             abi.make_wall((0, -1, 0), (0, 5, 0), 0.0, MVN=-1.0, MVT=-1.0),
+             abi.make_wall((0, 0, 1), (0, 0, 0), 0.0, DN=7.0),
+             abi.make_wall((0, 0, -1), (0, 0, 7), 0.0, DN=7.0)]
+    cfg = W.base_config(dim, L, coll_op=abi.COLL_LANG, fricco=0.7, species=sp, walls=w,
+                        seed=88)
+    cfgp = W.base_config(dim, L, coll_op=abi.COLL_LANG, fricco=0.7, species=sp, walls=w,
+                         seed=88, precision=prec)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=89)
+    if dim == 3:
+        Q[:, 1] = 0.02 + Q[:, 1] * (L[1] - 0.04) / L[1]  # off the walls' planes
+    spid = (np.arange(len(Q)) % 3 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, spid)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(cfg.L[:3], dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    g.close()
+    o.close()

@@ -121,3 +121,28 @@ def test_escape_replacement_tracks_reference(op, dim):
     if U is not None:
         np.testing.assert_allclose(uo, ur, rtol=0, atol=1e-11)
     assert np.all(qo[:, 1] > -1.0)  # nothing left outside the grid
+
+
+@pytest.mark.parametrize("dim,L,fricco,damp", [(3, (7, 6, 8), 1.0, 0.0), (2, (20, 16), 0.5, 0.2),
+                                                (3, (6, 6, 6), 2.0, 0.1)])
+def test_langevin_operator_tracks_reference(dim, L, fricco, damp):
+    """The Langevin MPC operator (langevinMPC, mpc.c:1674-1780: the plain mean
+    of the noise, friction factors a and b per species) of the oracle against
+    the reference's own, with two species."""
+    sp = [W._species(mass=1.0, damp=damp), W._species(mass=2.5, damp=damp)]
+    cfg = W.base_config(dim, L, coll_op=abi.COLL_LANG, fricco=fricco, species=sp, seed=515)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=516)
+    spid = (np.arange(len(Q)) % 3 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    r = Reference(cfg, Q, V, U, spid)
+    for s in range(1, 6):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
+    ko, _ = o.globals()
+    kr, _ = r.globals()
+    assert ko == pytest.approx(kr, rel=1e-12)
