@@ -523,6 +523,61 @@ __device__ __forceinline__ void srd_matrix(const DevCfg &c, const double *L,
     }
 }
 
+// Orthogonal-axis SRD rotation matrix about Cartesian axis ca (rotate,
+// mpc.c:1206-1236, with the angle's sign fixed as for srd_matrix). The
+// x-axis matrix carries the reference's -.1*S in row 2, column 1, so that
+// rotation about x does not preserve the norm; it is reproduced as written.
+// In 2D the axis is unused and the plane rotation of srd_matrix applies.
+template <int DIM, typename T>
+__device__ __forceinline__ void orth_matrix(const DevCfg &c, int ca, T R[9]) {
+    if (DIM != 3) {
+        const double L[3] = {0, 0, 1};
+        srd_matrix<DIM, T>(c, L, R);
+        return;
+    }
+    const T C = (T)c.cosA, S = (T)c.sinA, one = (T)1, zero = (T)0;
+    for (int r = 0; r < 9; r++) R[r] = zero;
+    if (ca == 0) {
+        R[0] = one;
+        R[4] = C;
+        R[5] = S;
+        R[7] = (T)(-.1 * c.sinA);
+        R[8] = C;
+    } else if (ca == 1) {
+        R[0] = C;
+        R[2] = S;
+        R[4] = one;
+        R[6] = (T)(-1. * c.sinA);
+        R[8] = C;
+    } else {
+        R[0] = C;
+        R[1] = S;
+        R[3] = (T)(-1. * c.sinA);
+        R[4] = C;
+        R[8] = one;
+    }
+}
+
+// A cell's SRD rotation matrix for either rotation operator: a random unit
+// axis (MPCD_COLL_ARBAXIS) or a random Cartesian axis (MPCD_COLL_ORTHAXIS).
+template <int DIM, typename T>
+__device__ __forceinline__ void srd_cell_matrix(const DevCfg &c, uint32_t step,
+                                                uint32_t cell, T R[9]) {
+    if (c.op == MPCD_COLL_ORTHAXIS) {
+        const int ca = DIM == 3 ? mpcd_rng_orth_axis(c.seed, c.replica, step, cell, DIM) : 0;
+        orth_matrix<DIM, T>(c, ca, R);
+        return;
+    }
+    double Lx[3] = {0, 0, 1};
+    if (DIM == 3) mpcd_rng_axis3(c.seed, c.replica, step, cell, Lx);
+    srd_matrix<DIM, T>(c, Lx, R);
+}
+
+// True for the two SRD rotation operators.
+__host__ __device__ __forceinline__ bool is_srd_op(int op) {
+    return op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS;
+}
+
 // Inverse of a symmetric-or-not 3x3 matrix by adjugate / determinant.
 __device__ __forceinline__ void inv3(const double m[9], double r[9]) {
     double c00 = m[4] * m[8] - m[5] * m[7];

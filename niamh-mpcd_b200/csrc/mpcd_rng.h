@@ -274,4 +274,14 @@ MPCD_HD double mpcd_rng_uniform(uint64_t seed, uint32_t replica, uint32_t step,
     return mpcd_u01(mpcd_lane(r, (int)(k & 3u)));
 }
 
+/* The Cartesian axis of a cell's orthogonal-axis SRD rotation: the
+ * reference's CA = (int)DIM * genrand_real() (stochrotMPC, mpc.c:1289) with
+ * the cell's first uniform of its own stream, in 0..dim-1. */
+MPCD_HD int mpcd_rng_orth_axis(uint64_t seed, uint32_t replica, uint32_t step,
+                               uint32_t cell, int dim) {
+    int ca = (int)(MPCD_DMUL((double)dim, mpcd_rng_uniform(seed, replica, step,
+                                                          MPCD_STREAM_ORTH, cell, 0u)));
+    return ca < dim ? ca : dim - 1;
+}
+
 #endif /* MPCD_RNG_H */

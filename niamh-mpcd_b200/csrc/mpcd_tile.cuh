@@ -306,11 +306,11 @@ static inline TileLayout tile_layout(int ct, int cap, int op, int nspecies) {
         return r;
     };
     L.off_rec = take(cap * (int)sizeof(typename T::Rec), 16);
-    bool and_ = op != MPCD_COLL_ARBAXIS;
+    bool and_ = !is_srd_op(op);
     L.off_rv = and_ ? take(cap * 3 * (int)sizeof(typename T::VT), 16) : -1;
     L.off_start = take((ct + 1) * 4, 16);
     L.off_u = take(ct * 3 * 8, 16);
-    L.off_R = op == MPCD_COLL_ARBAXIS ? take(ct * 9 * (int)sizeof(typename T::VT), 16) : -1;
+    L.off_R = is_srd_op(op) ? take(ct * 9 * (int)sizeof(typename T::VT), 16) : -1;
     L.off_cm = op == MPCD_COLL_RAT ? take(ct * 3 * 8, 16) : -1;
     L.off_rs = and_ ? take(ct * 3 * 8, 16) : -1;
     L.off_W = op == MPCD_COLL_RAT ? take(ct * 3 * 8, 16) : -1;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
     for (int k = tid; k <= nct; k += nth) s_start[k] = tb.start[c0 + k];
     __syncthreads();
 
-    const bool andersen = c.op != MPCD_COLL_ARBAXIS;
+    const bool andersen = !is_srd_op(c.op);
     const bool rat = c.op == MPCD_COLL_RAT;
     // Langevin: the cell's plain mean of the noise instead of the
     // mass-weighted one (langevinMPC, mpc.c:1689-1736)
@@ -492,11 +492,8 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                 for (int d = 0; d < 3; d++) s_u[3 * lc + d] = u[d];
             }
             if (!andersen) {
-                if (lead && pop > 1) {
-                    double Lx[3] = {0, 0, 1};
-                    if (DIM == 3) mpcd_rng_axis3(c.seed, c.replica, sa.step, (uint32_t)cell, Lx);
-                    srd_matrix<DIM, VT>(c, Lx, &s_R[9 * lc]);
-                }
+                if (lead && pop > 1)
+                    srd_cell_matrix<DIM, VT>(c, sa.step, (uint32_t)cell, &s_R[9 * lc]);
                 continue;
             }
             // Andersen: the cell's sum of thermal velocities (every group of

@@ -19,6 +19,7 @@ ERR_STATE = -5
 ERR_SIZE = -6
 
 COLL_ARBAXIS = 0
+COLL_ORTHAXIS = 1
 COLL_MPCAT = 2
 COLL_LANG = 4
 COLL_RAT = 3

@@ -461,12 +461,36 @@ static void ghost_part(oracle_t *o, uint32_t step) {
 /* ------------------------------------------------------------ collisions */
 /* SRD (stochrotMPC, mpc.c:1275-1333 with rotate, mpc.c:1181-1257): the
  * rotation sign draw (long)genrand_real() is always 0, so the angle is
- * always -RA; in 2D the random axis is unused. */
+ * always -RA; in 2D the random axis is unused.  The orthogonal-axis form
+ * (RTECH ORTHAXIS) rotates about Cartesian axis CA = (int)DIM*u
+ * (mpc.c:1289); rotate's x-axis matrix has -.1*S in row 2, column 1
+ * (mpc.c:1215), kept as the reference has it. */
 static void collide_srd(oracle_t *o, int c, uint32_t step) {
     int dim = o->dim;
     double Cs = cos(o->cfg.rot_ang), Sn = -1.0 * sin(o->cfg.rot_ang);
-    double R[9];
-    if (dim == 3) {
+    double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (dim == 3 && o->cfg.coll_op == MPCD_COLL_ORTHAXIS) {
+        int ca = mpcd_rng_orth_axis(o->cfg.seed, o->cfg.replica, step, (uint32_t)c, dim);
+        if (ca == 0) {
+            R[0] = 1.;
+            R[4] = Cs;
+            R[5] = Sn;
+            R[7] = -.1 * Sn;
+            R[8] = Cs;
+        } else if (ca == 1) {
+            R[0] = Cs;
+            R[2] = Sn;
+            R[4] = 1.;
+            R[6] = -1. * Sn;
+            R[8] = Cs;
+        } else {
+            R[0] = Cs;
+            R[1] = Sn;
+            R[3] = -1. * Sn;
+            R[4] = Cs;
+            R[8] = 1.;
+        }
+    } else if (dim == 3) {
         double L[3];
         mpcd_rng_axis3(o->cfg.seed, o->cfg.replica, step, (uint32_t)c, L);
         R[0] = L[0] * L[0] + (1. - L[0] * L[0]) * Cs;
@@ -1042,7 +1066,7 @@ int oracle_step(oracle_t *o, uint32_t step) {
         if (o->pop[c] <= 1) continue;
         if (o->cfg.lc != 0)
             collide_lc(o, c, step);
-        else if (op == MPCD_COLL_ARBAXIS)
+        else if (op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS)
             collide_srd(o, c, step);
         else if (op == MPCD_COLL_MPCAT)
             collide_mpcat(o, c, step);

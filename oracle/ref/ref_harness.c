@@ -79,6 +79,8 @@ static uint32_t g_replica = 0, g_step = 0;
 enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT, PH_RETHERM, PH_ESCAPE };
 static int g_phase = PH_NONE;
 static int g_cell = 0;
+static int g_rtech = 0;  /* RTECH of the collision in progress */
+static int g_ccount = 0; /* its uniform draws so far */
 static particleMPC *g_cursor = NULL;
 static int g_comp = 0;
 static uint32_t g_stream = 0; /* PH_INIT: the stream of the current draws */
@@ -667,9 +669,15 @@ double genrand_real(void) {
                                 (uint32_t)g_pid, g_k++);
     if (g_phase == PH_ESCAPE)
         return mpcd_rng_uniform(g_seed, g_replica, g_step, g_stream, (uint32_t)g_pid, g_k++);
-    /* stochrotMPC draws a uniform only for the rotation sign, which
+    /* stochrotMPC draws a uniform for the orthogonal axis (ORTHAXIS only,
+     * mpc.c:1289) and then one for the rotation sign, which
      * (long)genrand_real() truncates to 0 (mpc.c:1291) */
-    if (g_phase == PH_COLLIDE) return 0.0;
+    if (g_phase == PH_COLLIDE) {
+        if (g_rtech == ORTHAXIS && g_ccount++ == 0)
+            return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_ORTH,
+                                    (uint32_t)g_cell, 0u);
+        return 0.0;
+    }
     g_unexpected++;
     return 0.5;
 }
@@ -768,6 +776,8 @@ void MPCcollision(cell *CL, spec *SP, specSwimmer SS, double KBT, int RTECH,
     g_cell = cell_id(CL);
     g_cursor = CL->pp;
     g_comp = 0;
+    g_rtech = RTECH;
+    g_ccount = 0;
     orig(CL, SP, SS, KBT, RTECH, C, S, FRICCO, TimeStep, MD_mode, LC, RELAX, CLQ,
          outP);
     g_phase = PH_NONE;

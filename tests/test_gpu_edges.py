@@ -11,6 +11,8 @@ precision forms) through the C ABI, against the CPU oracle:
 - an empty state: the upload is accepted and a step is refused with an
   error status, without a launch.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -240,6 +242,35 @@ def test_langevin_operator_matches_the_oracle(prec, kernel, dim):
     if dim == 3:
         Q[:, 1] = 0.02 + Q[:, 1] * (L[1] - 0.04) / L[1]  # off the walls' planes
     spid = (np.arange(len(Q)) % 3 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, spid)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(cfg.L[:3], dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    g.close()
+    o.close()
+
+
+@pytest.mark.parametrize("prec,kernel,dim", [
+    (abi.PREC_FP64, abi.KERNEL_TILE, 3), (abi.PREC_FP64, abi.KERNEL_PERSIST, 3),
+    (abi.PREC_FP64, abi.KERNEL_AUTO, 2), (abi.PREC_MIXED, abi.KERNEL_TILE, 3),
+    (abi.PREC_MIXED, abi.KERNEL_AUTO, 3)])
+def test_orthogonal_axis_srd_matches_the_oracle(prec, kernel, dim):
+    """SRD about a random Cartesian axis (stochrotMPC with RTECH ORTHAXIS,
+    mpc.c:1289; rotate, mpc.c:1206-1236) on the tile and persistent kernel
+    families against the oracle (pinned to the reference)."""
+    L = (6, 5, 7) if dim == 3 else (12, 10)
+    cfg = W.base_config(dim, L, coll_op=abi.COLL_ORTHAXIS, rot_ang=math.radians(130), seed=91)
+    cfgp = W.base_config(dim, L, coll_op=abi.COLL_ORTHAXIS, rot_ang=math.radians(130),
+                         seed=91, precision=prec)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=92)
     o = Oracle(cfg, Q, V, U, spid)
     g = Solver(cfgp)
     g.set_kernel(kernel)

@@ -1,6 +1,8 @@
 """Live comparison of the CPU oracle with the reference's own timestep
 (oracle/_ref/libmpcdref.so, built from the reference sources) on cases larger
 than the golden ones; skipped where the reference build is absent."""
+import math
+
 import numpy as np
 import pytest
 
@@ -146,3 +148,28 @@ def test_langevin_operator_tracks_reference(dim, L, fricco, damp):
     ko, _ = o.globals()
     kr, _ = r.globals()
     assert ko == pytest.approx(kr, rel=1e-12)
+
+
+@pytest.mark.parametrize("dim,L,ra", [(3, (7, 6, 8), 130.0), (3, (6, 6, 6), 90.0),
+                                      (2, (20, 16), 120.0)])
+def test_orthogonal_axis_srd_tracks_reference(dim, L, ra):
+    """SRD about a random Cartesian axis (RTECH ORTHAXIS: stochrotMPC,
+    mpc.c:1289, with rotate's matrices, mpc.c:1206-1236, including the x-axis
+    matrix's -.1*S) of the oracle against the reference's own."""
+    cfg = W.base_config(dim, L, coll_op=abi.COLL_ORTHAXIS, rot_ang=math.radians(ra), seed=525)
+    Q, V, U, spid = W.synthetic_state(cfg, 10, seed=526)
+    o = Oracle(cfg, Q, V, U, spid)
+    r = Reference(cfg, Q, V, U, spid)
+    for s in range(1, 6):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
+    if dim == 3:
+        # the x-axis matrix shrinks |v - u| along z: kinetic energy is not conserved
+        ko, _ = o.globals()
+        kr, _ = r.globals()
+        assert ko == pytest.approx(kr, rel=1e-12)
