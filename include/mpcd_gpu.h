@@ -56,6 +56,8 @@ extern "C" {
 #define MPCD_COLL_MPCAT 2          /* Andersen MPC-AT                      */
 #define MPCD_COLL_LANG 4           /* Langevin MPC (langevinMPC)           */
 #define MPCD_COLL_RAT 3            /* Andersen MPC-AT+a                    */
+#define MPCD_COLL_ACT_ARBAXIS 9    /* active SRD, random axis (activeSRD)  */
+#define MPCD_COLL_ACT_ORTHAXIS 10  /* active SRD, random Cartesian axis    */
 #define MPCD_COLL_DIPOLE_DIR_SUM 16 /* nematic, dipole activity summed    */
 #define MPCD_COLL_DIPOLE_DIR_AV 17  /* nematic, dipole activity averaged  */
 

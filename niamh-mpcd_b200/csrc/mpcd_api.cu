@@ -210,6 +210,15 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         dc->sigpos[s] = cfg->species[s].sigpos;
         dc->minactratio[s] = cfg->species[s].minactratio;
     }
+    // activeSRD takes the cell's activity from the last particle of the
+    // cell's linked list (sumACT = ACT, mpc.c:2058-2062), an order that the
+    // reference's re-binning history sets: only species of one activity give
+    // a result that does not depend on it.
+    dc->act_srd = cfg->lc == MPCD_LC_ISOTROPIC && (cfg->coll_op == MPCD_COLL_ACT_ARBAXIS ||
+                                                   cfg->coll_op == MPCD_COLL_ACT_ORTHAXIS);
+    if (dc->act_srd)
+        for (int s = 1; s < cfg->n_species; s++)
+            if (cfg->species[s].act != cfg->species[0].act) return MPCD_ERR_UNSUPPORTED;
     dc->dt = cfg->dt;
     dc->kbt = cfg->kbt;
     dc->cosA = std::cos(cfg->rot_ang);

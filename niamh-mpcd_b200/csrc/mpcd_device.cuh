@@ -147,7 +147,7 @@ struct DevCfg {
     double sigpos[MPCD_MAX_SPECIES], minactratio[MPCD_MAX_SPECIES];
     uint64_t seed;
     uint32_t replica;
-    int pad_;
+    int act_srd;  // active SRD (collOp 9, 10): turn active particles toward VCM
     DevWall walls[MPCD_MAX_WALLS];
 };
 
@@ -563,7 +563,7 @@ __device__ __forceinline__ void orth_matrix(const DevCfg &c, int ca, T R[9]) {
 template <int DIM, typename T>
 __device__ __forceinline__ void srd_cell_matrix(const DevCfg &c, uint32_t step,
                                                 uint32_t cell, T R[9]) {
-    if (c.op == MPCD_COLL_ORTHAXIS) {
+    if (c.op == MPCD_COLL_ORTHAXIS || c.op == MPCD_COLL_ACT_ORTHAXIS) {
         const int ca = DIM == 3 ? mpcd_rng_orth_axis(c.seed, c.replica, step, cell, DIM) : 0;
         orth_matrix<DIM, T>(c, ca, R);
         return;
@@ -573,9 +573,65 @@ __device__ __forceinline__ void srd_cell_matrix(const DevCfg &c, uint32_t step,
     srd_matrix<DIM, T>(c, Lx, R);
 }
 
-// True for the two SRD rotation operators.
+// True for the SRD rotation operators, plain or active.
 __host__ __device__ __forceinline__ bool is_srd_op(int op) {
-    return op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS;
+    return op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS ||
+           op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS;
+}
+
+// Length of a 3-vector, summed in index order as the reference's length()
+// (mtools.c:230-236), without contraction.
+__device__ __forceinline__ double len3_rn(const double *x) {
+    double r = __dmul_rn(x[0], x[0]);
+    r = __dadd_rn(r, __dmul_rn(x[1], x[1]));
+    r = __dadd_rn(r, __dmul_rn(x[2], x[2]));
+    return sqrt(r);
+}
+
+__device__ __forceinline__ double dot3_rn(const double *x, const double *y) {
+    double r = __dmul_rn(x[0], y[0]);
+    r = __dadd_rn(r, __dmul_rn(x[1], y[1]));
+    return __dadd_rn(r, __dmul_rn(x[2], y[2]));
+}
+
+__device__ __forceinline__ void cross3_rn(const double *x, const double *y, double *r) {
+    r[0] = __dsub_rn(__dmul_rn(x[1], y[2]), __dmul_rn(x[2], y[1]));
+    r[1] = __dsub_rn(__dmul_rn(x[2], y[0]), __dmul_rn(x[0], y[2]));
+    r[2] = __dsub_rn(__dmul_rn(x[0], y[1]), __dmul_rn(x[1], y[0]));
+}
+
+// The active part of active SRD (activeSRD, mpc.c:2055-2076), after the
+// rotation: a particle whose species has ACT != 0 (fneq, |ACT| >= 1e-8) is
+// turned toward the cell's centre-of-mass velocity u by ACT times the angle
+// between them (absAngle: acos of the cosine, mtools.c:325-367), about the
+// normal v x u, by Rodrigues' formula with the length restored
+// (rodriguesRotation, mtools.c:1572-1585; the axis is normalised only when
+// its length is at least 1e-8).  Turns below 1e-5 rad (ROTTOL) are skipped,
+// and so is a NaN angle (a zero v or u).  v and u are 3-vectors (zero z in
+// 2D).  Out of line: only the active operators reach it.
+static __device__ __noinline__ void active_srd_turn(double act, const double *u, double *v) {
+    if (!(fabs(act) >= 1e-8)) return;
+    double cosa = dot3_rn(v, u);
+    cosa = __ddiv_rn(cosa, len3_rn(v));
+    cosa = __ddiv_rn(cosa, len3_rn(u));
+    const double theta = acos(cosa);
+    double ax[3];
+    cross3_rn(v, u, ax);
+    if (!(fabs(theta) > 1e-5)) return;
+    const double l = len3_rn(ax);
+    if (fabs(l) >= 1e-8)
+        for (int d = 0; d < 3; d++) ax[d] = __ddiv_rn(ax[d], l);
+    const double old = len3_rn(v);
+    double cp[3];
+    cross3_rn(ax, v, cp);
+    const double dp = dot3_rn(ax, v);
+    const double t = __dmul_rn(act, theta), ct = cos(t), st = sin(t);
+    for (int d = 0; d < 3; d++)
+        v[d] = __dadd_rn(__dadd_rn(__dmul_rn(v[d], ct), __dmul_rn(cp[d], st)),
+                         __dmul_rn(__dmul_rn(ax[d], dp), __dsub_rn(1.0, ct)));
+    const double now = len3_rn(v);
+    const double f = __ddiv_rn(old, now);
+    for (int d = 0; d < 3; d++) v[d] = __dmul_rn(v[d], f);
 }
 
 // Inverse of a symmetric-or-not 3x3 matrix by adjugate / determinant.

@@ -375,6 +375,7 @@ __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &
             for (int a = 0; a < DIM; a++)
                 for (int b = 0; b < DIM; b++) t[a] += R[a * 3 + b] * w[b];
             for (int d = 0; d < DIM; d++) vv[d] = u[d] + t[d];
+            if (c.act_srd) active_srd_turn(c.act[sp], u, vv);
         } else {
             const double damp = c.damp[sp];
             double rv[3] = {0, 0, 0};

@@ -576,15 +576,21 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                             nv[1] = uy + ((float)R[3] * wx + (float)R[4] * wy);
                             nv[2] = 0.f;
                         }
+                        if (c.act_srd) {
+                            double dv[3] = {nv[0], nv[1], nv[2]};
+                            active_srd_turn(c.act[sp], &s_u[3 * lc], dv);
+                            for (int d = 0; d < 3; d++) nv[d] = (float)dv[d];
+                        }
                         MixT<DIM>::set_velf(*(MixRec *)&r, nv);
                     } else {
-                        double v[3], w[3] = {0, 0, 0}, t[3] = {0, 0, 0}, nv[3];
+                        double v[3], w[3] = {0, 0, 0}, t[3] = {0, 0, 0}, nv[3] = {0, 0, 0};
                         T::vel(r, v);
                         const double *u = &s_u[3 * lc];
                         for (int d = 0; d < DIM; d++) w[d] = v[d] - u[d];
                         for (int x = 0; x < DIM; x++)
                             for (int y = 0; y < DIM; y++) t[x] += (double)R[x * 3 + y] * w[y];
                         for (int d = 0; d < DIM; d++) nv[d] = u[d] + t[d];
+                        if (c.act_srd) active_srd_turn(c.act[sp], u, nv);
                         T::set_vel(r, nv);
                     }
                 } else {

@@ -23,6 +23,8 @@ COLL_ORTHAXIS = 1
 COLL_MPCAT = 2
 COLL_LANG = 4
 COLL_RAT = 3
+COLL_ACT_ARBAXIS = 9
+COLL_ACT_ORTHAXIS = 10
 COLL_DIPOLE_DIR_SUM = 16
 COLL_DIPOLE_DIR_AV = 17
 

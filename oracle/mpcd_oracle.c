@@ -459,6 +459,32 @@ static void ghost_part(oracle_t *o, uint32_t step) {
 }
 
 /* ------------------------------------------------------------ collisions */
+/* The active part of active SRD (activeSRD, mpc.c:2055-2076) after the
+ * rotation: turn v toward the cell's VCM u by ACT times their angle (absAngle,
+ * mtools.c:325-367) about v x u by Rodrigues' formula with the length kept
+ * (rodriguesRotation, mtools.c:1572-1585); skipped for |ACT| < 1e-8 (fneq)
+ * and for angles not above ROTTOL = 1e-5.  The cell's activity is the last
+ * listed particle's ACT in the reference; the library admits only species
+ * of one activity, for which that is every particle's own. */
+static void active_turn(double act, const double *u, double *v) {
+    if (!(fabs(act) >= 1e-8)) return;
+    double cosa = dot3(v, u, 3);
+    cosa /= len3(v, 3);
+    cosa /= len3(u, 3);
+    double theta = acos(cosa), ax[3], cp[3];
+    cross3(v, u, ax);
+    if (!(fabs(theta) > 1e-5)) return;
+    double l = len3(ax, 3);
+    if (fabs(l) >= 1e-8)
+        for (int d = 0; d < 3; d++) ax[d] = ax[d] / l;
+    double old = len3(v, 3);
+    cross3(ax, v, cp);
+    double dp = dot3(ax, v, 3), t = act * theta;
+    for (int d = 0; d < 3; d++) v[d] = v[d] * cos(t) + cp[d] * sin(t) + ax[d] * dp * (1.0 - cos(t));
+    double now = len3(v, 3);
+    for (int d = 0; d < 3; d++) v[d] *= (old / now);
+}
+
 /* SRD (stochrotMPC, mpc.c:1275-1333 with rotate, mpc.c:1181-1257): the
  * rotation sign draw (long)genrand_real() is always 0, so the angle is
  * always -RA; in 2D the random axis is unused.  The orthogonal-axis form
@@ -469,7 +495,9 @@ static void collide_srd(oracle_t *o, int c, uint32_t step) {
     int dim = o->dim;
     double Cs = cos(o->cfg.rot_ang), Sn = -1.0 * sin(o->cfg.rot_ang);
     double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (dim == 3 && o->cfg.coll_op == MPCD_COLL_ORTHAXIS) {
+    const int op = o->cfg.coll_op;
+    const int active = op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS;
+    if (dim == 3 && (op == MPCD_COLL_ORTHAXIS || op == MPCD_COLL_ACT_ORTHAXIS)) {
         int ca = mpcd_rng_orth_axis(o->cfg.seed, o->cfg.replica, step, (uint32_t)c, dim);
         if (ca == 0) {
             R[0] = 1.;
@@ -516,6 +544,7 @@ static void collide_srd(oracle_t *o, int c, uint32_t step) {
         for (int a = 0; a < dim; a++)
             for (int b = 0; b < dim; b++) t[a] += R[a * 3 + b] * w[b];
         for (int d = 0; d < dim; d++) o->V[3 * i + d] = u[d] + t[d];
+        if (active) active_turn(o->cfg.species[o->spid[i]].act, u, &o->V[3 * i]);
     }
 }
 
@@ -1066,7 +1095,8 @@ int oracle_step(oracle_t *o, uint32_t step) {
         if (o->pop[c] <= 1) continue;
         if (o->cfg.lc != 0)
             collide_lc(o, c, step);
-        else if (op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS)
+        else if (op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS ||
+                 op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS)
             collide_srd(o, c, step);
         else if (op == MPCD_COLL_MPCAT)
             collide_mpcat(o, c, step);

@@ -673,7 +673,7 @@ double genrand_real(void) {
      * mpc.c:1289) and then one for the rotation sign, which
      * (long)genrand_real() truncates to 0 (mpc.c:1291) */
     if (g_phase == PH_COLLIDE) {
-        if (g_rtech == ORTHAXIS && g_ccount++ == 0)
+        if ((g_rtech == ORTHAXIS || g_rtech == ACT_ORTHAXIS) && g_ccount++ == 0)
             return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_ORTH,
                                     (uint32_t)g_cell, 0u);
         return 0.0;

@@ -285,3 +285,47 @@ def test_orthogonal_axis_srd_matches_the_oracle(prec, kernel, dim):
     assert st.escaped == 0 and st.nonfinite == 0
     g.close()
     o.close()
+
+
+@pytest.mark.parametrize("op,prec,kernel,dim", [
+    (abi.COLL_ACT_ARBAXIS, abi.PREC_FP64, abi.KERNEL_TILE, 3),
+    (abi.COLL_ACT_ORTHAXIS, abi.PREC_FP64, abi.KERNEL_PERSIST, 3),
+    (abi.COLL_ACT_ARBAXIS, abi.PREC_FP64, abi.KERNEL_AUTO, 2),
+    (abi.COLL_ACT_ORTHAXIS, abi.PREC_MIXED, abi.KERNEL_TILE, 3),
+    (abi.COLL_ACT_ARBAXIS, abi.PREC_MIXED, abi.KERNEL_AUTO, 2)])
+def test_active_srd_matches_the_oracle(op, prec, kernel, dim):
+    """Active SRD (activeSRD, mpc.c:2037-2077) on the tile and persistent
+    kernel families against the oracle (pinned to the reference), with a net
+    flow so that the cells' VCM have a direction."""
+    L = (6, 5, 7) if dim == 3 else (12, 10)
+    sp = [W._species(mass=1.0, act=0.3), W._species(mass=2.0, act=0.3)]
+    kw = dict(coll_op=op, rot_ang=math.radians(110), species=sp, seed=93)
+    cfg = W.base_config(dim, L, **kw)
+    cfgp = W.base_config(dim, L, precision=prec, **kw)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=94)
+    V[:, 0] += 0.4
+    spid = (np.arange(len(Q)) % 4 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, spid)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(cfg.L[:3], dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    g.close()
+    o.close()
+
+
+def test_active_srd_refuses_species_of_different_activity():
+    """activeSRD takes the cell's activity from the last particle of its list,
+    whose order the reference's re-binning sets: species of different
+    activity are refused."""
+    sp = [W._species(mass=1.0, act=0.3), W._species(mass=1.0, act=0.0)]
+    cfg = W.base_config(3, (4, 4, 4), coll_op=abi.COLL_ACT_ARBAXIS, species=sp)
+    with pytest.raises(MPCDError):
+        Solver(cfg)

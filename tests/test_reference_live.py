@@ -173,3 +173,27 @@ def test_orthogonal_axis_srd_tracks_reference(dim, L, ra):
         ko, _ = o.globals()
         kr, _ = r.globals()
         assert ko == pytest.approx(kr, rel=1e-12)
+
+
+@pytest.mark.parametrize("op,dim,L,act", [(9, 3, (7, 6, 8), 0.3), (10, 3, (6, 6, 6), 0.5),
+                                          (9, 2, (20, 16), 0.2)])
+def test_active_srd_tracks_reference(op, dim, L, act):
+    """Active SRD (activeSRD, mpc.c:2037-2077: the SRD rotation, then every
+    particle turned toward the cell's VCM by ACT times their angle) of the
+    oracle against the reference's own, random and Cartesian axes, two
+    species of one activity."""
+    sp = [W._species(mass=1.0, act=act), W._species(mass=2.0, act=act)]
+    cfg = W.base_config(dim, L, coll_op=op, rot_ang=math.radians(110), species=sp, seed=535)
+    Q, V, U, spid = W.synthetic_state(cfg, 10, seed=536)
+    V[:, 0] += 0.4  # a net flow, so that the cells' VCM have a direction
+    spid = (np.arange(len(Q)) % 4 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    r = Reference(cfg, Q, V, U, spid)
+    for s in range(1, 6):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
