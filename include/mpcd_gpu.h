@@ -58,6 +58,8 @@ extern "C" {
 #define MPCD_COLL_RAT 3            /* Andersen MPC-AT+a                    */
 #define MPCD_COLL_ACT_ARBAXIS 9    /* active SRD, random axis (activeSRD)  */
 #define MPCD_COLL_ACT_ORTHAXIS 10  /* active SRD, random Cartesian axis    */
+#define MPCD_COLL_VICSEK_MPCAT 11  /* MPC-AT with Vicsek alignment          */
+#define MPCD_COLL_VICSEK_LANG 12   /* Langevin MPC with Vicsek alignment    */
 #define MPCD_COLL_DIPOLE_DIR_SUM 16 /* nematic, dipole activity summed    */
 #define MPCD_COLL_DIPOLE_DIR_AV 17  /* nematic, dipole activity averaged  */
 
@@ -130,7 +132,8 @@ typedef struct mpcd_config {
     int n_walls;
     mpcd_wall walls[MPCD_MAX_WALLS];
     int capacity;     /* maximum number of particles                       */
-    double fricco;    /* in.FRICCO: friction of the Langevin operator      */
+    double fricco;    /* in.FRICCO: friction of the Langevin operators     */
+    double relax;     /* in.TAU: RELAX of the Vicsek-aligned operators     */
 } mpcd_config;
 
 /* Per-handle error counters (the reference prints warnings instead). */

@@ -170,10 +170,10 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     if (cfg->lc != MPCD_LC_ISOTROPIC && !(cfg->lc == MPCD_LC_LOCAL && cfg->dim == 2))
         return MPCD_ERR_UNSUPPORTED;
     if (cfg->lc == MPCD_LC_ISOTROPIC && !is_srd_op(cfg->coll_op) &&
-        cfg->coll_op != MPCD_COLL_MPCAT && cfg->coll_op != MPCD_COLL_RAT &&
-        cfg->coll_op != MPCD_COLL_LANG)
+        !is_mpcat_op(cfg->coll_op) && cfg->coll_op != MPCD_COLL_RAT &&
+        !is_lang_op(cfg->coll_op))
         return MPCD_ERR_UNSUPPORTED;
-    if (cfg->coll_op == MPCD_COLL_LANG && !(cfg->fricco >= 0.0)) return MPCD_ERR_ARG;
+    if (is_lang_op(cfg->coll_op) && !(cfg->fricco >= 0.0)) return MPCD_ERR_ARG;
     dc->dim = cfg->dim;
     dc->op = cfg->coll_op;
     dc->lc = cfg->lc;
@@ -195,12 +195,18 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         dc->mass[s] = cfg->species[s].mass;
         dc->sig[s] = std::sqrt(cfg->kbt / cfg->species[s].mass);
         {
-            // as langevinMPC evaluates them (mpc.c:1744-1745)
+            // as langevinMPC and vicsekLangevinMPC evaluate them (mpc.c:1744-1745)
             const double M = cfg->species[s].mass, F = cfg->fricco, step = cfg->dt;
             dc->lang_a[s] = (M - F * step * 0.5) / (M + 0.5 * F * step);
             dc->lang_b[s] = std::sqrt(F * step) / (M + 0.5 * F * step);
+            if (cfg->coll_op == MPCD_COLL_VICSEK_MPCAT) {
+                // V' = VCM + (RV - RS) + alignment: the Langevin update's form
+                dc->lang_a[s] = 0.0;
+                dc->lang_b[s] = 1.0;
+            }
         }
-        dc->damp[s] = cfg->species[s].damp;
+        // the Vicsek-aligned operators apply no damping (mpc.c:2204-2480)
+        dc->damp[s] = is_vicsek_op(cfg->coll_op) ? 0.0 : cfg->species[s].damp;
         dc->rfc[s] = cfg->species[s].rfc;
         dc->tumble[s] = cfg->species[s].tumble;
         dc->chihi[s] = cfg->species[s].chihi;
@@ -221,6 +227,7 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
             if (cfg->species[s].act != cfg->species[0].act) return MPCD_ERR_UNSUPPORTED;
     dc->dt = cfg->dt;
     dc->kbt = cfg->kbt;
+    dc->relax = cfg->relax;
     dc->cosA = std::cos(cfg->rot_ang);
     dc->sinA = -1.0 * std::sin(cfg->rot_ang);  // rotation sign draw is always 0
     for (int d = 0; d < 3; d++) dc->grav[d] = cfg->grav[d];

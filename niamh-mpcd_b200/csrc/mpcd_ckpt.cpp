@@ -338,7 +338,7 @@ extern "C" int mpcd_ckpt_create(const mpcd_config *cfg, mpcd_ckpt **out) {
     c->set_i(L_FLAGS, 4, cfg->coll_op);
     c->set_i(L_FLAGS, 5, cfg->lc);
     c->set_i(L_STEPS, 0, 2000);  // readJson defaults (read.c:1058-1130)
-    c->set_f(L_ANG, 0, 0.5);     // TAU
+    c->set_f(L_ANG, 0, cfg->relax);  // TAU
     c->set_f(L_ANG, 1, cfg->rot_ang);
     c->set_f(L_ANG, 2, cfg->fricco);  // FRICCO
     for (int d = 0; d < 3; d++) c->set_f(L_GRAV, d, cfg->grav[d]);
@@ -427,6 +427,7 @@ extern "C" int mpcd_ckpt_config(const mpcd_ckpt *ck, mpcd_config *cfg) {
     cfg->lc = (int)ck->i(L_FLAGS, 5);
     cfg->rot_ang = ck->f(L_ANG, 1);
     cfg->fricco = ck->f(L_ANG, 2);
+    cfg->relax = ck->f(L_ANG, 0);
     for (int d = 0; d < 3; d++) cfg->grav[d] = ck->f(L_GRAV, d);
     cfg->gndnst = ck->f(ck->dens, 0);
     cfg->seed = (uint64_t)ck->i(L_SEED, 0);

@@ -141,6 +141,7 @@ struct DevCfg {
     // Langevin MPC (langevinMPC, mpc.c:1674-1780): per species
     // a = (m - F dt / 2) / (m + F dt / 2), b = sqrt(F dt) / (m + F dt / 2)
     double lang_a[MPCD_MAX_SPECIES], lang_b[MPCD_MAX_SPECIES];
+    double relax;  // in.TAU: RELAX of the Vicsek-aligned operators
     int vdist[MPCD_MAX_SPECIES];   // VDIST: re-thermalisation velocities (push)
     double rfc[MPCD_MAX_SPECIES], tumble[MPCD_MAX_SPECIES], chihi[MPCD_MAX_SPECIES];
     double act[MPCD_MAX_SPECIES], mfpot[MPCD_MAX_SPECIES], sigwidth[MPCD_MAX_SPECIES];
@@ -579,6 +580,39 @@ __host__ __device__ __forceinline__ bool is_srd_op(int op) {
            op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS;
 }
 
+// Andersen MPC-AT and its Vicsek-aligned form (one weighting of the noise).
+__host__ __device__ __forceinline__ bool is_mpcat_op(int op) {
+    return op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT;
+}
+// Langevin MPC and its Vicsek-aligned form (the plain mean of the noise).
+__host__ __device__ __forceinline__ bool is_lang_op(int op) {
+    return op == MPCD_COLL_LANG || op == MPCD_COLL_VICSEK_LANG;
+}
+__host__ __device__ __forceinline__ bool is_vicsek_op(int op) {
+    return op == MPCD_COLL_VICSEK_MPCAT || op == MPCD_COLL_VICSEK_LANG;
+}
+
+// The Vicsek alignment of vicsekAndersenMPC (mpc.c:2204-2290) and
+// vicsekLangevinMPC (mpc.c:2409-2480): a particle whose species has
+// |ACT| > 1e-8 (not feq) gains RELAX (ACT VCMdir - V), with V its velocity
+// before the collision and VCMdir = VCM / |VCM| (normCopy, mtools.c:262-267);
+// for |VCM| < 1e-8 the reference leaves VCMdir unset, zero here.  Returns
+// the term to add.  Out of line and by value: only these operators reach
+// it, and the callers' arrays stay in registers.
+static __device__ __noinline__ double3 vicsek_term(double relax, double act, int dim,
+                                                   double3 u, double3 v) {
+    double3 t = make_double3(0.0, 0.0, 0.0);
+    if (!(fabs(act) > 1e-8)) return t;
+    double l = u.x * u.x + u.y * u.y;
+    if (dim == 3) l += u.z * u.z;
+    l = sqrt(l);
+    const bool unit = fabs(l) >= 1e-8;
+    t.x = relax * (act * (unit ? u.x / l : 0.0) - v.x);
+    t.y = relax * (act * (unit ? u.y / l : 0.0) - v.y);
+    if (dim == 3) t.z = relax * (act * (unit ? u.z / l : 0.0) - v.z);
+    return t;
+}
+
 // Length of a 3-vector, summed in index order as the reference's length()
 // (mtools.c:230-236), without contraction.
 __device__ __forceinline__ double len3_rn(const double *x) {
@@ -608,16 +642,19 @@ __device__ __forceinline__ void cross3_rn(const double *x, const double *y, doub
 // (rodriguesRotation, mtools.c:1572-1585; the axis is normalised only when
 // its length is at least 1e-8).  Turns below 1e-5 rad (ROTTOL) are skipped,
 // and so is a NaN angle (a zero v or u).  v and u are 3-vectors (zero z in
-// 2D).  Out of line: only the active operators reach it.
-static __device__ __noinline__ void active_srd_turn(double act, const double *u, double *v) {
-    if (!(fabs(act) >= 1e-8)) return;
+// 2D).  Out of line and by value: only the active operators reach it, and
+// the callers' arrays stay in registers.
+static __device__ __noinline__ double3 active_srd_turn(double act, double3 uu, double3 vv) {
+    if (!(fabs(act) >= 1e-8)) return vv;
+    const double u[3] = {uu.x, uu.y, uu.z};
+    double v[3] = {vv.x, vv.y, vv.z};
     double cosa = dot3_rn(v, u);
     cosa = __ddiv_rn(cosa, len3_rn(v));
     cosa = __ddiv_rn(cosa, len3_rn(u));
     const double theta = acos(cosa);
     double ax[3];
     cross3_rn(v, u, ax);
-    if (!(fabs(theta) > 1e-5)) return;
+    if (!(fabs(theta) > 1e-5)) return vv;
     const double l = len3_rn(ax);
     if (fabs(l) >= 1e-8)
         for (int d = 0; d < 3; d++) ax[d] = __ddiv_rn(ax[d], l);
@@ -632,6 +669,7 @@ static __device__ __noinline__ void active_srd_turn(double act, const double *u,
     const double now = len3_rn(v);
     const double f = __ddiv_rn(old, now);
     for (int d = 0; d < 3; d++) v[d] = __dmul_rn(v[d], f);
+    return make_double3(v[0], v[1], v[2]);
 }
 
 // Inverse of a symmetric-or-not 3x3 matrix by adjugate / determinant.

@@ -64,13 +64,13 @@ struct PerQ {
     static __host__ __device__ constexpr int nq(int op) {
         return is_srd_op(op)
                    ? 1 + DIM
-                   : (op == MPCD_COLL_MPCAT || op == MPCD_COLL_LANG ? 1 + 2 * DIM : Lr + NL);
+                   : (is_mpcat_op(op) || is_lang_op(op) ? 1 + 2 * DIM : Lr + NL);
     }
     // record: u[D], then SRD 3D: R[9]; Andersen: RS[D]; MPC-AT+a: CM[D], W[NL]
     static constexpr int U = 0, ROT = DIM, RS = DIM, CM = 2 * DIM, W = 3 * DIM;
     static __host__ __device__ constexpr int nr(int op) {
         return is_srd_op(op) ? (DIM == 3 ? DIM + 9 : DIM)
-                                       : (op == MPCD_COLL_MPCAT || op == MPCD_COLL_LANG
+                                       : (is_mpcat_op(op) || is_lang_op(op)
                                               ? 2 * DIM
                                               : 3 * DIM + NL);
     }
@@ -222,7 +222,7 @@ __device__ __forceinline__ void per_enter(const DevCfg &c, const PerLayout &l, c
     for (int d = 0; d < DIM; d++) add(Q::P + d, vv[d] * m);
     if (is_srd_op(c.op)) return;
     // Langevin: the plain sum of the noise (langevinMPC, mpc.c:1707-1710)
-    for (int d = 0; d < DIM; d++) add(Q::R + d, c.op == MPCD_COLL_LANG ? rv[d] : rv[d] * m);
+    for (int d = 0; d < DIM; d++) add(Q::R + d, is_lang_op(c.op) ? rv[d] : rv[d] * m);
     if (c.op != MPCD_COLL_RAT) return;
     for (int d = 0; d < DIM; d++) add(Q::Q1 + d, rel[d] * m);
     double dv[3] = {0, 0, 0};
@@ -291,7 +291,7 @@ __device__ __forceinline__ void per_cell(const DevCfg &c, const PerLayout &l, co
     double rs[3] = {0, 0, 0};
     if (n > 1)
         for (int d = 0; d < DIM; d++)
-            rs[d] = x[Q::R + d] / (c.op == MPCD_COLL_LANG ? (double)n : M);
+            rs[d] = x[Q::R + d] / (is_lang_op(c.op) ? (double)n : M);
     for (int d = 0; d < DIM; d++) put(Q::RS + d, rs[d]);
     if (c.op != MPCD_COLL_RAT) return;
     double cm[3] = {0, 0, 0}, W[3] = {0, 0, 0};
@@ -375,18 +375,33 @@ __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &
             for (int a = 0; a < DIM; a++)
                 for (int b = 0; b < DIM; b++) t[a] += R[a * 3 + b] * w[b];
             for (int d = 0; d < DIM; d++) vv[d] = u[d] + t[d];
-            if (c.act_srd) active_srd_turn(c.act[sp], u, vv);
+            if (c.act_srd) {
+                const double3 t = active_srd_turn(c.act[sp], make_double3(u[0], u[1], u[2]),
+                                                  make_double3(vv[0], vv[1], vv[2]));
+                vv[0] = t.x;
+                vv[1] = t.y;
+                vv[2] = t.z;
+            }
         } else {
             const double damp = c.damp[sp];
             double rv[3] = {0, 0, 0};
             for (int d = 0; d < DIM; d++) rv[d] = rvv[d * l.chunk + j];
-            if (c.op == MPCD_COLL_LANG) {
+            const double3 v0 = make_double3(vv[0], vv[1], vv[2]);
+            if (is_lang_op(c.op) || is_vicsek_op(c.op)) {
+                // the Vicsek-aligned MPC-AT takes this update with a = 0, b = 1
                 // langevinMPC, mpc.c:1739-1750
                 const double a = c.lang_a[sp], b = c.lang_b[sp];
                 for (int d = 0; d < DIM; d++)
                     vv[d] = u[d] + a * (vv[d] - u[d]) + b * (rv[d] - rc[Q::RS + d]) -
                             damp * u[d] / (double)n;
-            } else if (c.op == MPCD_COLL_MPCAT) {
+                if (is_vicsek_op(c.op)) {
+                    const double3 t = vicsek_term(c.relax, c.act[sp], DIM,
+                                                  make_double3(u[0], u[1], u[2]), v0);
+                    vv[0] += t.x;
+                    vv[1] += t.y;
+                    if (DIM == 3) vv[2] += t.z;
+                }
+            } else if (is_mpcat_op(c.op)) {
                 // andersenMPC, mpc.c:1353-1444 (damping over POP)
                 for (int d = 0; d < DIM; d++)
                     vv[d] = u[d] + rv[d] - rc[Q::RS + d] - damp * u[d] / (double)n;

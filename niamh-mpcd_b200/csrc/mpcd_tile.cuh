@@ -365,7 +365,10 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
     const bool rat = c.op == MPCD_COLL_RAT;
     // Langevin: the cell's plain mean of the noise instead of the
     // mass-weighted one (langevinMPC, mpc.c:1689-1736)
-    const bool lang = c.op == MPCD_COLL_LANG;
+    const bool plain = is_lang_op(c.op);
+    // the Vicsek-aligned MPC-AT takes the Langevin update with a = 0, b = 1
+    const bool vic = is_vicsek_op(c.op);
+    const bool lang = plain || vic;
     double ke = 0.0, av[3] = {0, 0, 0};
     int bounce = 0, esc = 0, overflow = 0;
 
@@ -501,13 +504,13 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             // have fewer than two particles and ignore the result)
             double rs[3] = {0, 0, 0};
             for (int j = j0 + sub; j < j1; j += kCellLanes) {
-                double m = lang ? 1.0 : c.mass[s_sp ? s_sp[j] : 0];
+                double m = plain ? 1.0 : c.mass[s_sp ? s_sp[j] : 0];
                 for (int d = 0; d < DIM; d++) rs[d] += m * (double)s_rv[3 * j + d];
             }
             for (int d = 0; d < DIM; d++) rs[d] = group_sum(rs[d]);
             if (lead && pop > 1)
                 for (int d = 0; d < 3; d++)
-                    s_rs[3 * lc + d] = d < DIM ? rs[d] / (lang ? (double)pop : M) : 0.0;
+                    s_rs[3 * lc + d] = d < DIM ? rs[d] / (plain ? (double)pop : M) : 0.0;
             if (!rat) continue;
             double I6[6] = {0, 0, 0, 0, 0, 0}, Lm[3] = {0, 0, 0};
             for (int j = j0 + sub; j < j1; j += kCellLanes) {
@@ -577,9 +580,12 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                             nv[2] = 0.f;
                         }
                         if (c.act_srd) {
-                            double dv[3] = {nv[0], nv[1], nv[2]};
-                            active_srd_turn(c.act[sp], &s_u[3 * lc], dv);
-                            for (int d = 0; d < 3; d++) nv[d] = (float)dv[d];
+                            const double3 t = active_srd_turn(
+                                c.act[sp], make_double3(s_u[3 * lc], s_u[3 * lc + 1], s_u[3 * lc + 2]),
+                                make_double3(nv[0], nv[1], nv[2]));
+                            nv[0] = (float)t.x;
+                            nv[1] = (float)t.y;
+                            nv[2] = (float)t.z;
                         }
                         MixT<DIM>::set_velf(*(MixRec *)&r, nv);
                     } else {
@@ -590,7 +596,13 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                         for (int x = 0; x < DIM; x++)
                             for (int y = 0; y < DIM; y++) t[x] += (double)R[x * 3 + y] * w[y];
                         for (int d = 0; d < DIM; d++) nv[d] = u[d] + t[d];
-                        if (c.act_srd) active_srd_turn(c.act[sp], u, nv);
+                        if (c.act_srd) {
+                            const double3 t = active_srd_turn(c.act[sp], make_double3(u[0], u[1], u[2]),
+                                                              make_double3(nv[0], nv[1], nv[2]));
+                            nv[0] = t.x;
+                            nv[1] = t.y;
+                            nv[2] = t.z;
+                        }
                         T::set_vel(r, nv);
                     }
                 } else {
@@ -606,6 +618,14 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                             nv[d] = u[d] + a * (v[d] - u[d]) +
                                     b * ((double)s_rv[3 * j + d] - rs[d]) -
                                     damp * u[d] / (double)pop;
+                        if (vic) {
+                            const double3 t = vicsek_term(c.relax, c.act[sp], DIM,
+                                                          make_double3(u[0], u[1], u[2]),
+                                                          make_double3(v[0], v[1], v[2]));
+                            nv[0] += t.x;
+                            nv[1] += t.y;
+                            if (DIM == 3) nv[2] += t.z;
+                        }
                     } else if (!rat) {
                         for (int d = 0; d < DIM; d++)
                             nv[d] = u[d] + (double)s_rv[3 * j + d] - rs[d] -

@@ -25,6 +25,8 @@ COLL_LANG = 4
 COLL_RAT = 3
 COLL_ACT_ARBAXIS = 9
 COLL_ACT_ORTHAXIS = 10
+COLL_VICSEK_MPCAT = 11
+COLL_VICSEK_LANG = 12
 COLL_DIPOLE_DIR_SUM = 16
 COLL_DIPOLE_DIR_AV = 17
 
@@ -114,6 +116,7 @@ class Config(C.Structure):
         ("walls", Wall * MAX_WALLS),
         ("capacity", C.c_int),
         ("fricco", C.c_double),
+        ("relax", C.c_double),
     ]
 
 

@@ -23,7 +23,8 @@ def _species(mass=1.0, **kw):
 
 def base_config(dim, L, *, coll_op, dt=0.1, kbt=1.0, rot_ang=math.pi / 2,
                 lc=0, grav=(0.0, 0.0, 0.0), walls=None, seed=12345,
-                precision=abi.PREC_FP64, species=None, gndnst=0.0, galinv=1, fricco=1.0):
+                precision=abi.PREC_FP64, species=None, gndnst=0.0, galinv=1, fricco=1.0,
+                relax=0.5):
     cfg = abi.Config()
     cfg.dim = dim
     for d in range(3):
@@ -49,6 +50,7 @@ def base_config(dim, L, *, coll_op, dt=0.1, kbt=1.0, rot_ang=math.pi / 2,
         cfg.walls[i] = wl
     cfg.capacity = 0
     cfg.fricco = fricco
+    cfg.relax = relax
     return cfg
 
 

@@ -559,10 +559,28 @@ static void thermal_draw(const oracle_t *o, int i, uint32_t step, double *rv) {
 
 /* Andersen MPC-AT (andersenMPC, mpc.c:1353-1444):
  * v' = VCM + RV - RS - DAMP*VCM/POP, RS = sum(m RV)/M. */
+/* The Vicsek alignment of vicsekAndersenMPC (mpc.c:2204-2290) and
+ * vicsekLangevinMPC (mpc.c:2409-2480): a particle whose species has
+ * |ACT| > 1e-8 (not feq) gains RELAX (ACT VCMdir - V), VCMdir = VCM/|VCM|
+ * (normCopy, mtools.c:262-267; the reference leaves VCMdir unset for
+ * |VCM| < 1e-8, taken as zero here).  Neither operator applies DAMP. */
+static int vicsek_op(int op) {
+    return op == MPCD_COLL_VICSEK_MPCAT || op == MPCD_COLL_VICSEK_LANG;
+}
+static void vicsek_dir(int dim, const double *u, double *dir) {
+    double l = len3(u, dim);
+    for (int d = 0; d < 3; d++) dir[d] = 0.0;
+    if (fabs(l - 0.0) >= 1e-8)
+        for (int d = 0; d < dim; d++) dir[d] = u[d] / l;
+}
+
 static void collide_mpcat(oracle_t *o, int c, uint32_t step) {
     int dim = o->dim, s = o->start[c], e = o->start[c + 1];
     double RS[3] = {0, 0, 0};
     const double *u = &o->vcm[3 * c];
+    const int vic = vicsek_op(o->cfg.coll_op);
+    double dir[3];
+    vicsek_dir(dim, u, dir);
     for (int j = s; j < e; j++) {
         int i = o->list[j];
         double rv[3];
@@ -575,10 +593,17 @@ static void collide_mpcat(oracle_t *o, int c, uint32_t step) {
         int i = o->list[j];
         double rv[3];
         thermal_draw(o, i, step, rv);
-        double damp = o->cfg.species[o->spid[i]].damp;
-        for (int d = 0; d < dim; d++)
-            o->V[3 * i + d] =
-                u[d] + rv[d] - RS[d] - damp * u[d] / (double)(e - s);
+        const mpcd_species *sp = &o->cfg.species[o->spid[i]];
+        if (vic && fabs(sp->act - 0.0) > 1e-8) {
+            for (int d = 0; d < dim; d++)
+                o->V[3 * i + d] = u[d] + o->cfg.relax * (sp->act * dir[d] - o->V[3 * i + d]) +
+                                  rv[d] - RS[d];
+        } else if (vic) {
+            for (int d = 0; d < dim; d++) o->V[3 * i + d] = u[d] + rv[d] - RS[d];
+        } else {
+            for (int d = 0; d < dim; d++)
+                o->V[3 * i + d] = u[d] + rv[d] - RS[d] - sp->damp * u[d] / (double)(e - s);
+        }
     }
 }
 
@@ -591,6 +616,9 @@ static void collide_lang(oracle_t *o, int c, uint32_t step) {
     double WNS[3] = {0, 0, 0};
     const double *u = &o->vcm[3 * c];
     const double F = o->cfg.fricco, dt = o->cfg.dt;
+    const int vic = vicsek_op(o->cfg.coll_op);
+    double dir[3];
+    vicsek_dir(dim, u, dir);
     for (int j = s; j < e; j++) {
         double rv[3];
         thermal_draw(o, o->list[j], step, rv);
@@ -605,9 +633,20 @@ static void collide_lang(oracle_t *o, int c, uint32_t step) {
         const double M = sp->mass;
         const double a = (M - F * dt * 0.5) / (M + 0.5 * F * dt);
         const double b = sqrt(F * dt) / (M + 0.5 * F * dt);
-        for (int d = 0; d < dim; d++)
-            o->V[3 * i + d] = u[d] + a * (o->V[3 * i + d] - u[d]) + b * (rv[d] - WNS[d]) -
-                              sp->damp * u[d] / (double)(e - s);
+        if (vic && fabs(sp->act - 0.0) > 1e-8) {
+            for (int d = 0; d < dim; d++) {
+                const double v = o->V[3 * i + d];
+                o->V[3 * i + d] = u[d] + o->cfg.relax * (sp->act * dir[d] - v) + a * (v - u[d]) +
+                                  b * (rv[d] - WNS[d]);
+            }
+        } else if (vic) {
+            for (int d = 0; d < dim; d++)
+                o->V[3 * i + d] = u[d] + a * (o->V[3 * i + d] - u[d]) + b * (rv[d] - WNS[d]);
+        } else {
+            for (int d = 0; d < dim; d++)
+                o->V[3 * i + d] = u[d] + a * (o->V[3 * i + d] - u[d]) + b * (rv[d] - WNS[d]) -
+                                  sp->damp * u[d] / (double)(e - s);
+        }
     }
 }
 
@@ -1098,9 +1137,9 @@ int oracle_step(oracle_t *o, uint32_t step) {
         else if (op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS ||
                  op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS)
             collide_srd(o, c, step);
-        else if (op == MPCD_COLL_MPCAT)
+        else if (op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT)
             collide_mpcat(o, c, step);
-        else if (op == MPCD_COLL_LANG)
+        else if (op == MPCD_COLL_LANG || op == MPCD_COLL_VICSEK_LANG)
             collide_lang(o, c, step);
         else if (op == MPCD_COLL_RAT)
             collide_rat(o, c, step);

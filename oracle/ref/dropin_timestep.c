@@ -72,6 +72,7 @@ static int fill_config(mpcd_config *c, inputList in, spec SP[], bc WALL[]) {
     c->kbt = in.KBT;
     c->coll_op = in.RTECH;
     c->fricco = in.FRICCO;
+    c->relax = in.TAU;
     c->lc = in.LC;
     c->rot_ang = in.RA;
     c->galinv = in.GALINV;

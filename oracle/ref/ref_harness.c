@@ -235,7 +235,7 @@ int ref_init(const mpcd_config *cfg, int n, const double *Q, const double *V,
     g_in.LC = cfg->lc;
     g_in.GALINV = cfg->galinv;
     g_in.TSTECH = NOTHERM;
-    g_in.TAU = 0.5;
+    g_in.TAU = cfg->relax;
     g_in.noHI = HION;
     g_in.inCOMP = INCOMPOFF;
     g_in.MULTIPHASE = MPHOFF;
@@ -395,6 +395,7 @@ int ref_checkpoint_read(const char *path, mpcd_config *cfg, int *n, int *runtime
     cfg->kbt = in.KBT;
     cfg->coll_op = in.RTECH;
     cfg->fricco = in.FRICCO;
+    cfg->relax = in.TAU;
     cfg->lc = in.LC;
     cfg->rot_ang = in.RA;
     cfg->galinv = in.GALINV;

@@ -329,3 +329,39 @@ def test_active_srd_refuses_species_of_different_activity():
     cfg = W.base_config(3, (4, 4, 4), coll_op=abi.COLL_ACT_ARBAXIS, species=sp)
     with pytest.raises(MPCDError):
         Solver(cfg)
+
+
+@pytest.mark.parametrize("op,prec,kernel,dim", [
+    (abi.COLL_VICSEK_MPCAT, abi.PREC_FP64, abi.KERNEL_TILE, 3),
+    (abi.COLL_VICSEK_LANG, abi.PREC_FP64, abi.KERNEL_PERSIST, 3),
+    (abi.COLL_VICSEK_MPCAT, abi.PREC_FP64, abi.KERNEL_AUTO, 2),
+    (abi.COLL_VICSEK_LANG, abi.PREC_FP64, abi.KERNEL_TILE, 2),
+    (abi.COLL_VICSEK_MPCAT, abi.PREC_MIXED, abi.KERNEL_TILE, 3),
+    (abi.COLL_VICSEK_LANG, abi.PREC_MIXED, abi.KERNEL_AUTO, 2)])
+def test_vicsek_aligned_operators_match_the_oracle(op, prec, kernel, dim):
+    """MPC-AT and Langevin MPC with Vicsek alignment (vicsekAndersenMPC,
+    mpc.c:2204-2290; vicsekLangevinMPC, mpc.c:2409-2480) on the tile and
+    persistent kernel families against the oracle (pinned to the
+    reference): an active and a passive species, a net flow."""
+    L = (6, 5, 7) if dim == 3 else (12, 10)
+    sp = [W._species(mass=1.0, act=0.8, damp=0.3), W._species(mass=2.0, act=0.0, damp=0.3)]
+    kw = dict(coll_op=op, species=sp, relax=0.5, fricco=0.8, seed=95)
+    cfg = W.base_config(dim, L, **kw)
+    cfgp = W.base_config(dim, L, precision=prec, **kw)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=96)
+    V[:, 0] += 0.3
+    spid = (np.arange(len(Q)) % 3 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, spid)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(cfg.L[:3], dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    g.close()
+    o.close()

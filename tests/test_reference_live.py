@@ -197,3 +197,27 @@ def test_active_srd_tracks_reference(op, dim, L, act):
     assert r.unexpected_draws() == 0
     np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
     np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
+
+
+@pytest.mark.parametrize("op,dim,L,relax", [(11, 3, (7, 6, 8), 0.5), (12, 3, (6, 6, 6), 0.3),
+                                            (11, 2, (20, 16), 0.7), (12, 2, (16, 14), 0.5)])
+def test_vicsek_aligned_operators_track_reference(op, dim, L, relax):
+    """MPC-AT and Langevin MPC with Vicsek alignment (vicsekAndersenMPC,
+    mpc.c:2204-2290; vicsekLangevinMPC, mpc.c:2409-2480: RELAX (ACT VCMdir -
+    V) for active species, no damping) of the oracle against the
+    reference's own: an active and a passive species, a net flow."""
+    sp = [W._species(mass=1.0, act=0.8, damp=0.3), W._species(mass=2.0, act=0.0, damp=0.3)]
+    cfg = W.base_config(dim, L, coll_op=op, species=sp, relax=relax, fricco=0.8, seed=545)
+    Q, V, U, spid = W.synthetic_state(cfg, 10, seed=546)
+    V[:, 0] += 0.3
+    spid = (np.arange(len(Q)) % 3 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    r = Reference(cfg, Q, V, U, spid)
+    for s in range(1, 6):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
