@@ -169,7 +169,7 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
     if (!(cfg->dt > 0.0) || !(cfg->kbt >= 0.0)) return MPCD_ERR_ARG;
     if (cfg->lc != MPCD_LC_ISOTROPIC && !(cfg->lc == MPCD_LC_LOCAL && cfg->dim == 2))
         return MPCD_ERR_UNSUPPORTED;
-    if (cfg->lc == MPCD_LC_ISOTROPIC && !is_srd_op(cfg->coll_op) &&
+    if (cfg->lc == MPCD_LC_ISOTROPIC && !is_vcm_op(cfg->coll_op) &&
         !is_mpcat_op(cfg->coll_op) && cfg->coll_op != MPCD_COLL_RAT &&
         !is_lang_op(cfg->coll_op))
         return MPCD_ERR_UNSUPPORTED;
@@ -1356,7 +1356,7 @@ static int run_step_r64(mpcd_handle *h, uint32_t step) {
 
 static int default_strategy(const mpcd_handle *h) {
     // recompute (96 B/particle) wins when the collision is cheap to redo
-    return is_srd_op(h->dc.op) ? MPCD_STRATEGY_RECOMPUTE : MPCD_STRATEGY_SCATTER;
+    return is_vcm_op(h->dc.op) ? MPCD_STRATEGY_RECOMPUTE : MPCD_STRATEGY_SCATTER;
 }
 
 // One nematic (2D) timestep: moments + order parameter, velocity gradient,

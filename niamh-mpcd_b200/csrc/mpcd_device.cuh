@@ -574,10 +574,12 @@ __device__ __forceinline__ void srd_cell_matrix(const DevCfg &c, uint32_t step,
     srd_matrix<DIM, T>(c, Lx, R);
 }
 
-// True for the SRD rotation operators, plain or active.
-__host__ __device__ __forceinline__ bool is_srd_op(int op) {
+// True for the operators that need only the cell's VCM and no thermal
+// draws: the SRD rotations, plain or active, and Vicsek.
+__host__ __device__ __forceinline__ bool is_vcm_op(int op) {
     return op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS ||
-           op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS;
+           op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS ||
+           op == MPCD_COLL_VICSEK;
 }
 
 // Andersen MPC-AT and its Vicsek-aligned form (one weighting of the noise).
@@ -634,6 +636,26 @@ __device__ __forceinline__ void cross3_rn(const double *x, const double *y, doub
     r[2] = __dsub_rn(__dmul_rn(x[0], y[1]), __dmul_rn(x[1], y[0]));
 }
 
+// Rodrigues' rotation of v about axis ax by t with v's length restored
+// (rodriguesRotation, mtools.c:1572-1585): the axis is normalised only when
+// its length is at least 1e-8 (norm, mtools.c:246-251), in place.
+__device__ __forceinline__ void rodrigues_keep(double *v, double *ax, double t) {
+    const double l = len3_rn(ax);
+    if (fabs(l) >= 1e-8)
+        for (int d = 0; d < 3; d++) ax[d] = __ddiv_rn(ax[d], l);
+    const double old = len3_rn(v);
+    double cp[3];
+    cross3_rn(ax, v, cp);
+    const double dp = dot3_rn(ax, v);
+    const double ct = cos(t), st = sin(t);
+    for (int d = 0; d < 3; d++)
+        v[d] = __dadd_rn(__dadd_rn(__dmul_rn(v[d], ct), __dmul_rn(cp[d], st)),
+                         __dmul_rn(__dmul_rn(ax[d], dp), __dsub_rn(1.0, ct)));
+    const double now = len3_rn(v);
+    const double f = __ddiv_rn(old, now);
+    for (int d = 0; d < 3; d++) v[d] = __dmul_rn(v[d], f);
+}
+
 // The active part of active SRD (activeSRD, mpc.c:2055-2076), after the
 // rotation: a particle whose species has ACT != 0 (fneq, |ACT| >= 1e-8) is
 // turned toward the cell's centre-of-mass velocity u by ACT times the angle
@@ -655,21 +677,61 @@ static __device__ __noinline__ double3 active_srd_turn(double act, double3 uu, d
     double ax[3];
     cross3_rn(v, u, ax);
     if (!(fabs(theta) > 1e-5)) return vv;
-    const double l = len3_rn(ax);
-    if (fabs(l) >= 1e-8)
-        for (int d = 0; d < 3; d++) ax[d] = __ddiv_rn(ax[d], l);
-    const double old = len3_rn(v);
-    double cp[3];
-    cross3_rn(ax, v, cp);
-    const double dp = dot3_rn(ax, v);
-    const double t = __dmul_rn(act, theta), ct = cos(t), st = sin(t);
-    for (int d = 0; d < 3; d++)
-        v[d] = __dadd_rn(__dadd_rn(__dmul_rn(v[d], ct), __dmul_rn(cp[d], st)),
-                         __dmul_rn(__dmul_rn(ax[d], dp), __dsub_rn(1.0, ct)));
-    const double now = len3_rn(v);
-    const double f = __ddiv_rn(old, now);
-    for (int d = 0; d < 3; d++) v[d] = __dmul_rn(v[d], f);
+    rodrigues_keep(v, ax, __dmul_rn(act, theta));
     return make_double3(v[0], v[1], v[2]);
+}
+
+// Vicsek (vicsek, mpc.c:2098-2135): the particle's velocity is redrawn
+// with its speed (length over DIM) and a direction uniform on the cone of
+// half-angle pi (1 - ACT) that genrand_cone (rand.c:438-454) builds about
+// VCMdir = VCM/|VCM| (normCopy over 3 components): a draw on the cone about
+// the x axis (genrand_coneNP, rand.c:397-425: 3D z = u0 (1 - cos t) + cos t,
+// phi = 2 pi u1, (z, sqrt(1-z^2) cos phi, sqrt(1-z^2) sin phi); 2D
+// phi = t (1 - 2 u0), (cos phi, sin phi)), then Rodrigues' rotation about
+// VCMdir x x by the angle between them, as the reference has it.  For
+// |VCM| < 1e-8 the reference leaves VCMdir unset; here the draw keeps the
+// x axis.  The uniforms are the particle's own (MPCD_STREAM_VICSEK).
+static __device__ __noinline__ double3 vicsek_cone(double act, int dim, uint64_t seed,
+                                                   uint32_t replica, uint32_t step,
+                                                   uint32_t pid, double3 uu, double3 vv) {
+    double u[3] = {uu.x, uu.y, dim == 3 ? uu.z : 0.0};
+    const double l = len3_rn(u);
+    const bool dir = fabs(l) >= 1e-8;
+    if (dir)
+        for (int d = 0; d < 3; d++) u[d] = __ddiv_rn(u[d], l);
+    double speed = __dadd_rn(__dmul_rn(vv.x, vv.x), __dmul_rn(vv.y, vv.y));
+    if (dim == 3) speed = __dadd_rn(speed, __dmul_rn(vv.z, vv.z));
+    speed = sqrt(speed);
+    const double theta = __dmul_rn(M_PI, __dsub_rn(1.0, act));
+    double r[3];
+    if (dim == 3) {
+        const double ct = cos(theta);
+        const double u0 = mpcd_rng_uniform(seed, replica, step, MPCD_STREAM_VICSEK, pid, 0u);
+        const double u1 = mpcd_rng_uniform(seed, replica, step, MPCD_STREAM_VICSEK, pid, 1u);
+        const double z = __dadd_rn(__dmul_rn(u0, __dsub_rn(1.0, ct)), ct);
+        const double phi = __dmul_rn(__dmul_rn(u1, 2.0), M_PI);
+        const double sz = sqrt(__dsub_rn(1.0, __dmul_rn(z, z)));
+        r[0] = z;
+        r[1] = __dmul_rn(sz, cos(phi));
+        r[2] = __dmul_rn(sz, sin(phi));
+    } else {
+        const double u0 = mpcd_rng_uniform(seed, replica, step, MPCD_STREAM_VICSEK, pid, 0u);
+        const double phi = __dmul_rn(theta, __dsub_rn(1.0, __dmul_rn(2.0, u0)));
+        r[0] = cos(phi);
+        r[1] = sin(phi);
+        r[2] = 0.0;
+    }
+    if (dir) {
+        const double x[3] = {1.0, 0.0, 0.0};
+        double ax[3];
+        cross3_rn(u, x, ax);
+        double cosa = dot3_rn(u, x);
+        cosa = __ddiv_rn(cosa, len3_rn(u));
+        cosa = __ddiv_rn(cosa, len3_rn(x));
+        rodrigues_keep(r, ax, acos(cosa));
+    }
+    return make_double3(__dmul_rn(r[0], speed), __dmul_rn(r[1], speed),
+                        dim == 3 ? __dmul_rn(r[2], speed) : vv.z);
 }
 
 // Inverse of a symmetric-or-not 3x3 matrix by adjugate / determinant.

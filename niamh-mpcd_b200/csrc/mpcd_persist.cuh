@@ -62,14 +62,14 @@ struct PerQ {
     static constexpr int Lr = Q2 + NQ2;
     static constexpr int NL = DIM == 3 ? 3 : 1;
     static __host__ __device__ constexpr int nq(int op) {
-        return is_srd_op(op)
+        return is_vcm_op(op)
                    ? 1 + DIM
                    : (is_mpcat_op(op) || is_lang_op(op) ? 1 + 2 * DIM : Lr + NL);
     }
     // record: u[D], then SRD 3D: R[9]; Andersen: RS[D]; MPC-AT+a: CM[D], W[NL]
     static constexpr int U = 0, ROT = DIM, RS = DIM, CM = 2 * DIM, W = 3 * DIM;
     static __host__ __device__ constexpr int nr(int op) {
-        return is_srd_op(op) ? (DIM == 3 ? DIM + 9 : DIM)
+        return is_vcm_op(op) ? (DIM == 3 ? DIM + 9 : DIM)
                                        : (is_mpcat_op(op) || is_lang_op(op)
                                               ? 2 * DIM
                                               : 3 * DIM + NL);
@@ -100,7 +100,7 @@ inline PerLayout per_layout(int n, int op, int n_species, int blocks) {
     l.chunk = (n + blocks - 1) / blocks;
     l.nq = PerQ<DIM>::nq(op);
     l.nr = PerQ<DIM>::nr(op);
-    const bool andersen = !is_srd_op(op);
+    const bool andersen = !is_vcm_op(op);
     size_t o = 0;
     auto take = [&](size_t bytes) {
         const int at = (int)o;
@@ -220,7 +220,7 @@ __device__ __forceinline__ void per_enter(const DevCfg &c, const PerLayout &l, c
     atomicAdd(g.pop + k, 1);
     add(Q::M, m);
     for (int d = 0; d < DIM; d++) add(Q::P + d, vv[d] * m);
-    if (is_srd_op(c.op)) return;
+    if (is_vcm_op(c.op)) return;
     // Langevin: the plain sum of the noise (langevinMPC, mpc.c:1707-1710)
     for (int d = 0; d < DIM; d++) add(Q::R + d, is_lang_op(c.op) ? rv[d] : rv[d] * m);
     if (c.op != MPCD_COLL_RAT) return;
@@ -280,10 +280,11 @@ __device__ __forceinline__ void per_cell(const DevCfg &c, const PerLayout &l, co
         }
     }
     for (int d = 0; d < DIM; d++) put(Q::U + d, u[d]);
-    if (is_srd_op(c.op)) {
+    if (is_vcm_op(c.op)) {
         if (DIM == 3) {
             double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            if (n > 1) srd_cell_matrix<DIM, double>(c, step, (uint32_t)k, R);
+            if (n > 1 && c.op != MPCD_COLL_VICSEK)
+                srd_cell_matrix<DIM, double>(c, step, (uint32_t)k, R);
             for (int r = 0; r < 9; r++) put(Q::ROT + r, R[r]);
         }
         return;
@@ -362,7 +363,15 @@ __device__ __forceinline__ double per_collide(const DevCfg &c, const PerLayout &
     if (n > 1) {
         double u[3] = {0, 0, 0};
         for (int d = 0; d < DIM; d++) u[d] = rc[Q::U + d];
-        if (is_srd_op(c.op)) {
+        if (c.op == MPCD_COLL_VICSEK) {
+            const uint32_t pid = (uint32_t)((const int *)(sm + l.off_pid))[j];
+            const double3 t = vicsek_cone(c.act[sp], DIM, c.seed, c.replica, step, pid,
+                                          make_double3(u[0], u[1], u[2]),
+                                          make_double3(vv[0], vv[1], vv[2]));
+            vv[0] = t.x;
+            vv[1] = t.y;
+            vv[2] = t.z;
+        } else if (is_vcm_op(c.op)) {
             double R[9];
             if (DIM == 3) {
                 for (int r = 0; r < 9; r++) R[r] = rc[Q::ROT + r];

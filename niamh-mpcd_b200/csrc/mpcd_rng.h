@@ -56,7 +56,9 @@ enum {
     /* re-placement of a particle that left the grid, per particle and step: */
     MPCD_STREAM_ESCAPE_POS = 11, /* position, DIM uniforms per attempt       */
     MPCD_STREAM_ESCAPE_VEL = 12, /* velocity, DIM normals                    */
-    MPCD_STREAM_ESCAPE_ORI = 13  /* nematic orientation, one uniform         */
+    MPCD_STREAM_ESCAPE_ORI = 13, /* nematic orientation, one uniform         */
+    MPCD_STREAM_VICSEK = 14      /* Vicsek cone, 2 (3D) or 1 (2D) uniforms per
+                                    particle                                   */
 };
 
 /* Maximum Philox blocks a rejection loop may consume (2 attempts per block).

@@ -306,11 +306,11 @@ static inline TileLayout tile_layout(int ct, int cap, int op, int nspecies) {
         return r;
     };
     L.off_rec = take(cap * (int)sizeof(typename T::Rec), 16);
-    bool and_ = !is_srd_op(op);
+    bool and_ = !is_vcm_op(op);
     L.off_rv = and_ ? take(cap * 3 * (int)sizeof(typename T::VT), 16) : -1;
     L.off_start = take((ct + 1) * 4, 16);
     L.off_u = take(ct * 3 * 8, 16);
-    L.off_R = is_srd_op(op) ? take(ct * 9 * (int)sizeof(typename T::VT), 16) : -1;
+    L.off_R = is_vcm_op(op) ? take(ct * 9 * (int)sizeof(typename T::VT), 16) : -1;
     L.off_cm = op == MPCD_COLL_RAT ? take(ct * 3 * 8, 16) : -1;
     L.off_rs = and_ ? take(ct * 3 * 8, 16) : -1;
     L.off_W = op == MPCD_COLL_RAT ? take(ct * 3 * 8, 16) : -1;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
     for (int k = tid; k <= nct; k += nth) s_start[k] = tb.start[c0 + k];
     __syncthreads();
 
-    const bool andersen = !is_srd_op(c.op);
+    const bool andersen = !is_vcm_op(c.op);
     const bool rat = c.op == MPCD_COLL_RAT;
     // Langevin: the cell's plain mean of the noise instead of the
     // mass-weighted one (langevinMPC, mpc.c:1689-1736)
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                 for (int d = 0; d < 3; d++) s_u[3 * lc + d] = u[d];
             }
             if (!andersen) {
-                if (lead && pop > 1)
+                if (lead && pop > 1 && c.op != MPCD_COLL_VICSEK)
                     srd_cell_matrix<DIM, VT>(c, sa.step, (uint32_t)cell, &s_R[9 * lc]);
                 continue;
             }
@@ -561,7 +561,16 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             const int sp = s_sp ? s_sp[j] : 0;
             Rec r = s_rec[j];
             if (pop > 1) {
-                if (!andersen) {
+                if (!andersen && c.op == MPCD_COLL_VICSEK) {
+                    double v[3] = {0, 0, 0};
+                    T::vel(r, v);
+                    const double3 t = vicsek_cone(
+                        c.act[sp], DIM, c.seed, c.replica, sa.step, T::pid(r),
+                        make_double3(s_u[3 * lc], s_u[3 * lc + 1], s_u[3 * lc + 2]),
+                        make_double3(v[0], v[1], v[2]));
+                    const double nv[3] = {t.x, t.y, t.z};
+                    T::set_vel(r, nv);
+                } else if (!andersen) {
                     const VT *R = &s_R[9 * lc];
                     if constexpr (sizeof(VT) == 4) {
                         float ux = (float)s_u[3 * lc], uy = (float)s_u[3 * lc + 1],

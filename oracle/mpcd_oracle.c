@@ -559,6 +559,63 @@ static void thermal_draw(const oracle_t *o, int i, uint32_t step, double *rv) {
 
 /* Andersen MPC-AT (andersenMPC, mpc.c:1353-1444):
  * v' = VCM + RV - RS - DAMP*VCM/POP, RS = sum(m RV)/M. */
+/* Vicsek (vicsek, mpc.c:2098-2135): every particle keeps its speed (length
+ * over DIM) and takes a direction uniform on the cone of half-angle
+ * pi (1 - ACT) that genrand_cone (rand.c:438-454) builds about
+ * VCMdir = VCM/|VCM| (normCopy over 3 components): a draw on the cone about
+ * the x axis (genrand_coneNP, rand.c:397-425), then Rodrigues' rotation
+ * about VCMdir x x-hat by the angle between them.  The reference leaves
+ * VCMdir unset for |VCM| < 1e-8; the draw keeps the x axis here. */
+static void rodrigues_keep(double *v, double *ax, double t) {
+    double l = len3(ax, 3);
+    if (fabs(l - 0.0) >= 1e-8)
+        for (int d = 0; d < 3; d++) ax[d] = ax[d] / l;
+    double old = len3(v, 3), cp[3];
+    cross3(ax, v, cp);
+    double dp = dot3(ax, v, 3);
+    for (int d = 0; d < 3; d++) v[d] = v[d] * cos(t) + cp[d] * sin(t) + ax[d] * dp * (1.0 - cos(t));
+    double now = len3(v, 3);
+    for (int d = 0; d < 3; d++) v[d] *= (old / now);
+}
+static void collide_vicsek(oracle_t *o, int c, uint32_t step) {
+    int dim = o->dim;
+    double u[3] = {0, 0, 0};
+    for (int d = 0; d < dim; d++) u[d] = o->vcm[3 * c + d];
+    double l = len3(u, 3);
+    int dir = fabs(l - 0.0) >= 1e-8;
+    if (dir)
+        for (int d = 0; d < 3; d++) u[d] = u[d] / l;
+    for (int j = o->start[c]; j < o->start[c + 1]; j++) {
+        int i = o->list[j];
+        double *v = &o->V[3 * i];
+        double speed = len3(v, dim), theta = MPCD_PI * (1.0 - o->cfg.species[o->spid[i]].act);
+        double r[3] = {0, 0, 0};
+        double u0 = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
+                                     (uint32_t)i, 0u);
+        if (dim == 3) {
+            double ct = cos(theta), z = u0 * (1.0 - ct) + ct;
+            double phi = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
+                                          (uint32_t)i, 1u) * 2.0 * MPCD_PI;
+            r[0] = z;
+            r[1] = sqrt(1.0 - z * z) * cos(phi);
+            r[2] = sqrt(1.0 - z * z) * sin(phi);
+        } else {
+            double phi = theta * (1. - 2. * u0);
+            r[0] = cos(phi);
+            r[1] = sin(phi);
+        }
+        if (dir) {
+            double x[3] = {1.0, 0.0, 0.0}, ax[3];
+            cross3(u, x, ax);
+            double cosa = dot3(u, x, 3);
+            cosa /= len3(u, 3);
+            cosa /= len3(x, 3);
+            rodrigues_keep(r, ax, acos(cosa));
+        }
+        for (int d = 0; d < dim; d++) v[d] = r[d] * speed;
+    }
+}
+
 /* The Vicsek alignment of vicsekAndersenMPC (mpc.c:2204-2290) and
  * vicsekLangevinMPC (mpc.c:2409-2480): a particle whose species has
  * |ACT| > 1e-8 (not feq) gains RELAX (ACT VCMdir - V), VCMdir = VCM/|VCM|
@@ -1137,6 +1194,8 @@ int oracle_step(oracle_t *o, uint32_t step) {
         else if (op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS ||
                  op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS)
             collide_srd(o, c, step);
+        else if (op == MPCD_COLL_VICSEK)
+            collide_vicsek(o, c, step);
         else if (op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT)
             collide_mpcat(o, c, step);
         else if (op == MPCD_COLL_LANG || op == MPCD_COLL_VICSEK_LANG)

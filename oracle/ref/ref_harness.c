@@ -58,6 +58,9 @@ void setPBC(bc *WALL);                         /* read.c:584 */
 void galileantrans(particleMPC *pp, bc WALL[], simptr simMD, spec SP[], double KBT,
                    double VEL[], int POP, int NBC, int MDmode, int dimension); /* mtools.c:673 */
 double calcW(bc WALL, particleMPC P);          /* bc.c:55    */
+void crossprod(double x[3], double y[3], double result[3]);          /* mtools.c:177  */
+double absAngle(double v1[], double v2[], int dimension);           /* mtools.c:365  */
+void rodriguesRotation(double vec[], double rotAx[], double theta); /* mtools.c:1572 */
 unsigned long RandomSeedSRD(unsigned long s);  /* rand.c:293 */
 
 /* ------------------------------------------------------------------ state */
@@ -76,7 +79,7 @@ static int g_ncells = 0;
 /* draw bookkeeping */
 static uint64_t g_seed = 0;
 static uint32_t g_replica = 0, g_step = 0;
-enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT, PH_RETHERM, PH_ESCAPE };
+enum { PH_NONE = 0, PH_COLLIDE, PH_GHOST, PH_LC, PH_INIT, PH_RETHERM, PH_ESCAPE, PH_CONE };
 static int g_phase = PH_NONE;
 static int g_cell = 0;
 static int g_rtech = 0;  /* RTECH of the collision in progress */
@@ -670,6 +673,9 @@ double genrand_real(void) {
                                 (uint32_t)g_pid, g_k++);
     if (g_phase == PH_ESCAPE)
         return mpcd_rng_uniform(g_seed, g_replica, g_step, g_stream, (uint32_t)g_pid, g_k++);
+    if (g_phase == PH_CONE)
+        return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_VICSEK, (uint32_t)g_pid,
+                                g_k++);
     /* stochrotMPC draws a uniform for the orthogonal axis (ORTHAXIS only,
      * mpc.c:1289) and then one for the rotation sign, which
      * (long)genrand_real() truncates to 0 (mpc.c:1291) */
@@ -710,7 +716,7 @@ void genrand_coneNP(double vec[], double theta, int dimension) {
         /* the orientation of an escaped nematic: the particle's own stream */
         g_stream = MPCD_STREAM_ESCAPE_ORI;
         g_k = 0;
-    } else if (g_phase != PH_INIT) {
+    } else if (g_phase != PH_INIT && g_phase != PH_CONE) {
         genrand_sphere(vec, dimension);
         return;
     }
@@ -730,9 +736,29 @@ void genrand_coneNP(double vec[], double theta, int dimension) {
         g_unexpected++;
     }
 }
+/* rand.c:438-454, restated: a draw on the cone about the x axis, then
+ * Rodrigues' rotation about axis x x-hat by the angle between them, with the
+ * reference's own crossprod, absAngle and rodriguesRotation.  In a collision
+ * (vicsek, mpc.c:2098-2135, one draw per listed particle) the uniforms are
+ * the particle's own stream. */
 void genrand_cone(double axis[], double vecOut[], double theta, int dimension) {
-    (void)axis;
-    genrand_coneNP(vecOut, theta, dimension);
+    double rotAx[_3D], randVec[_3D] = {0.0}, xaxis[_3D] = {0.0};
+    int cone = g_phase == PH_COLLIDE && g_cursor;
+    if (cone) {
+        g_pid = (int)(g_cursor - g_pp);
+        g_k = 0;
+        g_phase = PH_CONE;
+    }
+    xaxis[0] = 1.0;
+    genrand_coneNP(randVec, theta, dimension);
+    crossprod(axis, xaxis, rotAx);
+    double angle = absAngle(axis, xaxis, _3D);
+    rodriguesRotation(randVec, rotAx, angle);
+    for (int i = 0; i < dimension; i++) vecOut[i] = randVec[i];
+    if (cone) {
+        g_phase = PH_COLLIDE;
+        g_cursor = g_cursor->next;
+    }
 }
 double *ranvec3D(double *v) {
     mpcd_rng_axis3(g_seed, g_replica, g_step, (uint32_t)g_cell, v);

@@ -365,3 +365,34 @@ def test_vicsek_aligned_operators_match_the_oracle(op, prec, kernel, dim):
     assert st.escaped == 0 and st.nonfinite == 0
     g.close()
     o.close()
+
+
+@pytest.mark.parametrize("prec,kernel,dim", [
+    (abi.PREC_FP64, abi.KERNEL_TILE, 3), (abi.PREC_FP64, abi.KERNEL_PERSIST, 3),
+    (abi.PREC_FP64, abi.KERNEL_AUTO, 2), (abi.PREC_MIXED, abi.KERNEL_TILE, 3),
+    (abi.PREC_MIXED, abi.KERNEL_AUTO, 2)])
+def test_vicsek_matches_the_oracle(prec, kernel, dim):
+    """Vicsek (vicsek, mpc.c:2098-2135, with genrand_cone, rand.c:438-454)
+    on the tile and persistent kernel families against the oracle (pinned to
+    the reference), a net flow."""
+    L = (6, 5, 7) if dim == 3 else (12, 10)
+    sp = [W._species(mass=1.0, act=0.7)]
+    cfg = W.base_config(dim, L, coll_op=abi.COLL_VICSEK, species=sp, seed=97)
+    cfgp = W.base_config(dim, L, coll_op=abi.COLL_VICSEK, species=sp, seed=97, precision=prec)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=98)
+    V[:, 0] += 0.3
+    V[:, 1] += 0.2
+    o = Oracle(cfg, Q, V, U, spid)
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, spid)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(cfg.L[:3], dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    g.close()
+    o.close()

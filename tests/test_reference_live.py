@@ -221,3 +221,26 @@ def test_vicsek_aligned_operators_track_reference(op, dim, L, relax):
     assert r.unexpected_draws() == 0
     np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
     np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
+
+
+@pytest.mark.parametrize("dim,L,act", [(3, (7, 6, 8), 0.7), (3, (6, 6, 6), 0.2), (2, (20, 16), 0.6)])
+def test_vicsek_tracks_reference(dim, L, act):
+    """Vicsek (vicsek, mpc.c:2098-2135: each particle keeps its speed and
+    takes a direction on the cone genrand_cone, rand.c:438-454, builds about
+    the cell's VCM direction) of the oracle against the reference's own, a
+    net flow."""
+    sp = [W._species(mass=1.0, act=act)]
+    cfg = W.base_config(dim, L, coll_op=abi.COLL_VICSEK, species=sp, seed=555)
+    Q, V, U, spid = W.synthetic_state(cfg, 10, seed=556)
+    V[:, 0] += 0.3
+    V[:, 1] += 0.2
+    o = Oracle(cfg, Q, V, U, spid)
+    r = Reference(cfg, Q, V, U, spid)
+    for s in range(1, 6):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
