@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define MPCD_ABI_VERSION 3
+#define MPCD_ABI_VERSION 4
 
 #define MPCD_MAX_SPECIES 10 /* reference MAXSPECI, definitions.h:66 */
 #define MPCD_MAX_WALLS 16

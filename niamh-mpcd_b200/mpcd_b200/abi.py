@@ -5,7 +5,7 @@ checks their sizes against the compiled library's own sizeof().
 """
 import ctypes as C
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 MAX_SPECIES = 10
 MAX_WALLS = 16

@@ -117,6 +117,7 @@ def test_library_checkpoint_read_by_reference(tmp_path, name):
             (cfg.dim, list(cfg.L), cfg.coll_op, cfg.lc, cfg.n_walls, cfg.n_species)
         assert rc.rot_ang == pytest.approx(cfg.rot_ang, abs=tol)
         assert rc.dt == cfg.dt and rc.kbt == cfg.kbt and rc.seed == cfg.seed
+        assert (rc.fricco, rc.relax) == (cfg.fricco, cfg.relax)
         for w in range(cfg.n_walls):
             a, b = rc.walls[w], cfg.walls[w]
             assert list(a.A) == list(b.A) and list(a.Q) == list(b.Q)
@@ -129,6 +130,7 @@ def test_library_checkpoint_read_by_reference(tmp_path, name):
         back = gpu.Checkpoint(path)
         c2 = back.config()
         assert c2.rot_ang == pytest.approx(cfg.rot_ang, abs=tol)
+        assert (c2.fricco, c2.relax) == (cfg.fricco, cfg.relax)
         q2, v2, _, sp2 = back.particles()
         np.testing.assert_allclose(q2, Q, rtol=0, atol=tol)
         np.testing.assert_array_equal(sp2, sp)
@@ -200,3 +202,19 @@ def test_truncated_or_malformed_files_are_rejected(tmp_path):
         gpu.Checkpoint(bad)
     with pytest.raises(gpu.MPCDError, match=r"-1 "):
         gpu.Checkpoint(tmp_path / "missing.dat")
+
+
+def test_operator_parameters_travel_in_checkpoints(tmp_path):
+    """FRICCO (Langevin operators) and TAU (RELAX of the Vicsek-aligned
+    operators) are written where the reference's checkpoint keeps them and
+    read back, with the operator."""
+    cfg = W.base_config(3, (4, 4, 4), coll_op=abi.COLL_VICSEK_LANG, fricco=0.75, relax=0.25,
+                        species=[W._species(mass=1.0, act=0.5)])
+    Q, V, U, sp = W.synthetic_state(cfg, 3, seed=7)
+    ck = gpu.Checkpoint(cfg=cfg)
+    ck.set_particles(Q, V, None, sp)
+    path = tmp_path / "ops.dat"
+    ck.write(path, precise=True)
+    c2 = gpu.Checkpoint(path).config()
+    assert (c2.coll_op, c2.fricco, c2.relax) == (abi.COLL_VICSEK_LANG, 0.75, 0.25)
+    assert c2.species[0].act == 0.5
