@@ -54,6 +54,7 @@ extern "C" {
 #define MPCD_COLL_ARBAXIS 0        /* SRD, random axis                     */
 #define MPCD_COLL_ORTHAXIS 1       /* SRD, random Cartesian axis           */
 #define MPCD_COLL_VICSEK 7         /* Vicsek alignment in the cell (vicsek) */
+#define MPCD_COLL_CHATE 8          /* nematic Vicsek (chate), 2D           */
 #define MPCD_COLL_MPCAT 2          /* Andersen MPC-AT                      */
 #define MPCD_COLL_LANG 4           /* Langevin MPC (langevinMPC)           */
 #define MPCD_COLL_RAT 3            /* Andersen MPC-AT+a                    */

@@ -174,6 +174,8 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         !is_lang_op(cfg->coll_op))
         return MPCD_ERR_UNSUPPORTED;
     if (is_lang_op(cfg->coll_op) && !(cfg->fricco >= 0.0)) return MPCD_ERR_ARG;
+    // Chate's director needs the order tensor's eigenvectors: 2x2 only here
+    if (cfg->coll_op == MPCD_COLL_CHATE && cfg->dim != 2) return MPCD_ERR_UNSUPPORTED;
     dc->dim = cfg->dim;
     dc->op = cfg->coll_op;
     dc->lc = cfg->lc;
@@ -937,7 +939,8 @@ static int per_plan(mpcd_handle *h, bool *wanted = nullptr) {
 }
 
 static int kernel_family(mpcd_handle *h) {
-    if (h->dc.lc) return MPCD_KERNEL_TILE;
+    // the nematic and Chate (the cells' director) run on the tile kernel only
+    if (h->dc.lc || h->dc.op == MPCD_COLL_CHATE) return MPCD_KERNEL_TILE;
     if (h->kernel == MPCD_KERNEL_PERSIST) return MPCD_KERNEL_PERSIST;
     bool wanted = false;
     if (h->kernel == MPCD_KERNEL_AUTO && h->prec == MPCD_PREC_FP64 && per_plan(h, &wanted) > 0 &&

@@ -575,11 +575,12 @@ __device__ __forceinline__ void srd_cell_matrix(const DevCfg &c, uint32_t step,
 }
 
 // True for the operators that need only the cell's VCM and no thermal
-// draws: the SRD rotations, plain or active, and Vicsek.
+// draws: the SRD rotations, plain or active, Vicsek and Chate (which also
+// takes the cell's velocity director).
 __host__ __device__ __forceinline__ bool is_vcm_op(int op) {
     return op == MPCD_COLL_ARBAXIS || op == MPCD_COLL_ORTHAXIS ||
            op == MPCD_COLL_ACT_ARBAXIS || op == MPCD_COLL_ACT_ORTHAXIS ||
-           op == MPCD_COLL_VICSEK;
+           op == MPCD_COLL_VICSEK || op == MPCD_COLL_CHATE;
 }
 
 // Andersen MPC-AT and its Vicsek-aligned form (one weighting of the noise).
@@ -681,31 +682,18 @@ static __device__ __noinline__ double3 active_srd_turn(double act, double3 uu, d
     return make_double3(v[0], v[1], v[2]);
 }
 
-// Vicsek (vicsek, mpc.c:2098-2135): the particle's velocity is redrawn
-// with its speed (length over DIM) and a direction uniform on the cone of
-// half-angle pi (1 - ACT) that genrand_cone (rand.c:438-454) builds about
-// VCMdir = VCM/|VCM| (normCopy over 3 components): a draw on the cone about
-// the x axis (genrand_coneNP, rand.c:397-425: 3D z = u0 (1 - cos t) + cos t,
-// phi = 2 pi u1, (z, sqrt(1-z^2) cos phi, sqrt(1-z^2) sin phi); 2D
-// phi = t (1 - 2 u0), (cos phi, sin phi)), then Rodrigues' rotation about
-// VCMdir x x by the angle between them, as the reference has it.  For
-// |VCM| < 1e-8 the reference leaves VCMdir unset; here the draw keeps the
-// x axis.  The uniforms are the particle's own (MPCD_STREAM_VICSEK).
-static __device__ __noinline__ double3 vicsek_cone(double act, int dim, uint64_t seed,
-                                                   uint32_t replica, uint32_t step,
-                                                   uint32_t pid, double3 uu, double3 vv) {
-    double u[3] = {uu.x, uu.y, dim == 3 ? uu.z : 0.0};
-    const double l = len3_rn(u);
-    const bool dir = fabs(l) >= 1e-8;
-    if (dir)
-        for (int d = 0; d < 3; d++) u[d] = __ddiv_rn(u[d], l);
-    double speed = __dadd_rn(__dmul_rn(vv.x, vv.x), __dmul_rn(vv.y, vv.y));
-    if (dim == 3) speed = __dadd_rn(speed, __dmul_rn(vv.z, vv.z));
-    speed = sqrt(speed);
-    const double theta = __dmul_rn(M_PI, __dsub_rn(1.0, act));
-    double r[3];
+// genrand_cone (rand.c:438-454) with the particle's own uniforms
+// (MPCD_STREAM_VICSEK, from index 0): a direction on the cone of half-angle
+// t about the x axis (genrand_coneNP, rand.c:397-425: 3D z = u0 (1 - cos t)
+// + cos t, phi = 2 pi u1, (z, sqrt(1-z^2) cos phi, sqrt(1-z^2) sin phi); 2D
+// phi = t (1 - 2 u0), (cos phi, sin phi)), then, when `rotate`, Rodrigues'
+// rotation about axis x x-hat by the angle between them, as the reference
+// has it (the cone ends up about the axis mirrored about x).
+__device__ __forceinline__ void cone_draw(double t, int dim, uint64_t seed, uint32_t replica,
+                                          uint32_t step, uint32_t pid, const double *axis,
+                                          bool rotate, double *r) {
     if (dim == 3) {
-        const double ct = cos(theta);
+        const double ct = cos(t);
         const double u0 = mpcd_rng_uniform(seed, replica, step, MPCD_STREAM_VICSEK, pid, 0u);
         const double u1 = mpcd_rng_uniform(seed, replica, step, MPCD_STREAM_VICSEK, pid, 1u);
         const double z = __dadd_rn(__dmul_rn(u0, __dsub_rn(1.0, ct)), ct);
@@ -716,22 +704,104 @@ static __device__ __noinline__ double3 vicsek_cone(double act, int dim, uint64_t
         r[2] = __dmul_rn(sz, sin(phi));
     } else {
         const double u0 = mpcd_rng_uniform(seed, replica, step, MPCD_STREAM_VICSEK, pid, 0u);
-        const double phi = __dmul_rn(theta, __dsub_rn(1.0, __dmul_rn(2.0, u0)));
+        const double phi = __dmul_rn(t, __dsub_rn(1.0, __dmul_rn(2.0, u0)));
         r[0] = cos(phi);
         r[1] = sin(phi);
         r[2] = 0.0;
     }
-    if (dir) {
+    if (rotate) {
         const double x[3] = {1.0, 0.0, 0.0};
         double ax[3];
-        cross3_rn(u, x, ax);
-        double cosa = dot3_rn(u, x);
-        cosa = __ddiv_rn(cosa, len3_rn(u));
+        cross3_rn(axis, x, ax);
+        double cosa = dot3_rn(axis, x);
+        cosa = __ddiv_rn(cosa, len3_rn(axis));
         cosa = __ddiv_rn(cosa, len3_rn(x));
         rodrigues_keep(r, ax, acos(cosa));
     }
+}
+
+// Speed of a velocity (length over DIM).
+__device__ __forceinline__ double speed_dim(double3 v, int dim) {
+    double s = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
+    if (dim == 3) s = __dadd_rn(s, __dmul_rn(v.z, v.z));
+    return sqrt(s);
+}
+
+// Vicsek (vicsek, mpc.c:2098-2135): the particle keeps its speed and takes a
+// direction on the cone of half-angle pi (1 - ACT) about VCMdir = VCM/|VCM|
+// (normCopy over 3 components).  For |VCM| < 1e-8 the reference leaves
+// VCMdir unset; here the draw keeps the x axis.  Out of line and by value.
+static __device__ __noinline__ double3 vicsek_cone(double act, int dim, uint64_t seed,
+                                                   uint32_t replica, uint32_t step,
+                                                   uint32_t pid, double3 uu, double3 vv) {
+    double u[3] = {uu.x, uu.y, dim == 3 ? uu.z : 0.0};
+    const double l = len3_rn(u);
+    const bool dir = fabs(l) >= 1e-8;
+    if (dir)
+        for (int d = 0; d < 3; d++) u[d] = __ddiv_rn(u[d], l);
+    const double speed = speed_dim(vv, dim);
+    double r[3];
+    cone_draw(__dmul_rn(M_PI, __dsub_rn(1.0, act)), dim, seed, replica, step, pid, u, dir, r);
     return make_double3(__dmul_rn(r[0], speed), __dmul_rn(r[1], speed),
                         dim == 3 ? __dmul_rn(r[2], speed) : vv.z);
+}
+
+// Chate (chate, mpc.c:2153-2186): the particle keeps its speed and takes a
+// direction on the cone of half-angle pi/2 (1 - ACT) about the cell's
+// director DIR (used as it is), times a random sign genrand_pmOne
+// (rand.c:378-382: -1 for a uniform <= 0.5), the particle's next uniform.
+static __device__ __noinline__ double3 chate_cone(double act, int dim, uint64_t seed,
+                                                  uint32_t replica, uint32_t step, uint32_t pid,
+                                                  double3 dd, double3 vv) {
+    const double dir[3] = {dd.x, dd.y, dim == 3 ? dd.z : 0.0};
+    const double speed = speed_dim(vv, dim);
+    double r[3];
+    cone_draw(__dmul_rn(__dmul_rn(0.5, M_PI), __dsub_rn(1.0, act)), dim, seed, replica, step,
+              pid, dir, true, r);
+    const double pm = mpcd_rng_uniform(seed, replica, step, MPCD_STREAM_VICSEK, pid,
+                                       dim == 3 ? 2u : 1u) <= 0.5 ? -1.0 : 1.0;
+    const double f = __dmul_rn(pm, speed);
+    return make_double3(__dmul_rn(r[0], f), __dmul_rn(r[1], f),
+                        dim == 3 ? __dmul_rn(r[2], f) : vv.z);
+}
+
+// 2x2 eigen-decomposition of a symmetric order tensor (s00, s01; s01, s11)
+// as eigenvalues2x2 and eigenvectors2x2 do it (mtools.c:1225-1300), with
+// their special cases: returns the largest eigenvalue, (e0, e1) its
+// eigenvector (the director).
+__device__ __forceinline__ double order_eigen2(double s00, double s01, double s11, double &e0,
+                                              double &e1) {
+    const double s10 = s01;
+    double det = s00 * s11 - s10 * s01;
+    double tr = s00 + s11;
+    double sq = sqrt(tr * tr * 0.25 - det);
+    double ev0 = tr * 0.5 + sq;
+    e0 = 0.0;
+    e1 = 0.0;
+    if (fabs(s10 - 0.0) >= kTol) {
+        e0 = ev0 - s11;
+        e1 = s10;
+        double l = sqrt(e0 * e0 + e1 * e1);
+        if (fabs(l) >= kTol) {
+            e0 /= l;
+            e1 /= l;
+        }
+    } else if (fabs(s01 - 0.0) >= kTol) {
+        e0 = s01;
+        e1 = ev0 - s00;
+        double l = sqrt(e0 * e0 + e1 * e1);
+        if (fabs(l) >= kTol) {
+            e0 /= l;
+            e1 /= l;
+        }
+    } else if (fabs(s00 - s11) <= kTol) {
+        e0 = sqrt(2.);
+        e1 = e0;
+    } else {
+        e0 = 1.0;
+        e1 = 0.0;
+    }
+    return ev0;
 }
 
 // Inverse of a symmetric-or-not 3x3 matrix by adjugate / determinant.

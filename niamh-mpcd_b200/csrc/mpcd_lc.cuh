@@ -185,35 +185,8 @@ __device__ void lc_cell_moments(const DevCfg &c, const typename T::State &a, con
         s11 *= cc * 2.0 * pinv;
         s00 -= cc;
         s11 -= cc;
-        const double s10 = s01;
-        double det = s00 * s11 - s10 * s01;
-        double tr = s00 + s11;
-        double sq = sqrt(tr * tr * 0.25 - det);
-        double ev0 = tr * 0.5 + sq;
-        double e0 = 0.0, e1 = 0.0;
-        if (fabs(s10 - 0.0) >= kTol) {
-            e0 = ev0 - s11;
-            e1 = s10;
-            double l = sqrt(e0 * e0 + e1 * e1);
-            if (fabs(l) >= kTol) {
-                e0 /= l;
-                e1 /= l;
-            }
-        } else if (fabs(s01 - 0.0) >= kTol) {
-            e0 = s01;
-            e1 = ev0 - s00;
-            double l = sqrt(e0 * e0 + e1 * e1);
-            if (fabs(l) >= kTol) {
-                e0 /= l;
-                e1 /= l;
-            }
-        } else if (fabs(s00 - s11) <= kTol) {
-            e0 = sqrt(2.);
-            e1 = e0;
-        } else {
-            e0 = 1.0;
-            e1 = 0.0;
-        }
+        double e0, e1;
+        const double ev0 = order_eigen2(s00, s01, s11, e0, e1);
         lc.dir[2 * cell] = e0;
         lc.dir[2 * cell + 1] = e1;
         lc.S[cell] = ev0 > 1.0 ? 1.0 : ev0;

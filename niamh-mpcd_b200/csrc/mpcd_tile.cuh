@@ -495,7 +495,36 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                 for (int d = 0; d < 3; d++) s_u[3 * lc + d] = u[d];
             }
             if (!andersen) {
-                if (lead && pop > 1 && c.op != MPCD_COLL_VICSEK)
+                if (DIM == 2 && c.op == MPCD_COLL_CHATE) {
+                    // the director of the normalised velocities (tensOrderParam
+                    // with addToTensOrderParamVel, lc.c:1103-1148; localPROP,
+                    // mpc.c:176-206), 2D; normCopy leaves a velocity shorter
+                    // than 1e-8 unset in the reference, zero here
+                    double s00 = 0.0, s01 = 0.0, s11 = 0.0;
+                    for (int j = j0 + sub; j < j1; j += kCellLanes) {
+                        double v[3] = {0, 0, 0};
+                        T::vel(s_rec[j], v);
+                        const double l = sqrt(v[0] * v[0] + v[1] * v[1]);
+                        const double o0 = fabs(l) >= 1e-8 ? v[0] / l : 0.0;
+                        const double o1 = fabs(l) >= 1e-8 ? v[1] / l : 0.0;
+                        s00 += o0 * o0;
+                        s01 += o0 * o1;
+                        s11 += o1 * o1;
+                    }
+                    s00 = group_sum(s00);
+                    s01 = group_sum(s01);
+                    s11 = group_sum(s11);
+                    if (lead && pop > 1) {
+                        const double cc = 1. / (2.0 - 1.), pinv = 1. / (double)pop;
+                        s00 = s00 * (cc * 2.0 * pinv) - cc;
+                        s01 = s01 * (cc * 2.0 * pinv);
+                        s11 = s11 * (cc * 2.0 * pinv) - cc;
+                        double e0, e1;
+                        order_eigen2(s00, s01, s11, e0, e1);
+                        s_R[9 * lc] = (VT)e0;
+                        s_R[9 * lc + 1] = (VT)e1;
+                    }
+                } else if (lead && pop > 1 && c.op != MPCD_COLL_VICSEK)
                     srd_cell_matrix<DIM, VT>(c, sa.step, (uint32_t)cell, &s_R[9 * lc]);
                 continue;
             }
@@ -567,6 +596,15 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                     const double3 t = vicsek_cone(
                         c.act[sp], DIM, c.seed, c.replica, sa.step, T::pid(r),
                         make_double3(s_u[3 * lc], s_u[3 * lc + 1], s_u[3 * lc + 2]),
+                        make_double3(v[0], v[1], v[2]));
+                    const double nv[3] = {t.x, t.y, t.z};
+                    T::set_vel(r, nv);
+                } else if (DIM == 2 && !andersen && c.op == MPCD_COLL_CHATE) {
+                    double v[3] = {0, 0, 0};
+                    T::vel(r, v);
+                    const double3 t = chate_cone(
+                        c.act[sp], DIM, c.seed, c.replica, sa.step, T::pid(r),
+                        make_double3((double)s_R[9 * lc], (double)s_R[9 * lc + 1], 0.0),
                         make_double3(v[0], v[1], v[2]));
                     const double nv[3] = {t.x, t.y, t.z};
                     T::set_vel(r, nv);

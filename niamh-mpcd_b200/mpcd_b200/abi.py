@@ -21,6 +21,7 @@ ERR_SIZE = -6
 COLL_ARBAXIS = 0
 COLL_ORTHAXIS = 1
 COLL_VICSEK = 7
+COLL_CHATE = 8
 COLL_MPCAT = 2
 COLL_LANG = 4
 COLL_RAT = 3

@@ -577,6 +577,37 @@ static void rodrigues_keep(double *v, double *ax, double t) {
     double now = len3(v, 3);
     for (int d = 0; d < 3; d++) v[d] *= (old / now);
 }
+/* genrand_cone (rand.c:438-454) with particle i's own uniforms
+ * (MPCD_STREAM_VICSEK from index 0): a draw on the cone of half-angle t
+ * about x (genrand_coneNP, rand.c:397-425), then, when `rotate`, Rodrigues'
+ * rotation about axis x x-hat by the angle between them. */
+static void cone_draw(const oracle_t *o, int i, uint32_t step, double t, const double *axis,
+                      int rotate, double *r) {
+    double u0 = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
+                                 (uint32_t)i, 0u);
+    r[0] = r[1] = r[2] = 0.0;
+    if (o->dim == 3) {
+        double ct = cos(t), z = u0 * (1.0 - ct) + ct;
+        double phi = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
+                                      (uint32_t)i, 1u) * 2.0 * MPCD_PI;
+        r[0] = z;
+        r[1] = sqrt(1.0 - z * z) * cos(phi);
+        r[2] = sqrt(1.0 - z * z) * sin(phi);
+    } else {
+        double phi = t * (1. - 2. * u0);
+        r[0] = cos(phi);
+        r[1] = sin(phi);
+    }
+    if (rotate) {
+        double x[3] = {1.0, 0.0, 0.0}, ax[3];
+        cross3(axis, x, ax);
+        double cosa = dot3(axis, x, 3);
+        cosa /= len3(axis, 3);
+        cosa /= len3(x, 3);
+        rodrigues_keep(r, ax, acos(cosa));
+    }
+}
+
 static void collide_vicsek(oracle_t *o, int c, uint32_t step) {
     int dim = o->dim;
     double u[3] = {0, 0, 0};
@@ -587,32 +618,50 @@ static void collide_vicsek(oracle_t *o, int c, uint32_t step) {
         for (int d = 0; d < 3; d++) u[d] = u[d] / l;
     for (int j = o->start[c]; j < o->start[c + 1]; j++) {
         int i = o->list[j];
-        double *v = &o->V[3 * i];
+        double *v = &o->V[3 * i], r[3];
         double speed = len3(v, dim), theta = MPCD_PI * (1.0 - o->cfg.species[o->spid[i]].act);
-        double r[3] = {0, 0, 0};
-        double u0 = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
-                                     (uint32_t)i, 0u);
-        if (dim == 3) {
-            double ct = cos(theta), z = u0 * (1.0 - ct) + ct;
-            double phi = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
-                                          (uint32_t)i, 1u) * 2.0 * MPCD_PI;
-            r[0] = z;
-            r[1] = sqrt(1.0 - z * z) * cos(phi);
-            r[2] = sqrt(1.0 - z * z) * sin(phi);
-        } else {
-            double phi = theta * (1. - 2. * u0);
-            r[0] = cos(phi);
-            r[1] = sin(phi);
-        }
-        if (dir) {
-            double x[3] = {1.0, 0.0, 0.0}, ax[3];
-            cross3(u, x, ax);
-            double cosa = dot3(u, x, 3);
-            cosa /= len3(u, 3);
-            cosa /= len3(x, 3);
-            rodrigues_keep(r, ax, acos(cosa));
-        }
+        cone_draw(o, i, step, theta, u, dir, r);
         for (int d = 0; d < dim; d++) v[d] = r[d] * speed;
+    }
+}
+
+/* Chate (chate, mpc.c:2151-2186), 2D: the cell's director is the leading
+ * eigenvector of the order tensor of the normalised velocities
+ * (tensOrderParam with addToTensOrderParamVel, lc.c:1103-1148; localPROP,
+ * mpc.c:176-206; normCopy leaves a velocity shorter than 1e-8 unset, zero
+ * here); each particle keeps its speed and takes a direction on the cone of
+ * half-angle pi/2 (1 - ACT) about the director, times genrand_pmOne
+ * (rand.c:378-382), its next uniform. */
+static void collide_chate(oracle_t *o, int c, uint32_t step) {
+    int s = o->start[c], e = o->start[c + 1];
+    double Sm[4] = {0, 0, 0, 0}, cc = 1. / (2.0 - 1.), popinv = 1. / (double)(e - s);
+    for (int j = s; j < e; j++) {
+        const double *v = &o->V[3 * o->list[j]];
+        double l = len3(v, 2), U[2] = {0.0, 0.0};
+        if (fabs(l - 0.0) >= 1e-8) {
+            U[0] = v[0] / l;
+            U[1] = v[1] / l;
+        }
+        Sm[0] += U[0] * U[0];
+        Sm[1] += U[0] * U[1];
+        Sm[3] += U[1] * U[1];
+    }
+    Sm[0] *= cc * 2.0 * popinv;
+    Sm[1] *= cc * 2.0 * popinv;
+    Sm[3] *= cc * 2.0 * popinv;
+    Sm[0] -= cc;
+    Sm[3] -= cc;
+    Sm[2] = Sm[1];
+    double dir[3] = {0, 0, 0};
+    eigen2(Sm, dir);
+    for (int j = s; j < e; j++) {
+        int i = o->list[j];
+        double *v = &o->V[3 * i], r[3];
+        double speed = len3(v, 2);
+        cone_draw(o, i, step, 0.5 * MPCD_PI * (1.0 - o->cfg.species[o->spid[i]].act), dir, 1, r);
+        double pm = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
+                                     (uint32_t)i, 1u) <= 0.5 ? -1.0 : 1.0;
+        for (int d = 0; d < 2; d++) v[d] = r[d] * (pm * speed);
     }
 }
 
@@ -1196,6 +1245,8 @@ int oracle_step(oracle_t *o, uint32_t step) {
             collide_srd(o, c, step);
         else if (op == MPCD_COLL_VICSEK)
             collide_vicsek(o, c, step);
+        else if (op == MPCD_COLL_CHATE && dim == 2)
+            collide_chate(o, c, step);
         else if (op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT)
             collide_mpcat(o, c, step);
         else if (op == MPCD_COLL_LANG || op == MPCD_COLL_VICSEK_LANG)

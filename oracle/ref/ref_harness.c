@@ -680,6 +680,10 @@ double genrand_real(void) {
      * mpc.c:1289) and then one for the rotation sign, which
      * (long)genrand_real() truncates to 0 (mpc.c:1291) */
     if (g_phase == PH_COLLIDE) {
+        /* chate's genrand_pmOne: the last cone particle's next uniform */
+        if (g_rtech == CHATE)
+            return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_VICSEK,
+                                    (uint32_t)g_pid, g_k++);
         if ((g_rtech == ORTHAXIS || g_rtech == ACT_ORTHAXIS) && g_ccount++ == 0)
             return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_ORTH,
                                     (uint32_t)g_cell, 0u);

@@ -396,3 +396,40 @@ def test_vicsek_matches_the_oracle(prec, kernel, dim):
     assert st.escaped == 0 and st.nonfinite == 0
     g.close()
     o.close()
+
+
+@pytest.mark.parametrize("prec,kernel", [(abi.PREC_FP64, abi.KERNEL_TILE),
+                                         (abi.PREC_FP64, abi.KERNEL_PERSIST),
+                                         (abi.PREC_MIXED, abi.KERNEL_AUTO)])
+def test_chate_matches_the_oracle(prec, kernel):
+    """Chate (chate, mpc.c:2151-2186) against the oracle (pinned to the
+    reference), 2D: the cells' director from the normalised velocities, a
+    cone draw about it and a random sign.  A persistent-kernel request runs
+    on the tile kernel, which holds the cells' director."""
+    L = (12, 10)
+    sp = [W._species(mass=1.0, act=0.6)]
+    cfg = W.base_config(2, L, coll_op=abi.COLL_CHATE, species=sp, seed=99)
+    cfgp = W.base_config(2, L, coll_op=abi.COLL_CHATE, species=sp, seed=99, precision=prec)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=100)
+    V[:, 0] += 0.3
+    o = Oracle(cfg, Q, V, U, spid)
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, spid)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(cfg.L[:3], dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    g.close()
+    o.close()
+
+
+def test_chate_in_3d_is_refused():
+    """The 3D director needs the reference's 3x3 eigensystem, not built."""
+    cfg = W.base_config(3, (4, 4, 4), coll_op=abi.COLL_CHATE)
+    with pytest.raises(MPCDError):
+        Solver(cfg)

@@ -244,3 +244,24 @@ def test_vicsek_tracks_reference(dim, L, act):
     assert r.unexpected_draws() == 0
     np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
     np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
+
+
+@pytest.mark.parametrize("L,act,seed", [((20, 16), 0.6, 565), ((16, 18), 0.2, 566)])
+def test_chate_tracks_reference(L, act, seed):
+    """Chate (chate, mpc.c:2151-2186: the cells' director from the order
+    tensor of the normalised velocities, then a cone draw about it with a
+    random sign) of the oracle against the reference's own, 2D."""
+    sp = [W._species(mass=1.0, act=act)]
+    cfg = W.base_config(2, L, coll_op=abi.COLL_CHATE, species=sp, seed=seed)
+    Q, V, U, spid = W.synthetic_state(cfg, 10, seed=seed + 1)
+    V[:, 0] += 0.3
+    o = Oracle(cfg, Q, V, U, spid)
+    r = Reference(cfg, Q, V, U, spid)
+    for s in range(1, 6):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
