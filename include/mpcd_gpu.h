@@ -163,7 +163,12 @@ int mpcd_abi_version(void);
 
 /* Create a handle on the current CUDA device.  Replaces the reference's
  * readJson (read.c:973) + initializeSIM (init.c:2048) state set-up; the
- * particles are supplied separately by mpcd_upload_state. */
+ * particles are supplied separately by mpcd_upload_state.
+ * MPCD_ERR_UNSUPPORTED for a collision operator outside MPCD_COLL_*, for
+ * MPCD_COLL_CHATE or a nematic outside 2D, and for active SRD whose species
+ * differ in activity (the reference takes the cell's activity from the last
+ * particle of its list, an order set by its re-binning history);
+ * MPCD_ERR_ARG for a negative fricco with a Langevin operator. */
 int mpcd_create(const mpcd_config *cfg, mpcd_handle **out);
 
 /* Release all device memory of the handle. */
