@@ -334,6 +334,39 @@ __device__ __forceinline__ double block_sum256(double v, double *red) {
     return t;  // valid in thread 0
 }
 
+// Chate's cell director, 2D (tensOrderParam with addToTensOrderParamVel,
+// lc.c:1103-1148; localPROP, mpc.c:176-206): the order tensor of the
+// normalised velocities, summed by the cell's lane group (every lane of the
+// warp calls it), its leading eigenvector written by the lead lane to
+// R[0..1].  normCopy leaves a velocity shorter than 1e-8 unset in the
+// reference, zero here.  Out of line: only Chate reaches it.
+template <class T>
+static __device__ __noinline__ void chate_director(const typename T::Rec *rec, int j, int j1,
+                                                   bool lead, int pop, typename T::VT *R) {
+    double s00 = 0.0, s01 = 0.0, s11 = 0.0;
+    for (; j < j1; j += kCellLanes) {
+        double v[3] = {0, 0, 0};
+        T::vel(rec[j], v);
+        const double l = sqrt(v[0] * v[0] + v[1] * v[1]);
+        const double o0 = fabs(l) >= 1e-8 ? v[0] / l : 0.0;
+        const double o1 = fabs(l) >= 1e-8 ? v[1] / l : 0.0;
+        s00 += o0 * o0;
+        s01 += o0 * o1;
+        s11 += o1 * o1;
+    }
+    s00 = group_sum(s00);
+    s01 = group_sum(s01);
+    s11 = group_sum(s11);
+    if (lead) {
+        const double cc = 1. / (2.0 - 1.), pinv = 1. / (double)pop;
+        double e0, e1;
+        order_eigen2(s00 * (cc * 2.0 * pinv) - cc, s01 * (cc * 2.0 * pinv),
+                     s11 * (cc * 2.0 * pinv) - cc, e0, e1);
+        R[0] = (typename T::VT)e0;
+        R[1] = (typename T::VT)e1;
+    }
+}
+
 template <int DIM, class T, int MODE>
 __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
                                               typename T::State a, typename T::State b,
@@ -496,34 +529,7 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             }
             if (!andersen) {
                 if (DIM == 2 && c.op == MPCD_COLL_CHATE) {
-                    // the director of the normalised velocities (tensOrderParam
-                    // with addToTensOrderParamVel, lc.c:1103-1148; localPROP,
-                    // mpc.c:176-206), 2D; normCopy leaves a velocity shorter
-                    // than 1e-8 unset in the reference, zero here
-                    double s00 = 0.0, s01 = 0.0, s11 = 0.0;
-                    for (int j = j0 + sub; j < j1; j += kCellLanes) {
-                        double v[3] = {0, 0, 0};
-                        T::vel(s_rec[j], v);
-                        const double l = sqrt(v[0] * v[0] + v[1] * v[1]);
-                        const double o0 = fabs(l) >= 1e-8 ? v[0] / l : 0.0;
-                        const double o1 = fabs(l) >= 1e-8 ? v[1] / l : 0.0;
-                        s00 += o0 * o0;
-                        s01 += o0 * o1;
-                        s11 += o1 * o1;
-                    }
-                    s00 = group_sum(s00);
-                    s01 = group_sum(s01);
-                    s11 = group_sum(s11);
-                    if (lead && pop > 1) {
-                        const double cc = 1. / (2.0 - 1.), pinv = 1. / (double)pop;
-                        s00 = s00 * (cc * 2.0 * pinv) - cc;
-                        s01 = s01 * (cc * 2.0 * pinv);
-                        s11 = s11 * (cc * 2.0 * pinv) - cc;
-                        double e0, e1;
-                        order_eigen2(s00, s01, s11, e0, e1);
-                        s_R[9 * lc] = (VT)e0;
-                        s_R[9 * lc + 1] = (VT)e1;
-                    }
+                    chate_director<T>(s_rec, j0 + sub, j1, lead && pop > 1, pop, &s_R[9 * lc]);
                 } else if (lead && pop > 1 && c.op != MPCD_COLL_VICSEK)
                     srd_cell_matrix<DIM, VT>(c, sa.step, (uint32_t)cell, &s_R[9 * lc]);
                 continue;
