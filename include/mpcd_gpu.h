@@ -62,6 +62,7 @@ extern "C" {
 #define MPCD_COLL_ACT_ORTHAXIS 10  /* active SRD, random Cartesian axis    */
 #define MPCD_COLL_VICSEK_MPCAT 11  /* MPC-AT with Vicsek alignment          */
 #define MPCD_COLL_VICSEK_LANG 12   /* Langevin MPC with Vicsek alignment    */
+#define MPCD_COLL_CHATE_MPCAT 13   /* MPC-AT with Chate alignment, 2D       */
 #define MPCD_COLL_DIPOLE_DIR_SUM 16 /* nematic, dipole activity summed    */
 #define MPCD_COLL_DIPOLE_DIR_AV 17  /* nematic, dipole activity averaged  */
 
@@ -165,9 +166,10 @@ int mpcd_abi_version(void);
  * readJson (read.c:973) + initializeSIM (init.c:2048) state set-up; the
  * particles are supplied separately by mpcd_upload_state.
  * MPCD_ERR_UNSUPPORTED for a collision operator outside MPCD_COLL_*, for
- * MPCD_COLL_CHATE or a nematic outside 2D, and for active SRD whose species
- * differ in activity (the reference takes the cell's activity from the last
- * particle of its list, an order set by its re-binning history);
+ * MPCD_COLL_CHATE, MPCD_COLL_CHATE_MPCAT or a nematic outside 2D, and for
+ * active SRD whose species differ in activity (the reference takes the
+ * cell's activity from the last particle of its list, an order set by its
+ * re-binning history);
  * MPCD_ERR_ARG for a negative fricco with a Langevin operator. */
 int mpcd_create(const mpcd_config *cfg, mpcd_handle **out);
 

@@ -175,7 +175,9 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
         return MPCD_ERR_UNSUPPORTED;
     if (is_lang_op(cfg->coll_op) && !(cfg->fricco >= 0.0)) return MPCD_ERR_ARG;
     // Chate's director needs the order tensor's eigenvectors: 2x2 only here
-    if (cfg->coll_op == MPCD_COLL_CHATE && cfg->dim != 2) return MPCD_ERR_UNSUPPORTED;
+    if ((cfg->coll_op == MPCD_COLL_CHATE || cfg->coll_op == MPCD_COLL_CHATE_MPCAT) &&
+        cfg->dim != 2)
+        return MPCD_ERR_UNSUPPORTED;
     dc->dim = cfg->dim;
     dc->op = cfg->coll_op;
     dc->lc = cfg->lc;
@@ -207,8 +209,10 @@ static int build_devcfg(const mpcd_config *cfg, DevCfg *dc) {
                 dc->lang_b[s] = 1.0;
             }
         }
-        // the Vicsek-aligned operators apply no damping (mpc.c:2204-2480)
-        dc->damp[s] = is_vicsek_op(cfg->coll_op) ? 0.0 : cfg->species[s].damp;
+        // the Vicsek- and Chate-aligned operators apply no damping (mpc.c:2204-2480)
+        dc->damp[s] = is_vicsek_op(cfg->coll_op) || cfg->coll_op == MPCD_COLL_CHATE_MPCAT
+                          ? 0.0
+                          : cfg->species[s].damp;
         dc->rfc[s] = cfg->species[s].rfc;
         dc->tumble[s] = cfg->species[s].tumble;
         dc->chihi[s] = cfg->species[s].chihi;
@@ -940,7 +944,8 @@ static int per_plan(mpcd_handle *h, bool *wanted = nullptr) {
 
 static int kernel_family(mpcd_handle *h) {
     // the nematic and Chate (the cells' director) run on the tile kernel only
-    if (h->dc.lc || h->dc.op == MPCD_COLL_CHATE) return MPCD_KERNEL_TILE;
+    if (h->dc.lc || h->dc.op == MPCD_COLL_CHATE || h->dc.op == MPCD_COLL_CHATE_MPCAT)
+        return MPCD_KERNEL_TILE;
     if (h->kernel == MPCD_KERNEL_PERSIST) return MPCD_KERNEL_PERSIST;
     bool wanted = false;
     if (h->kernel == MPCD_KERNEL_AUTO && h->prec == MPCD_PREC_FP64 && per_plan(h, &wanted) > 0 &&

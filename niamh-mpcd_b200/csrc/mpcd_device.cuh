@@ -585,7 +585,7 @@ __host__ __device__ __forceinline__ bool is_vcm_op(int op) {
 
 // Andersen MPC-AT and its Vicsek-aligned form (one weighting of the noise).
 __host__ __device__ __forceinline__ bool is_mpcat_op(int op) {
-    return op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT;
+    return op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT || op == MPCD_COLL_CHATE_MPCAT;
 }
 // Langevin MPC and its Vicsek-aligned form (the plain mean of the noise).
 __host__ __device__ __forceinline__ bool is_lang_op(int op) {

@@ -341,8 +341,8 @@ __device__ __forceinline__ double block_sum256(double v, double *red) {
 // R[0..1].  normCopy leaves a velocity shorter than 1e-8 unset in the
 // reference, zero here.  Out of line: only Chate reaches it.
 template <class T>
-static __device__ __noinline__ void chate_director(const typename T::Rec *rec, int j, int j1,
-                                                   bool lead, int pop, typename T::VT *R) {
+static __device__ __noinline__ double2 chate_director(const typename T::Rec *rec, int j, int j1,
+                                                     int pop) {
     double s00 = 0.0, s01 = 0.0, s11 = 0.0;
     for (; j < j1; j += kCellLanes) {
         double v[3] = {0, 0, 0};
@@ -357,13 +357,37 @@ static __device__ __noinline__ void chate_director(const typename T::Rec *rec, i
     s00 = group_sum(s00);
     s01 = group_sum(s01);
     s11 = group_sum(s11);
-    if (lead) {
-        const double cc = 1. / (2.0 - 1.), pinv = 1. / (double)pop;
-        double e0, e1;
-        order_eigen2(s00 * (cc * 2.0 * pinv) - cc, s01 * (cc * 2.0 * pinv),
-                     s11 * (cc * 2.0 * pinv) - cc, e0, e1);
-        R[0] = (typename T::VT)e0;
-        R[1] = (typename T::VT)e1;
+    const double cc = 1. / (2.0 - 1.), pinv = 1. / (double)pop;
+    double e0, e1;
+    order_eigen2(s00 * (cc * 2.0 * pinv) - cc, s01 * (cc * 2.0 * pinv), s11 * (cc * 2.0 * pinv) - cc,
+                 e0, e1);
+    return make_double2(e0, e1);
+}
+
+// The active velocities of MPC-AT with Chate alignment (chateAndersenMPC,
+// mpc.c:2300-2408), 2D: a particle whose species has |ACT| >= 1e-8 (fneq)
+// takes AV = pmOne RELAX (ACT - |V|) DIR, pmOne from its own uniform
+// (genrand_pmOne, rand.c:378-382; MPCD_STREAM_VICSEK, index 0); AV joins its
+// thermal velocity, so that the cell's mass-weighted mean of the two is
+// RS + AS and the update VCM + RV - RS + AV - AS is the MPC-AT one.  Every
+// lane of the warp calls it; each lane touches only its own particles.
+template <class T>
+static __device__ __noinline__ void chate_active(const DevCfg &c, const typename T::Rec *rec,
+                                                 const unsigned char *spv, typename T::VT *rv,
+                                                 int j, int j1, int pop, uint32_t step) {
+    const double2 dir = chate_director<T>(rec, j, j1, pop);
+    for (; j < j1; j += kCellLanes) {
+        const int sp = spv ? spv[j] : 0;
+        const double act = c.act[sp];
+        if (!(fabs(act - 0.0) >= 1e-8)) continue;
+        double v[3] = {0, 0, 0};
+        T::vel(rec[j], v);
+        const double speed = sqrt(v[0] * v[0] + v[1] * v[1]);
+        const double pm = mpcd_rng_uniform(c.seed, c.replica, step, MPCD_STREAM_VICSEK,
+                                           T::pid(rec[j]), 0u) <= 0.5 ? -1.0 : 1.0;
+        const double f = pm * c.relax * (act - speed);
+        rv[3 * j] = (typename T::VT)((double)rv[3 * j] + f * dir.x);
+        rv[3 * j + 1] = (typename T::VT)((double)rv[3 * j + 1] + f * dir.y);
     }
 }
 
@@ -529,7 +553,11 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             }
             if (!andersen) {
                 if (DIM == 2 && c.op == MPCD_COLL_CHATE) {
-                    chate_director<T>(s_rec, j0 + sub, j1, lead && pop > 1, pop, &s_R[9 * lc]);
+                    const double2 dir = chate_director<T>(s_rec, j0 + sub, j1, pop);
+                    if (lead && pop > 1) {
+                        s_R[9 * lc] = (VT)dir.x;
+                        s_R[9 * lc + 1] = (VT)dir.y;
+                    }
                 } else if (lead && pop > 1 && c.op != MPCD_COLL_VICSEK)
                     srd_cell_matrix<DIM, VT>(c, sa.step, (uint32_t)cell, &s_R[9 * lc]);
                 continue;
@@ -537,6 +565,8 @@ __global__ void __launch_bounds__(256) k_tile(const __grid_constant__ DevCfg c,
             // Andersen: the cell's sum of thermal velocities (every group of
             // the warp takes part in the shuffles; a group's own cell may
             // have fewer than two particles and ignore the result)
+            if (DIM == 2 && c.op == MPCD_COLL_CHATE_MPCAT)
+                chate_active<T>(c, s_rec, s_sp, s_rv, j0 + sub, j1, pop, sa.step);
             double rs[3] = {0, 0, 0};
             for (int j = j0 + sub; j < j1; j += kCellLanes) {
                 double m = plain ? 1.0 : c.mass[s_sp ? s_sp[j] : 0];

@@ -29,6 +29,7 @@ COLL_ACT_ARBAXIS = 9
 COLL_ACT_ORTHAXIS = 10
 COLL_VICSEK_MPCAT = 11
 COLL_VICSEK_LANG = 12
+COLL_CHATE_MPCAT = 13
 COLL_DIPOLE_DIR_SUM = 16
 COLL_DIPOLE_DIR_AV = 17
 

@@ -632,7 +632,7 @@ static void collide_vicsek(oracle_t *o, int c, uint32_t step) {
  * here); each particle keeps its speed and takes a direction on the cone of
  * half-angle pi/2 (1 - ACT) about the director, times genrand_pmOne
  * (rand.c:378-382), its next uniform. */
-static void collide_chate(oracle_t *o, int c, uint32_t step) {
+static void chate_dir(const oracle_t *o, int c, double *dir) {
     int s = o->start[c], e = o->start[c + 1];
     double Sm[4] = {0, 0, 0, 0}, cc = 1. / (2.0 - 1.), popinv = 1. / (double)(e - s);
     for (int j = s; j < e; j++) {
@@ -652,8 +652,14 @@ static void collide_chate(oracle_t *o, int c, uint32_t step) {
     Sm[0] -= cc;
     Sm[3] -= cc;
     Sm[2] = Sm[1];
-    double dir[3] = {0, 0, 0};
+    dir[0] = dir[1] = dir[2] = 0.0;
     eigen2(Sm, dir);
+}
+
+static void collide_chate(oracle_t *o, int c, uint32_t step) {
+    int s = o->start[c], e = o->start[c + 1];
+    double dir[3];
+    chate_dir(o, c, dir);
     for (int j = s; j < e; j++) {
         int i = o->list[j];
         double *v = &o->V[3 * i], r[3];
@@ -680,27 +686,53 @@ static void vicsek_dir(int dim, const double *u, double *dir) {
         for (int d = 0; d < dim; d++) dir[d] = u[d] / l;
 }
 
+/* The active velocity of MPC-AT with Chate alignment (chateAndersenMPC,
+ * mpc.c:2300-2408), 2D: for |ACT| >= 1e-8 (fneq), AV = pmOne RELAX
+ * (ACT - |V|) DIR with pmOne the particle's uniform (genrand_pmOne,
+ * rand.c:378-382); returns whether the particle is active.  The update is
+ * VCM + RV - RS + AV - AS with AS the cell's mass-weighted mean of AV, and
+ * no damping. */
+static int chate_av(const oracle_t *o, int i, uint32_t step, const double *dir, double *av) {
+    double act = o->cfg.species[o->spid[i]].act;
+    av[0] = av[1] = av[2] = 0.0;
+    if (!(fabs(act - 0.0) >= 1e-8)) return 0;
+    double speed = len3(&o->V[3 * i], 2);
+    double pm = mpcd_rng_uniform(o->cfg.seed, o->cfg.replica, step, MPCD_STREAM_VICSEK,
+                                 (uint32_t)i, 0u) <= 0.5 ? -1.0 : 1.0;
+    for (int d = 0; d < 2; d++) av[d] = pm * o->cfg.relax * (act - speed) * dir[d];
+    return 1;
+}
+
 static void collide_mpcat(oracle_t *o, int c, uint32_t step) {
     int dim = o->dim, s = o->start[c], e = o->start[c + 1];
     double RS[3] = {0, 0, 0};
     const double *u = &o->vcm[3 * c];
     const int vic = vicsek_op(o->cfg.coll_op);
-    double dir[3];
+    const int cha = o->cfg.coll_op == MPCD_COLL_CHATE_MPCAT;
+    double dir[3], cdir[3] = {0, 0, 0}, AS[3] = {0, 0, 0};
     vicsek_dir(dim, u, dir);
+    if (cha) chate_dir(o, c, cdir);
     for (int j = s; j < e; j++) {
         int i = o->list[j];
-        double rv[3];
+        double rv[3], av[3];
         thermal_draw(o, i, step, rv);
         double m = o->cfg.species[o->spid[i]].mass;
         for (int d = 0; d < dim; d++) RS[d] += m * rv[d];
+        if (cha && chate_av(o, i, step, cdir, av))
+            for (int d = 0; d < dim; d++) AS[d] += m * av[d];
     }
     for (int d = 0; d < dim; d++) RS[d] /= o->mass[c];
+    for (int d = 0; d < dim; d++) AS[d] /= o->mass[c];
     for (int j = s; j < e; j++) {
         int i = o->list[j];
         double rv[3];
         thermal_draw(o, i, step, rv);
         const mpcd_species *sp = &o->cfg.species[o->spid[i]];
-        if (vic && fabs(sp->act - 0.0) > 1e-8) {
+        double av[3] = {0, 0, 0};
+        if (cha) {
+            chate_av(o, i, step, cdir, av);
+            for (int d = 0; d < dim; d++) o->V[3 * i + d] = u[d] + rv[d] - RS[d] + av[d] - AS[d];
+        } else if (vic && fabs(sp->act - 0.0) > 1e-8) {
             for (int d = 0; d < dim; d++)
                 o->V[3 * i + d] = u[d] + o->cfg.relax * (sp->act * dir[d] - o->V[3 * i + d]) +
                                   rv[d] - RS[d];
@@ -1247,7 +1279,8 @@ int oracle_step(oracle_t *o, uint32_t step) {
             collide_vicsek(o, c, step);
         else if (op == MPCD_COLL_CHATE && dim == 2)
             collide_chate(o, c, step);
-        else if (op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT)
+        else if (op == MPCD_COLL_MPCAT || op == MPCD_COLL_VICSEK_MPCAT ||
+                 (op == MPCD_COLL_CHATE_MPCAT && dim == 2))
             collide_mpcat(o, c, step);
         else if (op == MPCD_COLL_LANG || op == MPCD_COLL_VICSEK_LANG)
             collide_lang(o, c, step);

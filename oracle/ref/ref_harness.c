@@ -84,6 +84,7 @@ static int g_phase = PH_NONE;
 static int g_cell = 0;
 static int g_rtech = 0;  /* RTECH of the collision in progress */
 static int g_ccount = 0; /* its uniform draws so far */
+static int g_last = 0;   /* the particle whose thermal draws ended last */
 static particleMPC *g_cursor = NULL;
 static int g_comp = 0;
 static uint32_t g_stream = 0; /* PH_INIT: the stream of the current draws */
@@ -639,6 +640,7 @@ static float next_normal(void) {
                             (uint32_t)pid, (uint32_t)g_comp);
         if (++g_comp == DIM) {
             g_comp = 0;
+            g_last = pid;
             g_cursor = g_cursor->next;
         }
     } else if (g_phase == PH_GHOST && g_ghost_pos < g_ghost_n) {
@@ -684,6 +686,10 @@ double genrand_real(void) {
         if (g_rtech == CHATE)
             return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_VICSEK,
                                     (uint32_t)g_pid, g_k++);
+        /* chateAndersenMPC's genrand_pmOne follows the particle's normals */
+        if (g_rtech == CHATE_MPCAT)
+            return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_VICSEK,
+                                    (uint32_t)g_last, 0u);
         if ((g_rtech == ORTHAXIS || g_rtech == ACT_ORTHAXIS) && g_ccount++ == 0)
             return mpcd_rng_uniform(g_seed, g_replica, g_step, MPCD_STREAM_ORTH,
                                     (uint32_t)g_cell, 0u);

@@ -433,3 +433,34 @@ def test_chate_in_3d_is_refused():
     cfg = W.base_config(3, (4, 4, 4), coll_op=abi.COLL_CHATE)
     with pytest.raises(MPCDError):
         Solver(cfg)
+
+
+@pytest.mark.parametrize("prec,kernel", [(abi.PREC_FP64, abi.KERNEL_TILE),
+                                         (abi.PREC_FP64, abi.KERNEL_AUTO),
+                                         (abi.PREC_MIXED, abi.KERNEL_AUTO)])
+def test_chate_aligned_mpcat_matches_the_oracle(prec, kernel):
+    """MPC-AT with Chate alignment (chateAndersenMPC, mpc.c:2300-2408), 2D,
+    against the oracle (pinned to the reference): an active and a passive
+    species, a net flow."""
+    L = (12, 10)
+    sp = [W._species(mass=1.0, act=0.8, damp=0.2), W._species(mass=2.0, act=0.0, damp=0.2)]
+    kw = dict(coll_op=abi.COLL_CHATE_MPCAT, species=sp, relax=0.5, seed=101)
+    cfg = W.base_config(2, L, **kw)
+    cfgp = W.base_config(2, L, precision=prec, **kw)
+    Q, V, U, spid = W.synthetic_state(cfg, 12, seed=102)
+    V[:, 0] += 0.3
+    spid = (np.arange(len(Q)) % 3 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    g = Solver(cfgp)
+    g.set_kernel(kernel)
+    g.upload(Q, V, U, spid)
+    for s in (1, 2, 3):
+        o.step(s)
+        g.step(1, s)
+        qo, vo, _ = o.particles()
+        qg, vg, _ = g.download()
+        _compare(prec, qg, vg, qo, vo, np.array(cfg.L[:3], dtype=float), 1e-5)
+    st = g.status()
+    assert st.escaped == 0 and st.nonfinite == 0
+    g.close()
+    o.close()

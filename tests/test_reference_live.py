@@ -265,3 +265,26 @@ def test_chate_tracks_reference(L, act, seed):
     assert r.unexpected_draws() == 0
     np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
     np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
+
+
+@pytest.mark.parametrize("L,relax", [((20, 16), 0.5), ((16, 18), 0.2)])
+def test_chate_aligned_mpcat_tracks_reference(L, relax):
+    """MPC-AT with Chate alignment (chateAndersenMPC, mpc.c:2300-2408: the
+    active velocity pmOne RELAX (ACT - |V|) DIR joins the thermal one, no
+    damping) of the oracle against the reference's own, 2D, an active and a
+    passive species."""
+    sp = [W._species(mass=1.0, act=0.8, damp=0.2), W._species(mass=2.0, act=0.0, damp=0.2)]
+    cfg = W.base_config(2, L, coll_op=abi.COLL_CHATE_MPCAT, species=sp, relax=relax, seed=575)
+    Q, V, U, spid = W.synthetic_state(cfg, 10, seed=576)
+    V[:, 0] += 0.3
+    spid = (np.arange(len(Q)) % 3 == 0).astype(np.int32)
+    o = Oracle(cfg, Q, V, U, spid)
+    r = Reference(cfg, Q, V, U, spid)
+    for s in range(1, 6):
+        o.step(s)
+        r.step(s)
+    qo, vo, _ = o.particles()
+    qr, vr, _ = r.particles()
+    assert r.unexpected_draws() == 0
+    np.testing.assert_allclose(vo, vr, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(qo, qr, rtol=0, atol=1e-11 * max(L))
